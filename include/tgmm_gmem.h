@@ -1,0 +1,209 @@
+/*
+ * tgmm_gmem.h -- C ABI of the B200 variational-inference Gaussian-mixture EM
+ * over foreground supervoxels (one TGMM time point, or a batch of them).
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (TGMM_OK == 0).  Device pointers are marked "dev", host pointers "host".
+ * Nothing here allocates implicitly except tgmm_plan_create (and the legacy
+ * C++ shims declared in tgmm_legacy.h, which keep a cached plan).
+ *
+ * Reference interface each entry point replaces (paths inside the reference
+ * project nmeth.3036-S2/src):
+ *   struct TgmmGaussian      <- GaussianMixtureModelCUDA, UtilsCUDA/GMEMupdateCUDA.h:22-57
+ *   tgmm_em_run              <- GMEMvariationalInferenceCUDAWithSupervoxels,
+ *                               UtilsCUDA/GMEMupdateCUDA.h:92-98 (body GMEMupdateCUDA.cu:3985-4421)
+ *   tgmm_knn                 <- knnCUDAinPlace, UtilsCUDA/knnCuda.h:225-226 (knnCuda.cu:781-817)
+ *   tgmm_update_priors       <- GaussianMixtureModel::updatePriors, GaussianMixtureModel.cpp:892-910,
+ *                               plus the nu_k*=2, W_k/=2 step of mainTrackingGaussianMixtureModel.cpp:961-969
+ *   tgmm_frame_upload        <- GMEMinitializeMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:132-137
+ *   tgmm_frame_release       <- GMEMreleaseMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:140-144
+ *   tgmm_assign_supervoxels  <- post-loop rnk>0.5 assignment, GMEMupdateCUDA.cu:4310-4350
+ *   tgmm_write_rnk_file      <- rnk/ind debug dump, GMEMupdateCUDA.cu:4364-4384
+ */
+#ifndef TGMM_GMEM_H_
+#define TGMM_GMEM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- constants of the reference (constants.h:11-17, GMEMupdateCUDA.h:20) ---- */
+#define TGMM_DIMS 3
+#define TGMM_J 5                      /* maxGaussiansPerVoxel */
+#define TGMM_MAX_SV_PER_GAUSSIAN 16   /* MAX_SUPERVOXELS_PER_GAUSSIAN */
+#define TGMM_MIN_PI_FOR_DEAD 1e-5     /* minPi_kForDead */
+#define TGMM_DEAD_SENTINEL (-1e32)    /* m_o[0] < -1e31 marks a dead Gaussian */
+
+/* ---- status codes ---- */
+enum {
+  TGMM_OK = 0,
+  TGMM_ERR_INVALID_ARG = 1,   /* null pointer, negative size, bad parameter */
+  TGMM_ERR_BAD_SIZE = 2,      /* sizes beyond the plan capacity or the ABI limits */
+  TGMM_ERR_BAD_CSR = 3,       /* labelListPtr not monotone / out of range */
+  TGMM_ERR_NAN_INPUT = 4,     /* NaN/Inf in coordinates or Gaussian parameters */
+  TGMM_ERR_CUDA = 5,          /* a CUDA runtime call failed */
+  TGMM_ERR_OOM = 6,           /* device allocation failed */
+  TGMM_ERR_DEVICE_FLAG = 7,   /* a kernel reported an internal inconsistency */
+  TGMM_ERR_NOT_SET = 8,       /* regularisation constants not set (reference exit(3)) */
+  TGMM_ERR_ADMISSION = 9      /* served form: request does not fit in free HBM */
+};
+
+/* Per-Gaussian record.  Byte-for-byte the reference's 288-byte
+ * GaussianMixtureModelCUDA (offsets: beta_k 0, m_k 24, W_k 48, eLD 96, beta_o 120,
+ * m_o 144, W_o 168, fixed 216, supervoxelIdx 220, supervoxelNum 284).
+ * W is the upper triangle, row major: 00,01,02,11,12,22. */
+typedef struct TgmmGaussian {
+  double beta_k, nu_k, alpha_k;
+  double m_k[3];
+  double W_k[6];
+  double expectedLogDetCovarianceCUDA;
+  double expectedLogResponsivityCUDA;
+  double splitScore;
+  double beta_o, nu_o, alpha_o;
+  double m_o[3];
+  double W_o[6];
+  unsigned char fixed; /* C++ bool */
+  int32_t supervoxelIdx[TGMM_MAX_SV_PER_GAUSSIAN];
+  int32_t supervoxelNum;
+} TgmmGaussian;
+
+/* Log-likelihood flavour used by the convergence test. */
+enum {
+  TGMM_LL_AS_REFERENCE = 0, /* the reference's per-thread overwrite for supervoxels with
+                               more than 1024 voxels (GMEMupdateCUDA.cu:1961-1962) */
+  TGMM_LL_TRUE = 1          /* every foreground voxel counted */
+};
+
+/* Precision of the per-voxel log-likelihood terms (accumulation is always FP64). */
+enum {
+  TGMM_LLPREC_MIXED = 0, /* dominant component in FP64, log1p correction of the others in FP32 */
+  TGMM_LLPREC_FP64 = 1   /* every component in FP64 */
+};
+
+typedef struct TgmmEmParams {
+  int32_t max_iter_em;      /* maxIterEM (reference default 400) */
+  int32_t w4dof;            /* regularize_W4DOF (reference main sets true) */
+  double tol_likelihood;    /* tolLikelihood (default 1e-6; 0 = run max_iter_em unless ll repeats) */
+  double lambda_min;        /* regularizePrecisionMatrixConstants::lambdaMin (0.02) */
+  double lambda_max;        /* lambdaMax (0.2222) */
+  double max_excentricity;  /* maxExcentricity (9) */
+  float scale[3];           /* anisotropy scale of the kNN distance, e.g. {1,1,2}
+                               (the reference's scaleCUDA, uploadScaleCUDA) */
+  float reg_scale[3];       /* scale of the regularisation (scaleGMEMCUDA, copyScaleToDvice);
+                               all zero = same as scale */
+  int32_t ll_mode;          /* TGMM_LL_AS_REFERENCE or TGMM_LL_TRUE */
+  int32_t ll_precision;     /* TGMM_LLPREC_MIXED or TGMM_LLPREC_FP64 */
+  int32_t frame;            /* only echoed in logs */
+} TgmmEmParams;
+
+/* Fill *p with the reference defaults (parseConfigFile.h:152-195, main:124). */
+void tgmm_default_params(TgmmEmParams* p);
+
+/* One time point on the device.  Layout is the reference's:
+ *   query[d*n_vox + v]      voxel coordinates, SoA (x block, y block, z block), float
+ *   img[v]                  intensity in [0,1]
+ *   centroids[d*n_sv + s]   supervoxel centroids, SoA
+ *   label_ptr[0..n_sv]      CSR: voxels of supervoxel s are [label_ptr[s], label_ptr[s+1]) */
+typedef struct TgmmFrame {
+  const float* query;        /* dev */
+  const float* img;          /* dev */
+  const float* centroids;    /* dev */
+  const int64_t* label_ptr;  /* dev */
+  int64_t n_vox;
+  int32_t n_sv;
+  int32_t n_gauss;
+} TgmmFrame;
+
+typedef struct TgmmEmStats {
+  int32_t iterations;       /* EM iterations executed (numIterEM-1 in the reference) */
+  int32_t converged;        /* 1 if stopped by the tolerance test */
+  double ll;                /* log-likelihood used by the convergence test (last iteration) */
+  double ll_true;           /* every-voxel log-likelihood (last iteration) */
+  double ll_as_reference;   /* overwrite-quirk log-likelihood (last iteration) */
+  double total_alpha;       /* sum of alpha_k after the last kill step */
+  int32_t n_dead;           /* dead Gaussians after the call */
+  int32_t device_flags;     /* bit mask of device-side anomaly flags (0 = none) */
+} TgmmEmStats;
+
+/* ---- plans: all device workspace, sized once, reused by every call ---- */
+typedef struct TgmmPlan TgmmPlan;
+
+/* Capacity of one plan.  A batch may hold up to max_frames frames whose totals fit. */
+typedef struct TgmmPlanDesc {
+  int64_t max_vox;     /* total voxels over the batch */
+  int32_t max_sv;      /* total supervoxels */
+  int32_t max_gauss;   /* total Gaussians */
+  int32_t max_frames;  /* frames per batch */
+  int32_t device;      /* CUDA device ordinal */
+} TgmmPlanDesc;
+
+int tgmm_plan_create(const TgmmPlanDesc* desc, TgmmPlan** out);
+int tgmm_plan_destroy(TgmmPlan* plan);
+/* Bytes of device memory tgmm_plan_create would allocate for desc. */
+int64_t tgmm_plan_bytes(const TgmmPlanDesc* desc);
+
+/* Single time point, Gaussians in HOST memory (read, updated in place, including
+ * supervoxelIdx/supervoxelNum), rnk/ind written to DEVICE buffers of n_sv*5
+ * (slot-major: rnk[j*n_sv+s]); ind_tr_dev (optional, may be NULL) receives the
+ * Gaussian-sorted keys like the reference's indCUDAtr.  stream: cudaStream_t or NULL. */
+int tgmm_em_run(TgmmPlan* plan, const TgmmFrame* frame, TgmmGaussian* gm_host,
+                float* rnk_dev, int32_t* ind_dev, int32_t* ind_tr_dev,
+                const TgmmEmParams* params, TgmmEmStats* stats, void* stream);
+
+/* Same with the Gaussians already on the device (gm_dev, n_gauss records), updated in
+ * place on the device; supervoxelIdx/Num are filled on the device.  No host sync
+ * unless stats != NULL. */
+int tgmm_em_run_device(TgmmPlan* plan, const TgmmFrame* frame, TgmmGaussian* gm_dev,
+                       float* rnk_dev, int32_t* ind_dev, const TgmmEmParams* params,
+                       TgmmEmStats* stats, void* stream);
+
+/* Batched form: n_frames independent time points, each with its own frame and its own
+ * Gaussian array (device), run together, one launch per EM phase over all frames.
+ * rnk_dev[f]/ind_dev[f] are per-frame outputs.  stats may be NULL or an array of n_frames.
+ * Results are bit-identical to running each frame alone through tgmm_em_run_device. */
+int tgmm_em_run_batch(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
+                      TgmmGaussian* const* gm_dev, float* const* rnk_dev,
+                      int32_t* const* ind_dev, const TgmmEmParams* params,
+                      TgmmEmStats* stats, void* stream);
+
+/* kNN of n_query points (SoA, dev) against n_ref points (AoS xyz float, dev), ordered by
+ * (scaled squared distance, index); ind_dev[j*n_query+q].  Exact. */
+int tgmm_knn(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
+             int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
+
+/* Posterior -> prior for the next time point, on the device (served form):
+ * N_k = nu_k - nu_o; m_o = m_k; beta_o = max(beta_pct*N_k, 1e-5);
+ * nu_o = max(nu_pct*N_k, 3); W_o = W_k*nu_k/nu_o; alpha_o = alpha_total*1e-5*alpha_pct
+ * (unchanged when alpha_total < 0); then nu_k *= 2, W_k /= 2.  alpha_total < 0 and
+ * compute_alpha_total != 0 means "use the sum of alpha_k of this array". */
+int tgmm_update_priors(TgmmGaussian* gm_dev, int32_t n_gauss, double beta_pct,
+                       double nu_pct, double alpha_pct, double alpha_total,
+                       int32_t compute_alpha_total, void* stream);
+
+/* Allocate device buffers and upload one frame from host arrays (legacy ownership model). */
+int tgmm_frame_upload(const float* query_host, const float* img_host,
+                      const float* centroids_host, const int64_t* label_ptr_host,
+                      int64_t n_vox, int32_t n_sv, TgmmFrame* out_frame);
+int tgmm_frame_release(TgmmFrame* frame);
+
+/* Reference post-loop assignment on host arrays: for j in 0..4, s in 0..n_sv-1, if
+ * rnk[j*n_sv+s] > 0.5, append s to gm[ind].supervoxelIdx (at most 16). */
+int tgmm_assign_supervoxels(const float* rnk_host, const int32_t* ind_host, int32_t n_sv,
+                            TgmmGaussian* gm_host, int32_t n_gauss);
+
+/* Reference rnk dump: int n_sv, int 5, float rnk[5*n_sv], int ind[5*n_sv]. */
+int tgmm_write_rnk_file(const char* path, const float* rnk_host, const int32_t* ind_host,
+                        int32_t n_sv);
+
+/* Last CUDA error string recorded by this library on the calling thread. */
+const char* tgmm_last_error(void);
+/* Library version string. */
+const char* tgmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TGMM_GMEM_H_ */

@@ -1,0 +1,23 @@
+#!/bin/sh
+# TEST INFRASTRUCTURE ONLY.  Compiles the reference's own GPU path for sm_100a from its
+# sources where they lie (read-only) plus oracle/ref_harness.cu into
+# oracle/_ref/libtgmm_ref.so.  Nothing is copied from the reference tree.
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${TGMM_REFERENCE_SRC:-/root/reference/nmeth.3036-S2/src}
+OUT="$HERE/_ref"
+if [ ! -d "$REF/UtilsCUDA" ]; then
+  echo "reference sources not found at $REF; skipping" >&2
+  exit 0
+fi
+mkdir -p "$OUT"
+NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
+FLAGS="-std=c++17 -O2 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -w"
+$NVCC $FLAGS -c "$REF/UtilsCUDA/GMEMupdateCUDA.cu" -o "$OUT/GMEMupdateCUDA.o"
+$NVCC $FLAGS -c "$REF/UtilsCUDA/knnCuda.cu" -o "$OUT/knnCuda.o"
+g++ -O2 -fPIC -c "$REF/constants.cpp" -o "$OUT/constants.o"
+$NVCC $FLAGS -I"$REF/UtilsCUDA" -I"$REF" -c "$HERE/ref_harness.cu" -o "$OUT/ref_harness.o"
+$NVCC -gencode arch=compute_100a,code=sm_100a -shared -o "$OUT/libtgmm_ref.so" \
+  "$OUT/GMEMupdateCUDA.o" "$OUT/knnCuda.o" "$OUT/constants.o" "$OUT/ref_harness.o" -lcusparse -lcuda
+rm -f "$OUT"/*.o
+echo "built $OUT/libtgmm_ref.so"

@@ -1,0 +1,50 @@
+// ref_harness.cu -- TEST INFRASTRUCTURE ONLY.  A C entry point over the reference's own
+// GPU path (UtilsCUDA/GMEMupdateCUDA.cu + knnCuda.cu, compiled from the reference
+// sources by oracle/build_ref.sh into oracle/_ref/libtgmm_ref.so), so that tests can run
+// the unmodified reference on the same seeded inputs and pin the CPU oracle to it.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <string>
+
+#include "GMEMupdateCUDA.h"
+#include "knnCuda.h"
+
+extern "C" int ref_em_run(float* query, float* img, float* cent, long long* lptr, long long N, int S, void* gauss,
+                          int K, int max_iter, double tol, int w4dof, double lmin, double lmax, double maxexc,
+                          float* scale, float* rnk_out, int* ind_out) {
+  if (S < 1 || S > 65535 || K < 5) return 1;
+  regularizePrecisionMatrixConstants::setConstants(lmin, lmax, maxexc);
+  float *qc = 0, *ic = 0, *rc = 0, *cc = 0;
+  int *indc = 0, *indtr = 0;
+  long long* lc = 0;
+  GMEMinitializeMemoryWithSupervoxels(&qc, query, &ic, img, scale, N, &rc, &indc, &indtr, (unsigned short)S, &cc,
+                                      cent, &lc, lptr);
+  copyScaleToDvice(scale);
+  GMEMvariationalInferenceCUDAWithSupervoxels(qc, ic, rc, NULL, indc, indtr, cc, lc, (GaussianMixtureModelCUDA*)gauss,
+                                              N, K, (unsigned short)S, max_iter, tol, 0, 0, w4dof != 0,
+                                              std::string(""));
+  cudaError_t e = cudaMemcpy(rnk_out, rc, sizeof(float) * 5 * (size_t)S, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(ind_out, indc, sizeof(int) * 5 * (size_t)S, cudaMemcpyDeviceToHost);
+  GMEMreleaseMemoryWithSupervoxels(&qc, &ic, &rc, &indc, &indtr, &cc, &lc);
+  fflush(stdout);
+  return e == cudaSuccess ? 0 : 2;
+}
+
+// kNN only: query SoA (host, nq points), refs AoS xyz (host).
+extern "C" int ref_knn(float* query, long long nq, float* ref, int nref, float* scale, int* ind_out) {
+  float *qd = 0, *rd = 0;
+  int* id = 0;
+  cudaMalloc(&qd, sizeof(float) * 3 * nq);
+  cudaMalloc(&rd, sizeof(float) * 3 * nref);
+  cudaMalloc(&id, sizeof(int) * 5 * nq);
+  cudaMemcpy(qd, query, sizeof(float) * 3 * nq, cudaMemcpyHostToDevice);
+  cudaMemcpy(rd, ref, sizeof(float) * 3 * nref, cudaMemcpyHostToDevice);
+  uploadScaleCUDA(scale);
+  knnCUDAinPlace(id, qd, rd, nq, nref);
+  cudaError_t e = cudaMemcpy(ind_out, id, sizeof(int) * 5 * nq, cudaMemcpyDeviceToHost);
+  cudaFree(qd);
+  cudaFree(rd);
+  cudaFree(id);
+  return e == cudaSuccess ? 0 : 2;
+}

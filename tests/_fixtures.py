@@ -1,0 +1,61 @@
+"""Seeded workloads shared by the tests (inputs are generated, never read from outside)."""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+
+from tgmm_b200 import _lib as L
+from tgmm_b200 import synth
+
+SPEC_HARD = synth.VolumeSpec(dims=(96, 96, 48), n_nuclei=40, axis_min=3.0, axis_max=7.0, jitter=3.0)
+SPEC_BIG = synth.VolumeSpec(dims=(96, 96, 48), n_nuclei=6, axis_min=11.0, axis_max=14.0)
+SPEC_SMALL = synth.VolumeSpec(dims=(128, 128, 48), n_nuclei=60, axis_min=3.0, axis_max=6.0)
+
+
+def _perturb(frame, seed):
+    """Harder Gaussian sets: duplicated Gaussians (soft responsibilities, Gaussians that
+    die), a fixed Gaussian, one dead from the start, anisotropic precisions."""
+    rng = np.random.default_rng(seed)
+    g = frame.gauss.copy()
+    K = g.shape[0]
+    g["W_k"][:, 0] *= rng.uniform(0.6, 1.6, K)
+    g["W_k"][:, 3] *= rng.uniform(0.6, 1.6, K)
+    g["W_k"][:, 1] = 0.2 * np.sqrt(g["W_k"][:, 0] * g["W_k"][:, 3]) * rng.uniform(-1, 1, K)
+    dup = rng.choice(K, size=max(1, K // 4), replace=False)
+    extra = g[dup].copy()
+    extra["m_k"] += rng.normal(0, 2.5, size=(dup.size, 3))
+    extra["m_o"] = extra["m_k"]
+    extra["alpha_k"] *= 0.5
+    extra["alpha_o"] = 1e-3  # these lose their supervoxels and die through alpha/sum(alpha) < 1e-5
+    twins = g[rng.choice(K, size=3, replace=False)].copy()  # near-copies: split responsibilities
+    twins["m_k"] += rng.normal(0, 0.004, size=(3, 3))
+    g = np.concatenate([g, extra, twins]).astype(L.GAUSS_DTYPE)
+    g["fixed"][1] = 1
+    dead = 2
+    g["m_o"][dead] = -1e32
+    g["m_k"][dead] = -1e32
+    g["alpha_k"][dead] = 0.0
+    g["W_k"][dead] = [1, 0, 0, 1, 0, 1]
+    frame.gauss = g
+    return frame
+
+
+@functools.lru_cache(maxsize=None)
+def frame(name: str):
+    if name == "tiny":
+        return synth.generate(synth.TINY, seed=7)
+    if name == "small":
+        return synth.generate(SPEC_SMALL, seed=3)
+    if name == "c1":
+        return synth.generate(synth.C1, seed=1)
+    if name == "hard":
+        return _perturb(synth.generate(SPEC_HARD, seed=11), 11)
+    if name == "big":
+        return synth.generate(SPEC_BIG, seed=5)
+    raise KeyError(name)
+
+
+def params(iters=20, tol=-1.0, **kw):
+    """EM parameters of the workloads; tol < 0 runs exactly `iters` iterations."""
+    return synth.em_params(iters=iters, tol=tol, **kw)

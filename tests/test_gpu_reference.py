@@ -1,0 +1,56 @@
+"""Pins the CPU oracle to the reference itself: the reference's GPU path, compiled from
+its own sources for sm_100a (oracle/_ref), runs the same seeded inputs, and the oracle's
+REF32 mode (the reference's FP32 arithmetic and reduction order) must agree with it.
+Only frames with at most 1024 supervoxels are run on the reference: its kNN kernel
+returns early for surplus threads and then calls __syncthreads(), which is only
+well-defined when no thread of the block returns early."""
+import numpy as np
+import pytest
+
+import _fixtures as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["tiny", "small", "c1", "hard"]
+
+
+def needs_ref():
+    if not O.ref_available():
+        pytest.skip("oracle/_ref/libtgmm_ref.so not built (oracle/build_ref.sh needs the reference sources)")
+
+
+def canon_sets(ind, S):
+    return np.sort(ind.reshape(5, S), axis=0)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("iters", [1, 20])
+def test_reference_matches_oracle_ref32(cuda_ok, name, iters):
+    needs_ref()
+    f = F.frame(name)
+    assert f.n_sv <= 1024
+    r = O.ref_em_run(f.query, f.img, f.centroids, f.label_ptr, f.gauss, max_iter=iters, tol=-1.0)
+    o = O.em_run(f.query, f.img, f.centroids, f.label_ptr, f.gauss,
+                 O.params(max_iter=iters, tol=-1.0, mode=O.MODE_REF32))
+    # the same replacement rule and slot order -> identical candidate arrays
+    np.testing.assert_array_equal(r["ind"], o["ind"])
+    assert np.max(np.abs(r["rnk"] - o["rnk"])) <= 1e-4
+    rg, og = r["gauss"], o["gauss"]
+    alive = og["m_o"][:, 0] > -1e31
+    np.testing.assert_array_equal(rg["m_o"][:, 0] > -1e31, alive)
+    np.testing.assert_array_equal(rg["supervoxelNum"], og["supervoxelNum"])
+    assert np.max(np.abs(rg["m_k"][alive] - og["m_k"][alive])) <= 1e-3
+    ws = np.max(np.abs(og["W_k"][alive]), axis=1, keepdims=True)
+    assert np.max(np.abs(rg["W_k"][alive] - og["W_k"][alive]) / ws) <= 1e-3
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_knn_sets_equal_canonical(cuda_ok, name):
+    needs_ref()
+    f = F.frame(name)
+    ref_xyz = np.ascontiguousarray(f.gauss["m_k"].astype(np.float32)).reshape(-1)
+    got = O.ref_knn(f.centroids, ref_xyz)
+    S = f.n_sv
+    np.testing.assert_array_equal(canon_sets(got, S), canon_sets(O.knn(f.centroids, ref_xyz), S))
+    np.testing.assert_array_equal(got, O.knn(f.centroids, ref_xyz, reference_rule=True))

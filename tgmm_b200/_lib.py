@@ -1,0 +1,199 @@
+"""ctypes bindings of the C ABI (include/tgmm_gmem.h) and of the synthetic-data library.
+
+The CUDA engine lives in ``libtgmm_gmem.so`` next to this file (built in-tree by
+``tgmm_b200/csrc/Makefile``).  Loading fails loudly when it is missing: there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GMEM_SO = os.path.join(HERE, "libtgmm_gmem.so")
+SYNTH_SO = os.path.join(HERE, "libtgmm_synth.so")
+
+TGMM_J = 5
+TGMM_MAX_SV = 16
+
+# status codes (tgmm_gmem.h)
+TGMM_OK = 0
+TGMM_ERR_INVALID_ARG = 1
+TGMM_ERR_BAD_SIZE = 2
+TGMM_ERR_BAD_CSR = 3
+TGMM_ERR_NAN_INPUT = 4
+TGMM_ERR_CUDA = 5
+TGMM_ERR_OOM = 6
+TGMM_ERR_DEVICE_FLAG = 7
+TGMM_ERR_NOT_SET = 8
+TGMM_ERR_ADMISSION = 9
+
+TGMM_LL_AS_REFERENCE = 0
+TGMM_LL_TRUE = 1
+TGMM_LLPREC_MIXED = 0
+TGMM_LLPREC_FP64 = 1
+
+
+class TgmmGaussian(C.Structure):
+    _fields_ = [
+        ("beta_k", C.c_double), ("nu_k", C.c_double), ("alpha_k", C.c_double),
+        ("m_k", C.c_double * 3), ("W_k", C.c_double * 6),
+        ("expectedLogDetCovarianceCUDA", C.c_double), ("expectedLogResponsivityCUDA", C.c_double),
+        ("splitScore", C.c_double),
+        ("beta_o", C.c_double), ("nu_o", C.c_double), ("alpha_o", C.c_double),
+        ("m_o", C.c_double * 3), ("W_o", C.c_double * 6),
+        ("fixed", C.c_ubyte),
+        ("supervoxelIdx", C.c_int32 * TGMM_MAX_SV), ("supervoxelNum", C.c_int32),
+    ]
+
+
+assert C.sizeof(TgmmGaussian) == 288
+
+# numpy view of the 288-byte record (same offsets)
+GAUSS_DTYPE = np.dtype({
+    "names": ["beta_k", "nu_k", "alpha_k", "m_k", "W_k", "eLD", "eLR", "splitScore", "beta_o", "nu_o",
+              "alpha_o", "m_o", "W_o", "fixed", "supervoxelIdx", "supervoxelNum"],
+    "formats": ["<f8", "<f8", "<f8", ("<f8", 3), ("<f8", 6), "<f8", "<f8", "<f8", "<f8", "<f8", "<f8",
+                ("<f8", 3), ("<f8", 6), "u1", ("<i4", 16), "<i4"],
+    "offsets": [0, 8, 16, 24, 48, 96, 104, 112, 120, 128, 136, 144, 168, 216, 220, 284],
+    "itemsize": 288,
+})
+
+
+class TgmmEmParams(C.Structure):
+    _fields_ = [
+        ("max_iter_em", C.c_int32), ("w4dof", C.c_int32), ("tol_likelihood", C.c_double),
+        ("lambda_min", C.c_double), ("lambda_max", C.c_double), ("max_excentricity", C.c_double),
+        ("scale", C.c_float * 3), ("reg_scale", C.c_float * 3),
+        ("ll_mode", C.c_int32), ("ll_precision", C.c_int32), ("frame", C.c_int32),
+    ]
+
+
+class TgmmFrame(C.Structure):
+    _fields_ = [
+        ("query", C.c_void_p), ("img", C.c_void_p), ("centroids", C.c_void_p), ("label_ptr", C.c_void_p),
+        ("n_vox", C.c_int64), ("n_sv", C.c_int32), ("n_gauss", C.c_int32),
+    ]
+
+
+class TgmmEmStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32), ("converged", C.c_int32), ("ll", C.c_double), ("ll_true", C.c_double),
+        ("ll_as_reference", C.c_double), ("total_alpha", C.c_double), ("n_dead", C.c_int32),
+        ("device_flags", C.c_int32),
+    ]
+
+
+class TgmmPlanDesc(C.Structure):
+    _fields_ = [
+        ("max_vox", C.c_int64), ("max_sv", C.c_int32), ("max_gauss", C.c_int32), ("max_frames", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
+class TgmmSynthConfig(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int32 * 3), ("axis_min", C.c_float), ("axis_max", C.c_float), ("anisotropy", C.c_float),
+        ("peak_min", C.c_float), ("peak_max", C.c_float), ("background", C.c_float), ("threshold", C.c_float),
+        ("jitter", C.c_float), ("min_size", C.c_int32),
+    ]
+
+
+# every function declared in include/tgmm_gmem.h: name -> (restype, argtypes)
+_VP = C.c_void_p
+GMEM_FUNCS = {
+    "tgmm_default_params": (None, [C.POINTER(TgmmEmParams)]),
+    "tgmm_plan_create": (C.c_int, [C.POINTER(TgmmPlanDesc), C.POINTER(_VP)]),
+    "tgmm_plan_destroy": (C.c_int, [_VP]),
+    "tgmm_plan_bytes": (C.c_int64, [C.POINTER(TgmmPlanDesc)]),
+    "tgmm_em_run": (C.c_int, [_VP, C.POINTER(TgmmFrame), _VP, _VP, _VP, _VP, C.POINTER(TgmmEmParams),
+                              C.POINTER(TgmmEmStats), _VP]),
+    "tgmm_em_run_device": (C.c_int, [_VP, C.POINTER(TgmmFrame), _VP, _VP, _VP, C.POINTER(TgmmEmParams),
+                                     C.POINTER(TgmmEmStats), _VP]),
+    "tgmm_em_run_batch": (C.c_int, [_VP, C.c_int32, C.POINTER(TgmmFrame), C.POINTER(_VP), C.POINTER(_VP),
+                                    C.POINTER(_VP), C.POINTER(TgmmEmParams), C.POINTER(TgmmEmStats), _VP]),
+    "tgmm_knn": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.POINTER(C.c_float), _VP, _VP]),
+    "tgmm_update_priors": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                     _VP]),
+    "tgmm_frame_upload": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int64, C.c_int32, C.POINTER(TgmmFrame)]),
+    "tgmm_frame_release": (C.c_int, [C.POINTER(TgmmFrame)]),
+    "tgmm_assign_supervoxels": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_int32]),
+    "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
+    "tgmm_last_error": (C.c_char_p, []),
+    "tgmm_version": (C.c_char_p, []),
+}
+
+SYNTH_FUNCS = {
+    "tgmm_synth_nuclei": (None, [C.POINTER(TgmmSynthConfig), C.c_int32, C.c_uint64, _VP, _VP, _VP, _VP]),
+    "tgmm_synth_frame": (_VP, [C.POINTER(TgmmSynthConfig), C.c_int32, _VP, _VP, _VP, _VP, C.c_uint64]),
+    "tgmm_synth_n_vox": (C.c_int64, [_VP]),
+    "tgmm_synth_n_sv": (C.c_int32, [_VP]),
+    "tgmm_synth_max_fg": (C.c_float, [_VP]),
+    "tgmm_synth_copy": (None, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "tgmm_synth_free": (None, [_VP]),
+    "tgmm_synth_init_gaussians": (C.c_int32, [_VP, C.POINTER(TgmmSynthConfig), C.c_int32, _VP, C.c_uint64,
+                                              C.POINTER(TgmmEmParams), _VP, _VP]),
+}
+
+_gmem = None
+_synth = None
+
+
+def _bind(lib, table):
+    for name, (res, args) in table.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def gmem():
+    """The CUDA engine library (raises if it was not built)."""
+    global _gmem
+    if _gmem is None:
+        if not os.path.exists(GMEM_SO):
+            raise RuntimeError(f"{GMEM_SO} is missing: build it with `make -C tgmm_b200/csrc` "
+                               "(there is no CPU fallback for the EM engine)")
+        _gmem = _bind(C.CDLL(GMEM_SO), GMEM_FUNCS)
+    return _gmem
+
+
+def synth():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_SO):
+            raise RuntimeError(f"{SYNTH_SO} is missing: build it with `make -C tgmm_b200/csrc`")
+        _synth = _bind(C.CDLL(SYNTH_SO), SYNTH_FUNCS)
+    return _synth
+
+
+class TgmmError(RuntimeError):
+    def __init__(self, code, where):
+        msg = gmem().tgmm_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed with status {code}: {msg}")
+        self.code = code
+
+
+def check(code, where):
+    if code != TGMM_OK:
+        raise TgmmError(code, where)
+
+
+def default_params(**overrides) -> TgmmEmParams:
+    p = TgmmEmParams()
+    gmem().tgmm_default_params(C.byref(p))
+    for k, v in overrides.items():
+        if k in ("scale", "reg_scale"):
+            getattr(p, k)[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def ptr(a) -> int:
+    """Address of a numpy array or a torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

@@ -1,0 +1,550 @@
+// em_host.cu -- C ABI of the EM engine: plans (all device workspace), batch tables,
+// CUDA-graph capture of the whole fixed-length EM, and the reference-shaped entry points.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tgmm_internal.cuh"
+
+using namespace tgmm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
+  char buf[512];
+  if (e != cudaSuccess)
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  else
+    snprintf(buf, sizeof(buf), "%s", what);
+  g_last_error = buf;
+  return code;
+}
+
+#define TG_CUDA(call, what)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return fail(TGMM_ERR_CUDA, what, e_); \
+  } while (0)
+
+int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+struct Layout {
+  // byte offsets of every device array inside one allocation
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, ref_cell, cell_refs, cell_cnt, cell_start,
+      cell_cur, bcnt, bucket, acnt, abucket, ape, apf, dead, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
+};
+
+Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
+  Layout L;
+  int64_t o = 0;
+  auto take = [&](int64_t bytes) {
+    int64_t at = o;
+    o = align_up(o + std::max<int64_t>(bytes, 1), 256);
+    return at;
+  };
+  const int64_t G = d.max_gauss, S = d.max_sv, F = d.max_frames;
+  L.info = take(sizeof(BatchInfo));
+  L.frames = take(sizeof(FrameDesc) * F);
+  L.state = take(sizeof(FrameState) * F);
+  L.gchunks = take(sizeof(GChunk) * max_gchunks);
+  L.g_frame = take(4 * G);
+  L.gd = take(8 * G * G_NUM);
+  L.fixed = take(G);
+  L.ref_cell = take(4 * G);
+  L.cell_refs = take(16 * G);
+  L.cell_cnt = take(4 * (int64_t)max_cells);
+  L.cell_start = take(4 * ((int64_t)max_cells + F));
+  L.cell_cur = take(4 * (int64_t)max_cells);
+  L.bcnt = take(4 * G);
+  L.bucket = take(4 * G * kBucketCap);
+  L.acnt = take(4 * G);
+  L.abucket = take(4 * G * kBucketCap);
+  L.ape = take(8 * (int64_t)max_gchunks);
+  L.apf = take(8 * (int64_t)max_gchunks);
+  L.dead = take(4 * (int64_t)max_gchunks);
+  L.sv_frame = take(4 * S);
+  L.mom = take(8 * S * kNumMoments);
+  L.cand = take(4 * S * kJ);
+  L.rnk = take(4 * S * kJ);
+  L.llp = take(8 * 2 * S);
+  L.gm_scratch = take((int64_t)sizeof(TgmmGaussian) * G);
+  L.total = o;
+  return L;
+}
+
+int32_t gchunks_cap(const TgmmPlanDesc& d) { return (d.max_gauss + kGChunk - 1) / kGChunk + d.max_frames; }
+int32_t cells_cap(const TgmmPlanDesc& d) { return 2 * d.max_gauss + 2 * d.max_frames; }
+
+}  // namespace
+
+struct TgmmPlan {
+  TgmmPlanDesc desc;
+  Layout L;
+  char* base = nullptr;
+  DevPlan dev;
+  // pinned host staging of the batch tables
+  BatchInfo* h_info = nullptr;
+  FrameDesc* h_frames = nullptr;
+  GChunk* h_gchunks = nullptr;
+  FrameState* h_state = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  cudaEvent_t done_ev = nullptr;
+  bool pending = false;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (max_iter, ll_prec) -> exec
+  std::mutex mu;
+};
+
+extern "C" {
+
+void tgmm_default_params(TgmmEmParams* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->max_iter_em = 400;
+  p->w4dof = 1;
+  p->tol_likelihood = 1e-6;
+  p->lambda_min = 0.02;
+  p->lambda_max = 0.2222;
+  p->max_excentricity = 9.0;
+  p->scale[0] = p->scale[1] = p->scale[2] = 1.0f;
+  p->ll_mode = TGMM_LL_AS_REFERENCE;
+  p->ll_precision = TGMM_LLPREC_MIXED;
+}
+
+const char* tgmm_last_error(void) { return g_last_error.c_str(); }
+const char* tgmm_version(void) { return "tgmm_b200 0.1 (sm_100a)"; }
+
+int64_t tgmm_plan_bytes(const TgmmPlanDesc* d) {
+  if (!d || d->max_gauss <= 0 || d->max_sv < 0 || d->max_frames <= 0) return -1;
+  return make_layout(*d, gchunks_cap(*d), cells_cap(*d)).total;
+}
+
+int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
+  if (!d || !out) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_create: null argument");
+  if (d->max_gauss < TGMM_J || d->max_sv < 1 || d->max_frames < 1 || d->max_vox < 0)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_create: capacities must be positive (max_gauss >= 5)");
+  if ((int64_t)d->max_sv * kJ >= (1LL << 31) || (int64_t)d->max_gauss * kBucketCap >= (1LL << 31))
+    return fail(TGMM_ERR_BAD_SIZE, "tgmm_plan_create: capacities beyond 32-bit indexing");
+  *out = nullptr;
+  TG_CUDA(cudaSetDevice(d->device), "cudaSetDevice");
+  TgmmPlan* P = new TgmmPlan();
+  P->desc = *d;
+  const int32_t mgc = gchunks_cap(*d), mcl = cells_cap(*d);
+  P->L = make_layout(*d, mgc, mcl);
+  cudaError_t e = cudaMalloc(&P->base, P->L.total);
+  if (e != cudaSuccess) {
+    delete P;
+    return fail(TGMM_ERR_OOM, "tgmm_plan_create: cudaMalloc", e);
+  }
+  e = cudaMemset(P->base, 0, P->L.total);
+  if (e == cudaSuccess) e = cudaMallocHost(&P->h_info, sizeof(BatchInfo));
+  if (e == cudaSuccess) e = cudaMallocHost(&P->h_frames, sizeof(FrameDesc) * d->max_frames);
+  if (e == cudaSuccess) e = cudaMallocHost(&P->h_gchunks, sizeof(GChunk) * mgc);
+  if (e == cudaSuccess) e = cudaMallocHost(&P->h_state, sizeof(FrameState) * d->max_frames);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->done_ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    tgmm_plan_destroy(P);
+    return fail(TGMM_ERR_CUDA, "tgmm_plan_create: setup", e);
+  }
+  DevPlan& D = P->dev;
+  char* b = P->base;
+  D.max_vox = d->max_vox;
+  D.max_sv = d->max_sv;
+  D.max_gauss = d->max_gauss;
+  D.max_frames = d->max_frames;
+  D.max_gchunks = mgc;
+  D.max_cells = mcl;
+  D.info = (BatchInfo*)(b + P->L.info);
+  D.frames = (FrameDesc*)(b + P->L.frames);
+  D.state = (FrameState*)(b + P->L.state);
+  D.gchunks = (GChunk*)(b + P->L.gchunks);
+  D.g_frame = (int32_t*)(b + P->L.g_frame);
+  D.gd = (double*)(b + P->L.gd);
+  D.fixed = (uint8_t*)(b + P->L.fixed);
+  D.ref_cell = (int32_t*)(b + P->L.ref_cell);
+  D.cell_refs = (float4*)(b + P->L.cell_refs);
+  D.cell_cnt = (int32_t*)(b + P->L.cell_cnt);
+  D.cell_start = (int32_t*)(b + P->L.cell_start);
+  D.cell_cur = (int32_t*)(b + P->L.cell_cur);
+  D.bcnt = (int32_t*)(b + P->L.bcnt);
+  D.bucket = (int32_t*)(b + P->L.bucket);
+  D.acnt = (int32_t*)(b + P->L.acnt);
+  D.abucket = (int32_t*)(b + P->L.abucket);
+  D.alpha_part_e = (double*)(b + P->L.ape);
+  D.alpha_part_f = (double*)(b + P->L.apf);
+  D.dead_part = (int32_t*)(b + P->L.dead);
+  D.sv_frame = (int32_t*)(b + P->L.sv_frame);
+  D.mom = (double*)(b + P->L.mom);
+  D.cand = (int32_t*)(b + P->L.cand);
+  D.rnk = (float*)(b + P->L.rnk);
+  D.ll_part = (double*)(b + P->L.llp);
+  *out = P;
+  return TGMM_OK;
+}
+
+int tgmm_plan_destroy(TgmmPlan* P) {
+  if (!P) return TGMM_OK;
+  if (P->pending) cudaEventSynchronize(P->done_ev);
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
+  if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+  if (P->done_ev) cudaEventDestroy(P->done_ev);
+  if (P->h_info) cudaFreeHost(P->h_info);
+  if (P->h_frames) cudaFreeHost(P->h_frames);
+  if (P->h_gchunks) cudaFreeHost(P->h_gchunks);
+  if (P->h_state) cudaFreeHost(P->h_state);
+  if (P->base) cudaFree(P->base);
+  delete P;
+  return TGMM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int validate_params(const TgmmEmParams* p) {
+  if (!p) return fail(TGMM_ERR_INVALID_ARG, "params is null");
+  if (p->max_iter_em < 1) return fail(TGMM_ERR_INVALID_ARG, "max_iter_em must be >= 1");
+  if (!(p->lambda_min > 0) || !(p->lambda_max > 0) || !(p->max_excentricity > 0))
+    return fail(TGMM_ERR_NOT_SET,
+                "regularisation constants not set (lambda_min, lambda_max, max_excentricity must be > 0)");
+  for (int d = 0; d < 3; d++)
+    if (!(p->scale[d] >= 1e-3f)) return fail(TGMM_ERR_INVALID_ARG, "scale must be >= 1e-3");
+  const bool reg_zero = p->reg_scale[0] == 0.0f && p->reg_scale[1] == 0.0f && p->reg_scale[2] == 0.0f;
+  for (int d = 0; d < 3 && !reg_zero; d++)
+    if (!(p->reg_scale[d] >= 1e-3f)) return fail(TGMM_ERR_INVALID_ARG, "reg_scale must be >= 1e-3 (or all zero)");
+  if (p->ll_mode != TGMM_LL_AS_REFERENCE && p->ll_mode != TGMM_LL_TRUE)
+    return fail(TGMM_ERR_INVALID_ARG, "unknown ll_mode");
+  if (p->ll_precision != TGMM_LLPREC_MIXED && p->ll_precision != TGMM_LLPREC_FP64)
+    return fail(TGMM_ERR_INVALID_ARG, "unknown ll_precision");
+  return TGMM_OK;
+}
+
+// Fill the pinned batch tables.  Returns a status.
+int stage_batch(TgmmPlan* P, int32_t n, const TgmmFrame* fr, TgmmGaussian* const* gm, float* const* rnk,
+                int32_t* const* ind, const TgmmEmParams* prm) {
+  if (n < 1 || n > P->desc.max_frames) return fail(TGMM_ERR_BAD_SIZE, "frame count beyond plan capacity");
+  int64_t tv = 0;
+  int64_t ts = 0, tg = 0, tc = 0;
+  int32_t gc = 0;
+  for (int32_t f = 0; f < n; f++) {
+    const TgmmFrame& F = fr[f];
+    if (!F.query || !F.img || !F.centroids || !F.label_ptr || !gm[f] || !rnk[f] || !ind[f])
+      return fail(TGMM_ERR_INVALID_ARG, "null frame pointer");
+    if (F.n_vox < 0 || F.n_sv < 1 || F.n_gauss < 1) return fail(TGMM_ERR_INVALID_ARG, "frame sizes must be positive");
+    if (F.n_gauss < TGMM_J) return fail(TGMM_ERR_BAD_SIZE, "a frame needs at least 5 Gaussians");
+    tv += F.n_vox;
+    ts += F.n_sv;
+    tg += F.n_gauss;
+  }
+  if (tv > P->desc.max_vox || ts > P->desc.max_sv || tg > P->desc.max_gauss)
+    return fail(TGMM_ERR_BAD_SIZE, "batch exceeds plan capacity");
+  ts = tg = 0;
+  for (int32_t f = 0; f < n; f++) {
+    const TgmmFrame& F = fr[f];
+    FrameDesc& D = P->h_frames[f];
+    memset(&D, 0, sizeof(D));
+    D.query = F.query;
+    D.img = F.img;
+    D.cent = F.centroids;
+    D.lptr = F.label_ptr;
+    D.gm = gm[f];
+    D.rnk_out = rnk[f];
+    D.ind_out = ind[f];
+    D.n_vox = F.n_vox;
+    D.n_sv = F.n_sv;
+    D.n_gauss = F.n_gauss;
+    D.sv_base = (int32_t)ts;
+    D.g_base = (int32_t)tg;
+    D.cell_base = (int32_t)tc;
+    D.cell_budget = 2 * F.n_gauss + 2;
+    D.gchunk_base = gc;
+    D.n_gchunks = (F.n_gauss + kGChunk - 1) / kGChunk;
+    const bool reg_zero = prm->reg_scale[0] == 0.0f && prm->reg_scale[1] == 0.0f && prm->reg_scale[2] == 0.0f;
+    for (int d = 0; d < 3; d++) {
+      D.scale[d] = prm->scale[d];
+      D.reg_scale[d] = reg_zero ? prm->scale[d] : prm->reg_scale[d];
+    }
+    D.w4dof = prm->w4dof ? 1 : 0;
+    D.lambda_min = prm->lambda_min;
+    D.lambda_max = prm->lambda_max;
+    D.max_exc = prm->max_excentricity;
+    D.tol = prm->tol_likelihood;
+    D.max_iter = prm->max_iter_em;
+    D.ll_mode = prm->ll_mode;
+    D.ll_prec = prm->ll_precision;
+    for (int32_t c = 0; c < D.n_gchunks; c++) {
+      GChunk& C = P->h_gchunks[gc + c];
+      C.frame = f;
+      C.g_begin = D.g_base + c * kGChunk;
+      C.g_end = std::min(D.g_base + F.n_gauss, C.g_begin + kGChunk);
+      C.pad = 0;
+    }
+    gc += D.n_gchunks;
+    ts += F.n_sv;
+    tg += F.n_gauss;
+    tc += D.cell_budget;
+  }
+  BatchInfo& I = *P->h_info;
+  memset(&I, 0, sizeof(I));
+  I.n_frames = n;
+  I.total_sv = (int32_t)ts;
+  I.total_gauss = (int32_t)tg;
+  I.n_gchunks = gc;
+  I.total_cells = (int32_t)tc;
+  return TGMM_OK;
+}
+
+// The whole EM as a stream of async operations on `st`.
+int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
+  const DevPlan& D = P->dev;
+  TG_CUDA(cudaMemcpyAsync(D.info, P->h_info, sizeof(BatchInfo), cudaMemcpyHostToDevice, st), "stage info");
+  TG_CUDA(cudaMemcpyAsync(D.frames, P->h_frames, sizeof(FrameDesc) * P->desc.max_frames, cudaMemcpyHostToDevice, st),
+          "stage frames");
+  TG_CUDA(cudaMemcpyAsync(D.gchunks, P->h_gchunks, sizeof(GChunk) * D.max_gchunks, cudaMemcpyHostToDevice, st),
+          "stage chunks");
+  TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)D.max_gauss, st), "clear buckets");
+  TG_CUDA(cudaMemsetAsync(D.acnt, 0, 4 * (size_t)D.max_gauss, st), "clear assignment buckets");
+  launch_build_maps(D, st);
+  launch_import(D, st);
+  launch_frame_end(D, 0, st);
+  launch_moments(D, st);
+  for (int it = 0; it < max_iter; it++) {
+    launch_grid_fill(D, st);
+    launch_knn_estep(D, st);
+    launch_mstep_update(D, st);
+    launch_kill_prep(D, st);
+    launch_ll_pass(D, ll_prec == TGMM_LLPREC_FP64, st);
+    launch_frame_end(D, 1, st);
+  }
+  launch_assign(D, st);
+  launch_export(D, st);
+  TG_CUDA(cudaGetLastError(), "kernel launch");
+  return TGMM_OK;
+}
+
+bool use_graphs() {
+  const char* e = getenv("TGMM_NO_GRAPH");
+  return !(e && e[0] == '1');
+}
+
+int run_batch(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
+  if (!use_graphs()) return enqueue_em(P, max_iter, ll_prec, st);
+  auto key = std::make_pair(max_iter, ll_prec);
+  auto it = P->graphs.find(key);
+  if (it == P->graphs.end()) {
+    cudaGraph_t g = nullptr;
+    TG_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = enqueue_em(P, max_iter, ll_prec, P->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
+    if (rc != TGMM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(TGMM_ERR_CUDA, "end capture", e);
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(TGMM_ERR_CUDA, "graph instantiate", e);
+    it = P->graphs.emplace(key, ex).first;
+  }
+  TG_CUDA(cudaGraphLaunch(it->second, st), "graph launch");
+  return TGMM_OK;
+}
+
+int collect_stats(TgmmPlan* P, int32_t n, TgmmEmStats* stats, cudaStream_t st, int* flags_or) {
+  TG_CUDA(cudaMemcpyAsync(P->h_state, P->dev.state, sizeof(FrameState) * n, cudaMemcpyDeviceToHost, st),
+          "read state");
+  TG_CUDA(cudaStreamSynchronize(st), "synchronize");
+  int fo = 0;
+  for (int32_t f = 0; f < n; f++) {
+    const FrameState& S = P->h_state[f];
+    fo |= S.flags;
+    if (!stats) continue;
+    TgmmEmStats& o = stats[f];
+    o.iterations = S.iter - 1;
+    o.converged = S.converged;
+    o.ll = S.ll;
+    o.ll_true = S.ll_true;
+    o.ll_as_reference = S.ll_ref;
+    o.total_alpha = S.total_alpha;
+    o.n_dead = S.n_dead;
+    o.device_flags = S.flags;
+  }
+  if (flags_or) *flags_or = fo;
+  return TGMM_OK;
+}
+
+int flags_to_status(int flags) {
+  if (flags & F_BAD_CSR) return fail(TGMM_ERR_BAD_CSR, "labelListPtr is not a valid CSR over the voxels");
+  if (flags & F_FEW_GAUSS) return fail(TGMM_ERR_BAD_SIZE, "a frame has fewer than 5 Gaussians");
+  if (flags & F_NAN_INPUT) return fail(TGMM_ERR_NAN_INPUT, "NaN in voxel coordinates, intensities or Gaussians");
+  return TGMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
+                      float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params,
+                      TgmmEmStats* stats, void* stream) {
+  if (!P || !frames || !gm_dev || !rnk_dev || !ind_dev) return fail(TGMM_ERR_INVALID_ARG, "null argument");
+  int rc = validate_params(params);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(P->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  if (P->pending) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  P->pending = false;
+  rc = stage_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params);
+  if (rc) return rc;
+  rc = run_batch(P, params->max_iter_em, params->ll_precision, st);
+  if (rc) return rc;
+  TG_CUDA(cudaEventRecord(P->done_ev, st), "record");
+  P->pending = true;
+  if (stats) {
+    int fo = 0;
+    rc = collect_stats(P, n_frames, stats, st, &fo);
+    if (rc) return rc;
+    P->pending = false;
+    return flags_to_status(fo);
+  }
+  return TGMM_OK;
+}
+
+int tgmm_em_run_device(TgmmPlan* P, const TgmmFrame* frame, TgmmGaussian* gm_dev, float* rnk_dev, int32_t* ind_dev,
+                       const TgmmEmParams* params, TgmmEmStats* stats, void* stream) {
+  if (!frame) return fail(TGMM_ERR_INVALID_ARG, "null frame");
+  return tgmm_em_run_batch(P, 1, frame, &gm_dev, &rnk_dev, &ind_dev, params, stats, stream);
+}
+
+int tgmm_em_run(TgmmPlan* P, const TgmmFrame* frame, TgmmGaussian* gm_host, float* rnk_dev, int32_t* ind_dev,
+                int32_t* ind_tr_dev, const TgmmEmParams* params, TgmmEmStats* stats, void* stream) {
+  if (!P || !frame || !gm_host) return fail(TGMM_ERR_INVALID_ARG, "null argument");
+  if (frame->n_gauss > P->desc.max_gauss) return fail(TGMM_ERR_BAD_SIZE, "n_gauss beyond plan capacity");
+  cudaStream_t st = (cudaStream_t)stream;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  if (P->pending) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  P->pending = false;
+  TgmmGaussian* scratch = (TgmmGaussian*)(P->base + P->L.gm_scratch);
+  const size_t bytes = sizeof(TgmmGaussian) * (size_t)frame->n_gauss;
+  TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");
+  TgmmEmStats local;
+  int rc = tgmm_em_run_batch(P, 1, frame, &scratch, &rnk_dev, &ind_dev, params, stats ? stats : &local, stream);
+  if (rc != TGMM_OK && rc != TGMM_ERR_NAN_INPUT) return rc;
+  TG_CUDA(cudaMemcpyAsync(gm_host, scratch, bytes, cudaMemcpyDeviceToHost, st), "download Gaussians");
+  if (ind_tr_dev) {
+    // reference-compatible Gaussian-sorted copy of the candidate ids (indCUDAtr)
+    const size_t n = (size_t)TGMM_J * frame->n_sv;
+    std::vector<int32_t> h(n);
+    TG_CUDA(cudaMemcpyAsync(h.data(), ind_dev, n * 4, cudaMemcpyDeviceToHost, st), "read ind");
+    TG_CUDA(cudaStreamSynchronize(st), "synchronize");
+    std::stable_sort(h.begin(), h.end());
+    TG_CUDA(cudaMemcpyAsync(ind_tr_dev, h.data(), n * 4, cudaMemcpyHostToDevice, st), "write ind_tr");
+  }
+  TG_CUDA(cudaStreamSynchronize(st), "synchronize");
+  return rc;
+}
+
+int tgmm_frame_upload(const float* q, const float* img, const float* cent, const int64_t* lptr, int64_t n_vox,
+                      int32_t n_sv, TgmmFrame* out) {
+  if (!q || !img || !cent || !lptr || !out || n_vox < 0 || n_sv < 1) return fail(TGMM_ERR_INVALID_ARG, "bad frame");
+  memset(out, 0, sizeof(*out));
+  float *dq = nullptr, *di = nullptr, *dc = nullptr;
+  int64_t* dl = nullptr;
+  cudaError_t e = cudaMalloc(&dq, sizeof(float) * 3 * std::max<int64_t>(n_vox, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&di, sizeof(float) * std::max<int64_t>(n_vox, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&dc, sizeof(float) * 3 * n_sv);
+  if (e == cudaSuccess) e = cudaMalloc(&dl, sizeof(int64_t) * (n_sv + 1));
+  if (e != cudaSuccess) {
+    cudaFree(dq);
+    cudaFree(di);
+    cudaFree(dc);
+    cudaFree(dl);
+    return fail(TGMM_ERR_OOM, "tgmm_frame_upload", e);
+  }
+  e = cudaMemcpy(dq, q, sizeof(float) * 3 * n_vox, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(di, img, sizeof(float) * n_vox, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dc, cent, sizeof(float) * 3 * n_sv, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dl, lptr, sizeof(int64_t) * (n_sv + 1), cudaMemcpyHostToDevice);
+  out->query = dq;
+  out->img = di;
+  out->centroids = dc;
+  out->label_ptr = dl;
+  out->n_vox = n_vox;
+  out->n_sv = n_sv;
+  if (e != cudaSuccess) {
+    tgmm_frame_release(out);
+    return fail(TGMM_ERR_CUDA, "tgmm_frame_upload copy", e);
+  }
+  return TGMM_OK;
+}
+
+int tgmm_frame_release(TgmmFrame* f) {
+  if (!f) return TGMM_OK;
+  cudaFree((void*)f->query);
+  cudaFree((void*)f->img);
+  cudaFree((void*)f->centroids);
+  cudaFree((void*)f->label_ptr);
+  memset(f, 0, sizeof(*f));
+  return TGMM_OK;
+}
+
+int tgmm_assign_supervoxels(const float* rnk, const int32_t* ind, int32_t n_sv, TgmmGaussian* gm, int32_t n_gauss) {
+  if (!rnk || !ind || !gm || n_sv < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_assign_supervoxels");
+  for (int32_t k = 0; k < n_gauss; k++) gm[k].supervoxelNum = 0;
+  int64_t p = 0;
+  for (int j = 0; j < TGMM_J; j++)
+    for (int32_t s = 0; s < n_sv; s++, p++) {
+      if ((double)rnk[p] > 0.5) {
+        const int32_t k = ind[p];
+        if (k < 0 || k >= n_gauss) return fail(TGMM_ERR_INVALID_ARG, "ind out of range");
+        TgmmGaussian& g = gm[k];
+        if (g.supervoxelNum < TGMM_MAX_SV_PER_GAUSSIAN) g.supervoxelIdx[g.supervoxelNum++] = s;
+      }
+    }
+  return TGMM_OK;
+}
+
+int tgmm_write_rnk_file(const char* path, const float* rnk, const int32_t* ind, int32_t n_sv) {
+  if (!path || !rnk || !ind || n_sv < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_write_rnk_file");
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return fail(TGMM_ERR_INVALID_ARG, "cannot open rnk file");
+  const int32_t hdr[2] = {n_sv, TGMM_J};
+  size_t ok = fwrite(hdr, sizeof(int32_t), 2, fp);
+  ok += fwrite(rnk, sizeof(float), (size_t)TGMM_J * n_sv, fp);
+  ok += fwrite(ind, sizeof(int32_t), (size_t)TGMM_J * n_sv, fp);
+  fclose(fp);
+  if (ok != 2 + 2 * (size_t)TGMM_J * n_sv) return fail(TGMM_ERR_INVALID_ARG, "short write of rnk file");
+  return TGMM_OK;
+}
+
+int tgmm_knn(const float* query, int64_t nq, const float* ref, int32_t nref, const float scale[3], int32_t* ind,
+             void* stream) {
+  if (!query || !ref || !scale || !ind || nq < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_knn");
+  if (nref < TGMM_J) return fail(TGMM_ERR_BAD_SIZE, "tgmm_knn needs at least 5 reference points");
+  if (nq == 0) return TGMM_OK;
+  cudaError_t e = knn_grid_standalone(query, nq, ref, nref, scale, ind, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(TGMM_ERR_CUDA, "tgmm_knn", e);
+  return TGMM_OK;
+}
+
+int tgmm_update_priors(TgmmGaussian* gm, int32_t n, double bp, double np, double ap, double atot, int32_t compute,
+                       void* stream) {
+  if (!gm || n < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_update_priors");
+  if (n == 0) return TGMM_OK;
+  cudaError_t e = update_priors_device(gm, n, bp, np, ap, atot, compute, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(TGMM_ERR_CUDA, "tgmm_update_priors", e);
+  return TGMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1379 @@
+// em_kernels.cu -- the sm_100a kernels of the supervoxel VI-EM.
+//
+// One EM call is:  build_maps, import, frame_end(init), moments,
+//                  then per iteration: grid_fill, knn_estep, mstep_update, kill_prep,
+//                  ll_pass, frame_end(iter);  finally assign, export.
+// Every kernel loops over the whole batch (one or many frames); frames that have
+// converged are skipped through their FrameState::done flag, so a captured graph of
+// max_iter iterations serves any batch.  No kernel uses float atomics: per-frame sums
+// are fixed-order sums of frame-aligned chunk partials, the M-step visits each
+// Gaussian's (supervoxel, slot) pairs in ascending position order, and results are
+// bit-identical whether a frame runs alone or inside a batch.
+#include <float.h>
+#include <stdio.h>
+
+#include "tgmm_internal.cuh"
+
+namespace tgmm {
+
+namespace {
+
+constexpr float kInfF = __builtin_huge_valf();
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;  // identical in every lane: each butterfly level adds commutative pairs
+}
+
+__device__ __forceinline__ int warp_sum_i(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fixed-order sum of the partials [base, base+n) by one warp: lane l adds l, l+32, ...
+// in order, then a butterfly.  Every warp that calls it with the same data gets the
+// same bits.
+__device__ __forceinline__ double warp_sum_range(const double* a, int base, int n) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += a[base + i];
+  return warp_sum(s);
+}
+
+// Block (kGChunk threads) fixed-order sum; result valid in thread 0.
+__device__ __forceinline__ double block_sum_gchunk(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kGChunk / 32; i++) t += sh[i];
+  return t;
+}
+
+__device__ __forceinline__ int block_sum_gchunk_i(int v, int* sh) {
+  v = warp_sum_i(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int t = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kGChunk / 32; i++) t += sh[i];
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// kNN primitives.  Distance (FP32, the reference's formula and rounding):
+//   a = (q0 - r0) * s0;  d = a*a;  b = (q1 - r1) * s1;  d = fma(b, b, d);  c = ...; d = fma(c, c, d)
+// Order: (d, index) ascending, NaN as +inf -> ties go to the lower index.
+// ---------------------------------------------------------------------------
+struct Top5 {
+  float d[kJ];
+  int i[kJ];
+};
+
+__device__ __forceinline__ void top5_init(Top5& t) {
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+    t.d[j] = kInfF;
+    t.i[j] = 0x7fffffff;
+  }
+}
+
+__device__ __forceinline__ bool before(float da, int ia, float db, int ib) {
+  return da < db || (da == db && ia < ib);
+}
+
+__device__ __forceinline__ void top5_insert(Top5& t, float d, int idx) {
+  if (!before(d, idx, t.d[kJ - 1], t.i[kJ - 1])) return;
+  t.d[kJ - 1] = d;
+  t.i[kJ - 1] = idx;
+#pragma unroll
+  for (int p = kJ - 1; p > 0; --p) {
+    if (before(t.d[p], t.i[p], t.d[p - 1], t.i[p - 1])) {
+      float td = t.d[p];
+      t.d[p] = t.d[p - 1];
+      t.d[p - 1] = td;
+      int ti = t.i[p];
+      t.i[p] = t.i[p - 1];
+      t.i[p - 1] = ti;
+    }
+  }
+}
+
+__device__ __forceinline__ float knn_dist(float q0, float q1, float q2, float r0, float r1,
+                                          float r2, const float* s) {
+  float a = __fmul_rn(__fsub_rn(q0, r0), s[0]);
+  float d = __fmul_rn(a, a);
+  float b = __fmul_rn(__fsub_rn(q1, r1), s[1]);
+  d = __fmaf_rn(b, b, d);
+  float c = __fmul_rn(__fsub_rn(q2, r2), s[2]);
+  d = __fmaf_rn(c, c, d);
+  return isnan(d) ? kInfF : d;
+}
+
+// Grid geometry of one point set (the queries' bounding box in scaled space).
+struct GridGeom {
+  float lo[3];
+  float h, inv_h;
+  int dims[3];
+};
+
+__device__ __forceinline__ int cell_coord(float y, float lo, float inv_h, int dim) {
+  float u = (y - lo) * inv_h;
+  int c = (u > 0.0f) ? (u < (float)dim ? (int)u : dim - 1) : 0;  // NaN -> 0 (not used)
+  return c;
+}
+
+// Exact grid search: rings of cells at growing Chebyshev distance r around the query's
+// cell; stop after ring r once the fifth distance is strictly below the squared lower
+// bound (r*h + delta - eps)^2 of every unvisited cell.  eps absorbs float rounding of
+// the scaled coordinates and of the distance itself.  Refs outside the box sit in the
+// boundary cells, which keeps the bound valid for queries inside the box.
+__device__ void knn_grid_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
+                                const int32_t* __restrict__ cstart, const float4* __restrict__ refs,
+                                Top5& t) {
+  const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
+  int c[3];
+  float delta = kInfF;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    c[a] = cell_coord(y[a], g.lo[a], g.inv_h, g.dims[a]);
+    float f0 = y[a] - (g.lo[a] + c[a] * g.h);
+    float f1 = (g.lo[a] + (c[a] + 1) * g.h) - y[a];
+    delta = fminf(delta, fminf(f0, f1));
+  }
+  delta = fmaxf(delta, 0.0f);
+  const int maxr = max(g.dims[0], max(g.dims[1], g.dims[2]));
+  for (int r = 0; r <= maxr; ++r) {
+    const int z0 = max(c[2] - r, 0), z1 = min(c[2] + r, g.dims[2] - 1);
+    const int y0 = max(c[1] - r, 0), y1 = min(c[1] + r, g.dims[1] - 1);
+    for (int z = z0; z <= z1; ++z) {
+      const bool zedge = (z == c[2] - r) || (z == c[2] + r);
+      for (int yy = y0; yy <= y1; ++yy) {
+        const bool edge = zedge || (yy == c[1] - r) || (yy == c[1] + r);
+        const int row = (z * g.dims[1] + yy) * g.dims[0];
+        int xa, xb, step;
+        if (edge) {
+          xa = max(c[0] - r, 0);
+          xb = min(c[0] + r, g.dims[0] - 1);
+          step = 1;
+        } else {
+          xa = c[0] - r;
+          xb = c[0] + r;
+          step = 2 * r;
+        }
+        for (int x = xa; x <= xb; x += step) {
+          if (x < 0 || x >= g.dims[0]) continue;
+          const int cell = row + x;
+          const int b = cstart[cell], e = cstart[cell + 1];
+          for (int k = b; k < e; ++k) {
+            const float4 rr = refs[k];
+            top5_insert(t, knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s), __float_as_int(rr.w));
+          }
+        }
+      }
+    }
+    const float lb = r * g.h + delta;
+    const float eps = 4e-3f + 1e-6f * lb;
+    if (lb > eps) {
+      const float bound = (lb - eps) * (lb - eps);
+      if (t.d[kJ - 1] < bound) break;
+    }
+  }
+}
+
+__device__ __forceinline__ FrameDesc load_desc(const DevPlan& P, int f) { return P.frames[f]; }
+
+}  // namespace
+
+
+// Grid geometry over the bounding box [lo, hi] (scaled space): cubic cells of side h,
+// about one reference per cell, at most budget-1 cells in total.
+__device__ void set_geometry(FrameState* S, const float* lo, const float* hi, int n_ref, int cell_budget) {
+  float ext[3];
+  double vol = 1.0;
+  for (int d = 0; d < 3; d++) {
+    ext[d] = fmaxf(hi[d] - lo[d], 1.0f);
+    vol *= ext[d];
+  }
+  const int budget = max(cell_budget - 1, 1);
+  const int target = max(1, min(budget, n_ref));
+  float h = (float)cbrt(vol / target);
+  int dims[3] = {1, 1, 1};
+  for (int guard = 0; guard < 400; guard++) {
+    long long tot = 1;
+    for (int d = 0; d < 3; d++) {
+      dims[d] = max(1, min(1024, (int)ceilf(ext[d] / h)));
+      tot *= dims[d];
+    }
+    if (tot <= budget) break;
+    h *= 1.1f;
+  }
+  for (int d = 0; d < 3; d++) {
+    S->lo[d] = lo[d];
+    S->dims[d] = dims[d];
+  }
+  S->h = h;
+  S->inv_h = 1.0f / h;
+  S->n_cells = dims[0] * dims[1] * dims[2];
+}
+
+// ===========================================================================
+// build_maps: per frame -- supervoxel/Gaussian -> frame maps, CSR validation,
+// centroid bounding box and grid geometry, EM state reset.
+// ===========================================================================
+__global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
+  const int f = blockIdx.x;
+  if (f >= P.info->n_frames) return;
+  const FrameDesc D = load_desc(P, f);
+  FrameState* S = &P.state[f];
+  __shared__ float smin[3][32], smax[3][32];
+  __shared__ int sbad;
+  if (threadIdx.x == 0) sbad = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) P.sv_frame[D.sv_base + i] = f;
+  for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) P.g_frame[D.g_base + i] = f;
+  for (int i = threadIdx.x; i < D.cell_budget; i += blockDim.x) P.cell_cnt[D.cell_base + i] = 0;
+  int bad = 0;
+  float lo[3] = {kInfF, kInfF, kInfF}, hi[3] = {-kInfF, -kInfF, -kInfF};
+  for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
+    const int64_t a = D.lptr[i], b = D.lptr[i + 1];
+    if (a < 0 || b < a || b > D.n_vox) bad = 1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const float y = D.cent[(int64_t)d * D.n_sv + i] * D.scale[d];
+      if (!isfinite(y)) {
+        bad |= 2;
+        continue;
+      }
+      lo[d] = fminf(lo[d], y);
+      hi[d] = fmaxf(hi[d], y);
+    }
+  }
+  if (bad) atomicOr(&sbad, bad);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int d = 0; d < 3; d++) {
+      smin[d][w] = lo[d];
+      smax[d][w] = hi[d];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int d = 0; d < 3; d++) {
+      lo[d] = smin[d][0];
+      hi[d] = smax[d][0];
+      for (int i = 1; i < (int)(blockDim.x >> 5); i++) {
+        lo[d] = fminf(lo[d], smin[d][i]);
+        hi[d] = fmaxf(hi[d], smax[d][i]);
+      }
+      if (!(lo[d] <= hi[d])) {
+        lo[d] = 0.0f;
+        hi[d] = 0.0f;
+      }
+    }
+    int flags = 0;
+    if (sbad & 1) flags |= F_BAD_CSR;
+    if (sbad & 2) flags |= F_NAN_INPUT;
+    if (D.n_gauss < kJ) flags |= F_FEW_GAUSS;
+    set_geometry(S, lo, hi, D.n_gauss, D.cell_budget);
+    S->iter = 1;
+    S->done = (flags & (F_BAD_CSR | F_FEW_GAUSS)) ? 1 : 0;
+    S->converged = 0;
+    S->flags = flags;
+    S->n_dead = 0;
+    S->ll = -1.0;
+    S->ll1 = -10.0;
+    S->ll2 = -100.0;
+    S->ll3 = -1000.0;
+    S->ll_true = 0.0;
+    S->ll_ref = 0.0;
+    S->total_alpha = 0.0;
+    S->psi_total[0] = S->psi_total[1] = 0.0;
+  }
+}
+
+// Gaussian -> grid cell (or -1 when its float centre is unusable for pruning).
+__device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc& D, float x, float y,
+                                           float z) {
+  const float ys[3] = {x * D.scale[0], y * D.scale[1], z * D.scale[2]};
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    if (!isfinite(ys[d]) || fabsf(ys[d]) >= 1e25f) return -1;
+  const int cx = cell_coord(ys[0], S.lo[0], S.inv_h, S.dims[0]);
+  const int cy = cell_coord(ys[1], S.lo[1], S.inv_h, S.dims[1]);
+  const int cz = cell_coord(ys[2], S.lo[2], S.inv_h, S.dims[2]);
+  return (cz * S.dims[1] + cy) * S.dims[0] + cx;
+}
+
+// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], grid cell.
+__device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
+                                              int k, int parity) {
+  const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
+  double W[6];
+#pragma unroll
+  for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
+  const double nu = gcomp(P, G_NU, k);
+  gcomp(P, G_PSIA0 + parity, k) = digamma(gcomp(P, G_ALPHA, k));
+  gcomp(P, G_ELD0 + parity, k) = dead ? -1e32 : expected_log_det(W, nu);
+  int cell = -1;
+  if (!dead) {
+    const float x = __double2float_rn(gcomp(P, G_M0, k));
+    const float y = __double2float_rn(gcomp(P, G_M1, k));
+    const float z = __double2float_rn(gcomp(P, G_M2, k));
+    cell = ref_cell_of(S, D, x, y, z);
+    if (cell >= 0) atomicAdd(&P.cell_cnt[D.cell_base + cell], 1);
+  }
+  P.ref_cell[k] = cell;
+}
+
+// ===========================================================================
+// import: AoS (288-byte records) -> SoA, validation, preparation of iteration 1.
+// ===========================================================================
+__global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
+  const int c = blockIdx.x;
+  if (c >= P.info->n_gchunks) return;
+  const GChunk ch = P.gchunks[c];
+  const FrameDesc D = load_desc(P, ch.frame);
+  const FrameState S = P.state[ch.frame];
+  __shared__ double shd[kGChunk / 32];
+  __shared__ int shi[kGChunk / 32];
+  const int k = ch.g_begin + threadIdx.x;
+  double alpha = 0.0;
+  int dead = 0;
+  if (k < ch.g_end) {
+    const TgmmGaussian& g = D.gm[k - D.g_base];
+    bool bad = false;
+    gcomp(P, G_BETA, k) = g.beta_k;
+    gcomp(P, G_NU, k) = g.nu_k;
+    gcomp(P, G_ALPHA, k) = g.alpha_k;
+    for (int d = 0; d < 3; d++) gcomp(P, G_M0 + d, k) = g.m_k[d];
+    for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = g.W_k[e];
+    gcomp(P, G_BETAO, k) = g.beta_o;
+    gcomp(P, G_NUO, k) = g.nu_o;
+    gcomp(P, G_ALPHAO, k) = g.alpha_o;
+    for (int d = 0; d < 3; d++) gcomp(P, G_MO0 + d, k) = g.m_o[d];
+    for (int e = 0; e < 6; e++) gcomp(P, G_WO0 + e, k) = g.W_o[e];
+    P.fixed[k] = g.fixed ? 1 : 0;
+    bad = isnan(g.beta_k) || isnan(g.nu_k) || isnan(g.alpha_k);
+    for (int d = 0; d < 3; d++) bad = bad || isnan(g.m_k[d]);
+    for (int e = 0; e < 6; e++) bad = bad || isnan(g.W_k[e]);
+    if (bad) atomicOr(&P.state[ch.frame].flags, F_NAN_INPUT);
+    prep_gaussian(P, D, S, k, 1);
+    alpha = gcomp(P, G_ALPHA, k);
+    dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
+  }
+  const double a = block_sum_gchunk(alpha, shd);
+  const int nd = block_sum_gchunk_i(dead, shi);
+  if (threadIdx.x == 0) {
+    P.alpha_part_f[c] = a;
+    P.dead_part[c] = nd;
+  }
+}
+
+// ===========================================================================
+// frame_end: per frame.  mode 0 (after import): alpha total, psi, cell scan.
+// mode 1 (after an iteration): log-likelihood sums, convergence test of the
+// reference's loop (GMEMupdateCUDA.cu:4145-4148), alpha total, psi, cell scan.
+// ===========================================================================
+__global__ void __launch_bounds__(kFrameThreads) k_frame_end(DevPlan P, int mode) {
+  const int f = blockIdx.x;
+  if (f >= P.info->n_frames) return;
+  FrameState* S = &P.state[f];
+  if (S->done) return;
+  const FrameDesc D = load_desc(P, f);
+  __shared__ double sh[2][kFrameThreads / 32];
+  __shared__ int s_done;
+  __shared__ int scan[kFrameThreads];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = S->iter;  // the iteration that just ran (mode 1) or 1 (mode 0)
+
+  // alpha total after the kill step (or of the input for mode 0); dead count
+  __shared__ double s_alpha;
+  __shared__ int s_dead;
+  if (threadIdx.x < 32) {
+    const double a = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
+    int nd = 0;
+    for (int i = lane; i < D.n_gchunks; i += 32) nd += P.dead_part[D.gchunk_base + i];
+    nd = warp_sum_i(nd);
+    if (threadIdx.x == 0) {
+      s_alpha = a;
+      s_dead = nd;
+    }
+  }
+  double lt = 0.0, lr = 0.0;
+  if (mode == 1) {
+    for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
+      lt += P.ll_part[D.sv_base + i];
+      lr += P.ll_part[(int64_t)P.max_sv + D.sv_base + i];
+    }
+  }
+  lt = warp_sum(lt);
+  lr = warp_sum(lr);
+  if (lane == 0) sh[1][w] = lt;
+  __syncthreads();
+  double lt_tot = 0.0;
+  const double a_tot = s_alpha;
+  const int nd_tot = s_dead;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) lt_tot += sh[1][i];
+  __syncthreads();
+  if (lane == 0) sh[1][w] = lr;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double lr_tot = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) lr_tot += sh[1][i];
+    int done = 0;
+    int next = t;
+    if (mode == 1) {
+      S->ll3 = S->ll2;
+      S->ll2 = S->ll1;
+      S->ll1 = S->ll;
+      S->ll_true = lt_tot;
+      S->ll_ref = lr_tot;
+      S->ll = (D.ll_mode == TGMM_LL_TRUE) ? lt_tot : lr_tot;
+      next = t + 1;
+      S->iter = next;
+      const double ll = S->ll;
+      const bool go = fabs(ll - S->ll1) / fabs(S->ll1) > D.tol && fabs(ll - S->ll2) / fabs(S->ll2) > D.tol &&
+                      fabs(ll - S->ll3) / fabs(S->ll3) > D.tol;
+      if (!go) S->converged = 1;
+      done = (!go || next > D.max_iter) ? 1 : 0;
+    }
+    S->total_alpha = a_tot;
+    S->psi_total[next & 1] = digamma(a_tot);
+    S->n_dead = nd_tot;
+    S->done = done;
+    s_done = done;
+  }
+  __syncthreads();
+  if (s_done) return;
+  // exclusive scan of the cell counts -> absolute starts into cell_refs
+  const int n = S->n_cells;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
+  int local = 0;
+  for (int i = b0; i < b1; i++) local += P.cell_cnt[D.cell_base + i];
+  scan[threadIdx.x] = local;
+  __syncthreads();
+  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+    int v = (threadIdx.x >= (unsigned)off) ? scan[threadIdx.x - off] : 0;
+    __syncthreads();
+    scan[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = D.g_base + scan[threadIdx.x] - local;
+  for (int i = b0; i < b1; i++) {
+    const int cnt = P.cell_cnt[D.cell_base + i];
+    P.cell_start[D.cell_base + i] = run;
+    P.cell_cur[D.cell_base + i] = run;
+    P.cell_cnt[D.cell_base + i] = 0;
+    run += cnt;
+  }
+  if (threadIdx.x == blockDim.x - 1) P.cell_start[D.cell_base + n] = D.g_base + scan[blockDim.x - 1];
+}
+
+// ===========================================================================
+// moments: once per call.  Warp per supervoxel; centred at the supervoxel centroid
+// c_s: per-voxel differences e = x - c_s in FP32, accumulation in FP64 (B200 runs
+// FP64 at half the FP32 rate, cheaper here than compensated FP32).  19 moments:
+// sum e, sum e e', sum I, sum I e, sum I e e'.
+// ===========================================================================
+__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
+  const int total = P.info->total_sv;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = 0; q < kSvPerWarpV; q++) {
+    const int s = blockIdx.x * kSvPerBlockV + q * kWarpsPerBlockV + warp;
+    if (s >= total) return;
+    const int f = P.sv_frame[s];
+    const FrameDesc D = load_desc(P, f);
+    const int sl = s - D.sv_base;
+    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;  // flagged by build_maps
+    const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
+    const float* __restrict__ qx = D.query;
+    const float* __restrict__ qy = D.query + D.n_vox;
+    const float* __restrict__ qz = D.query + 2 * D.n_vox;
+    const float* __restrict__ im = D.img;
+    double m[kNumMoments];
+#pragma unroll
+    for (int i = 0; i < kNumMoments; i++) m[i] = 0.0;
+    bool nan_seen = false;
+    for (int64_t v = p0 + lane; v < p1; v += 32) {
+      const float x = __ldg(qx + v), y = __ldg(qy + v), z = __ldg(qz + v), I = __ldg(im + v);
+      nan_seen |= isnan(x) || isnan(y) || isnan(z) || isnan(I);
+      const double e0 = (double)(x - c0), e1 = (double)(y - c1), e2 = (double)(z - c2);
+      const double wI = (double)I;
+      m[M_E0] += e0;
+      m[M_E1] += e1;
+      m[M_E2] += e2;
+      m[M_EE00] = fma(e0, e0, m[M_EE00]);
+      m[M_EE01] = fma(e0, e1, m[M_EE01]);
+      m[M_EE02] = fma(e0, e2, m[M_EE02]);
+      m[M_EE11] = fma(e1, e1, m[M_EE11]);
+      m[M_EE12] = fma(e1, e2, m[M_EE12]);
+      m[M_EE22] = fma(e2, e2, m[M_EE22]);
+      m[M_I] += wI;
+      const double i0 = wI * e0, i1 = wI * e1, i2 = wI * e2;
+      m[M_IE0] += i0;
+      m[M_IE1] += i1;
+      m[M_IE2] += i2;
+      m[M_IEE00] = fma(i0, e0, m[M_IEE00]);
+      m[M_IEE01] = fma(i0, e1, m[M_IEE01]);
+      m[M_IEE02] = fma(i0, e2, m[M_IEE02]);
+      m[M_IEE11] = fma(i1, e1, m[M_IEE11]);
+      m[M_IEE12] = fma(i1, e2, m[M_IEE12]);
+      m[M_IEE22] = fma(i2, e2, m[M_IEE22]);
+    }
+    if (__any_sync(0xffffffffu, nan_seen) && lane == 0) atomicOr(&P.state[f].flags, F_NAN_INPUT);
+#pragma unroll
+    for (int i = 0; i < kNumMoments; i++) m[i] = warp_sum(m[i]);
+    // lane i writes component i
+#pragma unroll
+    for (int i = 0; i < kNumMoments; i++)
+      if (lane == i) P.mom[(int64_t)i * P.max_sv + s] = m[i];
+  }
+}
+
+// ===========================================================================
+// grid_fill: scatter each live Gaussian's float centre into its cell.
+// ===========================================================================
+__global__ void __launch_bounds__(kGChunk) k_grid_fill(DevPlan P) {
+  const int c = blockIdx.x;
+  if (c >= P.info->n_gchunks) return;
+  const GChunk ch = P.gchunks[c];
+  if (P.state[ch.frame].done) return;
+  const FrameDesc D = load_desc(P, ch.frame);
+  const int k = ch.g_begin + threadIdx.x;
+  if (k >= ch.g_end) return;
+  const int cell = P.ref_cell[k];
+  if (cell < 0) return;
+  const int pos = atomicAdd(&P.cell_cur[D.cell_base + cell], 1);
+  const float x = __double2float_rn(gcomp(P, G_M0, k));
+  const float y = __double2float_rn(gcomp(P, G_M1, k));
+  const float z = __double2float_rn(gcomp(P, G_M2, k));
+  P.cell_refs[pos] = make_float4(x, y, z, __int_as_float(k - D.g_base));
+}
+
+// ===========================================================================
+// knn_estep: thread per supervoxel.  Exact 5-NN of the centroid among the frame's
+// Gaussian centres, then the E-step from the supervoxel's moments:
+//   L_j = sum_v [-1/2 (3/beta + nu d'Wd) + E ln pi + 1/2 E ln|Lambda|]
+//       = -1/2 (3 n/beta + nu tr(W D)) + n (psi(alpha) - psi(sum alpha) + 1/2 E ln|Lambda|),
+//   D = sum_v (x_v - m)(x_v - m)' = G2 - G1 u' - u G1' + n u u',  u = m - c_s,
+// in FP64; then the reference's float-storage semantics (empty supervoxel -> 0, dead
+// candidate or |L| beyond float range -> -inf) and rnk_j = 1 / sum_i exp(L_i - L_j).
+// Pairs with rnk > 1e-3 go to the Gaussian's M-step bucket.
+// ===========================================================================
+__global__ void __launch_bounds__(kSvPerBlockT) k_knn_estep(DevPlan P) {
+  const int s = blockIdx.x * kSvPerBlockT + threadIdx.x;
+  if (s >= P.info->total_sv) return;
+  const int f = P.sv_frame[s];
+  const FrameState& S = P.state[f];
+  if (S.done) return;
+  const FrameDesc D = load_desc(P, f);
+  const int sl = s - D.sv_base;
+  const int Sf = D.n_sv;
+  const float q0 = D.cent[sl], q1 = D.cent[(int64_t)Sf + sl], q2 = D.cent[2 * (int64_t)Sf + sl];
+  GridGeom g;
+  for (int d = 0; d < 3; d++) {
+    g.lo[d] = S.lo[d];
+    g.dims[d] = S.dims[d];
+  }
+  g.h = S.h;
+  g.inv_h = S.inv_h;
+  Top5 t;
+  top5_init(t);
+  knn_grid_search(q0, q1, q2, D.scale, g, P.cell_start + D.cell_base, P.cell_refs, t);
+  if (!(t.d[kJ - 1] < kInfF)) {
+    // fewer than five finite distances: exact scan of every Gaussian of the frame
+    top5_init(t);
+    for (int kl = 0; kl < D.n_gauss; kl++) {
+      const int k = D.g_base + kl;
+      const float x = __double2float_rn(gcomp(P, G_M0, k));
+      const float y = __double2float_rn(gcomp(P, G_M1, k));
+      const float z = __double2float_rn(gcomp(P, G_M2, k));
+      top5_insert(t, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
+    }
+  }
+  const int par = S.iter & 1;
+  const double psiT = S.psi_total[par];
+  int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+  const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
+  double G1[3], G2[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
+#pragma unroll
+  for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
+  const double c[3] = {(double)q0, (double)q1, (double)q2};
+  double L[kJ];
+  int gk[kJ];
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+    const int kl = t.i[j];
+    const int k = D.g_base + kl;
+    gk[j] = k;
+    double Lj;
+    if (n == 0.0) {
+      Lj = 0.0;
+    } else if (is_dead_prior(gcomp(P, G_MO0, k))) {
+      Lj = -(double)kInfF;
+    } else {
+      const double beta = gcomp(P, G_BETA, k), nu = gcomp(P, G_NU, k);
+      const double u0 = gcomp(P, G_M0, k) - c[0], u1 = gcomp(P, G_M1, k) - c[1], u2 = gcomp(P, G_M2, k) - c[2];
+      const double D00 = G2[0] - 2.0 * G1[0] * u0 + n * u0 * u0;
+      const double D01 = G2[1] - (G1[0] * u1 + u0 * G1[1]) + n * u0 * u1;
+      const double D02 = G2[2] - (G1[0] * u2 + u0 * G1[2]) + n * u0 * u2;
+      const double D11 = G2[3] - 2.0 * G1[1] * u1 + n * u1 * u1;
+      const double D12 = G2[4] - (G1[1] * u2 + u1 * G1[2]) + n * u1 * u2;
+      const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
+      const double tr = gcomp(P, G_W0, k) * D00 + gcomp(P, G_W3, k) * D11 + gcomp(P, G_W5, k) * D22 +
+                        2.0 * (gcomp(P, G_W1, k) * D01 + gcomp(P, G_W2, k) * D02 + gcomp(P, G_W4, k) * D12);
+      const double eLR = gcomp(P, G_PSIA0 + par, k) - psiT;
+      const double eLD = gcomp(P, G_ELD0 + par, k);
+      Lj = -0.5 * (3.0 * n / beta + nu * tr) + n * (eLR + 0.5 * eLD);
+      if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
+      if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
+    }
+    L[j] = Lj;
+  }
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < kJ; i++) acc += exp(L[i] - L[j]);
+    const float r = __double2float_rn(1.0 / acc);
+    const int64_t pos = (int64_t)j * Sf + sl;
+    D.rnk_out[pos] = r;
+    D.ind_out[pos] = t.i[j];
+    P.cand[(int64_t)s * kJ + j] = gk[j];
+    P.rnk[(int64_t)s * kJ + j] = r;
+    if ((double)r > 1e-3) {
+      const int b = atomicAdd(&P.bcnt[gk[j]], 1);
+      if (b < kBucketCap) P.bucket[(int64_t)gk[j] * kBucketCap + b] = (int)pos;
+    }
+  }
+}
+
+// M-step contribution of one (supervoxel, slot) pair to Gaussian k, moments re-centred
+// from the supervoxel centroid to m_ref (the Gaussian's current mean):
+//   A0 += r H0;  A1 += r (H1 + H0 d);  A2 += r (H2 + H1 d' + d H1' + H0 d d'),  d = c_s - m_ref.
+__device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, int p, const double* mref,
+                                          double* A) {
+  const int Sf = D.n_sv;
+  const int j = p / Sf, sl = p - j * Sf;
+  const int s = D.sv_base + sl;
+  const double r = (double)P.rnk[(int64_t)s * kJ + j];
+  const double d0 = (double)D.cent[sl] - mref[0];
+  const double d1 = (double)D.cent[(int64_t)Sf + sl] - mref[1];
+  const double d2 = (double)D.cent[2 * (int64_t)Sf + sl] - mref[2];
+  const double h0 = P.mom[(int64_t)M_I * P.max_sv + s];
+  const double h1[3] = {P.mom[(int64_t)M_IE0 * P.max_sv + s], P.mom[(int64_t)M_IE1 * P.max_sv + s],
+                        P.mom[(int64_t)M_IE2 * P.max_sv + s]};
+  const double h2[6] = {P.mom[(int64_t)M_IEE00 * P.max_sv + s], P.mom[(int64_t)M_IEE01 * P.max_sv + s],
+                        P.mom[(int64_t)M_IEE02 * P.max_sv + s], P.mom[(int64_t)M_IEE11 * P.max_sv + s],
+                        P.mom[(int64_t)M_IEE12 * P.max_sv + s], P.mom[(int64_t)M_IEE22 * P.max_sv + s]};
+  const double d[3] = {d0, d1, d2};
+  A[0] += r * h0;
+  A[1] += r * (h1[0] + h0 * d0);
+  A[2] += r * (h1[1] + h0 * d1);
+  A[3] += r * (h1[2] + h0 * d2);
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int e = 0; e < 6; e++)
+    A[4 + e] += r * (h2[e] + h1[ia[e]] * d[ib[e]] + d[ia[e]] * h1[ib[e]] + h0 * d[ia[e]] * d[ib[e]]);
+}
+
+// Block-cooperative ordered scan for Gaussians whose bucket overflowed: visit every
+// position p = j*S + s of the frame in increasing order, keep those whose candidate is k
+// and whose rnk exceeds `thr`; `visit(p)` is called by thread 0 in increasing p order.
+template <typename F>
+__device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int k, double thr, int* sh_list,
+                             int* sh_cnt, F visit) {
+  const int64_t total = (int64_t)kJ * D.n_sv;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t base = 0; base < total; base += blockDim.x) {
+    const int64_t p = base + threadIdx.x;
+    bool pred = false;
+    if (p < total) {
+      const int j = (int)(p / D.n_sv), sl = (int)(p - (int64_t)j * D.n_sv);
+      const int64_t idx = (int64_t)(D.sv_base + sl) * kJ + j;
+      pred = (P.cand[idx] == k) && ((double)P.rnk[idx] > thr);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (lane == 0) sh_cnt[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+        const int c = sh_cnt[i];
+        sh_cnt[i] = run;
+        run += c;
+      }
+      sh_cnt[blockDim.x >> 5] = run;
+    }
+    __syncthreads();
+    if (pred) sh_list[sh_cnt[w] + __popc(m & ((1u << lane) - 1u))] = (int)p;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < sh_cnt[blockDim.x >> 5]; i++) visit(sh_list[i]);
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
+// mstep_update: thread per Gaussian.  Sorted bucket -> FP64 sufficient statistics ->
+// Dirichlet / Normal-Wishart update (GMEMupdateCUDA.cu:1601-1677) -> regularisation
+// (:1693-1809).  Writes the chunk's alpha sum for the kill step.
+// ===========================================================================
+__global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
+  const int c = blockIdx.x;
+  if (c >= P.info->n_gchunks) return;
+  const GChunk ch = P.gchunks[c];
+  if (P.state[ch.frame].done) return;
+  const FrameDesc D = load_desc(P, ch.frame);
+  __shared__ int sbuf[kBucketCap][kGChunk];
+  __shared__ int s_ovf[kGChunk];
+  __shared__ int s_novf;
+  __shared__ double s_ovf_acc[kGChunk][10];
+  __shared__ int s_list[kGChunk];
+  __shared__ int s_cnt[kGChunk / 32 + 1];
+  __shared__ double shd[kGChunk / 32];
+  if (threadIdx.x == 0) s_novf = 0;
+  __syncthreads();
+  const int k = ch.g_begin + threadIdx.x;
+  const bool valid = k < ch.g_end;
+  double A[10];
+#pragma unroll
+  for (int i = 0; i < 10; i++) A[i] = 0.0;
+  double mref[3] = {0, 0, 0};
+  bool ovf = false;
+  if (valid) {
+    for (int d = 0; d < 3; d++) mref[d] = gcomp(P, G_M0 + d, k);
+    const int n = P.bcnt[k];
+    P.bcnt[k] = 0;
+    if (n > kBucketCap) {
+      ovf = true;
+      const int o = atomicAdd(&s_novf, 1);
+      s_ovf[o] = threadIdx.x;
+      atomicOr(&P.state[ch.frame].flags, F_BUCKET_OVERFLOW);
+    } else {
+      for (int i = 0; i < n; i++) {  // insertion sort by position
+        int v = P.bucket[(int64_t)k * kBucketCap + i];
+        int q = i;
+        while (q > 0 && sbuf[q - 1][threadIdx.x] > v) {
+          sbuf[q][threadIdx.x] = sbuf[q - 1][threadIdx.x];
+          q--;
+        }
+        sbuf[q][threadIdx.x] = v;
+      }
+      for (int i = 0; i < n; i++) mstep_add(P, D, sbuf[i][threadIdx.x], mref, A);
+    }
+  }
+  __syncthreads();
+  const int novf = s_novf;
+  for (int o = 0; o < novf; o++) {
+    const int tk = s_ovf[o];
+    const int kk = ch.g_begin + tk;
+    double mr[3] = {gcomp(P, G_M0, kk), gcomp(P, G_M1, kk), gcomp(P, G_M2, kk)};
+    double acc[10];
+    for (int i = 0; i < 10; i++) acc[i] = 0.0;
+    ordered_scan(P, D, kk, 1e-3, s_list, s_cnt, [&](int p) { mstep_add(P, D, p, mr, acc); });
+    if (threadIdx.x == 0)
+      for (int i = 0; i < 10; i++) s_ovf_acc[tk][i] = acc[i];
+    __syncthreads();
+  }
+  if (ovf)
+    for (int i = 0; i < 10; i++) A[i] = s_ovf_acc[threadIdx.x][i];
+  double alpha = 0.0;
+  if (valid) {
+    const bool alive = !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k];
+    if (alive) {
+      const double N = A[0];
+      double xb[3] = {0, 0, 0}, Sk[6] = {0, 0, 0, 0, 0, 0};
+      if (N > 0.0) {
+        for (int d = 0; d < 3; d++) xb[d] = mref[d] + A[1 + d] / N;
+        const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+        for (int e = 0; e < 6; e++) Sk[e] = A[4 + e] - A[1 + ia[e]] * A[1 + ib[e]] / N;
+      }
+      const double bo = gcomp(P, G_BETAO, k);
+      const double beta = bo + N;
+      gcomp(P, G_BETA, k) = beta;
+      gcomp(P, G_NU, k) = gcomp(P, G_NUO, k) + N;
+      gcomp(P, G_ALPHA, k) = fmax(gcomp(P, G_ALPHAO, k) + N, 0.0);
+      double mo[3];
+      for (int d = 0; d < 3; d++) {
+        mo[d] = gcomp(P, G_MO0 + d, k);
+        gcomp(P, G_M0 + d, k) = (bo * mo[d] + N * xb[d]) / beta;
+      }
+      double Wo[6];
+      for (int e = 0; e < 6; e++) Wo[e] = gcomp(P, G_WO0 + e, k);
+      if (Wo[5] < 1e-8) {
+        Wo[5] = 0.5 * (Wo[0] + Wo[3]);
+        gcomp(P, G_WO5, k) = Wo[5];
+      }
+      double Winv[6];
+      inv3(Wo, Winv);
+      const double dx[3] = {xb[0] - mo[0], xb[1] - mo[1], xb[2] - mo[2]};
+      const double fct = N * (bo / (bo + N));
+      const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+      for (int e = 0; e < 6; e++) Winv[e] += Sk[e] + fct * dx[ia[e]] * dx[ib[e]];
+      double W[6];
+      inv3(Winv, W);
+      RegConst rc;
+      for (int d = 0; d < 3; d++) rc.scale[d] = D.reg_scale[d];
+      rc.w4dof = D.w4dof;
+      rc.lambda_min = D.lambda_min;
+      rc.lambda_max = D.lambda_max;
+      rc.max_exc = D.max_exc;
+      regularize_W(W, gcomp(P, G_NU, k), rc);
+      for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = W[e];
+    }
+    alpha = gcomp(P, G_ALPHA, k);
+  }
+  const double a = block_sum_gchunk(alpha, shd);
+  if (threadIdx.x == 0) P.alpha_part_e[c] = a;
+}
+
+// ===========================================================================
+// kill_prep: dead-Gaussian rule (GMEMcheckDeadCellsKernel, GMEMupdateCUDA.cu:1813-1843)
+// with the post-update alpha total, then the preparation of the next iteration.
+// ===========================================================================
+__global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
+  const int c = blockIdx.x;
+  if (c >= P.info->n_gchunks) return;
+  const GChunk ch = P.gchunks[c];
+  const FrameState S = P.state[ch.frame];
+  if (S.done) return;
+  const FrameDesc D = load_desc(P, ch.frame);
+  __shared__ double s_total;
+  __shared__ double shd[kGChunk / 32];
+  __shared__ int shi[kGChunk / 32];
+  if (threadIdx.x < 32) {
+    const double tot = warp_sum_range(P.alpha_part_e, D.gchunk_base, D.n_gchunks);
+    if (threadIdx.x == 0) s_total = tot;
+  }
+  __syncthreads();
+  const double total = s_total;
+  const int cur = S.iter & 1, nxt = (S.iter + 1) & 1;
+  const int k = ch.g_begin + threadIdx.x;
+  double alpha = 0.0;
+  int dead = 0;
+  if (k < ch.g_end) {
+    bool nanw = isnan(gcomp(P, G_ELD0 + cur, k));
+    for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
+    const double a = gcomp(P, G_ALPHA, k);
+    if (nanw || (a / total < TGMM_MIN_PI_FOR_DEAD && !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k])) {
+      gcomp(P, G_ALPHA, k) = 0.0;
+      for (int d = 0; d < 3; d++) {
+        gcomp(P, G_MO0 + d, k) = -1e32;
+        gcomp(P, G_M0 + d, k) = -1e32;
+      }
+      const double I6[6] = {1, 0, 0, 1, 0, 1};
+      for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = I6[e];
+    }
+    prep_gaussian(P, D, S, k, nxt);
+    alpha = gcomp(P, G_ALPHA, k);
+    dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
+  }
+  const double at = block_sum_gchunk(alpha, shd);
+  const int nd = block_sum_gchunk_i(dead, shi);
+  if (threadIdx.x == 0) {
+    P.alpha_part_f[c] = at;
+    P.dead_part[c] = nd;
+  }
+}
+
+// ===========================================================================
+// ll_pass: the per-iteration voxel stream.  Warp per supervoxel:
+//   ll_v = ln sum_j (alpha_j/A) sqrt(det(W_j) nu_j^3) (2 pi)^-3/2 exp(-nu_j d'W_j d / 2)
+// over the supervoxel's five candidates (GMEMcomputeLikelihoodKernelWithSupervoxels,
+// GMEMupdateCUDA.cu:1913-1978), I_v * ll_v summed in FP64 when the density is positive.
+// Two sums: every voxel (true) and the reference's per-thread overwrite for supervoxels
+// above 1024 voxels (as reference).  Precision: FP64 per component, or "mixed": every
+// component in FP32 to find the dominant one, the dominant one again in FP64, and
+// ln(1 + sum of the others' ratios) in FP32.
+// ===========================================================================
+struct LLConst {
+  double md[kJ][3];
+  double Ad[kJ][6];  // nu * W (FP64 mode) or -nu*W/2 with doubled off-diagonals (mixed)
+  double bd[kJ];     // FP64: c_j * alpha_j / A ; mixed: ln of it
+  float mhi[kJ][3], mlo[kJ][3];
+  float Af[kJ][6];
+  float bf[kJ];
+  int anynan;
+};
+
+template <bool kFp64>
+__device__ __forceinline__ double voxel_ll(const LLConst& C, float x0, float x1, float x2, bool& ok) {
+  if (kFp64) {
+    double dens = 0.0;
+#pragma unroll
+    for (int j = 0; j < kJ; j++) {
+      const double d0 = (double)x0 - C.md[j][0], d1 = (double)x1 - C.md[j][1], d2 = (double)x2 - C.md[j][2];
+      const double* A = C.Ad[j];
+      const double q = A[0] * d0 * d0 + A[3] * d1 * d1 + A[5] * d2 * d2 + 2.0 * A[1] * d0 * d1 +
+                       2.0 * A[2] * d0 * d2 + 2.0 * A[4] * d1 * d2;
+      dens += C.bd[j] * exp(-0.5 * q);
+    }
+    ok = dens > 0.0;
+    return ok ? log(dens) : 0.0;
+  } else {
+    float a[kJ];
+#pragma unroll
+    for (int j = 0; j < kJ; j++) {
+      const float d0 = __fsub_rn(__fsub_rn(x0, C.mhi[j][0]), C.mlo[j][0]);
+      const float d1 = __fsub_rn(__fsub_rn(x1, C.mhi[j][1]), C.mlo[j][1]);
+      const float d2 = __fsub_rn(__fsub_rn(x2, C.mhi[j][2]), C.mlo[j][2]);
+      const float* A = C.Af[j];
+      const float t0 = fmaf(A[0], d0, fmaf(A[1], d1, A[2] * d2));
+      const float t1 = fmaf(A[3], d1, A[4] * d2);
+      a[j] = fmaf(d0, t0, fmaf(d1, t1, fmaf(d2, A[5] * d2, C.bf[j])));
+    }
+    int js = 0;
+    float am = a[0];
+#pragma unroll
+    for (int j = 1; j < kJ; j++)
+      if (a[j] > am) {
+        am = a[j];
+        js = j;
+      }
+    float r = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kJ; j++)
+      if (j != js) r += __expf(a[j] - am);
+    const double d0 = (double)x0 - C.md[js][0], d1 = (double)x1 - C.md[js][1], d2 = (double)x2 - C.md[js][2];
+    const double* A = C.Ad[js];
+    const double q = fma(d0, fma(A[0], d0, fma(A[1], d1, A[2] * d2)), fma(d1, fma(A[3], d1, A[4] * d2), d2 * A[5] * d2));
+    const double astar = C.bd[js] + q;
+    ok = astar > -745.0 && !C.anynan;  // exp(astar) would be a positive double
+    return ok ? astar + (double)log1pf(r) : 0.0;
+  }
+}
+
+template <bool kFp64>
+__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
+  const int total = P.info->total_sv;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ LLConst shc[kWarpsPerBlockV];
+  LLConst& C = shc[warp];
+  for (int qi = 0; qi < kSvPerWarpV; qi++) {
+    const int s = blockIdx.x * kSvPerBlockV + qi * kWarpsPerBlockV + warp;
+    if (s >= total) return;
+    const int f = P.sv_frame[s];
+    if (P.state[f].done) continue;
+    const FrameDesc D = load_desc(P, f);
+    const double A = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
+    __syncwarp();
+    if (lane < kJ) {
+      const int k = P.cand[(int64_t)s * kJ + lane];
+      double W[6];
+      for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
+      const double nu = gcomp(P, G_NU, k);
+      const double alpha = gcomp(P, G_ALPHA, k);
+      for (int d = 0; d < 3; d++) {
+        const double m = gcomp(P, G_M0 + d, k);
+        C.md[lane][d] = m;
+        const float hi = __double2float_rn(m);
+        C.mhi[lane][d] = hi;
+        C.mlo[lane][d] = __double2float_rn(m - (double)hi);
+      }
+      const double dn = det3(W) * nu * nu * nu;
+      if (kFp64) {
+        for (int e = 0; e < 6; e++) C.Ad[lane][e] = nu * W[e];
+        C.bd[lane] = (sqrt(dn) / 15.74960994572241901324) * (alpha / A);
+      } else {
+        const double b = 0.5 * log(dn) - 1.5 * kLnTwoPi + log(alpha) - log(A);
+        const double h[6] = {-0.5 * nu * W[0], -nu * W[1], -nu * W[2], -0.5 * nu * W[3], -nu * W[4], -0.5 * nu * W[5]};
+        for (int e = 0; e < 6; e++) {
+          C.Ad[lane][e] = h[e];
+          C.Af[lane][e] = __double2float_rn(h[e]);
+        }
+        C.bd[lane] = b;
+        C.bf[lane] = __double2float_rn(b);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      int an = 0;
+      if (!kFp64)
+        for (int j = 0; j < kJ; j++) an |= isnan(C.bd[j]) ? 1 : 0;
+      C.anynan = an;
+    }
+    __syncwarp();
+    const int sl = s - D.sv_base;
+    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;
+    const int64_t nv = p1 - p0;
+    const float* __restrict__ qx = D.query;
+    const float* __restrict__ qy = D.query + D.n_vox;
+    const float* __restrict__ qz = D.query + 2 * D.n_vox;
+    const float* __restrict__ im = D.img;
+    double lt = 0.0, lr = 0.0;
+    for (int64_t v = p0 + lane; v < p1; v += 32) {
+      const float x = __ldg(qx + v), y = __ldg(qy + v), z = __ldg(qz + v), I = __ldg(im + v);
+      bool ok;
+      const double l = voxel_ll<kFp64>(C, x, y, z, ok);
+      const int64_t i = v - p0;
+      const bool tail = i >= nv - 1024;
+      if (ok) {
+        const double term = (double)I * l;
+        lt += term;
+        if (tail) lr += term;
+      } else if (tail && nv > 1024) {
+        // the reference keeps, per thread, the last voxel of its stride with a positive
+        // density: walk back through this stride
+        for (int64_t i2 = i - 1024; i2 >= 0; i2 -= 1024) {
+          const int64_t v2 = p0 + i2;
+          bool ok2;
+          const double l2 = voxel_ll<kFp64>(C, qx[v2], qy[v2], qz[v2], ok2);
+          if (ok2) {
+            lr += (double)im[v2] * l2;
+            break;
+          }
+        }
+      }
+    }
+    lt = warp_sum(lt);
+    lr = warp_sum(lr);
+    if (lane == 0) {
+      P.ll_part[s] = lt;
+      P.ll_part[(int64_t)P.max_sv + s] = lr;
+    }
+    __syncwarp();
+  }
+}
+
+// ===========================================================================
+// assign + export: post-loop supervoxel assignment (rnk > 0.5, at most 16 per Gaussian,
+// GMEMupdateCUDA.cu:4310-4350) and SoA -> AoS.
+// ===========================================================================
+__global__ void __launch_bounds__(kSvPerBlockT) k_assign(DevPlan P) {
+  const int s = blockIdx.x * kSvPerBlockT + threadIdx.x;
+  if (s >= P.info->total_sv) return;
+  const int f = P.sv_frame[s];
+  const FrameDesc D = load_desc(P, f);
+  if (P.state[f].flags & (F_BAD_CSR | F_FEW_GAUSS)) return;
+  const int sl = s - D.sv_base;
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+    const float r = P.rnk[(int64_t)s * kJ + j];
+    if ((double)r > 0.5) {
+      const int k = P.cand[(int64_t)s * kJ + j];
+      const int b = atomicAdd(&P.acnt[k], 1);
+      if (b < kBucketCap) P.abucket[(int64_t)k * kBucketCap + b] = j * D.n_sv + sl;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
+  const int c = blockIdx.x;
+  if (c >= P.info->n_gchunks) return;
+  const GChunk ch = P.gchunks[c];
+  const FrameDesc D = load_desc(P, ch.frame);
+  const FrameState S = P.state[ch.frame];
+  __shared__ int sbuf[kBucketCap][kGChunk];
+  __shared__ int s_ovf[kGChunk];
+  __shared__ int s_novf;
+  __shared__ int s_first[kGChunk][TGMM_MAX_SV_PER_GAUSSIAN + 1];
+  __shared__ int s_list[kGChunk];
+  __shared__ int s_cnt[kGChunk / 32 + 1];
+  if (threadIdx.x == 0) s_novf = 0;
+  __syncthreads();
+  const int k = ch.g_begin + threadIdx.x;
+  const bool valid = k < ch.g_end;
+  const bool ran = !(S.flags & (F_BAD_CSR | F_FEW_GAUSS));
+  int n = 0;
+  if (valid && ran) {
+    n = P.acnt[k];
+    P.acnt[k] = 0;
+    if (n > kBucketCap) {
+      const int o = atomicAdd(&s_novf, 1);
+      s_ovf[o] = threadIdx.x;
+      atomicOr(&P.state[ch.frame].flags, F_ASSIGN_OVERFLOW);
+    } else {
+      for (int i = 0; i < n; i++) {
+        int v = P.abucket[(int64_t)k * kBucketCap + i];
+        int q = i;
+        while (q > 0 && sbuf[q - 1][threadIdx.x] > v) {
+          sbuf[q][threadIdx.x] = sbuf[q - 1][threadIdx.x];
+          q--;
+        }
+        sbuf[q][threadIdx.x] = v;
+      }
+    }
+  }
+  __syncthreads();
+  const int novf = s_novf;
+  for (int o = 0; o < novf; o++) {
+    const int tk = s_ovf[o];
+    int taken = 0;
+    int* dst = s_first[tk];
+    ordered_scan(P, D, ch.g_begin + tk, 0.5, s_list, s_cnt, [&](int p) {
+      if (taken < TGMM_MAX_SV_PER_GAUSSIAN) dst[taken++] = p;
+    });
+    if (threadIdx.x == 0) dst[TGMM_MAX_SV_PER_GAUSSIAN] = taken;
+    __syncthreads();
+  }
+  if (!valid) return;
+  TgmmGaussian& g = D.gm[k - D.g_base];
+  if (ran) {
+    g.beta_k = gcomp(P, G_BETA, k);
+    g.nu_k = gcomp(P, G_NU, k);
+    g.alpha_k = gcomp(P, G_ALPHA, k);
+    for (int d = 0; d < 3; d++) g.m_k[d] = gcomp(P, G_M0 + d, k);
+    for (int e = 0; e < 6; e++) g.W_k[e] = gcomp(P, G_W0 + e, k);
+    const int last = (S.iter - 1) & 1;  // parity of the last iteration that ran
+    const double eld = gcomp(P, G_ELD0 + last, k);
+    g.expectedLogDetCovarianceCUDA = eld;
+    g.expectedLogResponsivityCUDA = (eld == -1e32) ? -1e32 : gcomp(P, G_PSIA0 + last, k) - S.psi_total[last];
+    for (int d = 0; d < 3; d++) g.m_o[d] = gcomp(P, G_MO0 + d, k);
+    g.W_o[5] = gcomp(P, G_WO5, k);
+    if (n > kBucketCap) {
+      const int taken = s_first[threadIdx.x][TGMM_MAX_SV_PER_GAUSSIAN];
+      for (int i = 0; i < taken; i++) g.supervoxelIdx[i] = s_first[threadIdx.x][i] % D.n_sv;
+      g.supervoxelNum = taken;
+    } else {
+      const int taken = min(n, TGMM_MAX_SV_PER_GAUSSIAN);
+      for (int i = 0; i < taken; i++) g.supervoxelIdx[i] = sbuf[i][threadIdx.x] % D.n_sv;
+      g.supervoxelNum = taken;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline int div_up(int a, int b) { return (a + b - 1) / b; }
+
+void launch_build_maps(const DevPlan& P, cudaStream_t st) {
+  k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
+}
+void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
+void launch_frame_end(const DevPlan& P, int mode, cudaStream_t st) {
+  k_frame_end<<<P.max_frames, kFrameThreads, 0, st>>>(P, mode);
+}
+void launch_moments(const DevPlan& P, cudaStream_t st) {
+  k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+}
+void launch_grid_fill(const DevPlan& P, cudaStream_t st) {
+  k_grid_fill<<<P.max_gchunks, kGChunk, 0, st>>>(P);
+}
+void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
+  k_knn_estep<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);
+}
+void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
+  k_mstep_update<<<P.max_gchunks, kGChunk, 0, st>>>(P);
+}
+void launch_kill_prep(const DevPlan& P, cudaStream_t st) {
+  k_kill_prep<<<P.max_gchunks, kGChunk, 0, st>>>(P);
+}
+void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st) {
+  if (fp64)
+    k_ll_pass<true><<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+  else
+    k_ll_pass<false><<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+}
+void launch_assign(const DevPlan& P, cudaStream_t st) {
+  k_assign<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);
+}
+void launch_export(const DevPlan& P, cudaStream_t st) { k_export<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
+
+
+// ---------------------------------------------------------------------------
+// Standalone exact kNN (tgmm_knn): the same grid search over one point set.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_sa_geometry(const float* q, int64_t nq, float s0, float s1, float s2,
+                                                      int nref, int budget, FrameState* S) {
+  __shared__ float smin[3][32], smax[3][32];
+  const float sc[3] = {s0, s1, s2};
+  float lo[3] = {kInfF, kInfF, kInfF}, hi[3] = {-kInfF, -kInfF, -kInfF};
+  for (int64_t i = threadIdx.x; i < nq; i += blockDim.x)
+    for (int d = 0; d < 3; d++) {
+      const float y = q[d * nq + i] * sc[d];
+      if (!isfinite(y)) continue;
+      lo[d] = fminf(lo[d], y);
+      hi[d] = fmaxf(hi[d], y);
+    }
+  for (int d = 0; d < 3; d++)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int d = 0; d < 3; d++) {
+      smin[d][w] = lo[d];
+      smax[d][w] = hi[d];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int d = 0; d < 3; d++) {
+      lo[d] = smin[d][0];
+      hi[d] = smax[d][0];
+      for (int i = 1; i < (int)(blockDim.x >> 5); i++) {
+        lo[d] = fminf(lo[d], smin[d][i]);
+        hi[d] = fmaxf(hi[d], smax[d][i]);
+      }
+      if (!(lo[d] <= hi[d])) lo[d] = hi[d] = 0.0f;
+    }
+    set_geometry(S, lo, hi, nref, budget);
+  }
+}
+
+__global__ void k_sa_count(const float* ref, int nref, float s0, float s1, float s2, const FrameState* S, int* cnt,
+                           int* rcell) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nref) return;
+  const float ys[3] = {ref[3 * k] * s0, ref[3 * k + 1] * s1, ref[3 * k + 2] * s2};
+  int cell = 0;
+  for (int d = 0; d < 3; d++)
+    if (!isfinite(ys[d]) || fabsf(ys[d]) >= 1e25f) cell = -1;
+  if (cell == 0) {
+    const int cx = cell_coord(ys[0], S->lo[0], S->inv_h, S->dims[0]);
+    const int cy = cell_coord(ys[1], S->lo[1], S->inv_h, S->dims[1]);
+    const int cz = cell_coord(ys[2], S->lo[2], S->inv_h, S->dims[2]);
+    cell = (cz * S->dims[1] + cy) * S->dims[0] + cx;
+    atomicAdd(&cnt[cell], 1);
+  }
+  rcell[k] = cell;
+}
+
+__global__ void __launch_bounds__(1024) k_sa_scan(const FrameState* S, int* cnt, int* start, int* cur) {
+  __shared__ int scan[1024];
+  const int n = S->n_cells;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
+  int local = 0;
+  for (int i = b0; i < b1; i++) local += cnt[i];
+  scan[threadIdx.x] = local;
+  __syncthreads();
+  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+    int v = (threadIdx.x >= (unsigned)off) ? scan[threadIdx.x - off] : 0;
+    __syncthreads();
+    scan[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = scan[threadIdx.x] - local;
+  for (int i = b0; i < b1; i++) {
+    start[i] = run;
+    cur[i] = run;
+    run += cnt[i];
+  }
+  if (threadIdx.x == blockDim.x - 1) start[n] = scan[blockDim.x - 1];
+}
+
+__global__ void k_sa_fill(const float* ref, int nref, const int* rcell, int* cur, float4* refs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nref || rcell[k] < 0) return;
+  const int pos = atomicAdd(&cur[rcell[k]], 1);
+  refs[pos] = make_float4(ref[3 * k], ref[3 * k + 1], ref[3 * k + 2], __int_as_float(k));
+}
+
+__global__ void k_sa_query(const float* q, int64_t nq, const float* ref, int nref, float s0, float s1, float s2,
+                           const FrameState* S, const int* start, const float4* refs, int32_t* ind) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  const float sc[3] = {s0, s1, s2};
+  const float q0 = q[i], q1 = q[nq + i], q2 = q[2 * nq + i];
+  GridGeom g;
+  for (int d = 0; d < 3; d++) {
+    g.lo[d] = S->lo[d];
+    g.dims[d] = S->dims[d];
+  }
+  g.h = S->h;
+  g.inv_h = S->inv_h;
+  Top5 t;
+  top5_init(t);
+  knn_grid_search(q0, q1, q2, sc, g, start, refs, t);
+  if (!(t.d[kJ - 1] < kInfF)) {
+    top5_init(t);
+    for (int k = 0; k < nref; k++) top5_insert(t, knn_dist(q0, q1, q2, ref[3 * k], ref[3 * k + 1], ref[3 * k + 2], sc), k);
+  }
+  for (int j = 0; j < kJ; j++) ind[(int64_t)j * nq + i] = t.i[j];
+}
+
+cudaError_t knn_grid_standalone(const float* q, int64_t nq, const float* ref, int32_t nref, const float scale[3],
+                                int32_t* ind, cudaStream_t st) {
+  const int budget = 2 * nref + 2;
+  char* buf = nullptr;
+  const size_t off_state = 0, off_cnt = 256, off_start = off_cnt + 4 * (size_t)budget,
+               off_cur = off_start + 4 * ((size_t)budget + 1), off_rc = off_cur + 4 * (size_t)budget,
+               off_refs = (off_rc + 4 * (size_t)nref + 255) / 256 * 256, total = off_refs + 16 * (size_t)nref;
+  cudaError_t e = cudaMallocAsync((void**)&buf, total, st);
+  if (e != cudaSuccess) return e;
+  FrameState* S = (FrameState*)(buf + off_state);
+  int* cnt = (int*)(buf + off_cnt);
+  int* start = (int*)(buf + off_start);
+  int* cur = (int*)(buf + off_cur);
+  int* rc = (int*)(buf + off_rc);
+  float4* refs = (float4*)(buf + off_refs);
+  cudaMemsetAsync(cnt, 0, 4 * (size_t)budget, st);
+  k_sa_geometry<<<1, 1024, 0, st>>>(q, nq, scale[0], scale[1], scale[2], nref, budget, S);
+  const int gb = (nref + 255) / 256;
+  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, scale[0], scale[1], scale[2], S, cnt, rc);
+  k_sa_scan<<<1, 1024, 0, st>>>(S, cnt, start, cur);
+  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, rc, cur, refs);
+  k_sa_query<<<(unsigned)((nq + 127) / 128), 128, 0, st>>>(q, nq, ref, nref, scale[0], scale[1], scale[2], S, start,
+                                                          refs, ind);
+  e = cudaGetLastError();
+  cudaFreeAsync(buf, st);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Posterior -> prior on the device (GaussianMixtureModel::updatePriors,
+// GaussianMixtureModel.cpp:892-910; N_k = nu_k - nu_o as copyFromGMEM_CUDA/updateNk
+// derive it; then nu_k *= 2, W_k /= 2 as mainTrackingGaussianMixtureModel.cpp:961-969).
+// One block: the optional alpha total is a fixed-order block sum.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_update_priors(TgmmGaussian* gm, int n, double bp, double np, double ap,
+                                                        double atot, int compute) {
+  __shared__ double sh[32];
+  __shared__ double s_tot;
+  if (compute && atot < 0.0) {
+    double a = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) a += gm[k].alpha_k;
+    a = warp_sum(a);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += sh[i];
+      s_tot = t;
+    }
+    __syncthreads();
+    atot = s_tot;
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    TgmmGaussian& g = gm[k];
+    const double Nk = g.nu_k - g.nu_o;
+    for (int d = 0; d < 3; d++) g.m_o[d] = g.m_k[d];
+    g.beta_o = fmax(bp * Nk, 1e-5);
+    g.nu_o = fmax(np * Nk, 3.0);
+    for (int e = 0; e < 6; e++) g.W_o[e] = g.W_k[e] * g.nu_k / g.nu_o;
+    if (atot >= 0.0) g.alpha_o = atot * TGMM_MIN_PI_FOR_DEAD * ap;
+    g.nu_k *= 2.0;
+    for (int e = 0; e < 6; e++) g.W_k[e] /= 2.0;
+  }
+}
+
+cudaError_t update_priors_device(TgmmGaussian* gm, int32_t n, double bp, double np, double ap, double atot,
+                                 int compute, cudaStream_t st) {
+  k_update_priors<<<1, 1024, 0, st>>>(gm, n, bp, np, ap, atot, compute);
+  return cudaGetLastError();
+}
+
+}  // namespace tgmm

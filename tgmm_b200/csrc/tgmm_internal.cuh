@@ -1,0 +1,177 @@
+// tgmm_internal.cuh -- device-side data layout of a plan (all workspace of the EM),
+// the per-frame descriptor/state records and the kernel entry points.
+//
+// Layout in HBM (capacities fixed at plan creation):
+//   per Gaussian, SoA doubles  [component][max_gauss]: beta, nu, alpha, m[3], W[6],
+//                              beta_o, nu_o, alpha_o, m_o[3], W_o[6], eLD[2], psiA[2]
+//   per supervoxel             moments [19][max_sv] doubles (centred at the supervoxel
+//                              centroid: sum e, sum e e', sum I, sum I e, sum I e e'),
+//                              cand/rnk [max_sv][5], ll partials [2][max_sv]
+//   kNN grid                   per frame a uniform grid over the centroid bounding box
+//                              (scaled space); cell counts/starts and the refs sorted by cell
+//   M-step buckets             [max_gauss][kBucketCap] (supervoxel, slot) positions
+//   chunk tables               frame-aligned chunks of kGChunk Gaussians, so that every
+//                              per-frame sum is a fixed-order sum of chunk partials.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/tgmm_gmem.h"
+#include "tgmm_math.cuh"
+
+namespace tgmm {
+
+constexpr int kJ = TGMM_J;
+constexpr int kBucketCap = 32;   // M-step pairs per Gaussian held in the fast bucket
+constexpr int kGChunk = 128;     // Gaussians per block in per-Gaussian kernels
+constexpr int kSvPerBlockT = 128;  // supervoxels per block, thread-per-supervoxel kernels
+constexpr int kWarpsPerBlockV = 8;   // warps per block, warp-per-supervoxel kernels
+constexpr int kSvPerWarpV = 2;
+constexpr int kSvPerBlockV = kWarpsPerBlockV * kSvPerWarpV;
+constexpr int kNumMoments = 19;
+constexpr int kFrameThreads = 1024;
+
+// moment component indices
+enum : int {
+  M_E0 = 0, M_E1, M_E2,                      // sum e
+  M_EE00, M_EE01, M_EE02, M_EE11, M_EE12, M_EE22,  // sum e e'
+  M_I,                                        // sum I
+  M_IE0, M_IE1, M_IE2,                       // sum I e
+  M_IEE00, M_IEE01, M_IEE02, M_IEE11, M_IEE12, M_IEE22  // sum I e e'
+};
+
+// device flags (per frame, OR-ed into FrameState::flags)
+enum : int {
+  F_BAD_CSR = 1,
+  F_NAN_INPUT = 2,
+  F_FEW_GAUSS = 4,
+  F_BUCKET_OVERFLOW = 8,
+  F_ASSIGN_OVERFLOW = 16
+};
+
+struct FrameDesc {
+  const float* query;
+  const float* img;
+  const float* cent;
+  const int64_t* lptr;
+  TgmmGaussian* gm;  // device AoS records of this frame
+  float* rnk_out;    // device, 5*n_sv, slot-major
+  int32_t* ind_out;  // device, 5*n_sv, slot-major, frame-local Gaussian ids
+  int64_t n_vox;
+  int32_t n_sv, n_gauss;
+  int32_t sv_base, g_base;
+  int32_t cell_base, cell_budget;
+  int32_t gchunk_base, n_gchunks;
+  float scale[3];      // kNN distance scale
+  float reg_scale[3];  // regularisation scale
+  int32_t w4dof;
+  double lambda_min, lambda_max, max_exc, tol;
+  int32_t max_iter, ll_mode, ll_prec, pad;
+};
+
+struct FrameState {
+  float lo[3];
+  float h;
+  float inv_h;
+  int32_t dims[3];
+  int32_t n_cells;
+  int32_t iter;  // numIterEM of the reference: the next iteration to run (starts at 1)
+  int32_t done;
+  int32_t converged;
+  int32_t flags;
+  int32_t n_dead;
+  double total_alpha;  // post-kill sum of alpha (the value the E-step and the ll use)
+  double psi_total[2];
+  double ll, ll1, ll2, ll3;
+  double ll_true, ll_ref;
+};
+
+struct BatchInfo {
+  int32_t n_frames;
+  int32_t total_sv;
+  int32_t total_gauss;
+  int32_t n_gchunks;
+  int32_t total_cells;
+  int32_t pad[3];
+};
+
+struct GChunk {
+  int32_t frame, g_begin, g_end, pad;
+};
+
+// Device pointers of a plan (passed by value to kernels).
+struct DevPlan {
+  int64_t max_vox;
+  int32_t max_sv, max_gauss, max_frames, max_gchunks, max_cells;
+  BatchInfo* info;
+  FrameDesc* frames;
+  FrameState* state;
+  GChunk* gchunks;
+  // per Gaussian
+  int32_t* g_frame;
+  double* gd;  // SoA block, see G_* offsets (component * max_gauss)
+  uint8_t* fixed;
+  int32_t* ref_cell;
+  float4* cell_refs;
+  int32_t* cell_cnt;
+  int32_t* cell_start;  // max_cells + max_frames entries (absolute positions into cell_refs)
+  int32_t* cell_cur;
+  int32_t* bcnt;
+  int32_t* bucket;
+  int32_t* acnt;
+  int32_t* abucket;
+  double* alpha_part_e;
+  double* alpha_part_f;
+  int32_t* dead_part;
+  // per supervoxel
+  int32_t* sv_frame;
+  double* mom;
+  int32_t* cand;
+  float* rnk;
+  double* ll_part;  // [2][max_sv]
+};
+
+// component offsets inside DevPlan::gd (each component is max_gauss doubles)
+enum : int {
+  G_BETA = 0, G_NU, G_ALPHA,
+  G_M0, G_M1, G_M2,
+  G_W0, G_W1, G_W2, G_W3, G_W4, G_W5,
+  G_BETAO, G_NUO, G_ALPHAO,
+  G_MO0, G_MO1, G_MO2,
+  G_WO0, G_WO1, G_WO2, G_WO3, G_WO4, G_WO5,
+  G_ELD0, G_ELD1,
+  G_PSIA0, G_PSIA1,
+  G_NUM
+};
+
+__device__ __forceinline__ double& gcomp(const DevPlan& P, int c, int k) {
+  return P.gd[(int64_t)c * P.max_gauss + k];
+}
+
+// ---- kernel launchers (em_kernels.cu) ----
+void launch_build_maps(const DevPlan& P, cudaStream_t st);
+void launch_import(const DevPlan& P, cudaStream_t st);
+void launch_frame_end(const DevPlan& P, int mode, cudaStream_t st);
+void launch_moments(const DevPlan& P, cudaStream_t st);
+void launch_grid_fill(const DevPlan& P, cudaStream_t st);
+void launch_knn_estep(const DevPlan& P, cudaStream_t st);
+void launch_mstep_update(const DevPlan& P, cudaStream_t st);
+void launch_kill_prep(const DevPlan& P, cudaStream_t st);
+void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st);
+void launch_assign(const DevPlan& P, cudaStream_t st);
+void launch_export(const DevPlan& P, cudaStream_t st);
+
+// standalone kNN (tgmm_knn): brute force over refs in shared memory tiles
+cudaError_t knn_bruteforce(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
+                           const float scale[3], int32_t* ind, cudaStream_t st);
+// grid kNN over a single point set, for tgmm_knn with large nref
+cudaError_t knn_grid_standalone(const float* query, int64_t nq, const float* ref_xyz,
+                                int32_t nref, const float scale[3], int32_t* ind,
+                                cudaStream_t st);
+
+// device-side posterior -> prior
+cudaError_t update_priors_device(TgmmGaussian* gm, int32_t n, double bp, double np, double ap,
+                                 double atot, int compute_total, cudaStream_t st);
+
+}  // namespace tgmm

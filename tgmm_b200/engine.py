@@ -1,0 +1,151 @@
+"""Engine wrapper: device buffers (torch) + the C ABI of libtgmm_gmem.so.
+
+PyTorch only provides device memory and streams here; every kernel is the engine's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+@dataclass
+class DeviceFrame:
+    query: torch.Tensor      # (3N,) float32
+    img: torch.Tensor        # (N,) float32
+    centroids: torch.Tensor  # (3S,) float32
+    label_ptr: torch.Tensor  # (S+1,) int64
+    n_gauss: int
+
+    @property
+    def n_vox(self):
+        return int(self.img.numel())
+
+    @property
+    def n_sv(self):
+        return int(self.label_ptr.numel() - 1)
+
+    def cframe(self) -> L.TgmmFrame:
+        f = L.TgmmFrame()
+        f.query, f.img = self.query.data_ptr(), self.img.data_ptr()
+        f.centroids, f.label_ptr = self.centroids.data_ptr(), self.label_ptr.data_ptr()
+        f.n_vox, f.n_sv, f.n_gauss = self.n_vox, self.n_sv, self.n_gauss
+        return f
+
+
+def to_device(frame, device="cuda", pin=False) -> DeviceFrame:
+    """Copy a synth.Frame (host arrays) to the device."""
+    def t(a):
+        x = torch.from_numpy(np.ascontiguousarray(a))
+        if pin:
+            x = x.pin_memory()
+        return x.to(device, non_blocking=pin)
+    return DeviceFrame(t(frame.query), t(frame.img), t(frame.centroids), t(frame.label_ptr), frame.n_gauss)
+
+
+def gauss_to_device(g: np.ndarray, device="cuda") -> torch.Tensor:
+    g = np.ascontiguousarray(np.asarray(g).astype(L.GAUSS_DTYPE))
+    return torch.from_numpy(g.view(np.uint8).copy()).to(device)
+
+
+def gauss_from_device(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().numpy().view(L.GAUSS_DTYPE).copy()
+
+
+def stats_dict(st: L.TgmmEmStats) -> dict:
+    return dict(iterations=st.iterations, converged=st.converged, ll=st.ll, ll_true=st.ll_true,
+                ll_as_reference=st.ll_as_reference, total_alpha=st.total_alpha, n_dead=st.n_dead,
+                device_flags=st.device_flags)
+
+
+class Plan:
+    """All device workspace of the EM for batches up to the given capacity."""
+
+    def __init__(self, max_vox: int, max_sv: int, max_gauss: int, max_frames: int = 1, device: int = 0):
+        self.lib = L.gmem()
+        d = L.TgmmPlanDesc()
+        d.max_vox, d.max_sv, d.max_gauss, d.max_frames, d.device = max_vox, max_sv, max(max_gauss, 5), max_frames, device
+        self.desc = d
+        h = C.c_void_p()
+        L.check(self.lib.tgmm_plan_create(C.byref(d), C.byref(h)), "tgmm_plan_create")
+        self.h = h
+
+    @staticmethod
+    def bytes_for(max_vox, max_sv, max_gauss, max_frames=1) -> int:
+        d = L.TgmmPlanDesc()
+        d.max_vox, d.max_sv, d.max_gauss, d.max_frames, d.device = max_vox, max_sv, max(max_gauss, 5), max_frames, 0
+        return int(L.gmem().tgmm_plan_bytes(C.byref(d)))
+
+    def close(self):
+        if self.h:
+            self.lib.tgmm_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- single frame, Gaussians on the host (the reference's ownership model) --
+    def run_host(self, df: DeviceFrame, gauss: np.ndarray, params: L.TgmmEmParams, stream=None, want_ind_tr=False):
+        g = np.ascontiguousarray(np.asarray(gauss).astype(L.GAUSS_DTYPE))
+        S = df.n_sv
+        rnk = torch.empty(5 * S, dtype=torch.float32, device=df.img.device)
+        ind = torch.empty(5 * S, dtype=torch.int32, device=df.img.device)
+        ind_tr = torch.empty(5 * S, dtype=torch.int32, device=df.img.device) if want_ind_tr else None
+        st = L.TgmmEmStats()
+        cf = df.cframe()
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        rc = self.lib.tgmm_em_run(self.h, C.byref(cf), g.ctypes.data, rnk.data_ptr(), ind.data_ptr(),
+                                  ind_tr.data_ptr() if ind_tr is not None else None, C.byref(params), C.byref(st), s)
+        L.check(rc, "tgmm_em_run")
+        out = dict(gauss=g, rnk=rnk.cpu().numpy(), ind=ind.cpu().numpy(), **stats_dict(st))
+        if ind_tr is not None:
+            out["ind_tr"] = ind_tr.cpu().numpy()
+        return out
+
+    # -- device-resident form --
+    def run_device(self, df: DeviceFrame, gm_dev: torch.Tensor, rnk: torch.Tensor, ind: torch.Tensor,
+                   params: L.TgmmEmParams, stats: bool = True, stream=None):
+        st = L.TgmmEmStats() if stats else None
+        cf = df.cframe()
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        rc = self.lib.tgmm_em_run_device(self.h, C.byref(cf), gm_dev.data_ptr(), rnk.data_ptr(), ind.data_ptr(),
+                                         C.byref(params), C.byref(st) if st is not None else None, s)
+        L.check(rc, "tgmm_em_run_device")
+        return stats_dict(st) if st is not None else None
+
+    def run_batch(self, frames, gms, rnks, inds, params: L.TgmmEmParams, stats: bool = True, stream=None):
+        n = len(frames)
+        cfs = (L.TgmmFrame * n)(*[f.cframe() for f in frames])
+        gp = (C.c_void_p * n)(*[g.data_ptr() for g in gms])
+        rp = (C.c_void_p * n)(*[r.data_ptr() for r in rnks])
+        ip = (C.c_void_p * n)(*[i.data_ptr() for i in inds])
+        st = (L.TgmmEmStats * n)() if stats else None
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        rc = self.lib.tgmm_em_run_batch(self.h, n, cfs, gp, rp, ip, C.byref(params), st, s)
+        L.check(rc, "tgmm_em_run_batch")
+        return [stats_dict(x) for x in st] if st is not None else None
+
+
+def knn(query: torch.Tensor, ref_xyz: torch.Tensor, scale=(1.0, 1.0, 2.0), stream=None) -> torch.Tensor:
+    """Exact 5-NN (scaled squared distance, ties to the lower index); ind[j*nq + q]."""
+    nq = query.numel() // 3
+    ind = torch.empty(5 * nq, dtype=torch.int32, device=query.device)
+    sc = (C.c_float * 3)(*scale)
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L.check(L.gmem().tgmm_knn(query.data_ptr(), nq, ref_xyz.data_ptr(), ref_xyz.numel() // 3, sc, ind.data_ptr(), s),
+            "tgmm_knn")
+    return ind
+
+
+def update_priors(gm_dev: torch.Tensor, n: int, beta_pct=0.01, nu_pct=1.0, alpha_pct=0.8, alpha_total=-1.0,
+                  compute_alpha_total=True, stream=None):
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L.check(L.gmem().tgmm_update_priors(gm_dev.data_ptr(), n, beta_pct, nu_pct, alpha_pct, alpha_total,
+                                        1 if compute_alpha_total else 0, s), "tgmm_update_priors")
