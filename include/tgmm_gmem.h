@@ -198,6 +198,16 @@ int tgmm_assign_supervoxels(const float* rnk_host, const int32_t* ind_host, int3
 int tgmm_write_rnk_file(const char* path, const float* rnk_host, const int32_t* ind_host,
                         int32_t n_sv);
 
+/* Measurement hook (no reference counterpart): launch one kernel of the EM `reps` times
+ * back to back on `stream` between two CUDA events, on the batch last run through this
+ * plan, and return the average milliseconds per launch.  The plan's per-frame EM state
+ * is restored afterwards.  Only kernels without lasting side effects are accepted. */
+enum {
+  TGMM_KERNEL_MOMENTS = 0, /* per-supervoxel moment pass (once per call) */
+  TGMM_KERNEL_LL_PASS = 2  /* log-likelihood voxel pass (per iteration) */
+};
+int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* ms_per_launch, void* stream);
+
 /* Last CUDA error string recorded by this library on the calling thread. */
 const char* tgmm_last_error(void);
 /* Library version string. */

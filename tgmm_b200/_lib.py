@@ -35,6 +35,9 @@ TGMM_LL_TRUE = 1
 TGMM_LLPREC_MIXED = 0
 TGMM_LLPREC_FP64 = 1
 
+TGMM_KERNEL_MOMENTS = 0
+TGMM_KERNEL_LL_PASS = 2
+
 
 class TgmmGaussian(C.Structure):
     _fields_ = [
@@ -121,6 +124,7 @@ GMEM_FUNCS = {
     "tgmm_frame_release": (C.c_int, [C.POINTER(TgmmFrame)]),
     "tgmm_assign_supervoxels": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_int32]),
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
+    "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
     "tgmm_last_error": (C.c_char_p, []),
     "tgmm_version": (C.c_char_p, []),
 }

@@ -202,8 +202,10 @@ __device__ void set_geometry(FrameState* S, const float* lo, const float* hi, in
     ext[d] = fmaxf(hi[d] - lo[d], 1.0f);
     vol *= ext[d];
   }
+  // about three references per cell: the fifth neighbour then usually lies within the
+  // first ring of cells around the query
   const int budget = max(cell_budget - 1, 1);
-  const int target = max(1, min(budget, n_ref));
+  const int target = max(1, min(budget, n_ref / 3));
   float h = (float)cbrt(vol / target);
   int dims[3] = {1, 1, 1};
   for (int guard = 0; guard < 400; guard++) {
@@ -415,6 +417,7 @@ __global__ void __launch_bounds__(kFrameThreads) k_frame_end(DevPlan P, int mode
   }
   double lt = 0.0, lr = 0.0;
   if (mode == 1) {
+#pragma unroll 4
     for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
       lt += P.ll_part[D.sv_base + i];
       lr += P.ll_part[(int64_t)P.max_sv + D.sv_base + i];
@@ -460,29 +463,41 @@ __global__ void __launch_bounds__(kFrameThreads) k_frame_end(DevPlan P, int mode
   }
   __syncthreads();
   if (s_done) return;
-  // exclusive scan of the cell counts -> absolute starts into cell_refs
+  // exclusive scan of the cell counts -> absolute starts into cell_refs, in coalesced
+  // tiles of one cell per thread
   const int n = S->n_cells;
-  const int per = (n + blockDim.x - 1) / blockDim.x;
-  const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
-  int local = 0;
-  for (int i = b0; i < b1; i++) local += P.cell_cnt[D.cell_base + i];
-  scan[threadIdx.x] = local;
-  __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    int v = (threadIdx.x >= (unsigned)off) ? scan[threadIdx.x - off] : 0;
+  int run = D.g_base;
+  for (int t0 = 0; t0 < n; t0 += blockDim.x) {
+    const int i = t0 + threadIdx.x;
+    const int cnt = i < n ? P.cell_cnt[D.cell_base + i] : 0;
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) scan[w] = x;
     __syncthreads();
-    scan[threadIdx.x] += v;
+    if (w == 0) {
+      int z = scan[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      scan[lane] = z;
+    }
+    __syncthreads();
+    const int start = run + (w > 0 ? scan[w - 1] : 0) + x - cnt;
+    if (i < n) {
+      P.cell_start[D.cell_base + i] = start;
+      P.cell_cur[D.cell_base + i] = start;
+      P.cell_cnt[D.cell_base + i] = 0;
+    }
+    run += scan[31];
     __syncthreads();
   }
-  int run = D.g_base + scan[threadIdx.x] - local;
-  for (int i = b0; i < b1; i++) {
-    const int cnt = P.cell_cnt[D.cell_base + i];
-    P.cell_start[D.cell_base + i] = run;
-    P.cell_cur[D.cell_base + i] = run;
-    P.cell_cnt[D.cell_base + i] = 0;
-    run += cnt;
-  }
-  if (threadIdx.x == blockDim.x - 1) P.cell_start[D.cell_base + n] = D.g_base + scan[blockDim.x - 1];
+  if (threadIdx.x == 0) P.cell_start[D.cell_base + n] = run;
 }
 
 // ===========================================================================
@@ -511,8 +526,22 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 #pragma unroll
     for (int i = 0; i < kNumMoments; i++) m[i] = 0.0;
     bool nan_seen = false;
-    for (int64_t v = p0 + lane; v < p1; v += 32) {
-      const float x = __ldg(qx + v), y = __ldg(qy + v), z = __ldg(qz + v), I = __ldg(im + v);
+    constexpr int U = 4;  // voxels in flight per lane
+    for (int64_t v0 = p0 + lane; v0 < p1; v0 += 32 * U) {
+      float xs[U], ys[U], zs[U], ws[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t v = v0 + 32 * u;
+        const bool in = v < p1;
+        xs[u] = in ? __ldcs(qx + v) : c0;
+        ys[u] = in ? __ldcs(qy + v) : c1;
+        zs[u] = in ? __ldcs(qz + v) : c2;
+        ws[u] = in ? __ldcs(im + v) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+      if (v0 + 32 * u >= p1) break;
+      const float x = xs[u], y = ys[u], z = zs[u], I = ws[u];
       nan_seen |= isnan(x) || isnan(y) || isnan(z) || isnan(I);
       const double e0 = (double)(x - c0), e1 = (double)(y - c1), e2 = (double)(z - c2);
       const double wI = (double)I;
@@ -536,6 +565,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
       m[M_IEE11] = fma(i1, e1, m[M_IEE11]);
       m[M_IEE12] = fma(i1, e2, m[M_IEE12]);
       m[M_IEE22] = fma(i2, e2, m[M_IEE22]);
+      }
     }
     if (__any_sync(0xffffffffu, nan_seen) && lane == 0) atomicOr(&P.state[f].flags, F_NAN_INPUT);
 #pragma unroll
@@ -568,8 +598,11 @@ __global__ void __launch_bounds__(kGChunk) k_grid_fill(DevPlan P) {
 }
 
 // ===========================================================================
-// knn_estep: thread per supervoxel.  Exact 5-NN of the centroid among the frame's
-// Gaussian centres, then the E-step from the supervoxel's moments:
+// knn_estep: warp per supervoxel.  Exact 5-NN of the centroid among the frame's
+// Gaussian centres: the lanes split each ring of grid cells, keep private top-5 lists
+// pruned by the warp's current fifth distance, and after each ring the lists are merged
+// by five rounds of a warp-wide (distance, index) arg-min.  Then the E-step from the
+// supervoxel's moments, candidate j on lane j:
 //   L_j = sum_v [-1/2 (3/beta + nu d'Wd) + E ln pi + 1/2 E ln|Lambda|]
 //       = -1/2 (3 n/beta + nu tr(W D)) + n (psi(alpha) - psi(sum alpha) + 1/2 E ln|Lambda|),
 //   D = sum_v (x_v - m)(x_v - m)' = G2 - G1 u' - u G1' + n u u',  u = m - c_s,
@@ -577,8 +610,100 @@ __global__ void __launch_bounds__(kGChunk) k_grid_fill(DevPlan P) {
 // candidate or |L| beyond float range -> -inf) and rnk_j = 1 / sum_i exp(L_i - L_j).
 // Pairs with rnk > 1e-3 go to the Gaussian's M-step bucket.
 // ===========================================================================
-__global__ void __launch_bounds__(kSvPerBlockT) k_knn_estep(DevPlan P) {
-  const int s = blockIdx.x * kSvPerBlockT + threadIdx.x;
+constexpr int kKnnWarps = 4;
+
+// warp-wide lexicographic arg-min of (d, i); every lane gets the winner
+__device__ __forceinline__ void warp_min_pair(float& d, int& i) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float od = __shfl_xor_sync(0xffffffffu, d, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (before(od, oi, d, i)) {
+      d = od;
+      i = oi;
+    }
+  }
+}
+
+// merge the 32 lanes' sorted lists into the warp's top-5 (identical in every lane)
+__device__ __forceinline__ void warp_merge_top5(Top5& mine, Top5& out) {
+#pragma unroll
+  for (int r = 0; r < kJ; r++) {
+    float d = mine.d[0];
+    int i = mine.i[0];
+    warp_min_pair(d, i);
+    out.d[r] = d;
+    out.i[r] = i;
+    if (mine.i[0] == i && mine.d[0] == d && i != 0x7fffffff) {  // pop the front of the winner
+#pragma unroll
+      for (int q = 0; q < kJ - 1; q++) {
+        mine.d[q] = mine.d[q + 1];
+        mine.i[q] = mine.i[q + 1];
+      }
+      mine.d[kJ - 1] = kInfF;
+      mine.i[kJ - 1] = 0x7fffffff;
+    }
+  }
+}
+
+__device__ void knn_warp_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
+                                const int32_t* __restrict__ cstart, const float4* __restrict__ refs, Top5& best) {
+  const int lane = threadIdx.x & 31;
+  const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
+  int c[3];
+  float delta = kInfF;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    c[a] = cell_coord(y[a], g.lo[a], g.inv_h, g.dims[a]);
+    const float f0 = y[a] - (g.lo[a] + c[a] * g.h);
+    const float f1 = (g.lo[a] + (c[a] + 1) * g.h) - y[a];
+    delta = fminf(delta, fminf(f0, f1));
+  }
+  delta = fmaxf(delta, 0.0f);
+  top5_init(best);
+  const int maxr = max(g.dims[0], max(g.dims[1], g.dims[2]));
+  for (int r = 0; r <= maxr; ++r) {
+    Top5 t;
+    top5_init(t);
+    // prune with the warp's current fifth: a ref must beat it to matter
+    const float td = best.d[kJ - 1];
+    const int ti = best.i[kJ - 1];
+    const int side = 2 * r + 1;
+    const int cube = side * side * side;
+    for (int idx = lane; idx < cube; idx += 32) {
+      const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
+      if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+      const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
+      if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) continue;
+      const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
+      const int b = cstart[cell], e = cstart[cell + 1];
+      for (int k = b; k < e; ++k) {
+        const float4 rr = refs[k];
+        const float d = knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s);
+        const int id = __float_as_int(rr.w);
+        if (before(d, id, td, ti)) top5_insert(t, d, id);
+      }
+    }
+    // lane 0 also carries the previous best (disjoint from this ring's refs)
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < kJ; q++) top5_insert(t, best.d[q], best.i[q]);
+    }
+    Top5 merged;
+    warp_merge_top5(t, merged);
+    best = merged;
+    const float lb = r * g.h + delta;
+    const float eps = 4e-3f + 1e-6f * lb;
+    if (lb > eps) {
+      const float bound = (lb - eps) * (lb - eps);
+      if (best.d[kJ - 1] < bound) break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * kKnnWarps + warp;
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
   const FrameState& S = P.state[f];
@@ -595,44 +720,42 @@ __global__ void __launch_bounds__(kSvPerBlockT) k_knn_estep(DevPlan P) {
   g.h = S.h;
   g.inv_h = S.inv_h;
   Top5 t;
-  top5_init(t);
-  knn_grid_search(q0, q1, q2, D.scale, g, P.cell_start + D.cell_base, P.cell_refs, t);
+  knn_warp_search(q0, q1, q2, D.scale, g, P.cell_start + D.cell_base, P.cell_refs, t);
   if (!(t.d[kJ - 1] < kInfF)) {
     // fewer than five finite distances: exact scan of every Gaussian of the frame
-    top5_init(t);
-    for (int kl = 0; kl < D.n_gauss; kl++) {
+    Top5 m;
+    top5_init(m);
+    for (int kl = lane; kl < D.n_gauss; kl += 32) {
       const int k = D.g_base + kl;
       const float x = __double2float_rn(gcomp(P, G_M0, k));
       const float y = __double2float_rn(gcomp(P, G_M1, k));
       const float z = __double2float_rn(gcomp(P, G_M2, k));
-      top5_insert(t, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
+      top5_insert(m, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
     }
+    warp_merge_top5(m, t);
   }
+  // E-step: candidate j on lane j
   const int par = S.iter & 1;
-  const double psiT = S.psi_total[par];
-  int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+  const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
   const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
-  double G1[3], G2[6];
+  int kl = 0;
 #pragma unroll
-  for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
-#pragma unroll
-  for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
-  const double c[3] = {(double)q0, (double)q1, (double)q2};
-  double L[kJ];
-  int gk[kJ];
-#pragma unroll
-  for (int j = 0; j < kJ; j++) {
-    const int kl = t.i[j];
-    const int k = D.g_base + kl;
-    gk[j] = k;
-    double Lj;
-    if (n == 0.0) {
-      Lj = 0.0;
-    } else if (is_dead_prior(gcomp(P, G_MO0, k))) {
+  for (int j = 0; j < kJ; j++)
+    if (lane == j) kl = t.i[j];
+  const int k = D.g_base + kl;
+  double Lj = 0.0;
+  if (lane < kJ && n != 0.0) {
+    if (is_dead_prior(gcomp(P, G_MO0, k))) {
       Lj = -(double)kInfF;
     } else {
+      double G1[3], G2[6];
+#pragma unroll
+      for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
+#pragma unroll
+      for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
       const double beta = gcomp(P, G_BETA, k), nu = gcomp(P, G_NU, k);
-      const double u0 = gcomp(P, G_M0, k) - c[0], u1 = gcomp(P, G_M1, k) - c[1], u2 = gcomp(P, G_M2, k) - c[2];
+      const double u0 = gcomp(P, G_M0, k) - (double)q0, u1 = gcomp(P, G_M1, k) - (double)q1,
+                   u2 = gcomp(P, G_M2, k) - (double)q2;
       const double D00 = G2[0] - 2.0 * G1[0] * u0 + n * u0 * u0;
       const double D01 = G2[1] - (G1[0] * u1 + u0 * G1[1]) + n * u0 * u1;
       const double D02 = G2[2] - (G1[0] * u2 + u0 * G1[2]) + n * u0 * u2;
@@ -641,34 +764,35 @@ __global__ void __launch_bounds__(kSvPerBlockT) k_knn_estep(DevPlan P) {
       const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
       const double tr = gcomp(P, G_W0, k) * D00 + gcomp(P, G_W3, k) * D11 + gcomp(P, G_W5, k) * D22 +
                         2.0 * (gcomp(P, G_W1, k) * D01 + gcomp(P, G_W2, k) * D02 + gcomp(P, G_W4, k) * D12);
-      const double eLR = gcomp(P, G_PSIA0 + par, k) - psiT;
+      const double eLR = gcomp(P, G_PSIA0 + par, k) - S.psi_total[par];
       const double eLD = gcomp(P, G_ELD0 + par, k);
       Lj = -0.5 * (3.0 * n / beta + nu * tr) + n * (eLR + 0.5 * eLD);
       if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
       if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
     }
-    L[j] = Lj;
   }
+  double acc = 0.0;
 #pragma unroll
-  for (int j = 0; j < kJ; j++) {
-    double acc = 0.0;
-#pragma unroll
-    for (int i = 0; i < kJ; i++) acc += exp(L[i] - L[j]);
+  for (int i = 0; i < kJ; i++) acc += exp(__shfl_sync(0xffffffffu, Lj, i) - Lj);
+  if (lane < kJ) {
     const float r = __double2float_rn(1.0 / acc);
+    const int j = lane;
     const int64_t pos = (int64_t)j * Sf + sl;
     D.rnk_out[pos] = r;
-    D.ind_out[pos] = t.i[j];
-    P.cand[(int64_t)s * kJ + j] = gk[j];
+    D.ind_out[pos] = kl;
+    P.cand[(int64_t)s * kJ + j] = k;
     P.rnk[(int64_t)s * kJ + j] = r;
     if ((double)r > 1e-3) {
-      const int b = atomicAdd(&P.bcnt[gk[j]], 1);
-      if (b < kBucketCap) P.bucket[(int64_t)gk[j] * kBucketCap + b] = (int)pos;
+      const int b = atomicAdd(&P.bcnt[k], 1);
+      if (b < kBucketCap) P.bucket[(int64_t)k * kBucketCap + b] = (int)pos;
     }
   }
 }
 
 // M-step contribution of one (supervoxel, slot) pair to Gaussian k, moments re-centred
-// from the supervoxel centroid to m_ref (the Gaussian's current mean):
+// from the supervoxel centroid to m_ref, the Gaussian's prior mean m_o.  m_o stays fixed
+// during a call, so responsibilities that repeat bit for bit give parameters that repeat
+// bit for bit -- the exact fixed point the reference's tol = 0 stopping rule looks for:
 //   A0 += r H0;  A1 += r (H1 + H0 d);  A2 += r (H2 + H1 d' + d H1' + H0 d d'),  d = c_s - m_ref.
 __device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, int p, const double* mref,
                                           double* A) {
@@ -761,7 +885,7 @@ __global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
   double mref[3] = {0, 0, 0};
   bool ovf = false;
   if (valid) {
-    for (int d = 0; d < 3; d++) mref[d] = gcomp(P, G_M0 + d, k);
+    for (int d = 0; d < 3; d++) mref[d] = gcomp(P, G_MO0 + d, k);
     const int n = P.bcnt[k];
     P.bcnt[k] = 0;
     if (n > kBucketCap) {
@@ -787,7 +911,7 @@ __global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
   for (int o = 0; o < novf; o++) {
     const int tk = s_ovf[o];
     const int kk = ch.g_begin + tk;
-    double mr[3] = {gcomp(P, G_M0, kk), gcomp(P, G_M1, kk), gcomp(P, G_M2, kk)};
+    double mr[3] = {gcomp(P, G_MO0, kk), gcomp(P, G_MO1, kk), gcomp(P, G_MO2, kk)};
     double acc[10];
     for (int i = 0; i < 10; i++) acc[i] = 0.0;
     ordered_scan(P, D, kk, 1e-3, s_list, s_cnt, [&](int p) { mstep_add(P, D, p, mr, acc); });
@@ -902,134 +1026,134 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
 // over the supervoxel's five candidates (GMEMcomputeLikelihoodKernelWithSupervoxels,
 // GMEMupdateCUDA.cu:1913-1978), I_v * ll_v summed in FP64 when the density is positive.
 // Two sums: every voxel (true) and the reference's per-thread overwrite for supervoxels
-// above 1024 voxels (as reference).  Precision: FP64 per component, or "mixed": every
-// component in FP32 to find the dominant one, the dominant one again in FP64, and
-// ln(1 + sum of the others' ratios) in FP32.
+// above 1024 voxels (as reference).
+// Voxels are centred at the supervoxel centroid c (e = x - c, exact in FP32 for voxel
+// coordinates near c); each candidate contributes through u_j = m_j - c, so FP32 keeps
+// full relative precision without splitting the means.  Precision modes:
+//   FP64   -- every component in FP64, the reference's formula;
+//   mixed  -- every component in FP32 to rank them, the dominant one again in FP64, and
+//             ln(sum_j exp(a_j - a*)) in FP32 (an O(1) correction with absolute error
+//             ~1e-7), accumulated in FP64.
+// Each lane keeps four voxels in flight (strides of 32); a supervoxel whose five
+// candidates all have W02 = W12 = 0 (the 4-DOF regularisation) takes the 4-DOF path.
 // ===========================================================================
-struct LLConst {
-  double md[kJ][3];
-  double Ad[kJ][6];  // nu * W (FP64 mode) or -nu*W/2 with doubled off-diagonals (mixed)
-  double bd[kJ];     // FP64: c_j * alpha_j / A ; mixed: ln of it
-  float mhi[kJ][3], mlo[kJ][3];
+struct LLShared {
+  double u[kJ][3];
+  double A[kJ][6];  // FP64 mode: nu*W; mixed: -nu*W/2 with doubled off-diagonals
+  double b[kJ];     // FP64 mode: c_j*alpha_j/A; mixed: its logarithm
+  float uf[kJ][3];
   float Af[kJ][6];
   float bf[kJ];
-  int anynan;
+  int anynan, w4;
 };
 
-template <bool kFp64>
-__device__ __forceinline__ double voxel_ll(const LLConst& C, float x0, float x1, float x2, bool& ok) {
-  if (kFp64) {
-    double dens = 0.0;
-#pragma unroll
-    for (int j = 0; j < kJ; j++) {
-      const double d0 = (double)x0 - C.md[j][0], d1 = (double)x1 - C.md[j][1], d2 = (double)x2 - C.md[j][2];
-      const double* A = C.Ad[j];
-      const double q = A[0] * d0 * d0 + A[3] * d1 * d1 + A[5] * d2 * d2 + 2.0 * A[1] * d0 * d1 +
-                       2.0 * A[2] * d0 * d2 + 2.0 * A[4] * d1 * d2;
-      dens += C.bd[j] * exp(-0.5 * q);
-    }
-    ok = dens > 0.0;
-    return ok ? log(dens) : 0.0;
+constexpr int kLLUnroll = 4;
+
+template <bool kW4>
+__device__ __forceinline__ float quad_f(const float* A, float d0, float d1, float d2) {
+  if (kW4) {
+    const float t0 = fmaf(A[1], d1, A[0] * d0);
+    return fmaf(d0, t0, fmaf(d1, A[3] * d1, d2 * (A[5] * d2)));
   } else {
-    float a[kJ];
-#pragma unroll
-    for (int j = 0; j < kJ; j++) {
-      const float d0 = __fsub_rn(__fsub_rn(x0, C.mhi[j][0]), C.mlo[j][0]);
-      const float d1 = __fsub_rn(__fsub_rn(x1, C.mhi[j][1]), C.mlo[j][1]);
-      const float d2 = __fsub_rn(__fsub_rn(x2, C.mhi[j][2]), C.mlo[j][2]);
-      const float* A = C.Af[j];
-      const float t0 = fmaf(A[0], d0, fmaf(A[1], d1, A[2] * d2));
-      const float t1 = fmaf(A[3], d1, A[4] * d2);
-      a[j] = fmaf(d0, t0, fmaf(d1, t1, fmaf(d2, A[5] * d2, C.bf[j])));
-    }
-    int js = 0;
-    float am = a[0];
-#pragma unroll
-    for (int j = 1; j < kJ; j++)
-      if (a[j] > am) {
-        am = a[j];
-        js = j;
-      }
-    float r = 0.0f;
-#pragma unroll
-    for (int j = 0; j < kJ; j++)
-      if (j != js) r += __expf(a[j] - am);
-    const double d0 = (double)x0 - C.md[js][0], d1 = (double)x1 - C.md[js][1], d2 = (double)x2 - C.md[js][2];
-    const double* A = C.Ad[js];
-    const double q = fma(d0, fma(A[0], d0, fma(A[1], d1, A[2] * d2)), fma(d1, fma(A[3], d1, A[4] * d2), d2 * A[5] * d2));
-    const double astar = C.bd[js] + q;
-    ok = astar > -745.0 && !C.anynan;  // exp(astar) would be a positive double
-    return ok ? astar + (double)log1pf(r) : 0.0;
+    const float t0 = fmaf(A[0], d0, fmaf(A[1], d1, A[2] * d2));
+    const float t1 = fmaf(A[3], d1, A[4] * d2);
+    return fmaf(d0, t0, fmaf(d1, t1, d2 * (A[5] * d2)));
   }
 }
 
-template <bool kFp64>
-__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
-  const int total = P.info->total_sv;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __shared__ LLConst shc[kWarpsPerBlockV];
-  LLConst& C = shc[warp];
-  for (int qi = 0; qi < kSvPerWarpV; qi++) {
-    const int s = blockIdx.x * kSvPerBlockV + qi * kWarpsPerBlockV + warp;
-    if (s >= total) return;
-    const int f = P.sv_frame[s];
-    if (P.state[f].done) continue;
-    const FrameDesc D = load_desc(P, f);
-    const double A = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
-    __syncwarp();
-    if (lane < kJ) {
-      const int k = P.cand[(int64_t)s * kJ + lane];
-      double W[6];
-      for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
-      const double nu = gcomp(P, G_NU, k);
-      const double alpha = gcomp(P, G_ALPHA, k);
-      for (int d = 0; d < 3; d++) {
-        const double m = gcomp(P, G_M0 + d, k);
-        C.md[lane][d] = m;
-        const float hi = __double2float_rn(m);
-        C.mhi[lane][d] = hi;
-        C.mlo[lane][d] = __double2float_rn(m - (double)hi);
-      }
-      const double dn = det3(W) * nu * nu * nu;
-      if (kFp64) {
-        for (int e = 0; e < 6; e++) C.Ad[lane][e] = nu * W[e];
-        C.bd[lane] = (sqrt(dn) / 15.74960994572241901324) * (alpha / A);
-      } else {
-        const double b = 0.5 * log(dn) - 1.5 * kLnTwoPi + log(alpha) - log(A);
-        const double h[6] = {-0.5 * nu * W[0], -nu * W[1], -nu * W[2], -0.5 * nu * W[3], -nu * W[4], -0.5 * nu * W[5]};
-        for (int e = 0; e < 6; e++) {
-          C.Ad[lane][e] = h[e];
-          C.Af[lane][e] = __double2float_rn(h[e]);
-        }
-        C.bd[lane] = b;
-        C.bf[lane] = __double2float_rn(b);
-      }
+template <bool kW4>
+__device__ __forceinline__ double quad_d(const double* A, double d0, double d1, double d2) {
+  if (kW4) {
+    return fma(d0, fma(A[1], d1, A[0] * d0), fma(d1, A[3] * d1, d2 * (A[5] * d2)));
+  } else {
+    return fma(d0, fma(A[0], d0, fma(A[1], d1, A[2] * d2)), fma(d1, fma(A[3], d1, A[4] * d2), d2 * (A[5] * d2)));
+  }
+}
+
+// ln of the mixture density at e = x - c (mixed precision); ok = density > 0.
+template <bool kW4>
+__device__ __forceinline__ double voxel_ll_mixed(const LLShared& C, const float (&uf)[kJ][3],
+                                                 const float (&Af)[kJ][6], const float (&bf)[kJ], float e0,
+                                                 float e1, float e2, bool& ok) {
+  float a[kJ];
+#pragma unroll
+  for (int j = 0; j < kJ; j++)
+    a[j] = bf[j] + quad_f<kW4>(Af[j], e0 - uf[j][0], e1 - uf[j][1], e2 - uf[j][2]);
+  int js = 0;
+  float am = a[0];
+#pragma unroll
+  for (int j = 1; j < kJ; j++)
+    if (a[j] > am) {
+      am = a[j];
+      js = j;
     }
-    __syncwarp();
-    if (lane == 0) {
-      int an = 0;
-      if (!kFp64)
-        for (int j = 0; j < kJ; j++) an |= isnan(C.bd[j]) ? 1 : 0;
-      C.anynan = an;
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < kJ; j++) s += __expf(a[j] - am);
+  const double d0 = (double)e0 - C.u[js][0], d1 = (double)e1 - C.u[js][1], d2 = (double)e2 - C.u[js][2];
+  const double astar = C.b[js] + quad_d<kW4>(C.A[js], d0, d1, d2);
+  ok = astar > -745.0 && !C.anynan;  // exp(astar) is a positive double
+  return astar + (double)__logf(s);
+}
+
+// FP64 mode: d = x - m exactly as the reference forms it (x - c in FP64, then - (m - c)).
+__device__ __forceinline__ double voxel_ll_fp64(const LLShared& C, float x0, float x1, float x2, float c0, float c1,
+                                                float c2, bool& ok) {
+  const double e0 = (double)x0 - (double)c0, e1 = (double)x1 - (double)c1, e2 = (double)x2 - (double)c2;
+  double dens = 0.0;
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+    const double d0 = e0 - C.u[j][0], d1 = e1 - C.u[j][1], d2 = e2 - C.u[j][2];
+    const double* A = C.A[j];
+    const double q = A[0] * d0 * d0 + A[3] * d1 * d1 + A[5] * d2 * d2 + 2.0 * A[1] * d0 * d1 +
+                     2.0 * A[2] * d0 * d2 + 2.0 * A[4] * d1 * d2;
+    dens += C.b[j] * exp(-0.5 * q);
+  }
+  ok = dens > 0.0;
+  return ok ? log(dens) : 0.0;
+}
+
+template <bool kFp64, bool kW4>
+__device__ __forceinline__ void ll_stream(const LLShared& C, const FrameDesc& D, float c0, float c1, float c2,
+                                          int64_t p0, int64_t p1, double& lt, double& lr) {
+  const int lane = threadIdx.x & 31;
+  float uf[kJ][3], Af[kJ][6], bf[kJ];
+#pragma unroll
+  for (int j = 0; j < kJ; j++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) uf[j][d] = C.uf[j][d];
+#pragma unroll
+    for (int e = 0; e < 6; e++) Af[j][e] = C.Af[j][e];
+    bf[j] = C.bf[j];
+  }
+  const float* __restrict__ qx = D.query;
+  const float* __restrict__ qy = D.query + D.n_vox;
+  const float* __restrict__ qz = D.query + 2 * D.n_vox;
+  const float* __restrict__ im = D.img;
+  const int64_t nv = p1 - p0;
+  for (int64_t v0 = p0 + lane; v0 < p1; v0 += 32 * kLLUnroll) {
+    float x[kLLUnroll], y[kLLUnroll], z[kLLUnroll], w[kLLUnroll];
+#pragma unroll
+    for (int u = 0; u < kLLUnroll; u++) {
+      const int64_t v = v0 + 32 * u;
+      const bool in = v < p1;
+      x[u] = in ? __ldcs(qx + v) : c0;
+      y[u] = in ? __ldcs(qy + v) : c1;
+      z[u] = in ? __ldcs(qz + v) : c2;
+      w[u] = in ? __ldcs(im + v) : 0.0f;
     }
-    __syncwarp();
-    const int sl = s - D.sv_base;
-    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
-    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;
-    const int64_t nv = p1 - p0;
-    const float* __restrict__ qx = D.query;
-    const float* __restrict__ qy = D.query + D.n_vox;
-    const float* __restrict__ qz = D.query + 2 * D.n_vox;
-    const float* __restrict__ im = D.img;
-    double lt = 0.0, lr = 0.0;
-    for (int64_t v = p0 + lane; v < p1; v += 32) {
-      const float x = __ldg(qx + v), y = __ldg(qy + v), z = __ldg(qz + v), I = __ldg(im + v);
+#pragma unroll
+    for (int u = 0; u < kLLUnroll; u++) {
+      const int64_t v = v0 + 32 * u;
+      if (v >= p1) break;
       bool ok;
-      const double l = voxel_ll<kFp64>(C, x, y, z, ok);
+      const float e0 = x[u] - c0, e1 = y[u] - c1, e2 = z[u] - c2;
+      const double l = kFp64 ? voxel_ll_fp64(C, x[u], y[u], z[u], c0, c1, c2, ok)
+                             : voxel_ll_mixed<kW4>(C, uf, Af, bf, e0, e1, e2, ok);
       const int64_t i = v - p0;
       const bool tail = i >= nv - 1024;
       if (ok) {
-        const double term = (double)I * l;
+        const double term = (double)w[u] * l;
         lt += term;
         if (tail) lr += term;
       } else if (tail && nv > 1024) {
@@ -1038,7 +1162,9 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
         for (int64_t i2 = i - 1024; i2 >= 0; i2 -= 1024) {
           const int64_t v2 = p0 + i2;
           bool ok2;
-          const double l2 = voxel_ll<kFp64>(C, qx[v2], qy[v2], qz[v2], ok2);
+          const float g0 = qx[v2], g1 = qy[v2], g2 = qz[v2];
+          const double l2 = kFp64 ? voxel_ll_fp64(C, g0, g1, g2, c0, c1, c2, ok2)
+                                  : voxel_ll_mixed<kW4>(C, uf, Af, bf, g0 - c0, g1 - c1, g2 - c2, ok2);
           if (ok2) {
             lr += (double)im[v2] * l2;
             break;
@@ -1046,6 +1172,72 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
         }
       }
     }
+  }
+}
+
+template <bool kFp64>
+__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
+  const int total = P.info->total_sv;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ LLShared shc[kWarpsPerBlockV];
+  LLShared& C = shc[warp];
+  for (int qi = 0; qi < kSvPerWarpV; qi++) {
+    const int s = blockIdx.x * kSvPerBlockV + qi * kWarpsPerBlockV + warp;
+    if (s >= total) return;
+    const int f = P.sv_frame[s];
+    if (P.state[f].done) continue;
+    const FrameDesc D = load_desc(P, f);
+    const int sl = s - D.sv_base;
+    const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
+    const double Atot = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
+    __syncwarp();
+    if (lane < kJ) {
+      const int k = P.cand[(int64_t)s * kJ + lane];
+      double W[6];
+      for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
+      const double nu = gcomp(P, G_NU, k);
+      const double alpha = gcomp(P, G_ALPHA, k);
+      const double cc[3] = {(double)c0, (double)c1, (double)c2};
+      for (int d = 0; d < 3; d++) {
+        const double u = gcomp(P, G_M0 + d, k) - cc[d];
+        C.u[lane][d] = u;
+        C.uf[lane][d] = __double2float_rn(u);
+      }
+      const double dn = det3(W) * nu * nu * nu;
+      if (kFp64) {
+        for (int e = 0; e < 6; e++) C.A[lane][e] = nu * W[e];
+        C.b[lane] = (sqrt(dn) / 15.74960994572241901324) * (alpha / Atot);
+      } else {
+        const double h[6] = {-0.5 * nu * W[0], -nu * W[1], -nu * W[2], -0.5 * nu * W[3], -nu * W[4], -0.5 * nu * W[5]};
+        for (int e = 0; e < 6; e++) {
+          C.A[lane][e] = h[e];
+          C.Af[lane][e] = __double2float_rn(h[e]);
+        }
+        const double b = 0.5 * log(dn) - 1.5 * kLnTwoPi + log(alpha) - log(Atot);
+        C.b[lane] = b;
+        C.bf[lane] = __double2float_rn(b);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      int an = 0, w4 = 1;
+      for (int j = 0; j < kJ; j++) {
+        if (!kFp64) an |= isnan(C.b[j]) ? 1 : 0;
+        w4 &= (C.A[j][2] == 0.0 && C.A[j][4] == 0.0) ? 1 : 0;
+      }
+      C.anynan = an;
+      C.w4 = w4;
+    }
+    __syncwarp();
+    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;
+    double lt = 0.0, lr = 0.0;
+    if (kFp64)
+      ll_stream<true, false>(C, D, c0, c1, c2, p0, p1, lt, lr);
+    else if (C.w4)
+      ll_stream<false, true>(C, D, c0, c1, c2, p0, p1, lt, lr);
+    else
+      ll_stream<false, false>(C, D, c0, c1, c2, p0, p1, lt, lr);
     lt = warp_sum(lt);
     lr = warp_sum(lr);
     if (lane == 0) {
@@ -1172,7 +1364,7 @@ void launch_grid_fill(const DevPlan& P, cudaStream_t st) {
   k_grid_fill<<<P.max_gchunks, kGChunk, 0, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
-  k_knn_estep<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);
+  k_knn_estep<<<div_up(P.max_sv, kKnnWarps), kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
   k_mstep_update<<<P.max_gchunks, kGChunk, 0, st>>>(P);

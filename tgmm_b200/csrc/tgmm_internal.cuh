@@ -24,7 +24,7 @@ namespace tgmm {
 
 constexpr int kJ = TGMM_J;
 constexpr int kBucketCap = 32;   // M-step pairs per Gaussian held in the fast bucket
-constexpr int kGChunk = 128;     // Gaussians per block in per-Gaussian kernels
+constexpr int kGChunk = 64;      // Gaussians per block in per-Gaussian kernels
 constexpr int kSvPerBlockT = 128;  // supervoxels per block, thread-per-supervoxel kernels
 constexpr int kWarpsPerBlockV = 8;   // warps per block, warp-per-supervoxel kernels
 constexpr int kSvPerWarpV = 2;
