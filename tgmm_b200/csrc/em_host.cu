@@ -40,7 +40,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 struct Layout {
   // byte offsets of every device array inside one allocation
   int64_t info, frames, state, gchunks, g_frame, gd, fixed, ref_cell, cell_refs, cell_cnt, cell_start,
-      cell_cur, bcnt, bucket, acnt, abucket, ape, apf, dead, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
+      cell_cur, bcnt, bucket, acnt, abucket, ape, apf, dead, llc, work, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -68,9 +68,11 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.bucket = take(4 * G * kBucketCap);
   L.acnt = take(4 * G);
   L.abucket = take(4 * G * kBucketCap);
-  L.ape = take(8 * (int64_t)max_gchunks);
+  L.ape = take(8 * 2 * (int64_t)max_gchunks);
   L.apf = take(8 * (int64_t)max_gchunks);
   L.dead = take(4 * (int64_t)max_gchunks);
+  L.llc = take(8 * 10 * G);
+  L.work = take(64);
   L.sv_frame = take(4 * S);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(4 * S * kJ);
@@ -191,6 +193,13 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.alpha_part_e = (double*)(b + P->L.ape);
   D.alpha_part_f = (double*)(b + P->L.apf);
   D.dead_part = (int32_t*)(b + P->L.dead);
+  D.llc = (double*)(b + P->L.llc);
+  D.work = (int32_t*)(b + P->L.work);
+  e = configure_kernels(D, d->device);
+  if (e != cudaSuccess) {
+    tgmm_plan_destroy(P);
+    return fail(TGMM_ERR_CUDA, "tgmm_plan_create: kernel configuration", e);
+  }
   D.sv_frame = (int32_t*)(b + P->L.sv_frame);
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);
@@ -324,15 +333,14 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
   TG_CUDA(cudaMemsetAsync(D.acnt, 0, 4 * (size_t)D.max_gauss, st), "clear assignment buckets");
   launch_build_maps(D, st);
   launch_import(D, st);
-  launch_frame_end(D, 0, st);
+  launch_grid_fill(D, st);
   launch_moments(D, st);
   for (int it = 0; it < max_iter; it++) {
-    launch_grid_fill(D, st);
     launch_knn_estep(D, st);
     launch_mstep_update(D, st);
     launch_kill_prep(D, st);
+    launch_grid_fill(D, st);
     launch_ll_pass(D, ll_prec == TGMM_LLPREC_FP64, st);
-    launch_frame_end(D, 1, st);
   }
   launch_assign(D, st);
   launch_export(D, st);
@@ -457,6 +465,13 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   for (auto& s : live)
     if (!(s.flags & (F_BAD_CSR | F_FEW_GAUSS))) s.done = 0;
   TG_CUDA(cudaMemcpy(P->dev.state, live.data(), sizeof(FrameState) * nf, cudaMemcpyHostToDevice), "write state");
+  // the voxel pass runs the convergence test; keep every frame running while timing
+  std::vector<FrameDesc> frames(P->h_frames, P->h_frames + nf);
+  for (auto& d : frames) {
+    d.max_iter = 0x7fffffff;
+    d.tol = -1.0;
+  }
+  TG_CUDA(cudaMemcpy(P->dev.frames, frames.data(), sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice), "write frames");
   cudaEvent_t a, b;
   TG_CUDA(cudaEventCreate(&a), "event");
   TG_CUDA(cudaEventCreate(&b), "event");
@@ -474,6 +489,8 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   *ms = t / reps;
   TG_CUDA(cudaMemcpyAsync(P->dev.state, backup.data(), sizeof(FrameState) * nf, cudaMemcpyHostToDevice, st),
           "restore state");
+  TG_CUDA(cudaMemcpyAsync(P->dev.frames, P->h_frames, sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice, st),
+          "restore frames");
   TG_CUDA(cudaStreamSynchronize(st), "synchronize");
   TG_CUDA(cudaGetLastError(), "kernel launch");
   return TGMM_OK;

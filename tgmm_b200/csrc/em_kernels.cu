@@ -1,8 +1,8 @@
 // em_kernels.cu -- the sm_100a kernels of the supervoxel VI-EM.
 //
-// One EM call is:  build_maps, import, frame_end(init), moments,
-//                  then per iteration: grid_fill, knn_estep, mstep_update, kill_prep,
-//                  ll_pass, frame_end(iter);  finally assign, export.
+// One EM call is:  build_maps, import (+ frame tail), grid_fill, moments,
+//                  then per iteration: knn_estep, mstep_update, kill_prep (+ frame tail),
+//                  grid_fill, ll_pass (+ convergence test);  finally assign, export.
 // Every kernel loops over the whole batch (one or many frames); frames that have
 // converged are skipped through their FrameState::done flag, so a captured graph of
 // max_iter iterations serves any batch.  No kernel uses float atomics: per-frame sums
@@ -40,6 +40,20 @@ __device__ __forceinline__ double warp_sum_range(const double* a, int base, int 
   double s = 0.0;
   for (int i = lane; i < n; i += 32) s += a[base + i];
   return warp_sum(s);
+}
+
+// Block (kN threads) fixed-order sum; result valid in thread 0.
+template <int kN>
+__device__ __forceinline__ double block_sum_n(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kN / 32; i++) t += sh[i];
+  return t;
 }
 
 // Block (kGChunk threads) fixed-order sum; result valid in thread 0.
@@ -303,7 +317,12 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
     S->ll_true = 0.0;
     S->ll_ref = 0.0;
     S->total_alpha = 0.0;
+    S->ln_alpha = 0.0;
     S->psi_total[0] = S->psi_total[1] = 0.0;
+    S->ll_int[0] = S->ll_int[1] = 0;
+    S->ll_frac[0] = S->ll_frac[1] = 0;
+    S->sv_done = 0;
+    S->blk_done = 0;
   }
 }
 
@@ -320,7 +339,9 @@ __device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc&
   return (cz * S.dims[1] + cy) * S.dims[0] + cx;
 }
 
-// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], grid cell.
+// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], the
+// log-likelihood constants (-nu W/2 with doubled off-diagonals, the log weight
+// 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the mean) and the grid cell.
 __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
                                               int k, int parity) {
   const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
@@ -328,8 +349,20 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
 #pragma unroll
   for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
   const double nu = gcomp(P, G_NU, k);
-  gcomp(P, G_PSIA0 + parity, k) = digamma(gcomp(P, G_ALPHA, k));
+  const double alpha = gcomp(P, G_ALPHA, k);
+  gcomp(P, G_PSIA0 + parity, k) = digamma(alpha);
   gcomp(P, G_ELD0 + parity, k) = dead ? -1e32 : expected_log_det(W, nu);
+  double* L = P.llc + (int64_t)k * 10;
+  L[0] = -0.5 * nu * W[0];
+  L[1] = -nu * W[1];
+  L[2] = -nu * W[2];
+  L[3] = -0.5 * nu * W[3];
+  L[4] = -nu * W[4];
+  L[5] = -0.5 * nu * W[5];
+  L[6] = 0.5 * log(det3(W) * nu * nu * nu) - 1.5 * kLnTwoPi + log(alpha);
+  L[7] = gcomp(P, G_M0, k);
+  L[8] = gcomp(P, G_M1, k);
+  L[9] = gcomp(P, G_M2, k);
   int cell = -1;
   if (!dead) {
     const float x = __double2float_rn(gcomp(P, G_M0, k));
@@ -339,6 +372,78 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
     if (cell >= 0) atomicAdd(&P.cell_cnt[D.cell_base + cell], 1);
   }
   P.ref_cell[k] = cell;
+}
+
+// Run by the last Gaussian chunk of a frame to finish (import or kill step): the alpha
+// total as a fixed-order sum of the chunk partials, psi and ln of it for the next
+// iteration, the dead count, and the exclusive scan of the grid-cell counts.
+__device__ void frame_tail(const DevPlan& P, int f, int next_parity) {
+  const FrameDesc D = load_desc(P, f);
+  FrameState* S = &P.state[f];
+  __shared__ int s_scan[kGChunk / 32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
+    const double a = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
+    int nd = 0;
+    for (int i = lane; i < D.n_gchunks; i += 32) nd += P.dead_part[D.gchunk_base + i];
+    nd = warp_sum_i(nd);
+    if (lane == 0) {
+      S->total_alpha = a;
+      S->ln_alpha = log(a);
+      S->psi_total[next_parity] = digamma(a);
+      S->n_dead = nd;
+    }
+  }
+  // exclusive scan of the cell counts -> absolute starts into cell_refs; each thread owns
+  // a contiguous segment of cells
+  const int n = S->n_cells;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
+  int local = 0;
+#pragma unroll 8
+  for (int i = b0; i < b1; i++) local += P.cell_cnt[D.cell_base + i];
+  int x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_scan[w] = x;
+  __syncthreads();
+  int before = 0, total = 0;
+#pragma unroll
+  for (int q = 0; q < kGChunk / 32; q++) {
+    const int v = s_scan[q];
+    if (q < w) before += v;
+    total += v;
+  }
+  int run = D.g_base + before + x - local;
+  for (int i = b0; i < b1; i++) {
+    const int cnt = P.cell_cnt[D.cell_base + i];
+    P.cell_start[D.cell_base + i] = run;
+    P.cell_cur[D.cell_base + i] = run;
+    P.cell_cnt[D.cell_base + i] = 0;
+    run += cnt;
+  }
+  run = D.g_base + total;
+  if (threadIdx.x == 0) {
+    P.cell_start[D.cell_base + n] = run;
+    S->blk_done = 0;
+  }
+}
+
+// The last-arriving chunk of frame f runs frame_tail.  Every chunk calls this after its
+// own writes; no thread waits on another.
+__device__ __forceinline__ void chunk_done(const DevPlan& P, int f, int n_chunks, int next_parity) {
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&P.state[f].blk_done, 1) == n_chunks - 1) ? 1 : 0;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    frame_tail(P, f, next_parity);
+  }
 }
 
 // ===========================================================================
@@ -383,121 +488,7 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
     P.alpha_part_f[c] = a;
     P.dead_part[c] = nd;
   }
-}
-
-// ===========================================================================
-// frame_end: per frame.  mode 0 (after import): alpha total, psi, cell scan.
-// mode 1 (after an iteration): log-likelihood sums, convergence test of the
-// reference's loop (GMEMupdateCUDA.cu:4145-4148), alpha total, psi, cell scan.
-// ===========================================================================
-__global__ void __launch_bounds__(kFrameThreads) k_frame_end(DevPlan P, int mode) {
-  const int f = blockIdx.x;
-  if (f >= P.info->n_frames) return;
-  FrameState* S = &P.state[f];
-  if (S->done) return;
-  const FrameDesc D = load_desc(P, f);
-  __shared__ double sh[2][kFrameThreads / 32];
-  __shared__ int s_done;
-  __shared__ int scan[kFrameThreads];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int t = S->iter;  // the iteration that just ran (mode 1) or 1 (mode 0)
-
-  // alpha total after the kill step (or of the input for mode 0); dead count
-  __shared__ double s_alpha;
-  __shared__ int s_dead;
-  if (threadIdx.x < 32) {
-    const double a = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
-    int nd = 0;
-    for (int i = lane; i < D.n_gchunks; i += 32) nd += P.dead_part[D.gchunk_base + i];
-    nd = warp_sum_i(nd);
-    if (threadIdx.x == 0) {
-      s_alpha = a;
-      s_dead = nd;
-    }
-  }
-  double lt = 0.0, lr = 0.0;
-  if (mode == 1) {
-#pragma unroll 4
-    for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
-      lt += P.ll_part[D.sv_base + i];
-      lr += P.ll_part[(int64_t)P.max_sv + D.sv_base + i];
-    }
-  }
-  lt = warp_sum(lt);
-  lr = warp_sum(lr);
-  if (lane == 0) sh[1][w] = lt;
-  __syncthreads();
-  double lt_tot = 0.0;
-  const double a_tot = s_alpha;
-  const int nd_tot = s_dead;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) lt_tot += sh[1][i];
-  __syncthreads();
-  if (lane == 0) sh[1][w] = lr;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double lr_tot = 0.0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) lr_tot += sh[1][i];
-    int done = 0;
-    int next = t;
-    if (mode == 1) {
-      S->ll3 = S->ll2;
-      S->ll2 = S->ll1;
-      S->ll1 = S->ll;
-      S->ll_true = lt_tot;
-      S->ll_ref = lr_tot;
-      S->ll = (D.ll_mode == TGMM_LL_TRUE) ? lt_tot : lr_tot;
-      next = t + 1;
-      S->iter = next;
-      const double ll = S->ll;
-      const bool go = fabs(ll - S->ll1) / fabs(S->ll1) > D.tol && fabs(ll - S->ll2) / fabs(S->ll2) > D.tol &&
-                      fabs(ll - S->ll3) / fabs(S->ll3) > D.tol;
-      if (!go) S->converged = 1;
-      done = (!go || next > D.max_iter) ? 1 : 0;
-    }
-    S->total_alpha = a_tot;
-    S->psi_total[next & 1] = digamma(a_tot);
-    S->n_dead = nd_tot;
-    S->done = done;
-    s_done = done;
-  }
-  __syncthreads();
-  if (s_done) return;
-  // exclusive scan of the cell counts -> absolute starts into cell_refs, in coalesced
-  // tiles of one cell per thread
-  const int n = S->n_cells;
-  int run = D.g_base;
-  for (int t0 = 0; t0 < n; t0 += blockDim.x) {
-    const int i = t0 + threadIdx.x;
-    const int cnt = i < n ? P.cell_cnt[D.cell_base + i] : 0;
-    int x = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) scan[w] = x;
-    __syncthreads();
-    if (w == 0) {
-      int z = scan[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, z, o);
-        if (lane >= o) z += y;
-      }
-      scan[lane] = z;
-    }
-    __syncthreads();
-    const int start = run + (w > 0 ? scan[w - 1] : 0) + x - cnt;
-    if (i < n) {
-      P.cell_start[D.cell_base + i] = start;
-      P.cell_cur[D.cell_base + i] = start;
-      P.cell_cnt[D.cell_base + i] = 0;
-    }
-    run += scan[31];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) P.cell_start[D.cell_base + n] = run;
+  chunk_done(P, ch.frame, D.n_gchunks, 1);
 }
 
 // ===========================================================================
@@ -661,8 +652,9 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
   }
   delta = fmaxf(delta, 0.0f);
   top5_init(best);
-  const int maxr = max(g.dims[0], max(g.dims[1], g.dims[2]));
-  for (int r = 0; r <= maxr; ++r) {
+  const int maxr = max(1, max(g.dims[0], max(g.dims[1], g.dims[2])));
+  // the first pass covers rings 0 and 1 (27 cells, one per lane), later passes one ring
+  for (int r = 1; r <= maxr; ++r) {
     Top5 t;
     top5_init(t);
     // prune with the warp's current fifth: a ref must beat it to matter
@@ -672,7 +664,7 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
     const int cube = side * side * side;
     for (int idx = lane; idx < cube; idx += 32) {
       const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
-      if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+      if (r > 1 && max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
       const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
       if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) continue;
       const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
@@ -862,22 +854,22 @@ __device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int k, double
 // Dirichlet / Normal-Wishart update (GMEMupdateCUDA.cu:1601-1677) -> regularisation
 // (:1693-1809).  Writes the chunk's alpha sum for the kill step.
 // ===========================================================================
-__global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
-  const int c = blockIdx.x;
+__global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
+  // two blocks per Gaussian chunk (twice the SMs busy): block b covers half b%2 of chunk b/2
+  const int c = blockIdx.x >> 1, half = blockIdx.x & 1;
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
   if (P.state[ch.frame].done) return;
   const FrameDesc D = load_desc(P, ch.frame);
-  __shared__ int sbuf[kBucketCap][kGChunk];
-  __shared__ int s_ovf[kGChunk];
+  __shared__ int s_ovf[kMChunk];
   __shared__ int s_novf;
-  __shared__ double s_ovf_acc[kGChunk][10];
-  __shared__ int s_list[kGChunk];
-  __shared__ int s_cnt[kGChunk / 32 + 1];
-  __shared__ double shd[kGChunk / 32];
+  __shared__ double s_ovf_acc[kMChunk][10];
+  __shared__ int s_list[kMChunk];
+  __shared__ int s_cnt[kMChunk / 32 + 1];
+  __shared__ double shd[kMChunk / 32];
   if (threadIdx.x == 0) s_novf = 0;
   __syncthreads();
-  const int k = ch.g_begin + threadIdx.x;
+  const int k = ch.g_begin + half * kMChunk + threadIdx.x;
   const bool valid = k < ch.g_end;
   double A[10];
 #pragma unroll
@@ -894,23 +886,24 @@ __global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
       s_ovf[o] = threadIdx.x;
       atomicOr(&P.state[ch.frame].flags, F_BUCKET_OVERFLOW);
     } else {
-      for (int i = 0; i < n; i++) {  // insertion sort by position
-        int v = P.bucket[(int64_t)k * kBucketCap + i];
+      int* bk = P.bucket + (int64_t)k * kBucketCap;  // this Gaussian's own bucket
+      for (int i = 1; i < n; i++) {                  // insertion sort by position
+        const int v = bk[i];
         int q = i;
-        while (q > 0 && sbuf[q - 1][threadIdx.x] > v) {
-          sbuf[q][threadIdx.x] = sbuf[q - 1][threadIdx.x];
+        while (q > 0 && bk[q - 1] > v) {
+          bk[q] = bk[q - 1];
           q--;
         }
-        sbuf[q][threadIdx.x] = v;
+        bk[q] = v;
       }
-      for (int i = 0; i < n; i++) mstep_add(P, D, sbuf[i][threadIdx.x], mref, A);
+      for (int i = 0; i < n; i++) mstep_add(P, D, bk[i], mref, A);
     }
   }
   __syncthreads();
   const int novf = s_novf;
   for (int o = 0; o < novf; o++) {
     const int tk = s_ovf[o];
-    const int kk = ch.g_begin + tk;
+    const int kk = ch.g_begin + half * kMChunk + tk;
     double mr[3] = {gcomp(P, G_MO0, kk), gcomp(P, G_MO1, kk), gcomp(P, G_MO2, kk)};
     double acc[10];
     for (int i = 0; i < 10; i++) acc[i] = 0.0;
@@ -967,8 +960,8 @@ __global__ void __launch_bounds__(kGChunk) k_mstep_update(DevPlan P) {
     }
     alpha = gcomp(P, G_ALPHA, k);
   }
-  const double a = block_sum_gchunk(alpha, shd);
-  if (threadIdx.x == 0) P.alpha_part_e[c] = a;
+  const double a = block_sum_n<kMChunk>(alpha, shd);
+  if (threadIdx.x == 0) P.alpha_part_e[blockIdx.x] = a;
 }
 
 // ===========================================================================
@@ -986,7 +979,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   __shared__ double shd[kGChunk / 32];
   __shared__ int shi[kGChunk / 32];
   if (threadIdx.x < 32) {
-    const double tot = warp_sum_range(P.alpha_part_e, D.gchunk_base, D.n_gchunks);
+    const double tot = warp_sum_range(P.alpha_part_e, 2 * D.gchunk_base, 2 * D.n_gchunks);
     if (threadIdx.x == 0) s_total = tot;
   }
   __syncthreads();
@@ -1018,86 +1011,120 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     P.alpha_part_f[c] = at;
     P.dead_part[c] = nd;
   }
+  chunk_done(P, ch.frame, D.n_gchunks, nxt);
 }
 
 // ===========================================================================
 // ll_pass: the per-iteration voxel stream.  Warp per supervoxel:
 //   ll_v = ln sum_j (alpha_j/A) sqrt(det(W_j) nu_j^3) (2 pi)^-3/2 exp(-nu_j d'W_j d / 2)
 // over the supervoxel's five candidates (GMEMcomputeLikelihoodKernelWithSupervoxels,
-// GMEMupdateCUDA.cu:1913-1978), I_v * ll_v summed in FP64 when the density is positive.
-// Two sums: every voxel (true) and the reference's per-thread overwrite for supervoxels
+// GMEMupdateCUDA.cu:1913-1978), I_v * ll_v summed when the density is positive.  Two
+// sums: every voxel (true) and the reference's per-thread overwrite for supervoxels
 // above 1024 voxels (as reference).
-// Voxels are centred at the supervoxel centroid c (e = x - c, exact in FP32 for voxel
-// coordinates near c); each candidate contributes through u_j = m_j - c, so FP32 keeps
-// full relative precision without splitting the means.  Precision modes:
-//   FP64   -- every component in FP64, the reference's formula;
-//   mixed  -- every component in FP32 to rank them, the dominant one again in FP64, and
-//             ln(sum_j exp(a_j - a*)) in FP32 (an O(1) correction with absolute error
-//             ~1e-7), accumulated in FP64.
-// Each lane keeps four voxels in flight (strides of 32); a supervoxel whose five
-// candidates all have W02 = W12 = 0 (the 4-DOF regularisation) takes the 4-DOF path.
+// With a_j = ln weight_j - nu_j d'W_j d/2, each voxel's term is written
+//   ll_v = a_0 + [ (a_max - a_0) + ln sum_j exp(a_j - a_max) ]
+// where candidate 0 is the anchor (the nearest candidate with a finite weight): a_0 in
+// FP64, the bracket -- an O(1) correction -- in FP32 with the five candidates evaluated
+// in packed FP32x2 pairs.  Voxels are centred at the supervoxel centroid c (e = x - c is
+// exact in FP32 for voxels near c) and candidates enter through u_j = m_j - c.  The FP64
+// mode evaluates every component in FP64 with the reference's formula.
+// Per-supervoxel results are added into per-frame 64-bit integer accumulators (integer
+// part and 2^-40 fraction), so the frame total does not depend on the order in which
+// warps finish; the warp that finishes a frame's last supervoxel runs the reference's
+// convergence test for that frame.
 // ===========================================================================
-struct LLShared {
-  double u[kJ][3];
-  double A[kJ][6];  // FP64 mode: nu*W; mixed: -nu*W/2 with doubled off-diagonals
-  double b[kJ];     // FP64 mode: c_j*alpha_j/A; mixed: its logarithm
-  float uf[kJ][3];
-  float Af[kJ][6];
-  float bf[kJ];
-  int anynan, w4;
+constexpr float kL2E = 1.4426950408889634f;  // log2(e)
+constexpr float kLN2F = 0.6931471805599453f;
+constexpr double kFracScale = 1099511627776.0;  // 2^40
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// FP32 constants of the five candidates (anchor first): two packed pairs and one single.
+struct CandF {
+  float2 u[2][3];
+  float2 A[2][6];
+  float2 b[2];
+  float u4[3], A4[6], b4;
 };
 
-constexpr int kLLUnroll = 4;
+template <bool kW4>
+__device__ __forceinline__ float2 eval_pair(const CandF& C, int q, float2 E0, float2 E1, float2 E2) {
+  const float2 d0 = __fadd2_rn(E0, C.u[q][0]);  // u stored negated
+  const float2 d1 = __fadd2_rn(E1, C.u[q][1]);
+  const float2 d2 = __fadd2_rn(E2, C.u[q][2]);
+  const float2* A = C.A[q];
+  if (kW4) {
+    const float2 t0 = __ffma2_rn(A[1], d1, __fmul2_rn(A[0], d0));
+    return __ffma2_rn(d0, t0, __ffma2_rn(d1, __fmul2_rn(A[3], d1), __ffma2_rn(d2, __fmul2_rn(A[5], d2), C.b[q])));
+  } else {
+    const float2 t0 = __ffma2_rn(A[0], d0, __ffma2_rn(A[1], d1, __fmul2_rn(A[2], d2)));
+    const float2 t1 = __ffma2_rn(A[3], d1, __fmul2_rn(A[4], d2));
+    return __ffma2_rn(d0, t0, __ffma2_rn(d1, t1, __ffma2_rn(d2, __fmul2_rn(A[5], d2), C.b[q])));
+  }
+}
 
 template <bool kW4>
-__device__ __forceinline__ float quad_f(const float* A, float d0, float d1, float d2) {
+__device__ __forceinline__ float eval_single(const CandF& C, float e0, float e1, float e2) {
+  const float d0 = e0 + C.u4[0], d1 = e1 + C.u4[1], d2 = e2 + C.u4[2];
+  const float* A = C.A4;
   if (kW4) {
     const float t0 = fmaf(A[1], d1, A[0] * d0);
-    return fmaf(d0, t0, fmaf(d1, A[3] * d1, d2 * (A[5] * d2)));
+    return fmaf(d0, t0, fmaf(d1, A[3] * d1, fmaf(d2, A[5] * d2, C.b4)));
   } else {
     const float t0 = fmaf(A[0], d0, fmaf(A[1], d1, A[2] * d2));
     const float t1 = fmaf(A[3], d1, A[4] * d2);
-    return fmaf(d0, t0, fmaf(d1, t1, d2 * (A[5] * d2)));
+    return fmaf(d0, t0, fmaf(d1, t1, fmaf(d2, A[5] * d2, C.b4)));
   }
 }
 
+struct Anchor {
+  double u0, u1, u2;  // u of the anchor (not negated)
+  double A[6];
+  double b;
+};
+
 template <bool kW4>
-__device__ __forceinline__ double quad_d(const double* A, double d0, double d1, double d2) {
-  if (kW4) {
-    return fma(d0, fma(A[1], d1, A[0] * d0), fma(d1, A[3] * d1, d2 * (A[5] * d2)));
-  } else {
-    return fma(d0, fma(A[0], d0, fma(A[1], d1, A[2] * d2)), fma(d1, fma(A[3], d1, A[4] * d2), d2 * (A[5] * d2)));
-  }
+__device__ __forceinline__ double voxel_ll_mixed(const CandF& C, const Anchor& Z, float e0, float e1, float e2,
+                                                 bool& ok) {
+  const float2 E0 = make_float2(e0, e0), E1 = make_float2(e1, e1), E2 = make_float2(e2, e2);
+  const float2 a01 = eval_pair<kW4>(C, 0, E0, E1, E2);
+  const float2 a23 = eval_pair<kW4>(C, 1, E0, E1, E2);
+  const float a4 = eval_single<kW4>(C, e0, e1, e2);
+  const float am = fmaxf(fmaxf(fmaxf(a01.x, a01.y), fmaxf(a23.x, a23.y)), a4);
+  const float nm = -am * kL2E;
+  const float2 t01 = __ffma2_rn(a01, make_float2(kL2E, kL2E), make_float2(nm, nm));
+  const float2 t23 = __ffma2_rn(a23, make_float2(kL2E, kL2E), make_float2(nm, nm));
+  const float s = (ex2_approx(t01.x) + ex2_approx(t01.y)) + (ex2_approx(t23.x) + ex2_approx(t23.y)) +
+                  ex2_approx(fmaf(a4, kL2E, nm));
+  const float br = (am - a01.x) + lg2_approx(s) * kLN2F;
+  const double d0 = (double)e0 - Z.u0, d1 = (double)e1 - Z.u1, d2 = (double)e2 - Z.u2;
+  double q;
+  if (kW4)
+    q = fma(d0, fma(Z.A[1], d1, Z.A[0] * d0), fma(d1, Z.A[3] * d1, d2 * (Z.A[5] * d2)));
+  else
+    q = fma(d0, fma(Z.A[0], d0, fma(Z.A[1], d1, Z.A[2] * d2)), fma(d1, fma(Z.A[3], d1, Z.A[4] * d2), d2 * (Z.A[5] * d2)));
+  const double ll = (Z.b + q) + (double)br;
+  ok = ll > -745.13;  // exp(ll) is a positive double
+  return ll;
 }
 
-// ln of the mixture density at e = x - c (mixed precision); ok = density > 0.
-template <bool kW4>
-__device__ __forceinline__ double voxel_ll_mixed(const LLShared& C, const float (&uf)[kJ][3],
-                                                 const float (&Af)[kJ][6], const float (&bf)[kJ], float e0,
-                                                 float e1, float e2, bool& ok) {
-  float a[kJ];
-#pragma unroll
-  for (int j = 0; j < kJ; j++)
-    a[j] = bf[j] + quad_f<kW4>(Af[j], e0 - uf[j][0], e1 - uf[j][1], e2 - uf[j][2]);
-  int js = 0;
-  float am = a[0];
-#pragma unroll
-  for (int j = 1; j < kJ; j++)
-    if (a[j] > am) {
-      am = a[j];
-      js = j;
-    }
-  float s = 0.0f;
-#pragma unroll
-  for (int j = 0; j < kJ; j++) s += __expf(a[j] - am);
-  const double d0 = (double)e0 - C.u[js][0], d1 = (double)e1 - C.u[js][1], d2 = (double)e2 - C.u[js][2];
-  const double astar = C.b[js] + quad_d<kW4>(C.A[js], d0, d1, d2);
-  ok = astar > -745.0 && !C.anynan;  // exp(astar) is a positive double
-  return astar + (double)__logf(s);
-}
+// FP64 verification mode: the reference's formula, every component in FP64.
+struct LLShared64 {
+  double u[kJ][3];
+  double A[kJ][6];  // nu * W
+  double w[kJ];     // c_j * alpha_j / A
+};
 
-// FP64 mode: d = x - m exactly as the reference forms it (x - c in FP64, then - (m - c)).
-__device__ __forceinline__ double voxel_ll_fp64(const LLShared& C, float x0, float x1, float x2, float c0, float c1,
+__device__ __forceinline__ double voxel_ll_fp64(const LLShared64& C, float x0, float x1, float x2, float c0, float c1,
                                                 float c2, bool& ok) {
   const double e0 = (double)x0 - (double)c0, e1 = (double)x1 - (double)c1, e2 = (double)x2 - (double)c2;
   double dens = 0.0;
@@ -1107,53 +1134,81 @@ __device__ __forceinline__ double voxel_ll_fp64(const LLShared& C, float x0, flo
     const double* A = C.A[j];
     const double q = A[0] * d0 * d0 + A[3] * d1 * d1 + A[5] * d2 * d2 + 2.0 * A[1] * d0 * d1 +
                      2.0 * A[2] * d0 * d2 + 2.0 * A[4] * d1 * d2;
-    dens += C.b[j] * exp(-0.5 * q);
+    dens += C.w[j] * exp(-0.5 * q);
   }
   ok = dens > 0.0;
   return ok ? log(dens) : 0.0;
 }
 
-template <bool kFp64, bool kW4>
-__device__ __forceinline__ void ll_stream(const LLShared& C, const FrameDesc& D, float c0, float c1, float c2,
-                                          int64_t p0, int64_t p1, double& lt, double& lr) {
+// Voxel tiles of one warp are staged through shared memory with asynchronous copies
+// (cp.async): kLLStages tiles of kLLTile voxels are in flight while the warp computes,
+// without holding registers.  Each lane copies and later reads only its own elements.
+constexpr int kLLTile = 128;   // voxels per tile (4 per lane)
+constexpr int kLLStages = 4;   // tiles in flight per warp
+constexpr int kLLWarpFloats = kLLStages * 4 * kLLTile;
+constexpr size_t kLLSmemBytes = sizeof(float) * kLLWarpFloats * kWarpsPerBlockV;
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int kMode>  // 0: mixed 4-DOF, 1: mixed general, 2: FP64
+__device__ __forceinline__ void ll_stream(const CandF& C, const Anchor& Z, const LLShared64& C64, const FrameDesc& D,
+                                          float c0, float c1, float c2, int64_t p0, int64_t p1, float* buf,
+                                          double& lt, double& lr) {
   const int lane = threadIdx.x & 31;
-  float uf[kJ][3], Af[kJ][6], bf[kJ];
-#pragma unroll
-  for (int j = 0; j < kJ; j++) {
-#pragma unroll
-    for (int d = 0; d < 3; d++) uf[j][d] = C.uf[j][d];
-#pragma unroll
-    for (int e = 0; e < 6; e++) Af[j][e] = C.Af[j][e];
-    bf[j] = C.bf[j];
-  }
   const float* __restrict__ qx = D.query;
   const float* __restrict__ qy = D.query + D.n_vox;
   const float* __restrict__ qz = D.query + 2 * D.n_vox;
   const float* __restrict__ im = D.img;
   const int64_t nv = p1 - p0;
-  for (int64_t v0 = p0 + lane; v0 < p1; v0 += 32 * kLLUnroll) {
-    float x[kLLUnroll], y[kLLUnroll], z[kLLUnroll], w[kLLUnroll];
+  const int ntiles = (int)((nv + kLLTile - 1) / kLLTile);
+  auto eval = [&](float x, float y, float z, bool& ok) -> double {
+    if (kMode == 2) return voxel_ll_fp64(C64, x, y, z, c0, c1, c2, ok);
+    if (kMode == 0) return voxel_ll_mixed<true>(C, Z, x - c0, y - c1, z - c2, ok);
+    return voxel_ll_mixed<false>(C, Z, x - c0, y - c1, z - c2, ok);
+  };
+  auto issue = [&](int t) {
+    if (t < ntiles) {
+      float* b = buf + (t % kLLStages) * 4 * kLLTile;
 #pragma unroll
-    for (int u = 0; u < kLLUnroll; u++) {
-      const int64_t v = v0 + 32 * u;
-      const bool in = v < p1;
-      x[u] = in ? __ldcs(qx + v) : c0;
-      y[u] = in ? __ldcs(qy + v) : c1;
-      z[u] = in ? __ldcs(qz + v) : c2;
-      w[u] = in ? __ldcs(im + v) : 0.0f;
+      for (int u = 0; u < kLLTile / 32; u++) {
+        const int64_t i = (int64_t)t * kLLTile + u * 32 + lane;
+        if (i < nv) {
+          const int64_t v = p0 + i;
+          const int o = u * 32 + lane;
+          cp_async4(b + o, qx + v);
+          cp_async4(b + kLLTile + o, qy + v);
+          cp_async4(b + 2 * kLLTile + o, qz + v);
+          cp_async4(b + 3 * kLLTile + o, im + v);
+        }
+      }
     }
+    cp_commit();  // one group per tile slot, empty past the end
+  };
 #pragma unroll
-    for (int u = 0; u < kLLUnroll; u++) {
-      const int64_t v = v0 + 32 * u;
-      if (v >= p1) break;
+  for (int t = 0; t < kLLStages - 1; t++) issue(t);
+  for (int t = 0; t < ntiles; t++) {
+    issue(t + kLLStages - 1);
+    cp_wait<kLLStages - 1>();
+    const float* b = buf + (t % kLLStages) * 4 * kLLTile;
+#pragma unroll
+    for (int u = 0; u < kLLTile / 32; u++) {
+      const int64_t i = (int64_t)t * kLLTile + u * 32 + lane;
+      if (i >= nv) break;
+      const int o = u * 32 + lane;
       bool ok;
-      const float e0 = x[u] - c0, e1 = y[u] - c1, e2 = z[u] - c2;
-      const double l = kFp64 ? voxel_ll_fp64(C, x[u], y[u], z[u], c0, c1, c2, ok)
-                             : voxel_ll_mixed<kW4>(C, uf, Af, bf, e0, e1, e2, ok);
-      const int64_t i = v - p0;
+      const double l = eval(b[o], b[kLLTile + o], b[2 * kLLTile + o], ok);
       const bool tail = i >= nv - 1024;
       if (ok) {
-        const double term = (double)w[u] * l;
+        const double term = (double)b[3 * kLLTile + o] * l;
         lt += term;
         if (tail) lr += term;
       } else if (tail && nv > 1024) {
@@ -1162,9 +1217,7 @@ __device__ __forceinline__ void ll_stream(const LLShared& C, const FrameDesc& D,
         for (int64_t i2 = i - 1024; i2 >= 0; i2 -= 1024) {
           const int64_t v2 = p0 + i2;
           bool ok2;
-          const float g0 = qx[v2], g1 = qy[v2], g2 = qz[v2];
-          const double l2 = kFp64 ? voxel_ll_fp64(C, g0, g1, g2, c0, c1, c2, ok2)
-                                  : voxel_ll_mixed<kW4>(C, uf, Af, bf, g0 - c0, g1 - c1, g2 - c2, ok2);
+          const double l2 = eval(qx[v2], qy[v2], qz[v2], ok2);
           if (ok2) {
             lr += (double)im[v2] * l2;
             break;
@@ -1173,78 +1226,157 @@ __device__ __forceinline__ void ll_stream(const LLShared& C, const FrameDesc& D,
       }
     }
   }
+  cp_wait<0>();
+}
+
+// Order-free accumulation of one double into an (integer, 2^-40 fraction) pair.
+__device__ __forceinline__ void fixed_add(long long* ip, unsigned long long* fp, double v) {
+  const double fl = floor(v);
+  const long long i = (long long)fl;
+  const unsigned long long fr = (unsigned long long)((v - fl) * kFracScale);
+  atomicAdd((unsigned long long*)ip, (unsigned long long)i);
+  atomicAdd(fp, fr);
+}
+
+__device__ __forceinline__ double fixed_read(const long long* ip, const unsigned long long* fp) {
+  const long long i = *(volatile const long long*)ip;
+  const unsigned long long f = *(volatile const unsigned long long*)fp;
+  return (double)i + (double)f / kFracScale;
+}
+
+// The reference's convergence test after iteration t (GMEMupdateCUDA.cu:4145-4148), run
+// by the warp that finished the frame's last supervoxel.
+__device__ void frame_converge(const DevPlan& P, int f) {
+  FrameState* S = &P.state[f];
+  const FrameDesc D = load_desc(P, f);
+  const double lt = fixed_read(&S->ll_int[0], &S->ll_frac[0]);
+  const double lr = fixed_read(&S->ll_int[1], &S->ll_frac[1]);
+  S->ll_int[0] = S->ll_int[1] = 0;
+  S->ll_frac[0] = S->ll_frac[1] = 0;
+  S->sv_done = 0;
+  S->ll3 = S->ll2;
+  S->ll2 = S->ll1;
+  S->ll1 = S->ll;
+  S->ll_true = lt;
+  S->ll_ref = lr;
+  S->ll = (D.ll_mode == TGMM_LL_TRUE) ? lt : lr;
+  const int next = S->iter + 1;
+  S->iter = next;
+  const double ll = S->ll;
+  const bool go = fabs(ll - S->ll1) / fabs(S->ll1) > D.tol && fabs(ll - S->ll2) / fabs(S->ll2) > D.tol &&
+                  fabs(ll - S->ll3) / fabs(S->ll3) > D.tol;
+  if (!go) S->converged = 1;
+  S->done = (!go || next > D.max_iter) ? 1 : 0;
 }
 
 template <bool kFp64>
-__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_ll_pass(DevPlan P) {
+__global__ void __launch_bounds__(kWarpsPerBlockV * 32, 2) k_ll_pass(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __shared__ LLShared shc[kWarpsPerBlockV];
-  LLShared& C = shc[warp];
-  for (int qi = 0; qi < kSvPerWarpV; qi++) {
-    const int s = blockIdx.x * kSvPerBlockV + qi * kWarpsPerBlockV + warp;
-    if (s >= total) return;
+  __shared__ LLShared64 sh64[kFp64 ? kWarpsPerBlockV : 1];
+  extern __shared__ float ll_tiles[];
+  float* buf = ll_tiles + warp * kLLWarpFloats;
+  // dynamic scheduling: warps take supervoxels from a counter; the last warp to leave
+  // the launch resets it for the next one
+  for (;;) {
+    int s = 0;
+    if (lane == 0) s = atomicAdd(&P.work[0], 1);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= total) break;
     const int f = P.sv_frame[s];
-    if (P.state[f].done) continue;
+    FrameState* S = &P.state[f];
+    if (S->done) continue;
     const FrameDesc D = load_desc(P, f);
     const int sl = s - D.sv_base;
     const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
-    const double Atot = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
-    __syncwarp();
+    const double lnA = S->ln_alpha;
+    // candidate j on lane j: u = m - c, weight b = ln(w) - ln(A), -nu W/2
+    double u[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, b = 0.0;
     if (lane < kJ) {
       const int k = P.cand[(int64_t)s * kJ + lane];
-      double W[6];
-      for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
-      const double nu = gcomp(P, G_NU, k);
-      const double alpha = gcomp(P, G_ALPHA, k);
-      const double cc[3] = {(double)c0, (double)c1, (double)c2};
-      for (int d = 0; d < 3; d++) {
-        const double u = gcomp(P, G_M0 + d, k) - cc[d];
-        C.u[lane][d] = u;
-        C.uf[lane][d] = __double2float_rn(u);
-      }
-      const double dn = det3(W) * nu * nu * nu;
-      if (kFp64) {
-        for (int e = 0; e < 6; e++) C.A[lane][e] = nu * W[e];
-        C.b[lane] = (sqrt(dn) / 15.74960994572241901324) * (alpha / Atot);
-      } else {
-        const double h[6] = {-0.5 * nu * W[0], -nu * W[1], -nu * W[2], -0.5 * nu * W[3], -nu * W[4], -0.5 * nu * W[5]};
-        for (int e = 0; e < 6; e++) {
-          C.A[lane][e] = h[e];
-          C.Af[lane][e] = __double2float_rn(h[e]);
-        }
-        const double b = 0.5 * log(dn) - 1.5 * kLnTwoPi + log(alpha) - log(Atot);
-        C.b[lane] = b;
-        C.bf[lane] = __double2float_rn(b);
-      }
+      const double* L = P.llc + (int64_t)k * 10;
+      for (int e = 0; e < 6; e++) h[e] = L[e];
+      b = L[6] - lnA;
+      u[0] = L[7] - (double)c0;
+      u[1] = L[8] - (double)c1;
+      u[2] = L[9] - (double)c2;
     }
-    __syncwarp();
-    if (lane == 0) {
-      int an = 0, w4 = 1;
-      for (int j = 0; j < kJ; j++) {
-        if (!kFp64) an |= isnan(C.b[j]) ? 1 : 0;
-        w4 &= (C.A[j][2] == 0.0 && C.A[j][4] == 0.0) ? 1 : 0;
-      }
-      C.anynan = an;
-      C.w4 = w4;
-    }
-    __syncwarp();
+    const unsigned fin = __ballot_sync(0xffffffffu, lane < kJ && isfinite(b));
+    const unsigned bad = __ballot_sync(0xffffffffu, lane < kJ && (isnan(b) || b == (double)kInfF));
+    const unsigned w4m = __ballot_sync(0xffffffffu, lane >= kJ || (h[2] == 0.0 && h[4] == 0.0));
     int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
     if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;
+    // a NaN weight makes the reference's density NaN for every voxel (skipped); no finite
+    // weight means a zero density everywhere
+    if (bad || !fin) p0 = p1;
     double lt = 0.0, lr = 0.0;
-    if (kFp64)
-      ll_stream<true, false>(C, D, c0, c1, c2, p0, p1, lt, lr);
-    else if (C.w4)
-      ll_stream<false, true>(C, D, c0, c1, c2, p0, p1, lt, lr);
-    else
-      ll_stream<false, false>(C, D, c0, c1, c2, p0, p1, lt, lr);
+    if (kFp64) {
+      LLShared64& C = sh64[warp];
+      if (lane < kJ) {
+        for (int d = 0; d < 3; d++) C.u[lane][d] = u[d];
+        for (int e = 0; e < 6; e++) C.A[lane][e] = (e == 0 || e == 3 || e == 5) ? -2.0 * h[e] : -h[e];
+        C.w[lane] = exp(b);
+      }
+      __syncwarp();
+      CandF cf;
+      Anchor z;
+      ll_stream<2>(cf, z, C, D, c0, c1, c2, p0, p1, buf, lt, lr);
+      __syncwarp();
+    } else if (p1 > p0) {
+      const int ja = __ffs(fin) - 1;  // anchor: nearest candidate with a finite weight
+      CandF cf;
+      Anchor z;
+      float uf[kJ][3], Af[kJ][6], bf[kJ];
+#pragma unroll
+      for (int p = 0; p < kJ; p++) {
+        const int src = (ja + p) % kJ;
+#pragma unroll
+        for (int d = 0; d < 3; d++) uf[p][d] = -__double2float_rn(__shfl_sync(0xffffffffu, u[d], src));
+#pragma unroll
+        for (int e = 0; e < 6; e++) Af[p][e] = __double2float_rn(__shfl_sync(0xffffffffu, h[e], src));
+        bf[p] = __double2float_rn(__shfl_sync(0xffffffffu, b, src));
+      }
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) cf.u[q][d] = make_float2(uf[2 * q][d], uf[2 * q + 1][d]);
+#pragma unroll
+        for (int e = 0; e < 6; e++) cf.A[q][e] = make_float2(Af[2 * q][e], Af[2 * q + 1][e]);
+        cf.b[q] = make_float2(bf[2 * q], bf[2 * q + 1]);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; d++) cf.u4[d] = uf[4][d];
+#pragma unroll
+      for (int e = 0; e < 6; e++) cf.A4[e] = Af[4][e];
+      cf.b4 = bf[4];
+      z.u0 = __shfl_sync(0xffffffffu, u[0], ja);
+      z.u1 = __shfl_sync(0xffffffffu, u[1], ja);
+      z.u2 = __shfl_sync(0xffffffffu, u[2], ja);
+#pragma unroll
+      for (int e = 0; e < 6; e++) z.A[e] = __shfl_sync(0xffffffffu, h[e], ja);
+      z.b = __shfl_sync(0xffffffffu, b, ja);
+      LLShared64& dummy = sh64[0];
+      if (w4m == 0xffffffffu)
+        ll_stream<0>(cf, z, dummy, D, c0, c1, c2, p0, p1, buf, lt, lr);
+      else
+        ll_stream<1>(cf, z, dummy, D, c0, c1, c2, p0, p1, buf, lt, lr);
+    }
     lt = warp_sum(lt);
     lr = warp_sum(lr);
     if (lane == 0) {
-      P.ll_part[s] = lt;
-      P.ll_part[(int64_t)P.max_sv + s] = lr;
+      fixed_add(&S->ll_int[0], &S->ll_frac[0], lt);
+      fixed_add(&S->ll_int[1], &S->ll_frac[1], lr);
+      __threadfence();
+      if (atomicAdd(&S->sv_done, 1) == D.n_sv - 1) {
+        __threadfence();
+        frame_converge(P, f);
+      }
     }
     __syncwarp();
+  }
+  if (lane == 0 && atomicAdd(&P.work[1], 1) == (int)(gridDim.x * kWarpsPerBlockV) - 1) {
+    P.work[0] = 0;
+    P.work[1] = 0;
   }
 }
 
@@ -1276,7 +1408,6 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
   const GChunk ch = P.gchunks[c];
   const FrameDesc D = load_desc(P, ch.frame);
   const FrameState S = P.state[ch.frame];
-  __shared__ int sbuf[kBucketCap][kGChunk];
   __shared__ int s_ovf[kGChunk];
   __shared__ int s_novf;
   __shared__ int s_first[kGChunk][TGMM_MAX_SV_PER_GAUSSIAN + 1];
@@ -1296,14 +1427,15 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
       s_ovf[o] = threadIdx.x;
       atomicOr(&P.state[ch.frame].flags, F_ASSIGN_OVERFLOW);
     } else {
-      for (int i = 0; i < n; i++) {
-        int v = P.abucket[(int64_t)k * kBucketCap + i];
+      int* bk = P.abucket + (int64_t)k * kBucketCap;  // this Gaussian's own bucket
+      for (int i = 1; i < n; i++) {                   // insertion sort by position
+        const int v = bk[i];
         int q = i;
-        while (q > 0 && sbuf[q - 1][threadIdx.x] > v) {
-          sbuf[q][threadIdx.x] = sbuf[q - 1][threadIdx.x];
+        while (q > 0 && bk[q - 1] > v) {
+          bk[q] = bk[q - 1];
           q--;
         }
-        sbuf[q][threadIdx.x] = v;
+        bk[q] = v;
       }
     }
   }
@@ -1339,7 +1471,8 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
       g.supervoxelNum = taken;
     } else {
       const int taken = min(n, TGMM_MAX_SV_PER_GAUSSIAN);
-      for (int i = 0; i < taken; i++) g.supervoxelIdx[i] = sbuf[i][threadIdx.x] % D.n_sv;
+      const int* bk = P.abucket + (int64_t)k * kBucketCap;
+      for (int i = 0; i < taken; i++) g.supervoxelIdx[i] = bk[i] % D.n_sv;
       g.supervoxelNum = taken;
     }
   }
@@ -1354,9 +1487,6 @@ void launch_build_maps(const DevPlan& P, cudaStream_t st) {
   k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
 }
 void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
-void launch_frame_end(const DevPlan& P, int mode, cudaStream_t st) {
-  k_frame_end<<<P.max_frames, kFrameThreads, 0, st>>>(P, mode);
-}
 void launch_moments(const DevPlan& P, cudaStream_t st) {
   k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
 }
@@ -1367,16 +1497,29 @@ void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
   k_knn_estep<<<div_up(P.max_sv, kKnnWarps), kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
-  k_mstep_update<<<P.max_gchunks, kGChunk, 0, st>>>(P);
+  k_mstep_update<<<2 * P.max_gchunks, kMChunk, 0, st>>>(P);
 }
 void launch_kill_prep(const DevPlan& P, cudaStream_t st) {
   k_kill_prep<<<P.max_gchunks, kGChunk, 0, st>>>(P);
 }
 void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st) {
+  const int grid = P.ll_blocks;
   if (fp64)
-    k_ll_pass<true><<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+    k_ll_pass<true><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
   else
-    k_ll_pass<false><<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+    k_ll_pass<false><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
+}
+
+cudaError_t configure_kernels(DevPlan& P, int device) {
+  cudaError_t e = cudaFuncSetAttribute(k_ll_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ll_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
+  int sms = 0, per = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ll_pass<false>, kWarpsPerBlockV * 32, kLLSmemBytes);
+  P.ll_blocks = sms * (per > 0 ? per : 1);
+  return e;
 }
 void launch_assign(const DevPlan& P, cudaStream_t st) {
   k_assign<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);

@@ -24,7 +24,8 @@ namespace tgmm {
 
 constexpr int kJ = TGMM_J;
 constexpr int kBucketCap = 32;   // M-step pairs per Gaussian held in the fast bucket
-constexpr int kGChunk = 64;      // Gaussians per block in per-Gaussian kernels
+constexpr int kGChunk = 256;     // Gaussians per block in per-Gaussian kernels
+constexpr int kMChunk = kGChunk / 2;  // Gaussians per block of the M-step (two per chunk)
 constexpr int kSvPerBlockT = 128;  // supervoxels per block, thread-per-supervoxel kernels
 constexpr int kWarpsPerBlockV = 8;   // warps per block, warp-per-supervoxel kernels
 constexpr int kSvPerWarpV = 2;
@@ -82,9 +83,16 @@ struct FrameState {
   int32_t flags;
   int32_t n_dead;
   double total_alpha;  // post-kill sum of alpha (the value the E-step and the ll use)
+  double ln_alpha;     // ln(total_alpha)
   double psi_total[2];
   double ll, ll1, ll2, ll3;
   double ll_true, ll_ref;
+  // order-free accumulation of the per-supervoxel log-likelihoods: integer parts and
+  // 2^-40 fractions in 64-bit integers (true, as reference)
+  long long ll_int[2];
+  unsigned long long ll_frac[2];
+  int32_t sv_done;   // supervoxels finished in this iteration's voxel pass
+  int32_t blk_done;  // Gaussian chunks finished in this iteration's kill step
 };
 
 struct BatchInfo {
@@ -124,6 +132,9 @@ struct DevPlan {
   double* alpha_part_e;
   double* alpha_part_f;
   int32_t* dead_part;
+  int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
+  int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
+  double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
   int32_t* sv_frame;
   double* mom;
@@ -152,7 +163,6 @@ __device__ __forceinline__ double& gcomp(const DevPlan& P, int c, int k) {
 // ---- kernel launchers (em_kernels.cu) ----
 void launch_build_maps(const DevPlan& P, cudaStream_t st);
 void launch_import(const DevPlan& P, cudaStream_t st);
-void launch_frame_end(const DevPlan& P, int mode, cudaStream_t st);
 void launch_moments(const DevPlan& P, cudaStream_t st);
 void launch_grid_fill(const DevPlan& P, cudaStream_t st);
 void launch_knn_estep(const DevPlan& P, cudaStream_t st);
@@ -160,6 +170,7 @@ void launch_mstep_update(const DevPlan& P, cudaStream_t st);
 void launch_kill_prep(const DevPlan& P, cudaStream_t st);
 void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st);
 void launch_assign(const DevPlan& P, cudaStream_t st);
+cudaError_t configure_kernels(DevPlan& P, int device);
 void launch_export(const DevPlan& P, cudaStream_t st);
 
 // standalone kNN (tgmm_knn): brute force over refs in shared memory tiles
