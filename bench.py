@@ -32,10 +32,10 @@ METRIC = "EM frames/s & voxel-iters/s at 1 Gvox/20k nuclei; p50/p99 frame latenc
 UNIT = "frames/s"
 WORKLOAD = "2048x1024x512 uint16 volume, 20000 nuclei (semi-axes 4-8, anisotropy 2), 5-NN, 20 EM iterations"
 EM_ITERS = 20
-# kernels the engine launches per EM call: build_maps, import, grid_fill, moments,
-# 5 per iteration (knn_estep, mstep_update, kill_prep, grid_fill, ll_pass),
+# kernels the engine launches per EM call: build_maps, import, moments,
+# 4 per iteration (knn_estep, mstep_update, kill_prep, ll_pass),
 # assign, export
-KERNELS_PER_CALL = 4 + 5 * EM_ITERS + 2
+KERNELS_PER_CALL = 3 + 4 * EM_ITERS + 2
 
 
 def parse():

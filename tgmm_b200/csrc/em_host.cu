@@ -39,8 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, ref_cell, cell_refs, cell_cnt, cell_start,
-      cell_cur, bcnt, bucket, acnt, abucket, ape, apf, dead, llc, work, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, work, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -59,11 +58,8 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.g_frame = take(4 * G);
   L.gd = take(8 * G * G_NUM);
   L.fixed = take(G);
-  L.ref_cell = take(4 * G);
-  L.cell_refs = take(16 * G);
+  L.cell_refs = take(16 * (int64_t)kCellCap * max_cells);
   L.cell_cnt = take(4 * (int64_t)max_cells);
-  L.cell_start = take(4 * ((int64_t)max_cells + F));
-  L.cell_cur = take(4 * (int64_t)max_cells);
   L.bcnt = take(4 * G);
   L.bucket = take(4 * G * kBucketCap);
   L.acnt = take(4 * G);
@@ -71,6 +67,7 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.ape = take(8 * 2 * (int64_t)max_gchunks);
   L.apf = take(8 * (int64_t)max_gchunks);
   L.dead = take(4 * (int64_t)max_gchunks);
+  L.ec = take(8 * kEcStride * G);
   L.llc = take(8 * 10 * G);
   L.work = take(64);
   L.sv_frame = take(4 * S);
@@ -84,7 +81,7 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
 }
 
 int32_t gchunks_cap(const TgmmPlanDesc& d) { return (d.max_gauss + kGChunk - 1) / kGChunk + d.max_frames; }
-int32_t cells_cap(const TgmmPlanDesc& d) { return 2 * d.max_gauss + 2 * d.max_frames; }
+int32_t cells_cap(const TgmmPlanDesc& d) { return d.max_gauss / 2 + 8 * d.max_frames; }
 
 }  // namespace
 
@@ -181,11 +178,8 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.g_frame = (int32_t*)(b + P->L.g_frame);
   D.gd = (double*)(b + P->L.gd);
   D.fixed = (uint8_t*)(b + P->L.fixed);
-  D.ref_cell = (int32_t*)(b + P->L.ref_cell);
   D.cell_refs = (float4*)(b + P->L.cell_refs);
   D.cell_cnt = (int32_t*)(b + P->L.cell_cnt);
-  D.cell_start = (int32_t*)(b + P->L.cell_start);
-  D.cell_cur = (int32_t*)(b + P->L.cell_cur);
   D.bcnt = (int32_t*)(b + P->L.bcnt);
   D.bucket = (int32_t*)(b + P->L.bucket);
   D.acnt = (int32_t*)(b + P->L.acnt);
@@ -193,6 +187,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.alpha_part_e = (double*)(b + P->L.ape);
   D.alpha_part_f = (double*)(b + P->L.apf);
   D.dead_part = (int32_t*)(b + P->L.dead);
+  D.ec = (double*)(b + P->L.ec);
   D.llc = (double*)(b + P->L.llc);
   D.work = (int32_t*)(b + P->L.work);
   e = configure_kernels(D, d->device);
@@ -283,7 +278,7 @@ int stage_batch(TgmmPlan* P, int32_t n, const TgmmFrame* fr, TgmmGaussian* const
     D.sv_base = (int32_t)ts;
     D.g_base = (int32_t)tg;
     D.cell_base = (int32_t)tc;
-    D.cell_budget = 2 * F.n_gauss + 2;
+    D.cell_budget = F.n_gauss / 2 + 8;
     D.gchunk_base = gc;
     D.n_gchunks = (F.n_gauss + kGChunk - 1) / kGChunk;
     const bool reg_zero = prm->reg_scale[0] == 0.0f && prm->reg_scale[1] == 0.0f && prm->reg_scale[2] == 0.0f;
@@ -299,6 +294,7 @@ int stage_batch(TgmmPlan* P, int32_t n, const TgmmFrame* fr, TgmmGaussian* const
     D.max_iter = prm->max_iter_em;
     D.ll_mode = prm->ll_mode;
     D.ll_prec = prm->ll_precision;
+    D.frame_id = f;
     for (int32_t c = 0; c < D.n_gchunks; c++) {
       GChunk& C = P->s_gchunks[gc + c];
       C.frame = f;
@@ -333,13 +329,11 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
   TG_CUDA(cudaMemsetAsync(D.acnt, 0, 4 * (size_t)D.max_gauss, st), "clear assignment buckets");
   launch_build_maps(D, st);
   launch_import(D, st);
-  launch_grid_fill(D, st);
   launch_moments(D, st);
   for (int it = 0; it < max_iter; it++) {
     launch_knn_estep(D, st);
     launch_mstep_update(D, st);
     launch_kill_prep(D, st);
-    launch_grid_fill(D, st);
     launch_ll_pass(D, ll_prec == TGMM_LLPREC_FP64, st);
   }
   launch_assign(D, st);

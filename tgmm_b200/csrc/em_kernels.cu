@@ -1,8 +1,8 @@
 // em_kernels.cu -- the sm_100a kernels of the supervoxel VI-EM.
 //
-// One EM call is:  build_maps, import (+ frame tail), grid_fill, moments,
+// One EM call is:  build_maps, import (+ frame tail), moments,
 //                  then per iteration: knn_estep, mstep_update, kill_prep (+ frame tail),
-//                  grid_fill, ll_pass (+ convergence test);  finally assign, export.
+//                  ll_pass (+ convergence test);  finally assign, export.
 // Every kernel loops over the whole batch (one or many frames); frames that have
 // converged are skipped through their FrameState::done flag, so a captured graph of
 // max_iter iterations serves any batch.  No kernel uses float atomics: per-frame sums
@@ -339,9 +339,12 @@ __device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc&
   return (cz * S.dims[1] + cy) * S.dims[0] + cx;
 }
 
-// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], the
-// log-likelihood constants (-nu W/2 with doubled off-diagonals, the log weight
-// 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the mean) and the grid cell.
+// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], the E-step
+// record (nu W, m, 3/beta, psi(alpha) + E[ln|Lambda|]/2, or -inf for a dead Gaussian), the
+// log-likelihood record (-nu W/2 with doubled off-diagonals, the log weight
+// 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the mean), and the Gaussian's float centre
+// inserted into its grid cell (capacity kCellCap; a full cell flags the frame, whose kNN
+// then scans every Gaussian).
 __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
                                               int k, int parity) {
   const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
@@ -350,8 +353,19 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
   for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
   const double nu = gcomp(P, G_NU, k);
   const double alpha = gcomp(P, G_ALPHA, k);
-  gcomp(P, G_PSIA0 + parity, k) = digamma(alpha);
-  gcomp(P, G_ELD0 + parity, k) = dead ? -1e32 : expected_log_det(W, nu);
+  const double m[3] = {gcomp(P, G_M0, k), gcomp(P, G_M1, k), gcomp(P, G_M2, k)};
+  const double psa = digamma(alpha);
+  const double eld = dead ? -1e32 : expected_log_det(W, nu);
+  gcomp(P, G_PSIA0 + parity, k) = psa;
+  gcomp(P, G_ELD0 + parity, k) = eld;
+  double* E = P.ec + (int64_t)k * kEcStride;
+#pragma unroll
+  for (int e = 0; e < 6; e++) E[e] = nu * W[e];
+  E[6] = m[0];
+  E[7] = m[1];
+  E[8] = m[2];
+  E[9] = 3.0 / gcomp(P, G_BETA, k);
+  E[10] = dead ? -(double)kInfF : psa + 0.5 * eld;
   double* L = P.llc + (int64_t)k * 10;
   L[0] = -0.5 * nu * W[0];
   L[1] = -nu * W[1];
@@ -360,27 +374,31 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
   L[4] = -nu * W[4];
   L[5] = -0.5 * nu * W[5];
   L[6] = 0.5 * log(det3(W) * nu * nu * nu) - 1.5 * kLnTwoPi + log(alpha);
-  L[7] = gcomp(P, G_M0, k);
-  L[8] = gcomp(P, G_M1, k);
-  L[9] = gcomp(P, G_M2, k);
-  int cell = -1;
+  L[7] = m[0];
+  L[8] = m[1];
+  L[9] = m[2];
   if (!dead) {
-    const float x = __double2float_rn(gcomp(P, G_M0, k));
-    const float y = __double2float_rn(gcomp(P, G_M1, k));
-    const float z = __double2float_rn(gcomp(P, G_M2, k));
-    cell = ref_cell_of(S, D, x, y, z);
-    if (cell >= 0) atomicAdd(&P.cell_cnt[D.cell_base + cell], 1);
+    const float x = __double2float_rn(m[0]);
+    const float y = __double2float_rn(m[1]);
+    const float z = __double2float_rn(m[2]);
+    const int cell = ref_cell_of(S, D, x, y, z);
+    if (cell >= 0) {
+      const int g = D.cell_base + cell;
+      const int pos = atomicAdd(&P.cell_cnt[g], 1);
+      if (pos < kCellCap)
+        P.cell_refs[(int64_t)g * kCellCap + pos] = make_float4(x, y, z, __int_as_float(k - D.g_base));
+      else
+        atomicOr(&P.state[D.frame_id].flags, F_CELL_OVERFLOW);
+    }
   }
-  P.ref_cell[k] = cell;
 }
 
 // Run by the last Gaussian chunk of a frame to finish (import or kill step): the alpha
 // total as a fixed-order sum of the chunk partials, psi and ln of it for the next
-// iteration, the dead count, and the exclusive scan of the grid-cell counts.
+// iteration, and the dead count.
 __device__ void frame_tail(const DevPlan& P, int f, int next_parity) {
   const FrameDesc D = load_desc(P, f);
   FrameState* S = &P.state[f];
-  __shared__ int s_scan[kGChunk / 32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (w == 0) {
     const double a = warp_sum_range(P.alpha_part_f, D.gchunk_base, D.n_gchunks);
@@ -392,43 +410,8 @@ __device__ void frame_tail(const DevPlan& P, int f, int next_parity) {
       S->ln_alpha = log(a);
       S->psi_total[next_parity] = digamma(a);
       S->n_dead = nd;
+      S->blk_done = 0;
     }
-  }
-  // exclusive scan of the cell counts -> absolute starts into cell_refs; each thread owns
-  // a contiguous segment of cells
-  const int n = S->n_cells;
-  const int per = (n + blockDim.x - 1) / blockDim.x;
-  const int b0 = min(n, (int)threadIdx.x * per), b1 = min(n, b0 + per);
-  int local = 0;
-#pragma unroll 8
-  for (int i = b0; i < b1; i++) local += P.cell_cnt[D.cell_base + i];
-  int x = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_scan[w] = x;
-  __syncthreads();
-  int before = 0, total = 0;
-#pragma unroll
-  for (int q = 0; q < kGChunk / 32; q++) {
-    const int v = s_scan[q];
-    if (q < w) before += v;
-    total += v;
-  }
-  int run = D.g_base + before + x - local;
-  for (int i = b0; i < b1; i++) {
-    const int cnt = P.cell_cnt[D.cell_base + i];
-    P.cell_start[D.cell_base + i] = run;
-    P.cell_cur[D.cell_base + i] = run;
-    P.cell_cnt[D.cell_base + i] = 0;
-    run += cnt;
-  }
-  run = D.g_base + total;
-  if (threadIdx.x == 0) {
-    P.cell_start[D.cell_base + n] = run;
-    S->blk_done = 0;
   }
 }
 
@@ -569,26 +552,6 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 }
 
 // ===========================================================================
-// grid_fill: scatter each live Gaussian's float centre into its cell.
-// ===========================================================================
-__global__ void __launch_bounds__(kGChunk) k_grid_fill(DevPlan P) {
-  const int c = blockIdx.x;
-  if (c >= P.info->n_gchunks) return;
-  const GChunk ch = P.gchunks[c];
-  if (P.state[ch.frame].done) return;
-  const FrameDesc D = load_desc(P, ch.frame);
-  const int k = ch.g_begin + threadIdx.x;
-  if (k >= ch.g_end) return;
-  const int cell = P.ref_cell[k];
-  if (cell < 0) return;
-  const int pos = atomicAdd(&P.cell_cur[D.cell_base + cell], 1);
-  const float x = __double2float_rn(gcomp(P, G_M0, k));
-  const float y = __double2float_rn(gcomp(P, G_M1, k));
-  const float z = __double2float_rn(gcomp(P, G_M2, k));
-  P.cell_refs[pos] = make_float4(x, y, z, __int_as_float(k - D.g_base));
-}
-
-// ===========================================================================
 // knn_estep: warp per supervoxel.  Exact 5-NN of the centroid among the frame's
 // Gaussian centres: the lanes split each ring of grid cells, keep private top-5 lists
 // pruned by the warp's current fifth distance, and after each ring the lists are merged
@@ -638,7 +601,7 @@ __device__ __forceinline__ void warp_merge_top5(Top5& mine, Top5& out) {
 }
 
 __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
-                                const int32_t* __restrict__ cstart, const float4* __restrict__ refs, Top5& best) {
+                                const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, Top5& best) {
   const int lane = threadIdx.x & 31;
   const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
   int c[3];
@@ -668,9 +631,10 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
       const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
       if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) continue;
       const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
-      const int b = cstart[cell], e = cstart[cell + 1];
-      for (int k = b; k < e; ++k) {
-        const float4 rr = refs[k];
+      const int e = min(ccnt[cell], kCellCap);
+      const float4* cr = refs + (int64_t)cell * kCellCap;
+      for (int k = 0; k < e; ++k) {
+        const float4 rr = cr[k];
         const float d = knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s);
         const int id = __float_as_int(rr.w);
         if (before(d, id, td, ti)) top5_insert(t, d, id);
@@ -712,8 +676,11 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
   g.h = S.h;
   g.inv_h = S.inv_h;
   Top5 t;
-  knn_warp_search(q0, q1, q2, D.scale, g, P.cell_start + D.cell_base, P.cell_refs, t);
-  if (!(t.d[kJ - 1] < kInfF)) {
+  top5_init(t);
+  const bool grid_ok = !(S.flags & F_CELL_OVERFLOW);
+  if (grid_ok)
+    knn_warp_search(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap, t);
+  if (!grid_ok || !(t.d[kJ - 1] < kInfF)) {
     // fewer than five finite distances: exact scan of every Gaussian of the frame
     Top5 m;
     top5_init(m);
@@ -737,7 +704,11 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
   const int k = D.g_base + kl;
   double Lj = 0.0;
   if (lane < kJ && n != 0.0) {
-    if (is_dead_prior(gcomp(P, G_MO0, k))) {
+    const double* E = P.ec + (int64_t)k * kEcStride;
+    const double2 e01 = *(const double2*)(E), e23 = *(const double2*)(E + 2), e45 = *(const double2*)(E + 4);
+    const double2 e67 = *(const double2*)(E + 6), e89 = *(const double2*)(E + 8), e10 = *(const double2*)(E + 10);
+    const double cst = e10.x;  // psi(alpha) + E[ln|Lambda|]/2, -inf when dead
+    if (cst == -(double)kInfF) {
       Lj = -(double)kInfF;
     } else {
       double G1[3], G2[6];
@@ -745,20 +716,16 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
       for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
 #pragma unroll
       for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
-      const double beta = gcomp(P, G_BETA, k), nu = gcomp(P, G_NU, k);
-      const double u0 = gcomp(P, G_M0, k) - (double)q0, u1 = gcomp(P, G_M1, k) - (double)q1,
-                   u2 = gcomp(P, G_M2, k) - (double)q2;
+      const double u0 = e67.x - (double)q0, u1 = e67.y - (double)q1, u2 = e89.x - (double)q2;
       const double D00 = G2[0] - 2.0 * G1[0] * u0 + n * u0 * u0;
       const double D01 = G2[1] - (G1[0] * u1 + u0 * G1[1]) + n * u0 * u1;
       const double D02 = G2[2] - (G1[0] * u2 + u0 * G1[2]) + n * u0 * u2;
       const double D11 = G2[3] - 2.0 * G1[1] * u1 + n * u1 * u1;
       const double D12 = G2[4] - (G1[1] * u2 + u1 * G1[2]) + n * u1 * u2;
       const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
-      const double tr = gcomp(P, G_W0, k) * D00 + gcomp(P, G_W3, k) * D11 + gcomp(P, G_W5, k) * D22 +
-                        2.0 * (gcomp(P, G_W1, k) * D01 + gcomp(P, G_W2, k) * D02 + gcomp(P, G_W4, k) * D12);
-      const double eLR = gcomp(P, G_PSIA0 + par, k) - S.psi_total[par];
-      const double eLD = gcomp(P, G_ELD0 + par, k);
-      Lj = -0.5 * (3.0 * n / beta + nu * tr) + n * (eLR + 0.5 * eLD);
+      // nu * tr(W D) with nu*W from the record: W00 D00 + W11 D11 + W22 D22 + 2 (W01 D01 + W02 D02 + W12 D12)
+      const double tr = e01.x * D00 + e23.y * D11 + e45.y * D22 + 2.0 * (e01.y * D01 + e23.x * D02 + e45.x * D12);
+      Lj = -0.5 * (n * e89.y + tr) + n * (cst - S.psi_total[par]);
       if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
       if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
     }
@@ -869,6 +836,13 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   __shared__ double shd[kMChunk / 32];
   if (threadIdx.x == 0) s_novf = 0;
   __syncthreads();
+  {
+    // the grid of this frame was read by this iteration's kNN and is refilled by the kill
+    // step: its 2*n_gchunks M-step blocks clear it
+    const int nb = 2 * D.n_gchunks, rank = 2 * (c - D.gchunk_base) + half;
+    const int ncell = P.state[ch.frame].n_cells;
+    for (int i = rank * kMChunk + threadIdx.x; i < ncell; i += nb * kMChunk) P.cell_cnt[D.cell_base + i] = 0;
+  }
   const int k = ch.g_begin + half * kMChunk + threadIdx.x;
   const bool valid = k < ch.g_end;
   double A[10];
@@ -1199,16 +1173,25 @@ __device__ __forceinline__ void ll_stream(const CandF& C, const Anchor& Z, const
     issue(t + kLLStages - 1);
     cp_wait<kLLStages - 1>();
     const float* b = buf + (t % kLLStages) * 4 * kLLTile;
+    // the lane's voxels of this tile as independent chains (out-of-range slots evaluate
+    // the centroid and are masked below), then the bookkeeping
+    constexpr int U = kLLTile / 32;
+    double l[U];
+    bool ok[U];
 #pragma unroll
-    for (int u = 0; u < kLLTile / 32; u++) {
-      const int64_t i = (int64_t)t * kLLTile + u * 32 + lane;
-      if (i >= nv) break;
+    for (int u = 0; u < U; u++) {
       const int o = u * 32 + lane;
-      bool ok;
-      const double l = eval(b[o], b[kLLTile + o], b[2 * kLLTile + o], ok);
+      const bool in = (int64_t)t * kLLTile + o < nv;
+      l[u] = eval(in ? b[o] : c0, in ? b[kLLTile + o] : c1, in ? b[2 * kLLTile + o] : c2, ok[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int o = u * 32 + lane;
+      const int64_t i = (int64_t)t * kLLTile + o;
+      if (i >= nv) break;
       const bool tail = i >= nv - 1024;
-      if (ok) {
-        const double term = (double)b[3 * kLLTile + o] * l;
+      if (ok[u]) {
+        const double term = (double)b[3 * kLLTile + o] * l[u];
         lt += term;
         if (tail) lr += term;
       } else if (tail && nv > 1024) {
@@ -1489,9 +1472,6 @@ void launch_build_maps(const DevPlan& P, cudaStream_t st) {
 void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
 void launch_moments(const DevPlan& P, cudaStream_t st) {
   k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
-}
-void launch_grid_fill(const DevPlan& P, cudaStream_t st) {
-  k_grid_fill<<<P.max_gchunks, kGChunk, 0, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
   k_knn_estep<<<div_up(P.max_sv, kKnnWarps), kKnnWarps * 32, 0, st>>>(P);

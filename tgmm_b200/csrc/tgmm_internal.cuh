@@ -8,7 +8,7 @@
 //                              centroid: sum e, sum e e', sum I, sum I e, sum I e e'),
 //                              cand/rnk [max_sv][5], ll partials [2][max_sv]
 //   kNN grid                   per frame a uniform grid over the centroid bounding box
-//                              (scaled space); cell counts/starts and the refs sorted by cell
+//                              (scaled space); per cell a count and kCellCap float centres
 //   M-step buckets             [max_gauss][kBucketCap] (supervoxel, slot) positions
 //   chunk tables               frame-aligned chunks of kGChunk Gaussians, so that every
 //                              per-frame sum is a fixed-order sum of chunk partials.
@@ -32,6 +32,8 @@ constexpr int kSvPerWarpV = 2;
 constexpr int kSvPerBlockV = kWarpsPerBlockV * kSvPerWarpV;
 constexpr int kNumMoments = 19;
 constexpr int kFrameThreads = 1024;
+constexpr int kCellCap = 32;   // Gaussian centres per kNN grid cell
+constexpr int kEcStride = 12;  // doubles per E-step record
 
 // moment component indices
 enum : int {
@@ -48,7 +50,8 @@ enum : int {
   F_NAN_INPUT = 2,
   F_FEW_GAUSS = 4,
   F_BUCKET_OVERFLOW = 8,
-  F_ASSIGN_OVERFLOW = 16
+  F_ASSIGN_OVERFLOW = 16,
+  F_CELL_OVERFLOW = 32
 };
 
 struct FrameDesc {
@@ -68,7 +71,7 @@ struct FrameDesc {
   float reg_scale[3];  // regularisation scale
   int32_t w4dof;
   double lambda_min, lambda_max, max_exc, tol;
-  int32_t max_iter, ll_mode, ll_prec, pad;
+  int32_t max_iter, ll_mode, ll_prec, frame_id;
 };
 
 struct FrameState {
@@ -120,11 +123,8 @@ struct DevPlan {
   int32_t* g_frame;
   double* gd;  // SoA block, see G_* offsets (component * max_gauss)
   uint8_t* fixed;
-  int32_t* ref_cell;
-  float4* cell_refs;
+  float4* cell_refs;  // [max_cells][kCellCap]: float centre + frame-local index
   int32_t* cell_cnt;
-  int32_t* cell_start;  // max_cells + max_frames entries (absolute positions into cell_refs)
-  int32_t* cell_cur;
   int32_t* bcnt;
   int32_t* bucket;
   int32_t* acnt;
@@ -134,6 +134,7 @@ struct DevPlan {
   int32_t* dead_part;
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
   int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
+  double* ec;   // per Gaussian E-step record, kEcStride doubles: nu W [6], m [3], 3/beta, psi(alpha)+eLD/2
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
   int32_t* sv_frame;
@@ -164,7 +165,6 @@ __device__ __forceinline__ double& gcomp(const DevPlan& P, int c, int k) {
 void launch_build_maps(const DevPlan& P, cudaStream_t st);
 void launch_import(const DevPlan& P, cudaStream_t st);
 void launch_moments(const DevPlan& P, cudaStream_t st);
-void launch_grid_fill(const DevPlan& P, cudaStream_t st);
 void launch_knn_estep(const DevPlan& P, cudaStream_t st);
 void launch_mstep_update(const DevPlan& P, cudaStream_t st);
 void launch_kill_prep(const DevPlan& P, cudaStream_t st);
