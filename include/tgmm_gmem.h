@@ -174,6 +174,20 @@ int tgmm_em_run_batch(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
 int tgmm_knn(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
              int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
 
+/* No counterpart in the reference.  The same exact kNN as tgmm_knn for callers that may not
+ * allocate device memory -- code whose device memory belongs to another allocator (a
+ * framework's caching pool, a host application's fixed arena) or that runs on a path where
+ * an allocation's latency or failure is not acceptable.  It calls no cudaMalloc, cudaFree or
+ * allocating library routine; its scratch is a file-scope device array of about 2.8 MB that
+ * every GPU which loads the library holds until the process exits.  At most
+ * TGMM_KNN_NOALLOC_MAX_REF reference points (TGMM_ERR_BAD_SIZE beyond).  The first call on a
+ * device looks the array's device address up with that device current; make that first call
+ * before any stream capture.  All calls share the one array: calls that overlap on the GPU
+ * (different streams, or different host threads) race and must be serialised by the caller. */
+#define TGMM_KNN_NOALLOC_MAX_REF 65535
+int tgmm_knn_noalloc(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
+                     int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
+
 /* Posterior -> prior for the next time point, on the device (served form):
  * N_k = nu_k - nu_o; m_o = m_k; beta_o = max(beta_pct*N_k, 1e-5);
  * nu_o = max(nu_pct*N_k, 3); W_o = W_k*nu_k/nu_o; alpha_o = alpha_total*1e-5*alpha_pct

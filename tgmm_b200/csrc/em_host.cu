@@ -85,6 +85,10 @@ int32_t cells_cap(const TgmmPlanDesc& d) { return d.max_gauss / 2 + 8 * d.max_fr
 
 }  // namespace
 
+namespace tgmm {
+int report_error(int code, const char* what, cudaError_t e) { return fail(code, what, e); }
+}  // namespace tgmm
+
 struct TgmmPlan {
   TgmmPlanDesc desc;
   Layout L;

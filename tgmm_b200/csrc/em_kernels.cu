@@ -1648,6 +1648,40 @@ cudaError_t knn_grid_standalone(const float* q, int64_t nq, const float* ref, in
   return e;
 }
 
+// Bytes of scratch the grid kNN needs for nref reference points.
+size_t knn_grid_scratch_bytes(int32_t nref) {
+  const size_t budget = 2 * (size_t)nref + 2;
+  const size_t refs_off = (256 + 4 * budget + 4 * (budget + 1) + 4 * budget + 4 * (size_t)nref + 255) / 256 * 256;
+  return refs_off + 16 * (size_t)nref;
+}
+
+// The grid kNN on caller-provided scratch (at least knn_grid_scratch_bytes(nref), 256-byte
+// aligned); allocates nothing.
+cudaError_t knn_grid_in_scratch(const float* q, int64_t nq, const float* ref, int32_t nref, const float scale[3],
+                                int32_t* ind, cudaStream_t st, void* scratch) {
+  const int budget = 2 * nref + 2;
+  char* buf = (char*)scratch;
+  const size_t off_state = 0, off_cnt = 256, off_start = off_cnt + 4 * (size_t)budget,
+               off_cur = off_start + 4 * ((size_t)budget + 1), off_rc = off_cur + 4 * (size_t)budget,
+               off_refs = (off_rc + 4 * (size_t)nref + 255) / 256 * 256;
+  FrameState* S = (FrameState*)(buf + off_state);
+  int* cnt = (int*)(buf + off_cnt);
+  int* start = (int*)(buf + off_start);
+  int* cur = (int*)(buf + off_cur);
+  int* rc = (int*)(buf + off_rc);
+  float4* refs = (float4*)(buf + off_refs);
+  cudaError_t e = cudaMemsetAsync(cnt, 0, 4 * (size_t)budget, st);  // counts start at zero every call
+  if (e != cudaSuccess) return e;
+  k_sa_geometry<<<1, 1024, 0, st>>>(q, nq, scale[0], scale[1], scale[2], nref, budget, S);
+  const int gb = (nref + 255) / 256;
+  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, scale[0], scale[1], scale[2], S, cnt, rc);
+  k_sa_scan<<<1, 1024, 0, st>>>(S, cnt, start, cur);
+  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, rc, cur, refs);
+  k_sa_query<<<(unsigned)((nq + 127) / 128), 128, 0, st>>>(q, nq, ref, nref, scale[0], scale[1], scale[2], S, start,
+                                                          refs, ind);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Posterior -> prior on the device (GaussianMixtureModel::updatePriors,
 // GaussianMixtureModel.cpp:892-910; N_k = nu_k - nu_o as copyFromGMEM_CUDA/updateNk

@@ -181,6 +181,13 @@ cudaError_t knn_grid_standalone(const float* query, int64_t nq, const float* ref
                                 int32_t nref, const float scale[3], int32_t* ind,
                                 cudaStream_t st);
 
+// grid kNN on caller-provided scratch (no allocation)
+size_t knn_grid_scratch_bytes(int32_t nref);
+cudaError_t knn_grid_in_scratch(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
+                                const float scale[3], int32_t* ind, cudaStream_t st, void* scratch);
+// records a failure for tgmm_last_error() and returns code
+int report_error(int code, const char* what, cudaError_t e);
+
 // device-side posterior -> prior
 cudaError_t update_priors_device(TgmmGaussian* gm, int32_t n, double bp, double np, double ap,
                                  double atot, int compute_total, cudaStream_t st);
