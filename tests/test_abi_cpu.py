@@ -1,0 +1,136 @@
+"""CPU checks of the C ABI library: it loads without a GPU, exports every entry point the
+headers declare (the C ABI and the reference's mangled C++ names), keeps the 288-byte record
+layout, and its host-only functions behave like the reference's post-loop code."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from tgmm_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+
+# the reference's C++ entry points, as the reference itself mangles them (g++, cxx11 ABI)
+LEGACY_SYMBOLS = [
+    "_Z13setDeviceCUDAi",
+    "_Z14knnCUDAinPlacePiPfS0_xi",
+    "_Z15uploadScaleCUDAPf",
+    "_Z16copyScaleToDvicePf",
+    "_Z25selectCUDAdeviceMaxMemoryv",
+    "_Z32GMEMreleaseMemoryWithSupervoxelsPPfS0_S0_PPiS2_S0_PPx",
+    "_Z35GMEMinitializeMemoryWithSupervoxelsPPfS_S0_S_S_xS0_PPiS2_tS0_S_PPxS3_",
+    "_Z43GMEMvariationalInferenceCUDAWithSupervoxelsPfS_S_S_PiS0_S_PxP24GaussianMixtureModelCUDAxitidiibNSt7__cxx11"
+    "12basic_stringIcSt11char_traitsIcESaIcEEE",
+    "_ZN24GaussianMixtureModelCUDA8writeXMLERSoi",
+    "_ZN34regularizePrecisionMatrixConstants9lambdaMinE",
+    "_ZN34regularizePrecisionMatrixConstants9lambdaMaxE",
+    "_ZN34regularizePrecisionMatrixConstants15maxExcentricityE",
+]
+
+
+def declared_c_functions():
+    names = set()
+    for h in ("tgmm_gmem.h",):
+        src = open(os.path.join(INC, h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(tgmm_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
+
+
+def test_library_loads_without_gpu():
+    lib = L.gmem()
+    assert lib.tgmm_version().startswith(b"tgmm_b200")
+
+
+@pytest.mark.parametrize("name", declared_c_functions())
+def test_every_declared_c_function_is_exported(name):
+    assert hasattr(L.gmem(), name), name
+    assert name in L.GMEM_FUNCS, f"{name} has no ctypes binding"
+
+
+@pytest.mark.parametrize("sym", LEGACY_SYMBOLS)
+def test_reference_cpp_entry_points_exported(sym):
+    out = subprocess.run(["nm", "-D", "--defined-only", L.GMEM_SO], capture_output=True, text=True).stdout
+    assert sym in out.split(), sym
+
+
+def test_record_layout_matches_reference():
+    assert C.sizeof(L.TgmmGaussian) == 288
+    offs = {"beta_k": 0, "m_k": 24, "W_k": 48, "expectedLogDetCovarianceCUDA": 96, "beta_o": 120, "m_o": 144,
+            "W_o": 168, "fixed": 216, "supervoxelIdx": 220, "supervoxelNum": 284}
+    for k, v in offs.items():
+        assert getattr(L.TgmmGaussian, k).offset == v, k
+    assert L.GAUSS_DTYPE.itemsize == 288
+    assert L.GAUSS_DTYPE.fields["supervoxelNum"][1] == 284
+
+
+def test_default_params_are_the_reference_defaults():
+    p = L.default_params()
+    assert p.max_iter_em == 400 and p.tol_likelihood == 1e-6 and p.w4dof == 1
+    assert (p.lambda_min, p.lambda_max, p.max_excentricity) == (0.02, 0.2222, 9.0)
+    assert p.ll_mode == L.TGMM_LL_AS_REFERENCE
+
+
+def test_plan_bytes_is_monotone():
+    def b(n, s, k, f=1):
+        d = L.TgmmPlanDesc()
+        d.max_vox, d.max_sv, d.max_gauss, d.max_frames, d.device = n, s, k, f, 0
+        return L.gmem().tgmm_plan_bytes(C.byref(d))
+    assert 0 < b(1000, 10, 10) < b(1000, 100, 100) < b(1000, 100, 100, 8)
+    assert b(1000, 10, 0) == -1
+
+
+def test_assign_supervoxels_matches_oracle():
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    S, K = 300, 40
+    rnk = rng.dirichlet(np.ones(5) * 0.3, size=S).T.astype(np.float32).reshape(-1)
+    ind = rng.integers(0, K, size=5 * S).astype(np.int32)
+    g = np.zeros(K, L.GAUSS_DTYPE)
+    g["supervoxelNum"] = 7  # overwritten
+    got = g.copy()
+    L.check(L.gmem().tgmm_assign_supervoxels(rnk.ctypes.data, ind.ctypes.data, S, got.ctypes.data, K), "assign")
+    want = g.copy()
+    O.lib().or_assign_supervoxels.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+    O.lib().or_assign_supervoxels(rnk.ctypes.data, ind.ctypes.data, S, want.ctypes.data, K)
+    np.testing.assert_array_equal(got["supervoxelNum"], want["supervoxelNum"])
+    for k in range(K):
+        n = want["supervoxelNum"][k]
+        np.testing.assert_array_equal(got["supervoxelIdx"][k][:n], want["supervoxelIdx"][k][:n])
+    assert (got["supervoxelNum"] <= 16).all()
+
+
+def test_rnk_file_is_the_reference_dump_format(tmp_path):
+    S = 37
+    rnk = np.linspace(0, 1, 5 * S).astype(np.float32)
+    ind = np.arange(5 * S, dtype=np.int32)
+    p = str(tmp_path / "rnk.bin")
+    L.check(L.gmem().tgmm_write_rnk_file(p.encode(), rnk.ctypes.data, ind.ctypes.data, S), "write")
+    raw = open(p, "rb").read()
+    hdr = np.frombuffer(raw[:8], np.int32)
+    assert tuple(hdr) == (S, 5)
+    np.testing.assert_array_equal(np.frombuffer(raw[8:8 + 20 * S], np.float32), rnk)
+    np.testing.assert_array_equal(np.frombuffer(raw[8 + 20 * S:], np.int32), ind)
+
+
+def test_host_functions_reject_bad_arguments():
+    lib = L.gmem()
+    assert lib.tgmm_assign_supervoxels(None, None, 3, None, 3) == L.TGMM_ERR_INVALID_ARG
+    assert lib.tgmm_write_rnk_file(None, None, None, 1) == L.TGMM_ERR_INVALID_ARG
+    assert b"tgmm_write_rnk_file" in lib.tgmm_last_error()
+
+
+def test_legacy_header_compiles_and_links(tmp_path):
+    """A C++ program written against the reference's interface builds against the library."""
+    src = tmp_path / "use_legacy.cpp"
+    src.write_text(open(os.path.join(ROOT, "tests", "legacy_harness.cpp")).read())
+    exe = tmp_path / "use_legacy"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", str(src), "-I" + INC, "-I/usr/local/cuda/include",
+                        L.GMEM_SO, "-L/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath," + os.path.dirname(L.GMEM_SO),
+                        "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
