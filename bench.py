@@ -67,7 +67,9 @@ def measured_peaks():
 
 
 def committed_traffic():
-    """DRAM bytes per launch of the voxel pass from the committed ncu summary (or None)."""
+    """DRAM bytes (read + write) per launch of the voxel pass from the committed ncu summary,
+    with the voxel count of the captured frame, or None.  The pass streams each voxel once,
+    so its traffic scales with the voxel count."""
     p = os.path.join(ROOT, "profiles", "ll_pass_traffic.json")
     try:
         with open(p) as f:
@@ -244,7 +246,7 @@ def run_ours(args):
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
                 "fallback 6650 GB/s", "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms_ll,
-                "traffic": (traffic or {}).get("bytes_per_launch_scaled"),
+                "traffic": (traffic["bytes_per_launch"] * N / traffic["n_vox"]) if traffic else None,
                 "moments_pass": {"ms_per_launch": ms_mom, "achieved": alg_bytes / (ms_mom * 1e-3) / 1e9,
                                  "frac": alg_bytes / (ms_mom * 1e-3) / 1e9 / peak}}
 
