@@ -39,7 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, work, sv_frame, mom, cand, rnk, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, work, sv_frame, sv_rec, mom, cand, rnk, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -71,6 +71,7 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.llc = take(8 * 10 * G);
   L.work = take(64);
   L.sv_frame = take(4 * S);
+  L.sv_rec = take((int64_t)sizeof(SvRec) * S);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(4 * S * kJ);
   L.rnk = take(4 * S * kJ);
@@ -200,6 +201,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
     return fail(TGMM_ERR_CUDA, "tgmm_plan_create: kernel configuration", e);
   }
   D.sv_frame = (int32_t*)(b + P->L.sv_frame);
+  D.sv_rec = (SvRec*)(b + P->L.sv_rec);
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);
   D.rnk = (float*)(b + P->L.rnk);
@@ -401,6 +403,8 @@ int collect_stats(TgmmPlan* P, int32_t n, TgmmEmStats* stats, cudaStream_t st, i
 int flags_to_status(int flags) {
   if (flags & F_BAD_CSR) return fail(TGMM_ERR_BAD_CSR, "labelListPtr is not a valid CSR over the voxels");
   if (flags & F_FEW_GAUSS) return fail(TGMM_ERR_BAD_SIZE, "a frame has fewer than 5 Gaussians");
+  if (flags & F_STAGE_TIMEOUT)
+    return fail(TGMM_ERR_DEVICE_FLAG, "a voxel tile copy did not complete within its wait limit");
   if (flags & F_NAN_INPUT) return fail(TGMM_ERR_NAN_INPUT, "NaN in voxel coordinates, intensities or Gaussians");
   return TGMM_OK;
 }

@@ -19,6 +19,7 @@ namespace tgmm {
 namespace {
 
 constexpr float kInfF = __builtin_huge_valf();
+constexpr double kInf = __builtin_huge_val();
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -273,6 +274,35 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
     }
   }
   if (bad) atomicOr(&sbad, bad);
+  // stream records of the voxel pass
+  for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
+    const int64_t a = D.lptr[i], b = D.lptr[i + 1];
+    const bool ok = !(a < 0 || b < a || b > D.n_vox || b - a >= (1 << 30));
+    const int nv = ok ? (int)(b - a) : 0;
+    const int nt = (nv + kVoxTile - 1) / kVoxTile;
+    const int r0 = nt ? nv - (nt - 1) * kVoxTile : 0;
+    SvRec r;
+    const float* comp[4] = {D.query, D.query + D.n_vox, D.query + 2 * D.n_vox, D.img};
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const uintptr_t a0 = nt ? (uintptr_t)(comp[c] + a) : 0;
+      const uintptr_t a1 = a0 + 4u * (unsigned)r0;  // first voxel of tile 1
+      r.lo0[c] = a0 & ~(uintptr_t)15;
+      r.lo1[c] = a1 & ~(uintptr_t)15;
+      r.n0[c] = nt ? (unsigned)(((a1 + 15) & ~(uintptr_t)15) - r.lo0[c]) : 0u;
+      r.nf[c] = (4u * kVoxTile + ((a1 & 15) ? 16u : 0u)) | ((unsigned)((a0 & 15) >> 2) << 16) |
+                ((unsigned)((a1 & 15) >> 2) << 20);
+    }
+    r.ntiles = nt;
+    r.nv = nv;
+    r.frame = f;
+    r.frame_nsv = D.n_sv;
+    r.c0 = D.cent[i];
+    r.c1 = D.cent[(int64_t)D.n_sv + i];
+    r.c2 = D.cent[2 * (int64_t)D.n_sv + i];
+    r.r0 = r0;
+    P.sv_rec[D.sv_base + i] = r;
+  }
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -995,13 +1025,18 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
 // GMEMupdateCUDA.cu:1913-1978), I_v * ll_v summed when the density is positive.  Two
 // sums: every voxel (true) and the reference's per-thread overwrite for supervoxels
 // above 1024 voxels (as reference).
-// With a_j = ln weight_j - nu_j d'W_j d/2, each voxel's term is written
-//   ll_v = a_0 + [ (a_max - a_0) + ln sum_j exp(a_j - a_max) ]
-// where candidate 0 is the anchor (the nearest candidate with a finite weight): a_0 in
-// FP64, the bracket -- an O(1) correction -- in FP32 with the five candidates evaluated
-// in packed FP32x2 pairs.  Voxels are centred at the supervoxel centroid c (e = x - c is
-// exact in FP32 for voxels near c) and candidates enter through u_j = m_j - c.  The FP64
-// mode evaluates every component in FP64 with the reference's formula.
+// Voxels are centred at the supervoxel centroid c (e = x - c is exact in FP32 for voxels
+// near c) and candidate j enters through u_j = m_j - c, formed in FP64 and rounded once.
+// With a_j = ln weight_j - nu_j d'W_j d/2 (d = e - u_j) each voxel's term
+//   ll_v = a_max + ln sum_j exp(a_j - a_max)
+// is evaluated in FP32, the five candidates in packed FP32x2 pairs (absolute error of a
+// term about 1e-6); a lane adds its voxels of a tile in FP32 and the tile sums in FP64.
+// The FP64 mode evaluates every component in FP64 with the reference's formula.
+// Voxel tiles reach shared memory through TMA bulk copies (cp.async.bulk, one per
+// component and tile, issued by one lane) that complete on a per-slot mbarrier:
+// kLLStages tiles of kLLTile voxels are in flight per warp while it computes.  A copy
+// covers the 16-byte aligned span around its tile and the lanes index it from the
+// component's offset.
 // Per-supervoxel results are added into per-frame 64-bit integer accumulators (integer
 // part and 2^-40 fraction), so the frame total does not depend on the order in which
 // warps finish; the warp that finishes a frame's last supervoxel runs the reference's
@@ -1022,7 +1057,7 @@ __device__ __forceinline__ float lg2_approx(float x) {
   return y;
 }
 
-// FP32 constants of the five candidates (anchor first): two packed pairs and one single.
+// FP32 constants of the five candidates: two packed pairs and one single.
 struct CandF {
   float2 u[2][3];
   float2 A[2][6];
@@ -1060,15 +1095,8 @@ __device__ __forceinline__ float eval_single(const CandF& C, float e0, float e1,
   }
 }
 
-struct Anchor {
-  double u0, u1, u2;  // u of the anchor (not negated)
-  double A[6];
-  double b;
-};
-
 template <bool kW4>
-__device__ __forceinline__ double voxel_ll_mixed(const CandF& C, const Anchor& Z, float e0, float e1, float e2,
-                                                 bool& ok) {
+__device__ __forceinline__ float voxel_ll_f32(const CandF& C, float e0, float e1, float e2) {
   const float2 E0 = make_float2(e0, e0), E1 = make_float2(e1, e1), E2 = make_float2(e2, e2);
   const float2 a01 = eval_pair<kW4>(C, 0, E0, E1, E2);
   const float2 a23 = eval_pair<kW4>(C, 1, E0, E1, E2);
@@ -1079,16 +1107,7 @@ __device__ __forceinline__ double voxel_ll_mixed(const CandF& C, const Anchor& Z
   const float2 t23 = __ffma2_rn(a23, make_float2(kL2E, kL2E), make_float2(nm, nm));
   const float s = (ex2_approx(t01.x) + ex2_approx(t01.y)) + (ex2_approx(t23.x) + ex2_approx(t23.y)) +
                   ex2_approx(fmaf(a4, kL2E, nm));
-  const float br = (am - a01.x) + lg2_approx(s) * kLN2F;
-  const double d0 = (double)e0 - Z.u0, d1 = (double)e1 - Z.u1, d2 = (double)e2 - Z.u2;
-  double q;
-  if (kW4)
-    q = fma(d0, fma(Z.A[1], d1, Z.A[0] * d0), fma(d1, Z.A[3] * d1, d2 * (Z.A[5] * d2)));
-  else
-    q = fma(d0, fma(Z.A[0], d0, fma(Z.A[1], d1, Z.A[2] * d2)), fma(d1, fma(Z.A[3], d1, Z.A[4] * d2), d2 * (Z.A[5] * d2)));
-  const double ll = (Z.b + q) + (double)br;
-  ok = ll > -745.13;  // exp(ll) is a positive double
-  return ll;
+  return fmaf(lg2_approx(s), kLN2F, am);
 }
 
 // FP64 verification mode: the reference's formula, every component in FP64.
@@ -1114,111 +1133,243 @@ __device__ __forceinline__ double voxel_ll_fp64(const LLShared64& C, float x0, f
   return ok ? log(dens) : 0.0;
 }
 
-// Voxel tiles of one warp are staged through shared memory with asynchronous copies
-// (cp.async): kLLStages tiles of kLLTile voxels are in flight while the warp computes,
-// without holding registers.  Each lane copies and later reads only its own elements.
-constexpr int kLLTile = 128;   // voxels per tile (4 per lane)
-constexpr int kLLStages = 4;   // tiles in flight per warp
-constexpr int kLLWarpFloats = kLLStages * 4 * kLLTile;
-constexpr size_t kLLSmemBytes = sizeof(float) * kLLWarpFloats * kWarpsPerBlockV;
+// --- TMA bulk staging --------------------------------------------------------
+constexpr int kLLTile = kVoxTile;             // voxels per tile (8 per lane)
+constexpr int kLLStages = 3;                  // tile slots per warp
+constexpr int kLLSpan = kLLTile + 4;          // floats per component in a slot (16-byte slack)
+constexpr int kLLSlotFloats = 4 * kLLSpan;    // x, y, z, I
+constexpr unsigned long long kLLWaitNs = 1000000000ull;  // a slot not filled within 1 s counts as lost
 
-__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase with the given parity; false after kLLWaitNs without it.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kLLWaitNs) return false;
+  return true;
+}
+// Global -> shared bulk copy (non-multicast) completing on the mbarrier at `bar`.
+__device__ __forceinline__ void bulk_g2s(unsigned dst, unsigned long long src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
+// Small global -> shared copies (cp.async) for the look-ahead records.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Tile t of a supervoxel (SvRec): one bulk copy per component of the 16-byte chunks
+// holding its voxels.  Every chunk copied holds a voxel of the tile, so no byte outside
+// its array's pages is read.
+__device__ __forceinline__ void ll_issue(const SvRec& R, int t, float* slot, unsigned bar) {
+  unsigned n[4], total = 0;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    n[c] = t == 0 ? R.n0[c] : (R.nf[c] & 0xffffu);
+    total += n[c];
+  }
+  mbar_expect_tx(bar, total);
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+    bulk_g2s(smem_addr(slot + c * kLLSpan),
+             t == 0 ? R.lo0[c] : R.lo1[c] + (unsigned long long)(4 * kLLTile) * (unsigned)(t - 1), n[c], bar);
 }
 
-template <int kMode>  // 0: mixed 4-DOF, 1: mixed general, 2: FP64
-__device__ __forceinline__ void ll_stream(const CandF& C, const Anchor& Z, const LLShared64& C64, const FrameDesc& D,
-                                          float c0, float c1, float c2, int64_t p0, int64_t p1, float* buf,
-                                          double& lt, double& lr) {
+// Look-ahead records, fetched with cp.async ahead of use: a supervoxel's stream record and
+// candidate ids (stage A, two supervoxels ahead) and its candidates' constants (10
+// doubles each) with its frame's ln(sum alpha) and done flag (stage B, one ahead).
+struct LLRec {
+  SvRec rec;
+  int32_t cand[8];
+};
+struct LLConst {
+  double llc[kJ][10];
+  double ln_alpha;
+  int32_t done, pad;
+};
+static_assert(sizeof(LLRec) % 16 == 0 && sizeof(LLConst) % 16 == 0, "look-ahead records stay 16-byte aligned");
+
+// Per-warp shared region: slots, one mbarrier per slot, three stage-A and two stage-B
+// records, and the current supervoxel's FP32 candidate constants.
+constexpr int kLLBarOff = kLLStages * kLLSlotFloats * 4;
+constexpr int kLLRecOff = (kLLBarOff + kLLStages * 8 + 15) / 16 * 16;
+constexpr int kLLConstOff = kLLRecOff + 3 * (int)sizeof(LLRec);
+constexpr int kLLCandOff = kLLConstOff + 2 * (int)sizeof(LLConst);
+constexpr int kLLWarpBytes = (kLLCandOff + (int)sizeof(CandF) + 15) / 16 * 16;
+constexpr size_t kLLSmemBytes = (size_t)kLLWarpBytes * kWarpsPerBlockV;
+static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOff % 16 == 0 && kLLCandOff % 16 == 0,
+              "slots and records stay 16-byte aligned");
+static_assert(2 * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "two blocks of the voxel pass fit an SM");
+
+// Stage A: the record and candidate ids of supervoxel s.
+__device__ __forceinline__ void ll_fetch_a(const DevPlan& P, LLRec& X, int s) {
   const int lane = threadIdx.x & 31;
-  const float* __restrict__ qx = D.query;
-  const float* __restrict__ qy = D.query + D.n_vox;
-  const float* __restrict__ qz = D.query + 2 * D.n_vox;
-  const float* __restrict__ im = D.img;
-  const int64_t nv = p1 - p0;
-  const int ntiles = (int)((nv + kLLTile - 1) / kLLTile);
-  auto eval = [&](float x, float y, float z, bool& ok) -> double {
-    if (kMode == 2) return voxel_ll_fp64(C64, x, y, z, c0, c1, c2, ok);
-    if (kMode == 0) return voxel_ll_mixed<true>(C, Z, x - c0, y - c1, z - c2, ok);
-    return voxel_ll_mixed<false>(C, Z, x - c0, y - c1, z - c2, ok);
-  };
-  auto issue = [&](int t) {
-    if (t < ntiles) {
-      float* b = buf + (t % kLLStages) * 4 * kLLTile;
+  constexpr int kRecChunks = (int)sizeof(SvRec) / 16;
+  if (lane < kRecChunks)
+    cp_async16(reinterpret_cast<char*>(&X.rec) + 16 * lane, reinterpret_cast<const char*>(P.sv_rec + s) + 16 * lane);
+  else if (lane < kRecChunks + kJ)
+    cp_async4(&X.cand[lane - kRecChunks], P.cand + (int64_t)s * kJ + (lane - kRecChunks));
+}
+// Stage B (after A landed): the candidates' constants and the frame scalars.
+__device__ __forceinline__ void ll_fetch_b(const DevPlan& P, const LLRec& A, LLConst& X) {
+  const int lane = threadIdx.x & 31;
+  if (lane < 5 * kJ) {
+    const int j = lane / 5, c = lane % 5;
+    cp_async16(&X.llc[j][2 * c], P.llc + (int64_t)A.cand[j] * 10 + 2 * c);
+  } else if (lane == 5 * kJ) {
+    cp_async8(&X.ln_alpha, &P.state[A.rec.frame].ln_alpha);
+  } else if (lane == 5 * kJ + 1) {
+    cp_async4(&X.done, &P.state[A.rec.frame].done);
+  }
+}
+
+// Evaluation of one voxel in the three modes: 0 FP32 4-DOF, 1 FP32 general, 2 FP64.
+template <int kMode>
+struct VoxelEval {
+  using T = float;
+  const CandF& C;
+  __device__ __forceinline__ float operator()(float x, float y, float z, float c0, float c1, float c2) const {
+    return voxel_ll_f32<kMode == 0>(C, x - c0, y - c1, z - c2);
+  }
+  __device__ __forceinline__ static bool ok(float l) { return l > -745.13f; }  // exp(l) is a positive double
+};
+template <>
+struct VoxelEval<2> {
+  using T = double;
+  const LLShared64& C;
+  __device__ __forceinline__ double operator()(float x, float y, float z, float c0, float c1, float c2) const {
+    bool ok;
+    const double l = voxel_ll_fp64(C, x, y, z, c0, c1, c2, ok);
+    return ok ? l : -kInf;
+  }
+  __device__ __forceinline__ static bool ok(double l) { return l > -kInf; }
+};
+
+// One staged tile: lane voxels o = u*32 + lane, sht[c] the offset of component c in the
+// slot.  kFull: all kLLTile voxels present (else the first rem).  allok turns false when
+// a present voxel has a zero density.
+template <class Eval, bool kFull>
+__device__ __forceinline__ void ll_tile(const Eval& eval, const float* __restrict__ slot, const int* sht, int rem,
+                                        float c0, float c1, float c2, typename Eval::T& tsum, bool& allok) {
+  using T = typename Eval::T;
+  const int lane = threadIdx.x & 31;
+  const float* bx = slot + sht[0] + lane;
+  const float* by = slot + kLLSpan + sht[1] + lane;
+  const float* bz = slot + 2 * kLLSpan + sht[2] + lane;
+  const float* bi = slot + 3 * kLLSpan + sht[3] + lane;
 #pragma unroll
-      for (int u = 0; u < kLLTile / 32; u++) {
-        const int64_t i = (int64_t)t * kLLTile + u * 32 + lane;
-        if (i < nv) {
-          const int64_t v = p0 + i;
-          const int o = u * 32 + lane;
-          cp_async4(b + o, qx + v);
-          cp_async4(b + kLLTile + o, qy + v);
-          cp_async4(b + 2 * kLLTile + o, qz + v);
-          cp_async4(b + 3 * kLLTile + o, im + v);
-        }
-      }
-    }
-    cp_commit();  // one group per tile slot, empty past the end
-  };
+  for (int u = 0; u < kLLTile / 32; u++) {
+    if (!kFull && u * 32 >= rem) break;
+    const T l = eval(bx[32 * u], by[32 * u], bz[32 * u], c0, c1, c2);
+    const bool ok = Eval::ok(l);
+    const bool in = kFull || u * 32 + lane < rem;
+    allok = allok && (ok || !in);
+    tsum += (in && ok) ? (T)bi[32 * u] * l : (T)0;
+  }
+}
+
+// A kept voxel (one of the last 1024 of a supervoxel above 1024 voxels) with a zero
+// density: the reference thread of its stride still holds the last voxel of the stride
+// with a positive density (GMEMupdateCUDA.cu:1961-1962).  Rare; reads global memory.
+template <class Eval>
+__device__ __forceinline__ double ll_walk_back(const Eval& eval, const SvRec& R, int i, float c0, float c1, float c2) {
+  const float* v[4];
 #pragma unroll
-  for (int t = 0; t < kLLStages - 1; t++) issue(t);
-  for (int t = 0; t < ntiles; t++) {
-    issue(t + kLLStages - 1);
-    cp_wait<kLLStages - 1>();
-    const float* b = buf + (t % kLLStages) * 4 * kLLTile;
-    // the lane's voxels of this tile as independent chains (out-of-range slots evaluate
-    // the centroid and are masked below), then the bookkeeping
-    constexpr int U = kLLTile / 32;
-    double l[U];
-    bool ok[U];
+  for (int c = 0; c < 4; c++) v[c] = reinterpret_cast<const float*>(R.lo0[c]) + ((R.nf[c] >> 16) & 3);
+  for (int i2 = i - 1024; i2 >= 0; i2 -= 1024) {
+    const typename Eval::T l2 = eval(v[0][i2], v[1][i2], v[2][i2], c0, c1, c2);
+    if (Eval::ok(l2)) return (double)v[3][i2] * (double)l2;
+  }
+  return 0.0;
+}
+
+// The kept tiles (bit t - (nt - 4) of `mask`) that hold voxels of zero density, after the
+// supervoxel's tiles: their voxels are read again from global memory and each one of zero
+// density adds the walk-back value.  Rare.
+template <class Eval>
+__device__ __forceinline__ double ll_fixup(const Eval& eval, const SvRec& R, unsigned mask, float c0, float c1,
+                                           float c2) {
+  const int lane = threadIdx.x & 31;
+  const float* v[4];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int o = u * 32 + lane;
-      const bool in = (int64_t)t * kLLTile + o < nv;
-      l[u] = eval(in ? b[o] : c0, in ? b[kLLTile + o] : c1, in ? b[2 * kLLTile + o] : c2, ok[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int o = u * 32 + lane;
-      const int64_t i = (int64_t)t * kLLTile + o;
-      if (i >= nv) break;
-      const bool tail = i >= nv - 1024;
-      if (ok[u]) {
-        const double term = (double)b[3 * kLLTile + o] * l[u];
-        lt += term;
-        if (tail) lr += term;
-      } else if (tail && nv > 1024) {
-        // the reference keeps, per thread, the last voxel of its stride with a positive
-        // density: walk back through this stride
-        for (int64_t i2 = i - 1024; i2 >= 0; i2 -= 1024) {
-          const int64_t v2 = p0 + i2;
-          bool ok2;
-          const double l2 = eval(qx[v2], qy[v2], qz[v2], ok2);
-          if (ok2) {
-            lr += (double)im[v2] * l2;
-            break;
-          }
-        }
-      }
+  for (int c = 0; c < 4; c++) v[c] = reinterpret_cast<const float*>(R.lo0[c]) + ((R.nf[c] >> 16) & 3);
+  double add = 0.0;
+  for (int k = 0; k < 4; k++) {
+    if (!(mask & (1u << k))) continue;
+    const int t = R.ntiles - 4 + k;
+    const int start = t == 0 ? 0 : R.r0 + (t - 1) * kLLTile;
+    const int rem = t == 0 ? R.r0 : kLLTile;
+    for (int o = lane; o < rem; o += 32) {
+      const int i = start + o;
+      const typename Eval::T l = eval(v[0][i], v[1][i], v[2][i], c0, c1, c2);
+      if (!Eval::ok(l)) add += ll_walk_back(eval, R, i, c0, c1, c2);
     }
   }
-  cp_wait<0>();
+  return add;
 }
 
-// Order-free accumulation of one double into an (integer, 2^-40 fraction) pair.
-__device__ __forceinline__ void fixed_add(long long* ip, unsigned long long* fp, double v) {
+// Tile t (landed in `slot`) of the current supervoxel: its sum goes to lt, and to lr when
+// the tile is one of the last four (the reference's kept window of 1024 voxels).  A kept
+// tile of a supervoxel above 1024 voxels with a voxel of zero density is marked in fix.
+template <class Eval>
+__device__ __forceinline__ void ll_consume(const Eval& eval, const float* slot, const int* pk, int t, int nt, int nv,
+                                           int r0, float c0, float c1, float c2, double& lt, double& lr,
+                                           unsigned& fix) {
+  using T = typename Eval::T;
+  const int sft = t == 0 ? 0 : 4;
+  const int sht[4] = {(pk[0] >> sft) & 3, (pk[1] >> sft) & 3, (pk[2] >> sft) & 3, (pk[3] >> sft) & 3};
+  const int rem = t == 0 ? r0 : kLLTile;
+  T tsum = (T)0;
+  bool allok = true;
+  if (rem == kLLTile)
+    ll_tile<Eval, true>(eval, slot, sht, rem, c0, c1, c2, tsum, allok);
+  else
+    ll_tile<Eval, false>(eval, slot, sht, rem, c0, c1, c2, tsum, allok);
+  lt += (double)tsum;
+  if (t >= nt - 4) {
+    lr += (double)tsum;
+    if (nv > 1024 && __any_sync(0xffffffffu, !allok)) fix |= 1u << (t - (nt - 4));
+  }
+}
+
+// Order-free accumulation: a double becomes an (integer, 2^-40 fraction) pair, and pairs
+// add as integers, so a total does not depend on the order of its parts.
+__device__ __forceinline__ void fixed_acc(long long& ip, unsigned long long& fp, double v) {
   const double fl = floor(v);
-  const long long i = (long long)fl;
-  const unsigned long long fr = (unsigned long long)((v - fl) * kFracScale);
-  atomicAdd((unsigned long long*)ip, (unsigned long long)i);
-  atomicAdd(fp, fr);
+  ip += (long long)fl;
+  fp += (unsigned long long)((v - fl) * kFracScale);
 }
 
 __device__ __forceinline__ double fixed_read(const long long* ip, const unsigned long long* fp) {
@@ -1252,111 +1403,200 @@ __device__ void frame_converge(const DevPlan& P, int f) {
   S->done = (!go || next > D.max_iter) ? 1 : 0;
 }
 
+// Each warp streams the supervoxels it takes from the work counter through a ring of
+// kLLStages tile slots; the ring runs on from one supervoxel into the next.  Tickets are
+// taken two supervoxels ahead: while the warp computes its i-th supervoxel, the stream
+// record and candidate ids of the (i+2)-th (stage A) and the candidates' constants of the
+// (i+1)-th (stage B) are on their way, so every wait is for copies issued a supervoxel
+// earlier.  A warp adds its supervoxels' sums into fixed-point registers and publishes
+// them (with the count of supervoxels) when its frame changes and when it leaves; the
+// warp that completes a frame's count runs the convergence test.
 template <bool kFp64>
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32, 2) k_ll_pass(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ LLShared64 sh64[kFp64 ? kWarpsPerBlockV : 1];
-  extern __shared__ float ll_tiles[];
-  float* buf = ll_tiles + warp * kLLWarpFloats;
-  // dynamic scheduling: warps take supervoxels from a counter; the last warp to leave
-  // the launch resets it for the next one
-  for (;;) {
-    int s = 0;
-    if (lane == 0) s = atomicAdd(&P.work[0], 1);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if (s >= total) break;
-    const int f = P.sv_frame[s];
-    FrameState* S = &P.state[f];
-    if (S->done) continue;
-    const FrameDesc D = load_desc(P, f);
-    const int sl = s - D.sv_base;
-    const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
-    const double lnA = S->ln_alpha;
+  extern __shared__ __align__(128) unsigned char ll_smem[];
+  unsigned char* wbase = ll_smem + (size_t)warp * kLLWarpBytes;
+  float* wbuf = reinterpret_cast<float*>(wbase);
+  const unsigned bar0 = smem_addr(wbase + kLLBarOff);
+  LLRec* RA = reinterpret_cast<LLRec*>(wbase + kLLRecOff);
+  LLConst* RB = reinterpret_cast<LLConst*>(wbase + kLLConstOff);
+  CandF* cs = reinterpret_cast<CandF*>(wbase + kLLCandOff);
+  if (lane == 0)
+    for (int q = 0; q < kLLStages; q++) mbar_init(bar0 + 8 * q, 1);
+  mbar_fence_init();
+  __syncwarp();
+  // lane 0: the fixed-point sums (true, as reference) of the warp's current frame run
+  int acc_f = -1, acc_nsv = 0, acc_n = 0;
+  long long acc_i0 = 0, acc_i1 = 0;
+  unsigned long long acc_r0 = 0, acc_r1 = 0;
+  auto publish = [&]() {
+    if (lane == 0 && acc_n > 0) {
+      FrameState* Sp = &P.state[acc_f];
+      atomicAdd((unsigned long long*)&Sp->ll_int[0], (unsigned long long)acc_i0);
+      atomicAdd((unsigned long long*)&Sp->ll_int[1], (unsigned long long)acc_i1);
+      atomicAdd(&Sp->ll_frac[0], acc_r0);
+      atomicAdd(&Sp->ll_frac[1], acc_r1);
+      __threadfence();
+      if (atomicAdd(&Sp->sv_done, acc_n) == acc_nsv - acc_n) {
+        __threadfence();
+        frame_converge(P, acc_f);
+      }
+    }
+    acc_n = 0;
+    acc_i0 = acc_i1 = 0;
+    acc_r0 = acc_r1 = 0;
+  };
+  // tiles issued / consumed by this warp in this launch (slot = count mod kLLStages,
+  // mbarrier phase = count / kLLStages), and tiles of the current and the next supervoxel
+  // already issued; every lane keeps the same counts
+  unsigned gi = 0, gc = 0;
+  int ic = 0;
+  FrameState* S = nullptr;
+  bool failed = false;
+  // tickets: the current, the next, and (lane 0) the one after
+  int tk = 0;
+  if (lane == 0) tk = atomicAdd(&P.work[0], 1);
+  int sc = __shfl_sync(0xffffffffu, tk, 0);
+  if (lane == 0 && sc < total) tk = atomicAdd(&P.work[0], 1);
+  int sn = sc < total ? __shfl_sync(0xffffffffu, tk, 0) : total;
+  if (lane == 0 && sn < total) tk = atomicAdd(&P.work[0], 1);
+  if (sc < total) {
+    ll_fetch_a(P, RA[0], sc);
+    if (sn < total) ll_fetch_a(P, RA[1], sn);
+    cp_commit();
+    cp_wait_all();
+    __syncwarp();
+    ll_fetch_b(P, RA[0], RB[0]);
+    cp_commit();
+  }
+  for (unsigned i = 0; sc < total; i++) {
+    // everything fetched so far was issued at least a supervoxel ago
+    cp_wait_all();
+    __syncwarp();
+    const LLRec& CA = RA[i % 3];
+    const LLConst& CB = RB[i & 1];
+    const LLRec& NA = RA[(i + 1) % 3];
+    const int s2 = __shfl_sync(0xffffffffu, tk, 0);
+    if (lane == 0 && s2 < total) tk = atomicAdd(&P.work[0], 1);
+    if (sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
+    if (s2 < total) ll_fetch_a(P, RA[(i + 2) % 3], s2);
+    cp_commit();
+    int in = 0;
+    const int n_nt = sn < total ? NA.rec.ntiles : 0;  // the next one's tiles may start early
+    const int nv = CA.rec.nv, nt = CA.rec.ntiles, f = CA.rec.frame, nsv = CA.rec.frame_nsv;
+    const float c0 = CA.rec.c0, c1 = CA.rec.c1, c2 = CA.rec.c2;
+    const bool run = CB.done == 0;
+    S = &P.state[f];
     // candidate j on lane j: u = m - c, weight b = ln(w) - ln(A), -nu W/2
     double u[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, b = 0.0;
     if (lane < kJ) {
-      const int k = P.cand[(int64_t)s * kJ + lane];
-      const double* L = P.llc + (int64_t)k * 10;
+      const double* L = CB.llc[lane];
       for (int e = 0; e < 6; e++) h[e] = L[e];
-      b = L[6] - lnA;
+      b = L[6] - CB.ln_alpha;
       u[0] = L[7] - (double)c0;
       u[1] = L[8] - (double)c1;
       u[2] = L[9] - (double)c2;
     }
     const unsigned fin = __ballot_sync(0xffffffffu, lane < kJ && isfinite(b));
-    const unsigned bad = __ballot_sync(0xffffffffu, lane < kJ && (isnan(b) || b == (double)kInfF));
+    const unsigned nan_w = __ballot_sync(0xffffffffu, lane < kJ && (isnan(b) || b == (double)kInfF));
     const unsigned w4m = __ballot_sync(0xffffffffu, lane >= kJ || (h[2] == 0.0 && h[4] == 0.0));
-    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
-    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;
     // a NaN weight makes the reference's density NaN for every voxel (skipped); no finite
-    // weight means a zero density everywhere
-    if (bad || !fin) p0 = p1;
-    double lt = 0.0, lr = 0.0;
+    // weight means a zero density everywhere: the tiles are consumed unread
+    const bool compute = run && fin && !nan_w;
     if (kFp64) {
-      LLShared64& C = sh64[warp];
+      LLShared64& Q = sh64[warp];
       if (lane < kJ) {
-        for (int d = 0; d < 3; d++) C.u[lane][d] = u[d];
-        for (int e = 0; e < 6; e++) C.A[lane][e] = (e == 0 || e == 3 || e == 5) ? -2.0 * h[e] : -h[e];
-        C.w[lane] = exp(b);
+        for (int d = 0; d < 3; d++) Q.u[lane][d] = u[d];
+        for (int e = 0; e < 6; e++) Q.A[lane][e] = (e == 0 || e == 3 || e == 5) ? -2.0 * h[e] : -h[e];
+        Q.w[lane] = exp(b);
       }
-      __syncwarp();
-      CandF cf;
-      Anchor z;
-      ll_stream<2>(cf, z, C, D, c0, c1, c2, p0, p1, buf, lt, lr);
-      __syncwarp();
-    } else if (p1 > p0) {
-      const int ja = __ffs(fin) - 1;  // anchor: nearest candidate with a finite weight
-      CandF cf;
-      Anchor z;
-      float uf[kJ][3], Af[kJ][6], bf[kJ];
-#pragma unroll
-      for (int p = 0; p < kJ; p++) {
-        const int src = (ja + p) % kJ;
-#pragma unroll
-        for (int d = 0; d < 3; d++) uf[p][d] = -__double2float_rn(__shfl_sync(0xffffffffu, u[d], src));
-#pragma unroll
-        for (int e = 0; e < 6; e++) Af[p][e] = __double2float_rn(__shfl_sync(0xffffffffu, h[e], src));
-        bf[p] = __double2float_rn(__shfl_sync(0xffffffffu, b, src));
-      }
-#pragma unroll
-      for (int q = 0; q < 2; q++) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) cf.u[q][d] = make_float2(uf[2 * q][d], uf[2 * q + 1][d]);
-#pragma unroll
-        for (int e = 0; e < 6; e++) cf.A[q][e] = make_float2(Af[2 * q][e], Af[2 * q + 1][e]);
-        cf.b[q] = make_float2(bf[2 * q], bf[2 * q + 1]);
-      }
-#pragma unroll
-      for (int d = 0; d < 3; d++) cf.u4[d] = uf[4][d];
-#pragma unroll
-      for (int e = 0; e < 6; e++) cf.A4[e] = Af[4][e];
-      cf.b4 = bf[4];
-      z.u0 = __shfl_sync(0xffffffffu, u[0], ja);
-      z.u1 = __shfl_sync(0xffffffffu, u[1], ja);
-      z.u2 = __shfl_sync(0xffffffffu, u[2], ja);
-#pragma unroll
-      for (int e = 0; e < 6; e++) z.A[e] = __shfl_sync(0xffffffffu, h[e], ja);
-      z.b = __shfl_sync(0xffffffffu, b, ja);
-      LLShared64& dummy = sh64[0];
-      if (w4m == 0xffffffffu)
-        ll_stream<0>(cf, z, dummy, D, c0, c1, c2, p0, p1, buf, lt, lr);
+    } else if (lane < kJ) {
+      // the five candidates' FP32 constants in the packed layout (pairs 0-1, 2-3; single 4)
+      float* fu = lane < 4 ? &cs->u[lane >> 1][0].x + (lane & 1) : cs->u4;
+      float* fa = lane < 4 ? &cs->A[lane >> 1][0].x + (lane & 1) : cs->A4;
+      const int st = lane < 4 ? 2 : 1;
+      for (int d = 0; d < 3; d++) fu[st * d] = -__double2float_rn(u[d]);
+      for (int e = 0; e < 6; e++) fa[st * e] = __double2float_rn(h[e]);
+      if (lane < 4)
+        (&cs->b[lane >> 1].x)[lane & 1] = __double2float_rn(b);
       else
-        ll_stream<1>(cf, z, dummy, D, c0, c1, c2, p0, p1, buf, lt, lr);
-    }
-    lt = warp_sum(lt);
-    lr = warp_sum(lr);
-    if (lane == 0) {
-      fixed_add(&S->ll_int[0], &S->ll_frac[0], lt);
-      fixed_add(&S->ll_int[1], &S->ll_frac[1], lr);
-      __threadfence();
-      if (atomicAdd(&S->sv_done, 1) == D.n_sv - 1) {
-        __threadfence();
-        frame_converge(P, f);
-      }
+        cs->b4 = __double2float_rn(b);
     }
     __syncwarp();
+    const CandF cf = *cs;
+    int pk[4];  // slot offsets of the components: tile 0 in bits 0-1, later tiles in bits 4-5
+#pragma unroll
+    for (int c = 0; c < 4; c++) pk[c] = (int)(CA.rec.nf[c] >> 16);
+    const int r0 = CA.rec.r0;
+    double lt = 0.0, lr = 0.0;
+    unsigned fix = 0;  // kept tiles with voxels of zero density
+    // a finished frame issues no more tiles; those issued early are consumed unread
+    const int ntr = run ? nt : ic;
+    for (int t = 0; t < ntr; t++) {
+      __syncwarp();  // every lane is done with the slots refilled below
+      // refill the ring: the current supervoxel's tiles, then the next one's
+      while (gi < gc + kLLStages) {
+        const bool mine = ic < ntr;
+        if (!mine && in >= n_nt) break;
+        const int tt = mine ? ic++ : in++;
+        if (lane == 0) {
+          const unsigned q = gi % kLLStages;
+          ll_issue(mine ? CA.rec : NA.rec, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
+        }
+        gi++;
+      }
+      const unsigned q = gc % kLLStages;
+      if (!__all_sync(0xffffffffu, mbar_wait(bar0 + 8 * q, (gc / kLLStages) & 1))) {
+        failed = true;
+        break;
+      }
+      const float* slot = wbuf + q * kLLSlotFloats;
+      if (compute) {
+        if (kFp64)
+          ll_consume(VoxelEval<2>{sh64[warp]}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+        else if (w4m == 0xffffffffu)
+          ll_consume(VoxelEval<0>{cf}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+        else
+          ll_consume(VoxelEval<1>{cf}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+      }
+      gc++;
+    }
+    if (failed) break;
+    if (fix) {
+      if (kFp64)
+        lr += ll_fixup(VoxelEval<2>{sh64[warp]}, CA.rec, fix, c0, c1, c2);
+      else if (w4m == 0xffffffffu)
+        lr += ll_fixup(VoxelEval<0>{cf}, CA.rec, fix, c0, c1, c2);
+      else
+        lr += ll_fixup(VoxelEval<1>{cf}, CA.rec, fix, c0, c1, c2);
+    }
+    if (run) {
+      lt = warp_sum(lt);
+      lr = warp_sum(lr);
+      if (lane == 0) {
+        if (f != acc_f) {
+          publish();
+          acc_f = f;
+          acc_nsv = nsv;
+        }
+        fixed_acc(acc_i0, acc_r0, lt);
+        fixed_acc(acc_i1, acc_r1, lr);
+        acc_n++;
+      }
+    }
+    __syncwarp();  // the records of this supervoxel are refilled from the next iteration on
+    sc = sn;
+    sn = s2;
+    ic = in;
   }
+  if (failed) {  // a tile never arrived: wait for the copies still in flight, report, leave
+    for (unsigned g = gc + 1; g < gi; g++) mbar_wait(bar0 + 8 * (g % kLLStages), (g / kLLStages) & 1);
+    if (lane == 0) atomicOr(&S->flags, F_STAGE_TIMEOUT);
+  }
+  cp_wait_all();
+  publish();
   if (lane == 0 && atomicAdd(&P.work[1], 1) == (int)(gridDim.x * kWarpsPerBlockV) - 1) {
     P.work[0] = 0;
     P.work[1] = 0;

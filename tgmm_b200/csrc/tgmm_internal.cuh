@@ -51,7 +51,8 @@ enum : int {
   F_FEW_GAUSS = 4,
   F_BUCKET_OVERFLOW = 8,
   F_ASSIGN_OVERFLOW = 16,
-  F_CELL_OVERFLOW = 32
+  F_CELL_OVERFLOW = 32,
+  F_STAGE_TIMEOUT = 64  // a voxel tile copy did not complete within its wait limit
 };
 
 struct FrameDesc {
@@ -98,6 +99,28 @@ struct FrameState {
   int32_t blk_done;  // Gaussian chunks finished in this iteration's kill step
 };
 
+// Voxel tiles of the per-iteration voxel pass: kVoxTile voxels of a supervoxel per copy.
+constexpr int kVoxTile = 256;
+
+// Per-supervoxel stream record of the voxel pass, built once per call (k_build_maps).
+// Tiles are aligned to the END of the supervoxel: tile 0 holds its first r0 voxels
+// (1 <= r0 <= kVoxTile) and every later tile kVoxTile voxels, so the reference's kept
+// window of the last 1024 voxels is exactly the last four tiles.  Component c (x, y, z,
+// I) of tile 0 is the 16-byte aligned span [lo0[c], + n0[c]); of tile t >= 1 the span
+// [lo1[c] + 4 kVoxTile (t - 1), + (nf[c] & 0xffff)).  The first voxel of tile 0 sits
+// (nf[c] >> 16) & 3 floats into its span, that of the later tiles (nf[c] >> 20) & 3.
+struct SvRec {
+  unsigned long long lo0[4];
+  unsigned long long lo1[4];
+  unsigned n0[4];
+  unsigned nf[4];
+  int32_t ntiles, nv;
+  int32_t frame, frame_nsv;
+  float c0, c1, c2;
+  int32_t r0;
+};
+static_assert(sizeof(SvRec) == 128, "SvRec is eight 16-byte chunks");
+
 struct BatchInfo {
   int32_t n_frames;
   int32_t total_sv;
@@ -138,6 +161,7 @@ struct DevPlan {
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
   int32_t* sv_frame;
+  SvRec* sv_rec;
   double* mom;
   int32_t* cand;
   float* rnk;
