@@ -274,35 +274,6 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
     }
   }
   if (bad) atomicOr(&sbad, bad);
-  // stream records of the voxel pass
-  for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
-    const int64_t a = D.lptr[i], b = D.lptr[i + 1];
-    const bool ok = !(a < 0 || b < a || b > D.n_vox || b - a >= (1 << 30));
-    const int nv = ok ? (int)(b - a) : 0;
-    const int nt = (nv + kVoxTile - 1) / kVoxTile;
-    const int r0 = nt ? nv - (nt - 1) * kVoxTile : 0;
-    SvRec r;
-    const float* comp[4] = {D.query, D.query + D.n_vox, D.query + 2 * D.n_vox, D.img};
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      const uintptr_t a0 = nt ? (uintptr_t)(comp[c] + a) : 0;
-      const uintptr_t a1 = a0 + 4u * (unsigned)r0;  // first voxel of tile 1
-      r.lo0[c] = a0 & ~(uintptr_t)15;
-      r.lo1[c] = a1 & ~(uintptr_t)15;
-      r.n0[c] = nt ? (unsigned)(((a1 + 15) & ~(uintptr_t)15) - r.lo0[c]) : 0u;
-      r.nf[c] = (4u * kVoxTile + ((a1 & 15) ? 16u : 0u)) | ((unsigned)((a0 & 15) >> 2) << 16) |
-                ((unsigned)((a1 & 15) >> 2) << 20);
-    }
-    r.ntiles = nt;
-    r.nv = nv;
-    r.frame = f;
-    r.frame_nsv = D.n_sv;
-    r.c0 = D.cent[i];
-    r.c1 = D.cent[(int64_t)D.n_sv + i];
-    r.c2 = D.cent[2 * (int64_t)D.n_sv + i];
-    r.r0 = r0;
-    P.sv_rec[D.sv_base + i] = r;
-  }
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -510,6 +481,36 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
 // FP64 at half the FP32 rate, cheaper here than compensated FP32).  19 moments:
 // sum e, sum e e', sum I, sum I e, sum I e e'.
 // ===========================================================================
+// The stream record (SvRec) of supervoxel s (frame-local sl) for the voxel pass.
+__device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s, int sl) {
+  const int64_t a = D.lptr[sl], b = D.lptr[sl + 1];
+  const bool ok = !(a < 0 || b < a || b > D.n_vox || b - a >= (1 << 30));
+  const int nv = ok ? (int)(b - a) : 0;
+  const int nt = (nv + kVoxTile - 1) / kVoxTile;
+  const int r0 = nt ? nv - (nt - 1) * kVoxTile : 0;
+  SvRec r;
+  const float* comp[4] = {D.query, D.query + D.n_vox, D.query + 2 * D.n_vox, D.img};
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const uintptr_t a0 = nt ? (uintptr_t)(comp[c] + a) : 0;
+    const uintptr_t a1 = a0 + 4u * (unsigned)r0;  // first voxel of tile 1
+    r.lo0[c] = a0 & ~(uintptr_t)15;
+    r.lo1[c] = a1 & ~(uintptr_t)15;
+    r.n0[c] = nt ? (unsigned)(((a1 + 15) & ~(uintptr_t)15) - r.lo0[c]) : 0u;
+    r.nf[c] = (4u * kVoxTile + ((a1 & 15) ? 16u : 0u)) | ((unsigned)((a0 & 15) >> 2) << 16) |
+              ((unsigned)((a1 & 15) >> 2) << 20);
+  }
+  r.ntiles = nt;
+  r.nv = nv;
+  r.frame = f;
+  r.frame_nsv = D.n_sv;
+  r.c0 = D.cent[sl];
+  r.c1 = D.cent[(int64_t)D.n_sv + sl];
+  r.c2 = D.cent[2 * (int64_t)D.n_sv + sl];
+  r.r0 = r0;
+  P.sv_rec[s] = r;
+}
+
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -519,6 +520,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
     const int f = P.sv_frame[s];
     const FrameDesc D = load_desc(P, f);
     const int sl = s - D.sv_base;
+    if (lane == 0) write_sv_rec(P, D, f, s, sl);
     int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
     if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;  // flagged by build_maps
     const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
@@ -653,13 +655,9 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
     // prune with the warp's current fifth: a ref must beat it to matter
     const float td = best.d[kJ - 1];
     const int ti = best.i[kJ - 1];
-    const int side = 2 * r + 1;
-    const int cube = side * side * side;
-    for (int idx = lane; idx < cube; idx += 32) {
-      const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
-      if (r > 1 && max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+    auto scan_cell = [&](int dx, int dy, int dz) {
       const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
-      if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) continue;
+      if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) return;
       const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
       const int e = min(ccnt[cell], kCellCap);
       const float4* cr = refs + (int64_t)cell * kCellCap;
@@ -668,6 +666,28 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
         const float d = knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s);
         const int id = __float_as_int(rr.w);
         if (before(d, id, td, ti)) top5_insert(t, d, id);
+      }
+    };
+    // the cells of ring r (the whole cube for r = 1), with constant divisors for the
+    // rings a search usually needs
+    if (r == 1) {
+      if (lane < 27) scan_cell(lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1);
+    } else if (r == 2) {
+      for (int idx = lane; idx < 125; idx += 32) {
+        const int dx = idx % 5 - 2, dy = (idx / 5) % 5 - 2, dz = idx / 25 - 2;
+        if (max(abs(dx), max(abs(dy), abs(dz))) == 2) scan_cell(dx, dy, dz);
+      }
+    } else if (r == 3) {
+      for (int idx = lane; idx < 343; idx += 32) {
+        const int dx = idx % 7 - 3, dy = (idx / 7) % 7 - 3, dz = idx / 49 - 3;
+        if (max(abs(dx), max(abs(dy), abs(dz))) == 3) scan_cell(dx, dy, dz);
+      }
+    } else {
+      const int side = 2 * r + 1;
+      const int cube = side * side * side;
+      for (int idx = lane; idx < cube; idx += 32) {
+        const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
+        if (max(abs(dx), max(abs(dy), abs(dz))) == r) scan_cell(dx, dy, dz);
       }
     }
     // lane 0 also carries the previous best (disjoint from this ring's refs)
@@ -760,9 +780,15 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
       if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
     }
   }
+  // rnk_j = 1 / sum_i exp(L_i - L_j): lane 5i + j evaluates exp(L_i - L_j), and the sum
+  // runs over i in increasing order
+  const int ei = lane / kJ, ej = lane - ei * kJ;
+  const double Li = __shfl_sync(0xffffffffu, Lj, ei < kJ ? ei : 0);
+  const double Lk = __shfl_sync(0xffffffffu, Lj, ej);
+  const double ex = lane < kJ * kJ ? exp(Li - Lk) : 0.0;
   double acc = 0.0;
 #pragma unroll
-  for (int i = 0; i < kJ; i++) acc += exp(__shfl_sync(0xffffffffu, Lj, i) - Lj);
+  for (int i = 0; i < kJ; i++) acc += __shfl_sync(0xffffffffu, ex, i * kJ + (lane < kJ ? lane : 0));
   if (lane < kJ) {
     const float r = __double2float_rn(1.0 / acc);
     const int j = lane;

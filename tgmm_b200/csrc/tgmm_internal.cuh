@@ -102,7 +102,7 @@ struct FrameState {
 // Voxel tiles of the per-iteration voxel pass: kVoxTile voxels of a supervoxel per copy.
 constexpr int kVoxTile = 256;
 
-// Per-supervoxel stream record of the voxel pass, built once per call (k_build_maps).
+// Per-supervoxel stream record of the voxel pass, built once per call (k_moments).
 // Tiles are aligned to the END of the supervoxel: tile 0 holds its first r0 voxels
 // (1 <= r0 <= kVoxTile) and every later tile kVoxTile voxels, so the reference's kept
 // window of the last 1024 voxels is exactly the last four tiles.  Component c (x, y, z,
