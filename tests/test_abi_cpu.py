@@ -34,7 +34,7 @@ LEGACY_SYMBOLS = [
 
 def declared_c_functions():
     names = set()
-    for h in ("tgmm_gmem.h",):
+    for h in ("tgmm_gmem.h", "tgmm_serve.h"):
         src = open(os.path.join(INC, h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         names |= set(re.findall(r"\b(tgmm_[a-z0-9_]+)\s*\(", src))
@@ -134,3 +134,39 @@ def test_legacy_header_compiles_and_links(tmp_path):
                         "-o", str(exe)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_server_arena_selftest_passes_on_cpu():
+    assert L.gmem().tgmm_server_selftest() == 0
+
+
+def test_serve_structs_match_the_c_header(tmp_path):
+    """ctypes mirrors of the serve structs have the C compiler's sizes and offsets."""
+    structs = {"TgmmServerDesc": L.TgmmServerDesc, "TgmmServeRequest": L.TgmmServeRequest,
+               "TgmmServeResult": L.TgmmServeResult, "TgmmServerStats": L.TgmmServerStats,
+               "TgmmEmParams": L.TgmmEmParams, "TgmmEmStats": L.TgmmEmStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "tgmm_serve.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for f, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", str(src), "-I" + INC, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
+    for name, cls in structs.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for f, _ in cls._fields_:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, f"{name}.{f}"
+
+
+def test_lineage_shard_covers_every_lineage_once():
+    from tgmm_b200.serve import lineage_shard
+    for n, w in [(4, 1), (4, 2), (7, 3), (2, 4)]:
+        parts = [lineage_shard(n, r, w) for r in range(w)]
+        flat = sorted(x for p in parts for x in p)
+        assert flat == list(range(n))
+        assert max(map(len, parts)) - min(map(len, parts)) <= 1

@@ -1,0 +1,161 @@
+"""The served form (tgmm_serve.h) on the GPU: every frame's result in the mix of lineages
+and batches is bit-identical to the same lineage run alone through tgmm_em_run_device +
+tgmm_update_priors; admission against a small HBM budget; answers for frames that can
+never run; a two-frame lineage against the FP64 oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import _fixtures as F
+from tgmm_b200 import _lib as L
+from tgmm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [synth.VolumeSpec(dims=(64, 64, 32), n_nuclei=12, axis_min=3.0, axis_max=5.0),
+         synth.VolumeSpec(dims=(96, 96, 48), n_nuclei=30, axis_min=3.0, axis_max=6.0),
+         synth.VolumeSpec(dims=(128, 128, 48), n_nuclei=60, axis_min=3.0, axis_max=6.0),
+         synth.VolumeSpec(dims=(80, 64, 40), n_nuclei=20, axis_min=3.0, axis_max=5.0)]
+N_FRAMES = 4
+
+
+def lineages():
+    return [synth.time_series(spec, seed=100 + i, n_frames=N_FRAMES, divide_frac=0.05) for i, spec in enumerate(SPECS)]
+
+
+def params(tol=1e-6):
+    return F.params(iters=20, tol=tol)
+
+
+def run_alone(frames, prm):
+    """The lineage frame after frame through the plain device API."""
+    import torch
+    from tgmm_b200 import engine as E
+    K = frames[0].n_gauss
+    plan = E.Plan(max(f.n_vox for f in frames), max(f.n_sv for f in frames), K)
+    gm = E.gauss_to_device(frames[0].gauss)
+    out = []
+    for f in frames:
+        df = E.to_device(f, n_gauss=K)
+        rnk = torch.empty(5 * f.n_sv, dtype=torch.float32, device="cuda")
+        ind = torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda")
+        st = plan.run_device(df, gm, rnk, ind, prm, stats=True)
+        out.append(dict(rnk=rnk.cpu().numpy(), ind=ind.cpu().numpy(), gauss=E.gauss_from_device(gm), stats=st))
+        E.update_priors(gm, K, 0.01, 1.0, 0.8, -1.0, True)
+    torch.cuda.synchronize()
+    plan.close()
+    return out
+
+
+def same_records(a, b):
+    for name in L.GAUSS_DTYPE.names:
+        np.testing.assert_array_equal(a[name], b[name], err_msg=name)
+
+
+def test_served_mix_is_bit_identical_to_alone(cuda_ok):
+    from tgmm_b200.serve import Server
+    prm = params()
+    series = lineages()
+    alone = [run_alone(fr, prm) for fr in series]
+    with Server(params=prm, lanes=2, max_batch_frames=8) as srv:
+        ids = [srv.open_lineage(fr[0].gauss) for fr in series]
+        tag = 0
+        for t in range(N_FRAMES):  # interleaved arrivals of all lineages
+            for li, fr in enumerate(series):
+                srv.submit(ids[li], fr[t], tag=li * 100 + t)
+                tag += 1
+        res = {r.tag: r for r in srv.drain()}
+        st = srv.stats()
+    assert len(res) == len(series) * N_FRAMES
+    assert st["batches"] < len(series) * N_FRAMES  # frames of different lineages shared batches
+    for li in range(len(series)):
+        for t in range(N_FRAMES):
+            r = res[li * 100 + t]
+            assert r.status == L.TGMM_OK
+            a = alone[li][t]
+            np.testing.assert_array_equal(r.ind, a["ind"])
+            np.testing.assert_array_equal(r.rnk, a["rnk"])
+            same_records(r.gauss, a["gauss"])
+            assert r.stats["iterations"] == a["stats"]["iterations"]
+            assert r.stats["ll"] == a["stats"]["ll"]
+
+
+def test_admission_against_a_small_budget(cuda_ok):
+    from tgmm_b200.serve import Server
+    prm = params()
+    series = lineages()[:3]
+    alone = [run_alone(fr, prm) for fr in series]
+    lineage_bytes = sum(((fr[0].n_gauss * 288 + 255) // 256) * 256 for fr in series)
+    biggest = max(16 * f.n_vox + 60 * f.n_sv + 2048 for fr in series for f in fr)
+    budget = lineage_bytes + int(1.5 * biggest)  # room for about one frame at a time
+    with Server(params=prm, lanes=2, hbm_budget=budget) as srv:
+        ids = [srv.open_lineage(fr[0].gauss) for fr in series]
+        for t in range(N_FRAMES):
+            for li, fr in enumerate(series):
+                srv.submit(ids[li], fr[t], tag=li * 100 + t)
+        res = {r.tag: r for r in srv.drain()}
+        st = srv.stats()
+    assert st["hbm_peak"] <= st["hbm_budget"]
+    for li in range(len(series)):
+        for t in range(N_FRAMES):
+            r = res[li * 100 + t]
+            assert r.status == L.TGMM_OK
+            np.testing.assert_array_equal(r.rnk, alone[li][t]["rnk"])
+            same_records(r.gauss, alone[li][t]["gauss"])
+
+
+def test_frames_that_can_never_run_are_answered(cuda_ok):
+    from tgmm_b200.serve import Server
+    fr = lineages()[0]
+    K = fr[0].n_gauss
+    small = ((K * 288 + 255) // 256) * 256 + 4096
+    with Server(params=params(), lanes=1, hbm_budget=small, max_batch_sv=50) as srv:
+        lid = srv.open_lineage(fr[0].gauss)
+        srv.submit(lid, fr[0], tag=1)            # needs more than the budget holds
+        srv.submit(lid + 7, fr[0], tag=2)        # unknown lineage
+        res = {r.tag: r for r in srv.drain()}
+    assert res[1].status == L.TGMM_ERR_ADMISSION
+    assert res[2].status == L.TGMM_ERR_INVALID_ARG
+
+
+def test_two_frame_lineage_against_the_oracle(cuda_ok):
+    from oracle import oracle as O
+    from tgmm_b200.serve import Server
+    fr = lineages()[1][:2]
+    prm = params(tol=-1.0)
+    with Server(params=prm, lanes=1) as srv:
+        lid = srv.open_lineage(fr[0].gauss)
+        for t, f in enumerate(fr):
+            srv.submit(lid, f, tag=t)
+        res = {r.tag: r for r in srv.drain()}
+    g = fr[0].gauss.copy()
+    for t, f in enumerate(fr):
+        o = O.em_run(f.query, f.img, f.centroids, f.label_ptr, g, O.params(max_iter=20, tol=-1.0))
+        r = res[t]
+        np.testing.assert_array_equal(r.ind, o["ind"])
+        assert np.max(np.abs(r.rnk - o["rnk"])) <= 1e-5
+        alive = o["gauss"]["m_o"][:, 0] > -1e31
+        assert np.max(np.abs(r.gauss["m_k"][alive] - o["gauss"]["m_k"][alive])) <= 1e-3
+        ws = np.max(np.abs(o["gauss"]["W_k"][alive]), axis=1, keepdims=True)
+        assert np.max(np.abs(r.gauss["W_k"][alive] - o["gauss"]["W_k"][alive]) / ws) <= 1e-4
+        g = o["gauss"].copy()
+        atot = float(g["alpha_k"].sum())
+        O.lib().or_update_priors(g.ctypes.data, g.shape[0], 0.01, 1.0, 0.8, atot)
+
+
+def test_read_lineage_returns_the_next_prior(cuda_ok):
+    import torch
+    from tgmm_b200 import engine as E
+    from tgmm_b200.serve import Server
+    fr = lineages()[0][:1]
+    prm = params()
+    with Server(params=prm, lanes=1) as srv:
+        lid = srv.open_lineage(fr[0].gauss)
+        srv.submit(lid, fr[0], tag=0)
+        post = srv.drain()[0].gauss
+        prior = srv.read_lineage(lid)
+    gm = E.gauss_to_device(post)
+    E.update_priors(gm, post.shape[0], 0.01, 1.0, 0.8, -1.0, True)
+    torch.cuda.synchronize()
+    same_records(prior, E.gauss_from_device(gm))

@@ -104,7 +104,39 @@ class TgmmSynthConfig(C.Structure):
     ]
 
 
-# every function declared in include/tgmm_gmem.h: name -> (restype, argtypes)
+class TgmmServerDesc(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("hbm_budget", C.c_int64), ("lanes", C.c_int32), ("max_batch_frames", C.c_int32),
+        ("max_batch_vox", C.c_int64), ("max_batch_sv", C.c_int32), ("max_batch_gauss", C.c_int32),
+        ("params", TgmmEmParams), ("beta_pct", C.c_double), ("nu_pct", C.c_double), ("alpha_pct", C.c_double),
+    ]
+
+
+class TgmmServeRequest(C.Structure):
+    _fields_ = [
+        ("lineage", C.c_int32), ("tag", C.c_uint64), ("query", C.c_void_p), ("img", C.c_void_p),
+        ("centroids", C.c_void_p), ("label_ptr", C.c_void_p), ("n_vox", C.c_int64), ("n_sv", C.c_int32),
+        ("rnk_out", C.c_void_p), ("ind_out", C.c_void_p), ("gm_out", C.c_void_p),
+    ]
+
+
+class TgmmServeResult(C.Structure):
+    _fields_ = [
+        ("tag", C.c_uint64), ("lineage", C.c_int32), ("status", C.c_int32), ("stats", TgmmEmStats),
+        ("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double), ("batch_id", C.c_int32),
+        ("batch_frames", C.c_int32),
+    ]
+
+
+class TgmmServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("completed", C.c_int64), ("rejected", C.c_int64), ("batches", C.c_int64),
+        ("frames_in_batches", C.c_int64), ("hbm_budget", C.c_int64), ("hbm_in_use", C.c_int64),
+        ("hbm_peak", C.c_int64), ("queued", C.c_int32), ("in_flight", C.c_int32),
+    ]
+
+
+# every function declared in include/tgmm_gmem.h and include/tgmm_serve.h: name -> (restype, argtypes)
 _VP = C.c_void_p
 GMEM_FUNCS = {
     "tgmm_default_params": (None, [C.POINTER(TgmmEmParams)]),
@@ -126,6 +158,16 @@ GMEM_FUNCS = {
     "tgmm_assign_supervoxels": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_int32]),
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
+    "tgmm_server_default_desc": (None, [C.POINTER(TgmmServerDesc)]),
+    "tgmm_server_create": (C.c_int, [C.POINTER(TgmmServerDesc), C.POINTER(_VP)]),
+    "tgmm_server_destroy": (C.c_int, [_VP]),
+    "tgmm_server_open_lineage": (C.c_int, [_VP, _VP, C.c_int32, C.POINTER(C.c_int32)]),
+    "tgmm_server_close_lineage": (C.c_int, [_VP, C.c_int32]),
+    "tgmm_server_read_lineage": (C.c_int, [_VP, C.c_int32, _VP]),
+    "tgmm_server_submit": (C.c_int, [_VP, C.POINTER(TgmmServeRequest)]),
+    "tgmm_server_poll": (C.c_int, [_VP, C.POINTER(TgmmServeResult), C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "tgmm_server_stats": (C.c_int, [_VP, C.POINTER(TgmmServerStats)]),
+    "tgmm_server_selftest": (C.c_int, []),
     "tgmm_last_error": (C.c_char_p, []),
     "tgmm_version": (C.c_char_p, []),
 }

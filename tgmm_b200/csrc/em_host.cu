@@ -400,6 +400,46 @@ int collect_stats(TgmmPlan* P, int32_t n, TgmmEmStats* stats, cudaStream_t st, i
   return TGMM_OK;
 }
 
+}  // namespace
+
+namespace tgmm {
+
+size_t frame_state_bytes() { return sizeof(FrameState); }
+
+int plan_enqueue_state(TgmmPlan* P, int32_t n, void* dst, cudaStream_t st) {
+  if (!P || !dst || n < 1 || n > P->desc.max_frames) return fail(TGMM_ERR_INVALID_ARG, "plan_enqueue_state");
+  TG_CUDA(cudaMemcpyAsync(dst, P->dev.state, sizeof(FrameState) * n, cudaMemcpyDeviceToHost, st), "read state");
+  return TGMM_OK;
+}
+
+int frame_state_to_stats(const void* state, TgmmEmStats* o) {
+  const FrameState& S = *static_cast<const FrameState*>(state);
+  if (o) {
+    o->iterations = S.iter - 1;
+    o->converged = S.converged;
+    o->ll = S.ll;
+    o->ll_true = S.ll_true;
+    o->ll_as_reference = S.ll_ref;
+    o->total_alpha = S.total_alpha;
+    o->n_dead = S.n_dead;
+    o->device_flags = S.flags;
+  }
+  int rc = TGMM_OK;
+  if (S.flags & F_BAD_CSR)
+    rc = TGMM_ERR_BAD_CSR;
+  else if (S.flags & F_FEW_GAUSS)
+    rc = TGMM_ERR_BAD_SIZE;
+  else if (S.flags & F_STAGE_TIMEOUT)
+    rc = TGMM_ERR_DEVICE_FLAG;
+  else if (S.flags & F_NAN_INPUT)
+    rc = TGMM_ERR_NAN_INPUT;
+  return rc;
+}
+
+}  // namespace tgmm
+
+namespace {
+
 int flags_to_status(int flags) {
   if (flags & F_BAD_CSR) return fail(TGMM_ERR_BAD_CSR, "labelListPtr is not a valid CSR over the voxels");
   if (flags & F_FEW_GAUSS) return fail(TGMM_ERR_BAD_SIZE, "a frame has fewer than 5 Gaussians");

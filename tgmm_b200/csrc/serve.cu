@@ -1,0 +1,617 @@
+// serve.cu -- the served form of the EM (tgmm_serve.h): lineages resident on the device,
+// a worker thread that admits submitted frames against an HBM budget, packs ready frames
+// of different lineages into batches and runs each batch through tgmm_em_run_batch on one
+// of several lanes (stream + plan), then turns each lineage's posterior into the prior of
+// its next frame on the device.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/tgmm_serve.h"
+#include "em_plan.h"
+
+namespace {
+
+constexpr int64_t kGranule = 256;
+int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+// First-fit allocator over byte offsets of one device allocation; neighbouring free
+// ranges are merged on release.
+class Arena {
+ public:
+  explicit Arena(int64_t capacity) : cap_(capacity) {
+    if (cap_ > 0) free_[0] = cap_;
+  }
+  int64_t alloc(int64_t n) {
+    n = round_up(std::max<int64_t>(n, 1), kGranule);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      const int64_t off = it->first, rest = it->second - n;
+      free_.erase(it);
+      if (rest) free_[off + n] = rest;
+      used_ += n;
+      peak_ = std::max(peak_, used_);
+      return off;
+    }
+    return -1;
+  }
+  void release(int64_t off, int64_t n) {
+    n = round_up(std::max<int64_t>(n, 1), kGranule);
+    used_ -= n;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  int64_t capacity() const { return cap_; }
+  int64_t used() const { return used_; }
+  int64_t peak() const { return peak_; }
+  size_t fragments() const { return free_.size(); }
+
+ private:
+  int64_t cap_, used_ = 0, peak_ = 0;
+  std::map<int64_t, int64_t> free_;
+};
+
+// Device bytes of one frame: inputs and outputs, each 256-byte aligned.
+struct FrameLayout {
+  int64_t query, img, cent, lptr, rnk, ind, total;
+  FrameLayout(int64_t n_vox, int32_t n_sv) {
+    int64_t o = 0;
+    auto take = [&](int64_t b) {
+      const int64_t at = o;
+      o += round_up(std::max<int64_t>(b, 1), kGranule);
+      return at;
+    };
+    query = take(12 * n_vox);
+    img = take(4 * n_vox);
+    cent = take(12 * (int64_t)n_sv);
+    lptr = take(8 * ((int64_t)n_sv + 1));
+    rnk = take(4 * (int64_t)TGMM_J * n_sv);
+    ind = take(4 * (int64_t)TGMM_J * n_sv);
+    total = o;
+  }
+};
+
+struct Request {
+  TgmmServeRequest r;
+  uint64_t seq = 0;
+  double t_submit = 0.0, t_start = 0.0;
+  int64_t off = -1, bytes = 0;
+};
+
+struct Lineage {
+  int32_t n_gauss = 0;
+  int64_t off = -1, bytes = 0;
+  TgmmGaussian* gm_dev = nullptr;
+  std::deque<Request*> queue;  // the front one is in flight when in_flight
+  bool in_flight = false;
+};
+
+struct Lane {
+  TgmmPlan* plan = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool busy = false;
+  int launch_rc = TGMM_OK;
+  int32_t batch_id = 0;
+  std::vector<Request*> reqs;
+  std::vector<int32_t> lineage_ids;
+  std::vector<TgmmGaussian*> gm_dev;  // the batch's lineages, captured when it is formed
+  std::vector<int32_t> n_gauss;
+  // pinned staging of the batch outputs
+  float* h_rnk = nullptr;
+  int32_t* h_ind = nullptr;
+  TgmmGaussian* h_gm = nullptr;
+  unsigned char* h_state = nullptr;
+  std::vector<int64_t> sv_off, g_off;
+};
+
+}  // namespace
+
+struct TgmmServer {
+  TgmmServerDesc desc{};
+  char* dev = nullptr;
+  Arena* arena = nullptr;
+  std::vector<Lane> lanes;
+  std::map<int32_t, Lineage> lineages;
+  int32_t next_lineage = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> inbox;
+  std::deque<TgmmServeResult> results;
+  std::thread worker;
+  bool stop = false;
+  uint64_t seq = 0;
+  int64_t submitted = 0, completed = 0, rejected = 0, batches = 0, frames_in_batches = 0;
+  int32_t queued = 0, in_flight = 0;  // in the inbox; in lineage queues (waiting or running)
+  int64_t lineage_bytes = 0;          // arena bytes held by resident lineages
+  std::chrono::steady_clock::time_point t0;
+
+  double now_ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  void run();
+  void finish(Request* q, int status, const TgmmEmStats* st, int32_t batch_id, int32_t batch_frames);
+  bool form_batch(Lane& L, std::vector<Request*>& batch);
+  void launch(Lane& L);
+  void complete(Lane& L);
+};
+
+namespace {
+
+int fail(int code, const char* what, cudaError_t e = cudaSuccess) { return tgmm::report_error(code, what, e); }
+
+#define SV_CUDA(call, what)                                     \
+  do {                                                          \
+    cudaError_t e_ = (call);                                    \
+    if (e_ != cudaSuccess) return fail(TGMM_ERR_CUDA, what, e_); \
+  } while (0)
+
+}  // namespace
+
+// Result of one request (lock held).  The request leaves its lineage's queue.
+void TgmmServer::finish(Request* q, int status, const TgmmEmStats* st, int32_t batch_id, int32_t batch_frames) {
+  TgmmServeResult res;
+  memset(&res, 0, sizeof(res));
+  res.tag = q->r.tag;
+  res.lineage = q->r.lineage;
+  res.status = status;
+  if (st) res.stats = *st;
+  res.submit_ms = q->t_submit;
+  res.start_ms = q->t_start;
+  res.done_ms = now_ms();
+  res.batch_id = batch_id;
+  res.batch_frames = batch_frames;
+  results.push_back(res);
+  completed++;
+  if (status == TGMM_ERR_ADMISSION || status == TGMM_ERR_BAD_SIZE || status == TGMM_ERR_INVALID_ARG) rejected++;
+  delete q;
+  cv_done.notify_all();
+}
+
+// Frames for lane L: the oldest ready frame of each lineage with nothing in flight, in
+// submission order, while the batch capacity and the HBM budget allow (lock held).
+bool TgmmServer::form_batch(Lane& L, std::vector<Request*>& batch) {
+  std::vector<std::pair<uint64_t, int32_t>> ready;
+  for (auto& kv : lineages)
+    if (!kv.second.in_flight && !kv.second.queue.empty()) ready.push_back({kv.second.queue.front()->seq, kv.first});
+  std::sort(ready.begin(), ready.end());
+  int64_t vox = 0, sv = 0, gauss = 0;
+  for (auto& rd : ready) {
+    if ((int32_t)batch.size() >= desc.max_batch_frames) break;
+    Lineage& G = lineages[rd.second];
+    Request* q = G.queue.front();
+    if (vox + q->r.n_vox > desc.max_batch_vox || sv + q->r.n_sv > desc.max_batch_sv ||
+        gauss + G.n_gauss > desc.max_batch_gauss)
+      continue;
+    const FrameLayout lay(q->r.n_vox, q->r.n_sv);
+    const int64_t off = arena->alloc(lay.total);
+    if (off < 0) continue;  // waits for memory: admitted once enough is released
+    q->off = off;
+    q->bytes = lay.total;
+    G.in_flight = true;
+    batch.push_back(q);
+    L.lineage_ids.push_back(rd.second);
+    L.gm_dev.push_back(G.gm_dev);
+    L.n_gauss.push_back(G.n_gauss);
+    vox += q->r.n_vox;
+    sv += q->r.n_sv;
+    gauss += G.n_gauss;
+  }
+  return !batch.empty();
+}
+
+// Enqueue the batch on the lane (lock not held; only the lane and its requests are used).
+void TgmmServer::launch(Lane& L) {
+  const int n = (int)L.reqs.size();
+  std::vector<TgmmFrame> fr(n);
+  std::vector<TgmmGaussian*> gm(n);
+  std::vector<float*> rnk(n);
+  std::vector<int32_t*> ind(n);
+  L.sv_off.assign(n, 0);
+  L.g_off.assign(n, 0);
+  int rc = TGMM_OK;
+  int64_t so = 0, go = 0;
+  for (int i = 0; i < n && rc == TGMM_OK; i++) {
+    Request* q = L.reqs[i];
+    const FrameLayout lay(q->r.n_vox, q->r.n_sv);
+    char* base = dev + q->off;
+    const int64_t N = q->r.n_vox, S = q->r.n_sv;
+    cudaError_t e = cudaMemcpyAsync(base + lay.query, q->r.query, 12 * N, cudaMemcpyHostToDevice, L.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.img, q->r.img, 4 * N, cudaMemcpyHostToDevice, L.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.cent, q->r.centroids, 12 * S, cudaMemcpyHostToDevice, L.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, L.st);
+    if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: upload", e);
+    fr[i].query = (const float*)(base + lay.query);
+    fr[i].img = (const float*)(base + lay.img);
+    fr[i].centroids = (const float*)(base + lay.cent);
+    fr[i].label_ptr = (const int64_t*)(base + lay.lptr);
+    fr[i].n_vox = N;
+    fr[i].n_sv = (int32_t)S;
+    fr[i].n_gauss = L.n_gauss[i];
+    gm[i] = L.gm_dev[i];
+    rnk[i] = (float*)(base + lay.rnk);
+    ind[i] = (int32_t*)(base + lay.ind);
+    L.sv_off[i] = so;
+    L.g_off[i] = go;
+    so += TGMM_J * S;
+    go += L.n_gauss[i];
+  }
+  if (rc == TGMM_OK)
+    rc = tgmm_em_run_batch(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, nullptr, L.st);
+  if (rc == TGMM_OK) rc = tgmm::plan_enqueue_state(L.plan, n, L.h_state, L.st);
+  for (int i = 0; i < n && rc == TGMM_OK; i++) {
+    Request* q = L.reqs[i];
+    const int64_t S = q->r.n_sv;
+    const int32_t K = fr[i].n_gauss;
+    cudaError_t e = cudaSuccess;
+    if (q->r.rnk_out)
+      e = cudaMemcpyAsync(L.h_rnk + L.sv_off[i], rnk[i], 4 * TGMM_J * S, cudaMemcpyDeviceToHost, L.st);
+    if (e == cudaSuccess && q->r.ind_out)
+      e = cudaMemcpyAsync(L.h_ind + L.sv_off[i], ind[i], 4 * TGMM_J * S, cudaMemcpyDeviceToHost, L.st);
+    if (e == cudaSuccess && q->r.gm_out)
+      e = cudaMemcpyAsync(L.h_gm + L.g_off[i], gm[i], sizeof(TgmmGaussian) * K, cudaMemcpyDeviceToHost, L.st);
+    if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: download", e);
+    // posterior -> prior of the lineage's next frame
+    if (rc == TGMM_OK)
+      rc = tgmm_update_priors(gm[i], K, desc.beta_pct, desc.nu_pct, desc.alpha_pct, -1.0, 1, L.st);
+  }
+  if (rc == TGMM_OK) {
+    cudaError_t e = cudaEventRecord(L.ev, L.st);
+    if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: record", e);
+  }
+  L.launch_rc = rc;
+}
+
+// The lane's batch has finished on the device (lock held).
+void TgmmServer::complete(Lane& L) {
+  const int n = (int)L.reqs.size();
+  const size_t sb = tgmm::frame_state_bytes();
+  for (int i = 0; i < n; i++) {
+    Request* q = L.reqs[i];
+    Lineage& G = lineages.at(L.lineage_ids[i]);
+    TgmmEmStats st;
+    memset(&st, 0, sizeof(st));
+    int status = L.launch_rc;
+    if (status == TGMM_OK) {
+      status = tgmm::frame_state_to_stats(L.h_state + sb * i, &st);
+      const int64_t S = q->r.n_sv;
+      if (q->r.rnk_out) memcpy(q->r.rnk_out, L.h_rnk + L.sv_off[i], 4 * TGMM_J * S);
+      if (q->r.ind_out) memcpy(q->r.ind_out, L.h_ind + L.sv_off[i], 4 * TGMM_J * S);
+      if (q->r.gm_out) memcpy(q->r.gm_out, L.h_gm + L.g_off[i], sizeof(TgmmGaussian) * G.n_gauss);
+    }
+    arena->release(q->off, q->bytes);
+    G.in_flight = false;
+    G.queue.pop_front();
+    in_flight--;
+    finish(q, status, status == TGMM_OK || status == TGMM_ERR_NAN_INPUT ? &st : nullptr, L.batch_id, n);
+  }
+  L.reqs.clear();
+  L.lineage_ids.clear();
+  L.gm_dev.clear();
+  L.n_gauss.clear();
+  L.busy = false;
+}
+
+void TgmmServer::run() {
+  cudaSetDevice(desc.device);
+  std::unique_lock<std::mutex> lk(mu);
+  for (;;) {
+    // intake: frames join their lineage's queue; frames that can never run are answered
+    while (!inbox.empty()) {
+      Request* q = inbox.front();
+      inbox.pop_front();
+      queued--;
+      auto it = lineages.find(q->r.lineage);
+      if (it == lineages.end()) {
+        finish(q, TGMM_ERR_INVALID_ARG, nullptr, -1, 0);
+        continue;
+      }
+      const FrameLayout lay(q->r.n_vox, q->r.n_sv);
+      if (q->r.n_vox > desc.max_batch_vox || q->r.n_sv > desc.max_batch_sv ||
+          it->second.n_gauss > desc.max_batch_gauss) {
+        finish(q, TGMM_ERR_BAD_SIZE, nullptr, -1, 0);
+        continue;
+      }
+      if (lay.total > arena->capacity() - lineage_bytes) {  // could never be admitted
+        finish(q, TGMM_ERR_ADMISSION, nullptr, -1, 0);
+        continue;
+      }
+      it->second.queue.push_back(q);
+      in_flight++;
+    }
+    bool progressed = false;
+    for (Lane& L : lanes) {
+      if (!L.busy) continue;
+      const cudaError_t e = L.launch_rc == TGMM_OK ? cudaEventQuery(L.ev) : cudaSuccess;
+      if (e == cudaErrorNotReady) continue;
+      if (e != cudaSuccess && L.launch_rc == TGMM_OK) L.launch_rc = fail(TGMM_ERR_CUDA, "serve: batch", e);
+      complete(L);
+      progressed = true;
+    }
+    for (Lane& L : lanes) {
+      if (L.busy) continue;
+      std::vector<Request*> batch;
+      if (!form_batch(L, batch)) break;
+      L.reqs = batch;
+      L.busy = true;
+      L.batch_id = (int32_t)batches++;
+      frames_in_batches += (int64_t)batch.size();
+      const double t = now_ms();
+      for (Request* q : batch) q->t_start = t;
+      lk.unlock();
+      launch(L);
+      lk.lock();
+      if (L.launch_rc != TGMM_OK) {  // nothing to wait for: answer the batch now
+        cudaStreamSynchronize(L.st);
+        complete(L);
+      }
+      progressed = true;
+    }
+    bool any_busy = false, any_queued = false;
+    for (Lane& L : lanes) any_busy |= L.busy;
+    for (auto& kv : lineages) any_queued |= !kv.second.queue.empty();
+    if (stop && !any_busy && !any_queued && inbox.empty()) break;
+    if (progressed) continue;
+    if (any_busy)
+      cv_work.wait_for(lk, std::chrono::microseconds(20));
+    else
+      cv_work.wait(lk, [&] { return !inbox.empty() || stop; });
+  }
+}
+
+extern "C" {
+
+void tgmm_server_default_desc(TgmmServerDesc* d) {
+  if (!d) return;
+  memset(d, 0, sizeof(*d));
+  d->device = 0;
+  d->hbm_budget = 0;
+  d->lanes = 2;
+  d->max_batch_frames = 64;
+  d->max_batch_vox = (int64_t)1 << 25;
+  d->max_batch_sv = 1 << 17;
+  d->max_batch_gauss = 1 << 17;
+  tgmm_default_params(&d->params);
+  d->beta_pct = 0.01;
+  d->nu_pct = 1.0;
+  d->alpha_pct = 0.8;
+}
+
+int tgmm_server_create(const TgmmServerDesc* d, TgmmServer** out) {
+  if (!d || !out) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_create: null argument");
+  *out = nullptr;
+  if (d->lanes < 1 || d->max_batch_frames < 1 || d->max_batch_vox < 1 || d->max_batch_sv < 1 ||
+      d->max_batch_gauss < TGMM_J || d->hbm_budget < 0)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_create: capacities must be positive");
+  SV_CUDA(cudaSetDevice(d->device), "cudaSetDevice");
+  TgmmServer* S = new TgmmServer();
+  S->desc = *d;
+  S->t0 = std::chrono::steady_clock::now();
+  auto bail = [&](int rc) {
+    tgmm_server_destroy(S);
+    return rc;
+  };
+  TgmmPlanDesc pd;
+  pd.max_vox = d->max_batch_vox;
+  pd.max_sv = d->max_batch_sv;
+  pd.max_gauss = d->max_batch_gauss;
+  pd.max_frames = d->max_batch_frames;
+  pd.device = d->device;
+  S->lanes.resize(d->lanes);
+  const size_t sb = tgmm::frame_state_bytes();
+  for (Lane& L : S->lanes) {
+    int rc = tgmm_plan_create(&pd, &L.plan);
+    if (rc) return bail(rc);
+    cudaError_t e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h_rnk, 4 * (size_t)TGMM_J * d->max_batch_sv);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h_ind, 4 * (size_t)TGMM_J * d->max_batch_sv);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h_gm, sizeof(TgmmGaussian) * (size_t)d->max_batch_gauss);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h_state, sb * (size_t)d->max_batch_frames);
+    if (e != cudaSuccess) return bail(fail(TGMM_ERR_CUDA, "tgmm_server_create: lane", e));
+  }
+  int64_t budget = d->hbm_budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    if (e != cudaSuccess) return bail(fail(TGMM_ERR_CUDA, "tgmm_server_create: cudaMemGetInfo", e));
+    budget = (int64_t)(0.8 * (double)fr);
+  }
+  budget = round_up(budget, kGranule);
+  cudaError_t e = cudaMalloc(&S->dev, budget);
+  if (e != cudaSuccess) return bail(fail(TGMM_ERR_OOM, "tgmm_server_create: HBM budget", e));
+  S->desc.hbm_budget = budget;
+  S->arena = new Arena(budget);
+  S->worker = std::thread([S] { S->run(); });
+  *out = S;
+  return TGMM_OK;
+}
+
+int tgmm_server_destroy(TgmmServer* S) {
+  if (!S) return TGMM_OK;
+  if (S->worker.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->stop = true;
+    }
+    S->cv_work.notify_all();
+    S->worker.join();
+  }
+  cudaSetDevice(S->desc.device);
+  for (Lane& L : S->lanes) {
+    if (L.st) cudaStreamSynchronize(L.st);
+    if (L.plan) tgmm_plan_destroy(L.plan);
+    if (L.ev) cudaEventDestroy(L.ev);
+    if (L.st) cudaStreamDestroy(L.st);
+    if (L.h_rnk) cudaFreeHost(L.h_rnk);
+    if (L.h_ind) cudaFreeHost(L.h_ind);
+    if (L.h_gm) cudaFreeHost(L.h_gm);
+    if (L.h_state) cudaFreeHost(L.h_state);
+  }
+  for (Request* q : S->inbox) delete q;
+  for (auto& kv : S->lineages)
+    for (Request* q : kv.second.queue) delete q;
+  if (S->dev) cudaFree(S->dev);
+  delete S->arena;
+  delete S;
+  return TGMM_OK;
+}
+
+int tgmm_server_open_lineage(TgmmServer* S, const TgmmGaussian* gm, int32_t n_gauss, int32_t* id) {
+  if (!S || !gm || !id) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_open_lineage: null argument");
+  if (n_gauss < TGMM_J) return fail(TGMM_ERR_BAD_SIZE, "tgmm_server_open_lineage: a lineage needs 5 Gaussians");
+  if (n_gauss > S->desc.max_batch_gauss) return fail(TGMM_ERR_BAD_SIZE, "tgmm_server_open_lineage: beyond batch capacity");
+  std::lock_guard<std::mutex> lk(S->mu);
+  const int64_t bytes = (int64_t)sizeof(TgmmGaussian) * n_gauss;
+  const int64_t off = S->arena->alloc(bytes);
+  if (off < 0) return fail(TGMM_ERR_ADMISSION, "tgmm_server_open_lineage: HBM budget exhausted");
+  SV_CUDA(cudaSetDevice(S->desc.device), "cudaSetDevice");
+  cudaError_t e = cudaMemcpy(S->dev + off, gm, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    S->arena->release(off, bytes);
+    return fail(TGMM_ERR_CUDA, "tgmm_server_open_lineage: upload", e);
+  }
+  Lineage G;
+  G.n_gauss = n_gauss;
+  G.off = off;
+  G.bytes = bytes;
+  G.gm_dev = (TgmmGaussian*)(S->dev + off);
+  S->lineage_bytes += round_up(bytes, kGranule);
+  *id = S->next_lineage++;
+  S->lineages.emplace(*id, std::move(G));
+  return TGMM_OK;
+}
+
+int tgmm_server_close_lineage(TgmmServer* S, int32_t id) {
+  if (!S) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_close_lineage: null server");
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->lineages.find(id);
+  if (it == S->lineages.end()) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_close_lineage: unknown lineage");
+  for (Request* q : S->inbox)
+    if (q->r.lineage == id) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_close_lineage: frames pending");
+  if (!it->second.queue.empty()) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_close_lineage: frames pending");
+  S->arena->release(it->second.off, it->second.bytes);
+  S->lineage_bytes -= round_up(it->second.bytes, kGranule);
+  S->lineages.erase(it);
+  return TGMM_OK;
+}
+
+int tgmm_server_read_lineage(TgmmServer* S, int32_t id, TgmmGaussian* gm) {
+  if (!S || !gm) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_read_lineage: null argument");
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto pending = [&] {
+    auto it = S->lineages.find(id);
+    if (it == S->lineages.end()) return false;
+    if (!it->second.queue.empty()) return true;
+    for (Request* q : S->inbox)
+      if (q->r.lineage == id) return true;
+    return false;
+  };
+  S->cv_done.wait(lk, [&] { return !pending(); });
+  auto it = S->lineages.find(id);
+  if (it == S->lineages.end()) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_read_lineage: unknown lineage");
+  SV_CUDA(cudaSetDevice(S->desc.device), "cudaSetDevice");
+  SV_CUDA(cudaMemcpy(gm, it->second.gm_dev, sizeof(TgmmGaussian) * it->second.n_gauss, cudaMemcpyDeviceToHost),
+          "tgmm_server_read_lineage: download");
+  return TGMM_OK;
+}
+
+int tgmm_server_submit(TgmmServer* S, const TgmmServeRequest* r) {
+  if (!S || !r) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: null argument");
+  if (!r->query || !r->img || !r->centroids || !r->label_ptr || r->n_vox < 0 || r->n_sv < 1)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad frame");
+  Request* q = new Request();
+  q->r = *r;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) {
+      delete q;
+      return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: server stopping");
+    }
+    q->seq = S->seq++;
+    q->t_submit = S->now_ms();
+    S->inbox.push_back(q);
+    S->queued++;
+    S->submitted++;
+  }
+  S->cv_work.notify_one();
+  return TGMM_OK;
+}
+
+int tgmm_server_poll(TgmmServer* S, TgmmServeResult* out, int32_t max, int32_t wait_ms, int32_t* n_out) {
+  if (!S || !out || max < 1 || !n_out) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_poll: bad argument");
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto ready = [&] { return !S->results.empty() || (S->queued == 0 && S->in_flight == 0); };
+  if (wait_ms < 0)
+    S->cv_done.wait(lk, ready);
+  else if (wait_ms > 0)
+    S->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), ready);
+  int32_t n = 0;
+  while (n < max && !S->results.empty()) {
+    out[n++] = S->results.front();
+    S->results.pop_front();
+  }
+  *n_out = n;
+  return TGMM_OK;
+}
+
+int tgmm_server_stats(TgmmServer* S, TgmmServerStats* o) {
+  if (!S || !o) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_stats: null argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  o->submitted = S->submitted;
+  o->completed = S->completed;
+  o->rejected = S->rejected;
+  o->batches = S->batches;
+  o->frames_in_batches = S->frames_in_batches;
+  o->hbm_budget = S->arena->capacity();
+  o->hbm_in_use = S->arena->used();
+  o->hbm_peak = S->arena->peak();
+  o->queued = S->queued;
+  o->in_flight = S->in_flight;
+  return TGMM_OK;
+}
+
+int tgmm_server_selftest(void) {
+  int bad = 0;
+  auto check = [&](bool c) { bad += c ? 0 : 1; };
+  Arena a(10 * kGranule);
+  const int64_t x = a.alloc(1), y = a.alloc(kGranule + 1), z = a.alloc(3 * kGranule);
+  check(x == 0 && y == kGranule && z == 3 * kGranule);
+  check(a.used() == 6 * kGranule);
+  check(a.alloc(5 * kGranule) == -1);  // 4 granules left
+  a.release(y, kGranule + 1);
+  check(a.alloc(3 * kGranule) == 6 * kGranule);  // first fit skips the 2-granule hole
+  check(a.alloc(2 * kGranule) == kGranule);      // and fills it next
+  a.release(x, 1);
+  a.release(kGranule, 2 * kGranule);
+  a.release(z, 3 * kGranule);
+  a.release(6 * kGranule, 3 * kGranule);
+  check(a.used() == 0 && a.fragments() == 1);  // fully coalesced
+  check(a.alloc(10 * kGranule) == 0);
+  check(a.peak() == 10 * kGranule);
+  const FrameLayout lay(1000, 10);
+  check(lay.total % kGranule == 0 && lay.img >= 12 * 1000 && lay.ind + 4 * 5 * 10 <= lay.total);
+  return bad;
+}
+
+}  // extern "C"

@@ -37,14 +37,16 @@ class DeviceFrame:
         return f
 
 
-def to_device(frame, device="cuda", pin=False) -> DeviceFrame:
-    """Copy a synth.Frame (host arrays) to the device."""
+def to_device(frame, device="cuda", pin=False, n_gauss: int | None = None) -> DeviceFrame:
+    """Copy a synth.Frame (host arrays) to the device.  n_gauss: the Gaussians the frame
+    runs with (default: the frame's own first-frame Gaussians)."""
     def t(a):
         x = torch.from_numpy(np.ascontiguousarray(a))
         if pin:
             x = x.pin_memory()
         return x.to(device, non_blocking=pin)
-    return DeviceFrame(t(frame.query), t(frame.img), t(frame.centroids), t(frame.label_ptr), frame.n_gauss)
+    return DeviceFrame(t(frame.query), t(frame.img), t(frame.centroids), t(frame.label_ptr),
+                       frame.n_gauss if n_gauss is None else n_gauss)
 
 
 def gauss_to_device(g: np.ndarray, device="cuda") -> torch.Tensor:
