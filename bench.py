@@ -44,7 +44,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "batch64", "series", "mixed"], default="c2",
+                    help="c2: the 1-Gvoxel frame (default, the headline); c1: 256x256x64; batch64: 64 uneven "
+                         "volumes in one batched call vs one at a time; series: one served time series of "
+                         "1024x1024x256 frames; mixed: four served time series of four sizes vs the plain form")
+    ap.add_argument("--frames", type=int, default=0, help="frames per time series (series/mixed; 0 = default sample)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2000)
@@ -335,10 +339,228 @@ def run_e2e(frame, df, plan, params, dev, args):
             "wall_frames_per_s": args.steps / wall, "path": "tgmm_em_run (C ABI) with pinned host buffers"}
 
 
+# ---------------------------------------------------------------------------
+# Batched and served forms (non-default workloads; one JSON line each)
+# ---------------------------------------------------------------------------
+def _pin(frame):
+    """The frame's host arrays, and its compact voxel codes, copied once into page-locked
+    memory (numpy views)."""
+    import torch
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    out = {k: pinned(getattr(frame, k)) for k in ("query", "img", "centroids", "label_ptr")}
+    lin, raw, dims, off, den = frame.compact()
+    out.update(lin=pinned(lin), raw=pinned(raw.view(np.int16)).view(np.uint16), dims=dims, raw_offset=off,
+               raw_denom=den)
+    return type("PinnedFrame", (), out)
+
+
+def run_batch64(args):
+    """64 independent volumes (uneven sizes): one tgmm_em_run_batch call per step (one
+    launch per EM phase for all volumes) against the same volumes one at a time through
+    tgmm_em_run_device; inputs resident on the device, 20 iterations each."""
+    import torch
+    from tgmm_b200 import engine as E
+    from tgmm_b200 import synth
+    torch.cuda.set_device(0)
+    specs = synth.batch_specs(64, seed=args.seed)
+    frames = [synth.generate(sp, seed=args.seed + i) for i, sp in enumerate(specs)]
+    prm = synth.em_params(iters=EM_ITERS, tol=-1.0)
+    dfs = [E.to_device(f) for f in frames]
+    gm0 = [E.gauss_to_device(f.gauss) for f in frames]
+    gms = [g.clone() for g in gm0]
+    rnks = [torch.empty(5 * f.n_sv, device="cuda") for f in frames]
+    inds = [torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda") for f in frames]
+    tv, ts, tg = sum(f.n_vox for f in frames), sum(f.n_sv for f in frames), sum(f.n_gauss for f in frames)
+    batch_plan = E.Plan(tv, ts, tg, max_frames=len(frames))
+    one_plan = E.Plan(max(f.n_vox for f in frames), max(f.n_sv for f in frames), max(f.n_gauss for f in frames))
+
+    def batched():
+        for g, g0 in zip(gms, gm0):
+            g.copy_(g0)
+        batch_plan.run_batch(dfs, gms, rnks, inds, prm, stats=False)
+
+    def plain():
+        for df, g, g0, r, i in zip(dfs, gms, gm0, rnks, inds):
+            g.copy_(g0)
+            one_plan.run_device(df, g, r, i, prm, stats=False)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    ms_b = timed(batched)
+    out_b = [(r.cpu().numpy(), i.cpu().numpy()) for r, i in zip(rnks, inds)]
+    ms_p = timed(plain)
+    same = all(np.array_equal(rb, r.cpu().numpy()) and np.array_equal(ib, i.cpu().numpy())
+               for (rb, ib), r, i in zip(out_b, rnks, inds))
+    n = len(frames)
+    line = {"metric": "EM frames/s, 64 uneven volumes batched", "value": n / (ms_b / 1e3), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "64 volumes, dims uniform in [128..512]x[128..512]x[64..128], one nucleus per "
+                                   "~3000 voxels clipped to [100, 5000], 20 EM iterations",
+                       "total_vox": tv, "total_sv": ts, "total_gauss": tg},
+            "plain": {"value": n / (ms_p / 1e3), "ms_per_sweep": ms_p, "path": "tgmm_em_run_device, one at a time"},
+            "batched_over_plain": ms_p / ms_b, "voxel_iters_per_s": tv * EM_ITERS / (ms_b / 1e3),
+            "rnk_ind_identical_to_alone": bool(same)}
+    print(json.dumps(line), flush=True)
+
+
+SERIES_SPECS = {
+    "series": [((1024, 1024, 256), 5000)],
+    "mixed": [((256, 256, 64), 300), ((512, 512, 128), 2000), ((1024, 1024, 256), 8000), ((2048, 1024, 512), 20000)],
+}
+
+
+def _series(args):
+    from tgmm_b200 import synth
+    nf = args.frames or (12 if args.workload == "series" else 6)
+    out = []
+    for i, (dims, n) in enumerate(SERIES_SPECS[args.workload]):
+        spec = synth.VolumeSpec(dims=dims, n_nuclei=n, axis_min=4.0, axis_max=8.0)
+        out.append(synth.time_series(spec, seed=args.seed + 17 * i, n_frames=nf, divide_frac=0.01))
+    return out
+
+
+def run_served(args):
+    """Served time series: the server (tgmm_serve.h) against the plain form, both over the
+    same pinned host frames, both returning rnk/ind and the posterior of every frame and
+    carrying each lineage's posterior into its next frame's prior on the device.
+    Closed loop (every frame submitted at once) gives throughput; Poisson arrivals at the
+    configured rate give per-frame latency."""
+    import torch
+    from tgmm_b200 import _lib as L
+    from tgmm_b200 import engine as E
+    from tgmm_b200.serve import Server
+    torch.cuda.set_device(0)
+    series = _series(args)
+    from tgmm_b200 import synth
+    prm = synth.em_params(iters=EM_ITERS, tol=1e-6)
+    pinned = [[_pin(f) for f in fr] for fr in series]
+    order = [(li, t) for t in range(len(series[0])) for li in range(len(series))]  # interleaved arrivals
+    n_frames = len(order)
+    rate = 2.0 if args.workload == "series" else 8.0
+
+    # plain form: one frame at a time
+    K = [fr[0].n_gauss for fr in series]
+    maxN = max(f.n_vox for fr in series for f in fr)
+    maxS = max(f.n_sv for fr in series for f in fr)
+    plan = E.Plan(maxN, maxS, max(K))
+    q = torch.empty(3 * maxN, device="cuda")
+    im = torch.empty(maxN, device="cuda")
+    ce = torch.empty(3 * maxS, device="cuda")
+    lp = torch.empty(maxS + 1, dtype=torch.int64, device="cuda")
+    rnk = torch.empty(5 * maxS, device="cuda")
+    ind = torch.empty(5 * maxS, dtype=torch.int32, device="cuda")
+    rnk_h = torch.empty(5 * maxS).pin_memory()
+    ind_h = torch.empty(5 * maxS, dtype=torch.int32).pin_memory()
+
+    def plain_sweep():
+        gms = [E.gauss_to_device(fr[0].gauss) for fr in series]
+        gm_h = [torch.empty(k * 288, dtype=torch.uint8).pin_memory() for k in K]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for li, t in order:
+            f = pinned[li][t]
+            N, S = f.img.shape[0], f.label_ptr.shape[0] - 1
+            q[:3 * N].copy_(torch.from_numpy(f.query), non_blocking=True)
+            im[:N].copy_(torch.from_numpy(f.img), non_blocking=True)
+            ce[:3 * S].copy_(torch.from_numpy(f.centroids), non_blocking=True)
+            lp[:S + 1].copy_(torch.from_numpy(f.label_ptr), non_blocking=True)
+            df = E.DeviceFrame(q[:3 * N], im[:N], ce[:3 * S], lp[:S + 1], K[li])
+            plan.run_device(df, gms[li], rnk, ind, prm, stats=True)
+            rnk_h[:5 * S].copy_(rnk[:5 * S], non_blocking=True)
+            ind_h[:5 * S].copy_(ind[:5 * S], non_blocking=True)
+            gm_h[li].copy_(gms[li].view(torch.uint8), non_blocking=True)
+            E.update_priors(gms[li], K[li])
+            torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    for _ in range(max(1, args.warmup)):
+        plain_sweep()
+    plain_s = min(plain_sweep() for _ in range(max(1, min(args.steps, 3))))
+
+    # served form; outputs into page-locked buffers, as the plain form's
+    srv = Server(params=prm, lanes=2, max_batch_frames=16, max_batch_vox=max(1 << 25, 2 * maxN))
+
+    def pinned_out(S, K):
+        return (torch.empty(5 * S).pin_memory().numpy(), torch.empty(5 * S, dtype=torch.int32).pin_memory().numpy(),
+                torch.empty(K * 288, dtype=torch.uint8).pin_memory().numpy().view(L.GAUSS_DTYPE))
+    outs = [[pinned_out(f.n_sv, K[li]) for f in fr] for li, fr in enumerate(series)]
+
+    def served(arrival_rate=None, seed=0, compact=True):
+        ids = [srv.open_lineage(fr[0].gauss) for fr in series]
+        rng = np.random.default_rng(seed)
+        t0 = time.perf_counter()
+        t_next = 0.0
+        for n, (li, t) in enumerate(order):
+            if arrival_rate:
+                t_next += rng.exponential(1.0 / arrival_rate)
+                while time.perf_counter() - t0 < t_next:
+                    time.sleep(0.0005)
+            srv.submit(ids[li], pinned[li][t], tag=n, compact=compact, out=outs[li][t])
+        res = srv.drain()
+        wall = time.perf_counter() - t0
+        for i in ids:
+            srv.close_lineage(i)
+        bad = [r.status for r in res if r.status != L.TGMM_OK]
+        return wall, res, bad
+
+    for _ in range(max(1, args.warmup)):
+        served()
+    closed = [served() for _ in range(max(1, min(args.steps, 3)))]
+    wall_c, res_c, bad_c = min(closed, key=lambda x: x[0])
+    h2d0 = srv.stats()["h2d_bytes"]
+    closed_f = [served(compact=False) for _ in range(max(1, min(args.steps, 3)))]
+    wall_f = min(x[0] for x in closed_f)
+    h2d_float = (srv.stats()["h2d_bytes"] - h2d0) / len(closed_f)
+    wall_o, res_o, bad_o = served(arrival_rate=rate, seed=args.seed)
+    lat = sorted(r.latency_ms for r in res_o)
+    st = srv.stats()
+    srv.close()
+    pct = lambda a, p: float(np.percentile(a, p))
+    line = {"metric": f"served EM frames/s ({args.workload} stream)", "value": n_frames / wall_c, "unit": UNIT,
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": [f"{d[0]}x{d[1]}x{d[2]}, {n} nuclei" for d, n in SERIES_SPECS[args.workload]],
+                       "frames_per_series": len(series[0]), "frames": n_frames, "em": "max 20 iterations, tol 1e-6",
+                       "n_vox": [[f.n_vox for f in fr] for fr in series], "lanes": 2},
+            "plain": {"value": n_frames / plain_s, "unit": UNIT,
+                      "path": "one frame at a time: pinned upload, tgmm_em_run_device, download, prior update"},
+            "served_over_plain": (n_frames / wall_c) / (n_frames / plain_s),
+            "served_float_frames": {"value": n_frames / wall_f, "unit": UNIT,
+                                    "over_plain": (n_frames / wall_f) / (n_frames / plain_s),
+                                    "h2d_bytes_per_frame": h2d_float / n_frames,
+                                    "path": "same server, frames uploaded as float query/img (16 B/voxel)"},
+            "h2d_bytes_per_frame": h2d0 / (max(1, args.warmup) + len(closed)) / n_frames,
+            "latency_ms": {"arrivals_per_s": rate, "p50": pct(lat, 50), "p99": pct(lat, 99), "max": lat[-1]},
+            "closed_loop_latency_ms": {"p50": pct([r.latency_ms for r in res_c], 50),
+                                       "p99": pct([r.latency_ms for r in res_c], 99)},
+            "mean_batch_frames": st["frames_in_batches"] / max(1, st["batches"]),
+            "mean_em_iterations_per_series": [float(np.mean([r.stats["iterations"] for r in res_c
+                                                             if order[r.tag][0] == li]))
+                                              for li in range(len(series))],
+            "hbm_peak_bytes": st["hbm_peak"], "errors": bad_c + bad_o}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch64":
+        run_batch64(args)
+    elif args.workload in ("series", "mixed"):
+        run_served(args)
     else:
         run_ours(args)
 

@@ -10,12 +10,13 @@
  * lineage runs with the current Gaussians as posterior-and-prior, and after it the update
  * above runs on the device (tgmm_update_priors).
  *
- * Frames of different lineages are independent.  A worker thread takes submitted frames
- * whose lineage has no frame in flight, admits them against the server's HBM budget
- * (their input and output buffers), packs as many as fit into a batch and runs the batch
- * through tgmm_em_run_batch -- one launch per EM phase for all its frames -- on one of
- * `lanes` streams, each with its own plan, so that a batch uploads and starts while
- * others run.  Results are bit-identical to running each frame alone.
+ * Frames of different lineages are independent.  A worker thread admits submitted frames
+ * against the server's HBM budget (their input and output buffers) in arrival order and
+ * uploads each on a copy stream as soon as it is admitted; it packs the ready frames whose
+ * lineage has no frame in flight into a batch and runs the batch through
+ * tgmm_em_run_batch -- one launch per EM phase for all its frames -- on one of `lanes`
+ * streams, each with its own plan.  Uploads, batches and downloads of different frames
+ * overlap.  Results are bit-identical to running each frame alone.
  *
  * Every entry point returns an int status (tgmm_gmem.h); results carry their own status.
  */
@@ -63,11 +64,21 @@ int tgmm_server_close_lineage(TgmmServer* s, int32_t lineage);
  * for its frames in flight. */
 int tgmm_server_read_lineage(TgmmServer* s, int32_t lineage, TgmmGaussian* gm_host);
 
-/* One frame of a lineage, in host memory with the layout of TgmmFrame.  The arrays must
- * stay valid and unchanged until the frame's result has been polled; page-locked host
- * memory makes the upload asynchronous.  Outputs (each optional, NULL to skip): rnk_out,
- * ind_out (5*n_sv, slot-major like tgmm_em_run) and gm_out (n_gauss records: the frame's
- * posterior, before the prior update), written before the result is returned. */
+/* One frame of a lineage, in host memory with the layout of TgmmFrame, or with its voxels
+ * in the compact form below.  The arrays must stay valid and unchanged until the frame's
+ * result has been polled; page-locked host memory makes the upload asynchronous.  A frame
+ * is admitted -- its device buffers taken from the HBM budget and its upload started --
+ * as soon as the budget allows, before its lineage is ready to run it.  Outputs (each
+ * optional, NULL to skip): rnk_out, ind_out (5*n_sv, slot-major like tgmm_em_run) and
+ * gm_out (n_gauss records: the frame's posterior, before the prior update), written before
+ * the result is returned; outputs in page-locked memory are downloaded in place, others
+ * through page-locked staging and a host copy.
+ *
+ * Compact voxels (used when query and img are NULL): lin[v] = x + X (y + Y z) and the raw
+ * intensity raw[v]; the device expands them into query (float x, y, z) and
+ * img = (float)(((double)raw - raw_offset) / raw_denom), the rescale of the reference's
+ * input build (mainTrackingGaussianMixtureModel.cpp:664-669).  6 bytes a voxel cross the
+ * host link instead of 16, and the expanded frame is bit-identical to the float one. */
 typedef struct TgmmServeRequest {
   int32_t lineage;
   uint64_t tag;                 /* echoed in the result */
@@ -80,6 +91,11 @@ typedef struct TgmmServeRequest {
   float* rnk_out;               /* host or NULL */
   int32_t* ind_out;             /* host or NULL */
   TgmmGaussian* gm_out;         /* host or NULL */
+  const uint32_t* lin;          /* host, n_vox (compact form) */
+  const uint16_t* raw;          /* host, n_vox (compact form) */
+  int32_t dims[3];              /* X, Y, Z of the volume (compact form) */
+  double raw_offset;            /* compact form: intensity offset (the foreground threshold) */
+  double raw_denom;             /* compact form: intensity denominator (max - threshold) */
 } TgmmServeRequest;
 
 int tgmm_server_submit(TgmmServer* s, const TgmmServeRequest* r);
@@ -105,6 +121,7 @@ typedef struct TgmmServerStats {
   int64_t submitted, completed, rejected, batches;
   int64_t frames_in_batches;    /* sum of batch sizes */
   int64_t hbm_budget, hbm_in_use, hbm_peak;
+  int64_t h2d_bytes;            /* bytes uploaded from host memory */
   int32_t queued, in_flight;
 } TgmmServerStats;
 

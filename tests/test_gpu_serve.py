@@ -53,18 +53,17 @@ def same_records(a, b):
         np.testing.assert_array_equal(a[name], b[name], err_msg=name)
 
 
-def test_served_mix_is_bit_identical_to_alone(cuda_ok):
+@pytest.mark.parametrize("compact", [False, True])
+def test_served_mix_is_bit_identical_to_alone(cuda_ok, compact):
     from tgmm_b200.serve import Server
     prm = params()
     series = lineages()
     alone = [run_alone(fr, prm) for fr in series]
     with Server(params=prm, lanes=2, max_batch_frames=8) as srv:
         ids = [srv.open_lineage(fr[0].gauss) for fr in series]
-        tag = 0
         for t in range(N_FRAMES):  # interleaved arrivals of all lineages
             for li, fr in enumerate(series):
-                srv.submit(ids[li], fr[t], tag=li * 100 + t)
-                tag += 1
+                srv.submit(ids[li], fr[t], tag=li * 100 + t, compact=compact)
         res = {r.tag: r for r in srv.drain()}
         st = srv.stats()
     assert len(res) == len(series) * N_FRAMES
@@ -159,3 +158,31 @@ def test_read_lineage_returns_the_next_prior(cuda_ok):
     E.update_priors(gm, post.shape[0], 0.01, 1.0, 0.8, -1.0, True)
     torch.cuda.synchronize()
     same_records(prior, E.gauss_from_device(gm))
+
+
+def test_outputs_in_page_locked_memory_are_written_in_place(cuda_ok):
+    import torch
+    from tgmm_b200.serve import Server
+    prm = params()
+    series = lineages()[:2]
+    alone = [run_alone(fr, prm) for fr in series]
+
+    def pinned_out(S, K):
+        return (torch.empty(5 * S).pin_memory().numpy(), torch.empty(5 * S, dtype=torch.int32).pin_memory().numpy(),
+                torch.empty(K * 288, dtype=torch.uint8).pin_memory().numpy().view(L.GAUSS_DTYPE))
+    with Server(params=prm, lanes=2) as srv:
+        ids = [srv.open_lineage(fr[0].gauss) for fr in series]
+        outs = {}
+        for t in range(N_FRAMES):
+            for li, fr in enumerate(series):
+                outs[li * 100 + t] = pinned_out(fr[t].n_sv, fr[0].n_gauss)
+                srv.submit(ids[li], fr[t], tag=li * 100 + t, out=outs[li * 100 + t])
+        res = {r.tag: r for r in srv.drain()}
+    for li in range(len(series)):
+        for t in range(N_FRAMES):
+            r, o = res[li * 100 + t], outs[li * 100 + t]
+            assert r.status == L.TGMM_OK
+            assert r.rnk.ctypes.data == o[0].ctypes.data
+            np.testing.assert_array_equal(o[0], alone[li][t]["rnk"])
+            np.testing.assert_array_equal(o[1], alone[li][t]["ind"])
+            same_records(o[2], alone[li][t]["gauss"])

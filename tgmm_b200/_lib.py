@@ -116,7 +116,8 @@ class TgmmServeRequest(C.Structure):
     _fields_ = [
         ("lineage", C.c_int32), ("tag", C.c_uint64), ("query", C.c_void_p), ("img", C.c_void_p),
         ("centroids", C.c_void_p), ("label_ptr", C.c_void_p), ("n_vox", C.c_int64), ("n_sv", C.c_int32),
-        ("rnk_out", C.c_void_p), ("ind_out", C.c_void_p), ("gm_out", C.c_void_p),
+        ("rnk_out", C.c_void_p), ("ind_out", C.c_void_p), ("gm_out", C.c_void_p), ("lin", C.c_void_p),
+        ("raw", C.c_void_p), ("dims", C.c_int32 * 3), ("raw_offset", C.c_double), ("raw_denom", C.c_double),
     ]
 
 
@@ -132,7 +133,7 @@ class TgmmServerStats(C.Structure):
     _fields_ = [
         ("submitted", C.c_int64), ("completed", C.c_int64), ("rejected", C.c_int64), ("batches", C.c_int64),
         ("frames_in_batches", C.c_int64), ("hbm_budget", C.c_int64), ("hbm_in_use", C.c_int64),
-        ("hbm_peak", C.c_int64), ("queued", C.c_int32), ("in_flight", C.c_int32),
+        ("hbm_peak", C.c_int64), ("h2d_bytes", C.c_int64), ("queued", C.c_int32), ("in_flight", C.c_int32),
     ]
 
 
@@ -179,6 +180,7 @@ SYNTH_FUNCS = {
     "tgmm_synth_n_sv": (C.c_int32, [_VP]),
     "tgmm_synth_max_fg": (C.c_float, [_VP]),
     "tgmm_synth_copy": (None, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "tgmm_synth_copy_raw": (None, [_VP, _VP]),
     "tgmm_synth_free": (None, [_VP]),
     "tgmm_synth_init_gaussians": (C.c_int32, [_VP, C.POINTER(TgmmSynthConfig), C.c_int32, _VP, C.c_uint64,
                                               C.POINTER(TgmmEmParams), _VP, _VP]),

@@ -95,16 +95,13 @@ struct TgmmPlan {
   Layout L;
   char* base = nullptr;
   DevPlan dev;
-  // pinned host staging of the batch tables
-  BatchInfo* h_info = nullptr;
-  FrameDesc* h_frames = nullptr;
-  GChunk* h_gchunks = nullptr;
-  FrameState* h_state = nullptr;
+  FrameState* h_state = nullptr;  // pinned: per-frame state read back for stats
   cudaStream_t cap_stream = nullptr;
-  cudaEvent_t done_ev = nullptr;
-  bool pending = false;
+  cudaEvent_t done_ev = nullptr;       // end of the last call
+  cudaStream_t last_stream = nullptr;  // its stream
+  bool used = false;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (max_iter, ll_prec) -> exec
-  // pageable shadow of the tables being staged
+  // host copy of the tables of the last staged batch
   BatchInfo s_info{};
   std::vector<FrameDesc> s_frames;
   std::vector<GChunk> s_gchunks;
@@ -153,9 +150,6 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
     return fail(TGMM_ERR_OOM, "tgmm_plan_create: cudaMalloc", e);
   }
   e = cudaMemset(P->base, 0, P->L.total);
-  if (e == cudaSuccess) e = cudaMallocHost(&P->h_info, sizeof(BatchInfo));
-  if (e == cudaSuccess) e = cudaMallocHost(&P->h_frames, sizeof(FrameDesc) * d->max_frames);
-  if (e == cudaSuccess) e = cudaMallocHost(&P->h_gchunks, sizeof(GChunk) * mgc);
   if (e == cudaSuccess) e = cudaMallocHost(&P->h_state, sizeof(FrameState) * d->max_frames);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->done_ev, cudaEventDisableTiming);
@@ -165,9 +159,6 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   }
   P->s_frames.assign(d->max_frames, FrameDesc{});
   P->s_gchunks.assign(mgc, GChunk{});
-  memset(P->h_frames, 0, sizeof(FrameDesc) * d->max_frames);
-  memset(P->h_gchunks, 0, sizeof(GChunk) * mgc);
-  memset(P->h_info, 0, sizeof(BatchInfo));
   DevPlan& D = P->dev;
   char* b = P->base;
   D.max_vox = d->max_vox;
@@ -212,13 +203,10 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
 
 int tgmm_plan_destroy(TgmmPlan* P) {
   if (!P) return TGMM_OK;
-  if (P->pending) cudaEventSynchronize(P->done_ev);
+  if (P->used) cudaEventSynchronize(P->done_ev);
   for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   if (P->done_ev) cudaEventDestroy(P->done_ev);
-  if (P->h_info) cudaFreeHost(P->h_info);
-  if (P->h_frames) cudaFreeHost(P->h_frames);
-  if (P->h_gchunks) cudaFreeHost(P->h_gchunks);
   if (P->h_state) cudaFreeHost(P->h_state);
   if (P->base) cudaFree(P->base);
   delete P;
@@ -323,16 +311,26 @@ int stage_batch(TgmmPlan* P, int32_t n, const TgmmFrame* fr, TgmmGaussian* const
   return TGMM_OK;
 }
 
-// The whole EM as a stream of async operations on `st`.
+// A call on `st` starts after the plan's previous call, even on another stream.
+int order_after_previous(TgmmPlan* P, cudaStream_t st) {
+  if (P->used && P->last_stream != st) TG_CUDA(cudaStreamWaitEvent(st, P->done_ev, 0), "order after previous call");
+  return TGMM_OK;
+}
+
+// The staged batch tables to the device (kernel launches, no copy engine).
+int stage_tables(TgmmPlan* P, cudaStream_t st) {
+  const DevPlan& D = P->dev;
+  TG_CUDA(launch_stage_bytes(D.info, &P->s_info, sizeof(BatchInfo), st), "stage info");
+  TG_CUDA(launch_stage_bytes(D.frames, P->s_frames.data(), sizeof(FrameDesc) * P->s_info.n_frames, st),
+          "stage frames");
+  TG_CUDA(launch_stage_bytes(D.gchunks, P->s_gchunks.data(), sizeof(GChunk) * P->s_info.n_gchunks, st),
+          "stage chunks");
+  return TGMM_OK;
+}
+
+// The whole EM (after the tables are staged) as a stream of async operations on `st`.
 int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
   const DevPlan& D = P->dev;
-  TG_CUDA(cudaMemcpyAsync(D.info, P->h_info, sizeof(BatchInfo), cudaMemcpyHostToDevice, st), "stage info");
-  TG_CUDA(cudaMemcpyAsync(D.frames, P->h_frames, sizeof(FrameDesc) * P->desc.max_frames, cudaMemcpyHostToDevice, st),
-          "stage frames");
-  TG_CUDA(cudaMemcpyAsync(D.gchunks, P->h_gchunks, sizeof(GChunk) * D.max_gchunks, cudaMemcpyHostToDevice, st),
-          "stage chunks");
-  TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)D.max_gauss, st), "clear buckets");
-  TG_CUDA(cudaMemsetAsync(D.acnt, 0, 4 * (size_t)D.max_gauss, st), "clear assignment buckets");
   launch_build_maps(D, st);
   launch_import(D, st);
   launch_moments(D, st);
@@ -462,29 +460,21 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
   std::lock_guard<std::mutex> lock(P->mu);
   cudaStream_t st = (cudaStream_t)stream;
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
-  // Stage the batch tables; the pinned copies are read by the previous call's graph until
-  // it finishes, so wait for it only when the tables change.
   rc = stage_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params);
   if (rc) return rc;
-  const size_t fb = sizeof(FrameDesc) * P->desc.max_frames, cb = sizeof(GChunk) * P->dev.max_gchunks;
-  const bool same = P->pending && memcmp(&P->s_info, P->h_info, sizeof(BatchInfo)) == 0 &&
-                    memcmp(P->s_frames.data(), P->h_frames, fb) == 0 && memcmp(P->s_gchunks.data(), P->h_gchunks, cb) == 0;
-  if (!same) {
-    if (P->pending) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
-    memcpy(P->h_info, &P->s_info, sizeof(BatchInfo));
-    memcpy(P->h_frames, P->s_frames.data(), fb);
-    memcpy(P->h_gchunks, P->s_gchunks.data(), cb);
-  }
-  P->pending = false;
+  rc = order_after_previous(P, st);
+  if (rc) return rc;
+  rc = stage_tables(P, st);
+  if (rc) return rc;
   rc = run_batch(P, params->max_iter_em, params->ll_precision, st);
   if (rc) return rc;
   TG_CUDA(cudaEventRecord(P->done_ev, st), "record");
-  P->pending = true;
+  P->used = true;
+  P->last_stream = st;
   if (stats) {
     int fo = 0;
     rc = collect_stats(P, n_frames, stats, st, &fo);
     if (rc) return rc;
-    P->pending = false;
     return flags_to_status(fo);
   }
   return TGMM_OK;
@@ -497,9 +487,8 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   std::lock_guard<std::mutex> lock(P->mu);
   cudaStream_t st = (cudaStream_t)stream;
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
-  if (P->pending) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
-  P->pending = false;
-  const int nf = P->h_info->n_frames;
+  if (P->used) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  const int nf = P->s_info.n_frames;
   if (nf < 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_time_kernel: run a batch first");
   std::vector<FrameState> backup(nf), live(nf);
   TG_CUDA(cudaMemcpy(backup.data(), P->dev.state, sizeof(FrameState) * nf, cudaMemcpyDeviceToHost), "read state");
@@ -508,7 +497,7 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
     if (!(s.flags & (F_BAD_CSR | F_FEW_GAUSS))) s.done = 0;
   TG_CUDA(cudaMemcpy(P->dev.state, live.data(), sizeof(FrameState) * nf, cudaMemcpyHostToDevice), "write state");
   // the voxel pass runs the convergence test; keep every frame running while timing
-  std::vector<FrameDesc> frames(P->h_frames, P->h_frames + nf);
+  std::vector<FrameDesc> frames(P->s_frames.begin(), P->s_frames.begin() + nf);
   for (auto& d : frames) {
     d.max_iter = 0x7fffffff;
     d.tol = -1.0;
@@ -520,7 +509,7 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   TG_CUDA(cudaEventRecord(a, st), "record");
   for (int r = 0; r < reps; r++) {
     if (kernel == TGMM_KERNEL_MOMENTS) launch_moments(P->dev, st);
-    if (kernel == TGMM_KERNEL_LL_PASS) launch_ll_pass(P->dev, P->h_frames[0].ll_prec == TGMM_LLPREC_FP64, st);
+    if (kernel == TGMM_KERNEL_LL_PASS) launch_ll_pass(P->dev, P->s_frames[0].ll_prec == TGMM_LLPREC_FP64, st);
   }
   TG_CUDA(cudaEventRecord(b, st), "record");
   TG_CUDA(cudaEventSynchronize(b), "synchronize");
@@ -531,7 +520,7 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   *ms = t / reps;
   TG_CUDA(cudaMemcpyAsync(P->dev.state, backup.data(), sizeof(FrameState) * nf, cudaMemcpyHostToDevice, st),
           "restore state");
-  TG_CUDA(cudaMemcpyAsync(P->dev.frames, P->h_frames, sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice, st),
+  TG_CUDA(cudaMemcpyAsync(P->dev.frames, P->s_frames.data(), sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice, st),
           "restore frames");
   TG_CUDA(cudaStreamSynchronize(st), "synchronize");
   TG_CUDA(cudaGetLastError(), "kernel launch");
@@ -550,8 +539,8 @@ int tgmm_em_run(TgmmPlan* P, const TgmmFrame* frame, TgmmGaussian* gm_host, floa
   if (frame->n_gauss > P->desc.max_gauss) return fail(TGMM_ERR_BAD_SIZE, "n_gauss beyond plan capacity");
   cudaStream_t st = (cudaStream_t)stream;
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
-  if (P->pending) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
-  P->pending = false;
+  int orc = order_after_previous(P, st);  // the scratch Gaussians may still be in use
+  if (orc) return orc;
   TgmmGaussian* scratch = (TgmmGaussian*)(P->base + P->L.gm_scratch);
   const size_t bytes = sizeof(TgmmGaussian) * (size_t)frame->n_gauss;
   TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");

@@ -11,6 +11,9 @@
 // bit-identical whether a frame runs alone or inside a batch.
 #include <float.h>
 #include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "tgmm_internal.cuh"
 
@@ -255,7 +258,11 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
   if (threadIdx.x == 0) sbad = 0;
   __syncthreads();
   for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) P.sv_frame[D.sv_base + i] = f;
-  for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) P.g_frame[D.g_base + i] = f;
+  for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) {
+    P.g_frame[D.g_base + i] = f;
+    P.bcnt[D.g_base + i] = 0;  // M-step and assignment buckets start empty
+    P.acnt[D.g_base + i] = 0;
+  }
   for (int i = threadIdx.x; i < D.cell_budget; i += blockDim.x) P.cell_cnt[D.cell_base + i] = 0;
   int bad = 0;
   float lo[3] = {kInfF, kInfF, kInfF}, hi[3] = {-kInfF, -kInfF, -kInfF};
@@ -1754,6 +1761,35 @@ void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st) {
     k_ll_pass<true><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
   else
     k_ll_pass<false><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
+}
+
+// Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging
+// a batch takes no copy engine: a batch is not queued behind large uploads of other frames.
+constexpr int kStageChunk16 = 1536;
+struct StageArgs {
+  uint4* dst;
+  int n16;
+  int pad;
+  uint4 data[kStageChunk16];
+};
+
+__global__ void __launch_bounds__(256) k_stage(const __grid_constant__ StageArgs a) {
+  for (int i = threadIdx.x; i < a.n16; i += blockDim.x) a.dst[i] = a.data[i];
+}
+
+cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  StageArgs a;
+  const unsigned char* s = static_cast<const unsigned char*>(src);
+  for (size_t off = 0; off < bytes; off += 16 * (size_t)kStageChunk16) {
+    const size_t n = std::min(bytes - off, 16 * (size_t)kStageChunk16);
+    memset(a.data, 0, 16 * ((n + 15) / 16));
+    memcpy(a.data, s + off, n);
+    a.dst = reinterpret_cast<uint4*>(static_cast<unsigned char*>(dst) + off);
+    a.n16 = (int)((n + 15) / 16);
+    a.pad = 0;
+    k_stage<<<1, 256, 0, st>>>(a);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t configure_kernels(DevPlan& P, int device) {

@@ -71,10 +71,11 @@ class Arena {
   std::map<int64_t, int64_t> free_;
 };
 
-// Device bytes of one frame: inputs and outputs, each 256-byte aligned.
+// Device bytes of one frame: inputs, outputs and (compact form) the uploaded voxel codes,
+// each 256-byte aligned.
 struct FrameLayout {
-  int64_t query, img, cent, lptr, rnk, ind, total;
-  FrameLayout(int64_t n_vox, int32_t n_sv) {
+  int64_t query, img, cent, lptr, rnk, ind, lin, raw, total;
+  FrameLayout(int64_t n_vox, int32_t n_sv, bool compact = false) {
     int64_t o = 0;
     auto take = [&](int64_t b) {
       const int64_t at = o;
@@ -87,15 +88,47 @@ struct FrameLayout {
     lptr = take(8 * ((int64_t)n_sv + 1));
     rnk = take(4 * (int64_t)TGMM_J * n_sv);
     ind = take(4 * (int64_t)TGMM_J * n_sv);
+    lin = compact ? take(4 * n_vox) : -1;
+    raw = compact ? take(2 * n_vox) : -1;
     total = o;
   }
 };
 
+bool is_compact(const TgmmServeRequest& r) { return !r.query && !r.img && r.lin && r.raw; }
+
+// Host memory the device can copy into directly (page-locked or registered).
+bool page_locked(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Compact voxels -> the float frame (x, y, z blocks and intensities), exactly as the host
+// builds them.
+__global__ void k_expand_frame(const uint32_t* __restrict__ lin, const uint16_t* __restrict__ raw, int64_t n,
+                               uint32_t X, uint32_t Y, double off, double den, float* __restrict__ query,
+                               float* __restrict__ img) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = lin[i];
+    const uint32_t q = v / X;
+    query[i] = (float)(v - q * X);
+    query[n + i] = (float)(q % Y);
+    query[2 * n + i] = (float)(q / Y);
+    img[i] = (float)(((double)raw[i] - off) / den);
+  }
+}
+
 struct Request {
   TgmmServeRequest r;
+  bool direct[3] = {false, false, false};  // rnk, ind, gm outputs downloaded in place
   uint64_t seq = 0;
   double t_submit = 0.0, t_start = 0.0;
-  int64_t off = -1, bytes = 0;
+  int64_t off = -1, bytes = 0;  // arena range once admitted
+  cudaEvent_t ready = nullptr;  // its upload (and expansion) done
 };
 
 struct Lineage {
@@ -140,6 +173,9 @@ struct TgmmServer {
   std::deque<TgmmServeResult> results;
   std::thread worker;
   bool stop = false;
+  cudaStream_t copy = nullptr;         // uploads of admitted frames
+  std::vector<cudaEvent_t> free_events;
+  int64_t h2d_bytes = 0;
   uint64_t seq = 0;
   int64_t submitted = 0, completed = 0, rejected = 0, batches = 0, frames_in_batches = 0;
   int32_t queued = 0, in_flight = 0;  // in the inbox; in lineage queues (waiting or running)
@@ -150,6 +186,8 @@ struct TgmmServer {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   void run();
+  void admit();
+  int upload(Request* q);
   void finish(Request* q, int status, const TgmmEmStats* st, int32_t batch_id, int32_t batch_frames);
   bool form_batch(Lane& L, std::vector<Request*>& batch);
   void launch(Lane& L);
@@ -182,6 +220,8 @@ void TgmmServer::finish(Request* q, int status, const TgmmEmStats* st, int32_t b
   res.batch_id = batch_id;
   res.batch_frames = batch_frames;
   results.push_back(res);
+  if (q->off >= 0) arena->release(q->off, q->bytes);
+  if (q->ready) free_events.push_back(q->ready);
   completed++;
   if (status == TGMM_ERR_ADMISSION || status == TGMM_ERR_BAD_SIZE || status == TGMM_ERR_INVALID_ARG) rejected++;
   delete q;
@@ -193,7 +233,8 @@ void TgmmServer::finish(Request* q, int status, const TgmmEmStats* st, int32_t b
 bool TgmmServer::form_batch(Lane& L, std::vector<Request*>& batch) {
   std::vector<std::pair<uint64_t, int32_t>> ready;
   for (auto& kv : lineages)
-    if (!kv.second.in_flight && !kv.second.queue.empty()) ready.push_back({kv.second.queue.front()->seq, kv.first});
+    if (!kv.second.in_flight && !kv.second.queue.empty() && kv.second.queue.front()->off >= 0)
+      ready.push_back({kv.second.queue.front()->seq, kv.first});
   std::sort(ready.begin(), ready.end());
   int64_t vox = 0, sv = 0, gauss = 0;
   for (auto& rd : ready) {
@@ -203,11 +244,6 @@ bool TgmmServer::form_batch(Lane& L, std::vector<Request*>& batch) {
     if (vox + q->r.n_vox > desc.max_batch_vox || sv + q->r.n_sv > desc.max_batch_sv ||
         gauss + G.n_gauss > desc.max_batch_gauss)
       continue;
-    const FrameLayout lay(q->r.n_vox, q->r.n_sv);
-    const int64_t off = arena->alloc(lay.total);
-    if (off < 0) continue;  // waits for memory: admitted once enough is released
-    q->off = off;
-    q->bytes = lay.total;
     G.in_flight = true;
     batch.push_back(q);
     L.lineage_ids.push_back(rd.second);
@@ -233,14 +269,11 @@ void TgmmServer::launch(Lane& L) {
   int64_t so = 0, go = 0;
   for (int i = 0; i < n && rc == TGMM_OK; i++) {
     Request* q = L.reqs[i];
-    const FrameLayout lay(q->r.n_vox, q->r.n_sv);
+    const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
     char* base = dev + q->off;
     const int64_t N = q->r.n_vox, S = q->r.n_sv;
-    cudaError_t e = cudaMemcpyAsync(base + lay.query, q->r.query, 12 * N, cudaMemcpyHostToDevice, L.st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.img, q->r.img, 4 * N, cudaMemcpyHostToDevice, L.st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.cent, q->r.centroids, 12 * S, cudaMemcpyHostToDevice, L.st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, L.st);
-    if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: upload", e);
+    const cudaError_t e = cudaStreamWaitEvent(L.st, q->ready, 0);  // its upload
+    if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: wait for upload", e);
     fr[i].query = (const float*)(base + lay.query);
     fr[i].img = (const float*)(base + lay.img);
     fr[i].centroids = (const float*)(base + lay.cent);
@@ -264,12 +297,20 @@ void TgmmServer::launch(Lane& L) {
     const int64_t S = q->r.n_sv;
     const int32_t K = fr[i].n_gauss;
     cudaError_t e = cudaSuccess;
+    // outputs in page-locked memory are written in place, the others through the lane's
+    // staging and a host copy when the batch is done
+    q->direct[0] = page_locked(q->r.rnk_out);
+    q->direct[1] = page_locked(q->r.ind_out);
+    q->direct[2] = page_locked(q->r.gm_out);
     if (q->r.rnk_out)
-      e = cudaMemcpyAsync(L.h_rnk + L.sv_off[i], rnk[i], 4 * TGMM_J * S, cudaMemcpyDeviceToHost, L.st);
+      e = cudaMemcpyAsync(q->direct[0] ? q->r.rnk_out : L.h_rnk + L.sv_off[i], rnk[i], 4 * TGMM_J * S,
+                          cudaMemcpyDeviceToHost, L.st);
     if (e == cudaSuccess && q->r.ind_out)
-      e = cudaMemcpyAsync(L.h_ind + L.sv_off[i], ind[i], 4 * TGMM_J * S, cudaMemcpyDeviceToHost, L.st);
+      e = cudaMemcpyAsync(q->direct[1] ? q->r.ind_out : L.h_ind + L.sv_off[i], ind[i], 4 * TGMM_J * S,
+                          cudaMemcpyDeviceToHost, L.st);
     if (e == cudaSuccess && q->r.gm_out)
-      e = cudaMemcpyAsync(L.h_gm + L.g_off[i], gm[i], sizeof(TgmmGaussian) * K, cudaMemcpyDeviceToHost, L.st);
+      e = cudaMemcpyAsync(q->direct[2] ? q->r.gm_out : L.h_gm + L.g_off[i], gm[i], sizeof(TgmmGaussian) * K,
+                          cudaMemcpyDeviceToHost, L.st);
     if (e != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "serve: download", e);
     // posterior -> prior of the lineage's next frame
     if (rc == TGMM_OK)
@@ -295,11 +336,10 @@ void TgmmServer::complete(Lane& L) {
     if (status == TGMM_OK) {
       status = tgmm::frame_state_to_stats(L.h_state + sb * i, &st);
       const int64_t S = q->r.n_sv;
-      if (q->r.rnk_out) memcpy(q->r.rnk_out, L.h_rnk + L.sv_off[i], 4 * TGMM_J * S);
-      if (q->r.ind_out) memcpy(q->r.ind_out, L.h_ind + L.sv_off[i], 4 * TGMM_J * S);
-      if (q->r.gm_out) memcpy(q->r.gm_out, L.h_gm + L.g_off[i], sizeof(TgmmGaussian) * G.n_gauss);
+      if (q->r.rnk_out && !q->direct[0]) memcpy(q->r.rnk_out, L.h_rnk + L.sv_off[i], 4 * TGMM_J * S);
+      if (q->r.ind_out && !q->direct[1]) memcpy(q->r.ind_out, L.h_ind + L.sv_off[i], 4 * TGMM_J * S);
+      if (q->r.gm_out && !q->direct[2]) memcpy(q->r.gm_out, L.h_gm + L.g_off[i], sizeof(TgmmGaussian) * G.n_gauss);
     }
-    arena->release(q->off, q->bytes);
     G.in_flight = false;
     G.queue.pop_front();
     in_flight--;
@@ -310,6 +350,71 @@ void TgmmServer::complete(Lane& L) {
   L.gm_dev.clear();
   L.n_gauss.clear();
   L.busy = false;
+}
+
+// Upload of an admitted frame on the copy stream (lock held; the copies are asynchronous
+// from page-locked memory).
+int TgmmServer::upload(Request* q) {
+  const bool cpt = is_compact(q->r);
+  const FrameLayout lay(q->r.n_vox, q->r.n_sv, cpt);
+  char* base = dev + q->off;
+  const int64_t N = q->r.n_vox, S = q->r.n_sv;
+  cudaError_t e = cudaSuccess;
+  if (cpt) {
+    e = cudaMemcpyAsync(base + lay.lin, q->r.lin, 4 * N, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.raw, q->r.raw, 2 * N, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess && N > 0) {
+      const int threads = 256;
+      const int64_t blocks = std::min<int64_t>((N + threads - 1) / threads, 148 * 16);
+      k_expand_frame<<<(int)blocks, threads, 0, copy>>>(
+          (const uint32_t*)(base + lay.lin), (const uint16_t*)(base + lay.raw), N, (uint32_t)q->r.dims[0],
+          (uint32_t)q->r.dims[1], q->r.raw_offset, q->r.raw_denom, (float*)(base + lay.query),
+          (float*)(base + lay.img));
+      e = cudaGetLastError();
+    }
+    h2d_bytes += 6 * N;
+  } else {
+    e = cudaMemcpyAsync(base + lay.query, q->r.query, 12 * N, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.img, q->r.img, 4 * N, cudaMemcpyHostToDevice, copy);
+    h2d_bytes += 16 * N;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.cent, q->r.centroids, 12 * S, cudaMemcpyHostToDevice, copy);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, copy);
+  h2d_bytes += 12 * S + 8 * (S + 1);
+  if (e == cudaSuccess) {
+    if (free_events.empty()) {
+      cudaEvent_t ev;
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess) free_events.push_back(ev);
+    }
+    if (e == cudaSuccess) {
+      q->ready = free_events.back();
+      free_events.pop_back();
+      e = cudaEventRecord(q->ready, copy);
+    }
+  }
+  return e == cudaSuccess ? TGMM_OK : fail(TGMM_ERR_CUDA, "serve: upload", e);
+}
+
+// Admission in arrival order: every queued frame that fits the HBM budget gets its buffers
+// and its upload, whether or not its lineage is ready (lock held).
+void TgmmServer::admit() {
+  std::vector<Request*> waiting;
+  for (auto& kv : lineages)
+    for (Request* q : kv.second.queue)
+      if (q->off < 0) waiting.push_back(q);
+  std::sort(waiting.begin(), waiting.end(), [](const Request* a, const Request* b) { return a->seq < b->seq; });
+  for (Request* q : waiting) {
+    const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
+    const int64_t off = arena->alloc(lay.total);
+    if (off < 0) break;  // later frames wait behind this one: admission keeps arrival order
+    q->off = off;
+    q->bytes = lay.total;
+    if (upload(q) != TGMM_OK) {
+      q->ready = nullptr;
+      // leaves the frame admitted; its batch reports the failure through the lane
+    }
+  }
 }
 
 void TgmmServer::run() {
@@ -326,7 +431,7 @@ void TgmmServer::run() {
         finish(q, TGMM_ERR_INVALID_ARG, nullptr, -1, 0);
         continue;
       }
-      const FrameLayout lay(q->r.n_vox, q->r.n_sv);
+      const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
       if (q->r.n_vox > desc.max_batch_vox || q->r.n_sv > desc.max_batch_sv ||
           it->second.n_gauss > desc.max_batch_gauss) {
         finish(q, TGMM_ERR_BAD_SIZE, nullptr, -1, 0);
@@ -339,6 +444,7 @@ void TgmmServer::run() {
       it->second.queue.push_back(q);
       in_flight++;
     }
+    admit();
     bool progressed = false;
     for (Lane& L : lanes) {
       if (!L.busy) continue;
@@ -442,6 +548,8 @@ int tgmm_server_create(const TgmmServerDesc* d, TgmmServer** out) {
   if (e != cudaSuccess) return bail(fail(TGMM_ERR_OOM, "tgmm_server_create: HBM budget", e));
   S->desc.hbm_budget = budget;
   S->arena = new Arena(budget);
+  e = cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(fail(TGMM_ERR_CUDA, "tgmm_server_create: copy stream", e));
   S->worker = std::thread([S] { S->run(); });
   *out = S;
   return TGMM_OK;
@@ -468,9 +576,15 @@ int tgmm_server_destroy(TgmmServer* S) {
     if (L.h_gm) cudaFreeHost(L.h_gm);
     if (L.h_state) cudaFreeHost(L.h_state);
   }
+  if (S->copy) cudaStreamSynchronize(S->copy);
   for (Request* q : S->inbox) delete q;
   for (auto& kv : S->lineages)
-    for (Request* q : kv.second.queue) delete q;
+    for (Request* q : kv.second.queue) {
+      if (q->ready) cudaEventDestroy(q->ready);
+      delete q;
+    }
+  for (cudaEvent_t ev : S->free_events) cudaEventDestroy(ev);
+  if (S->copy) cudaStreamDestroy(S->copy);
   if (S->dev) cudaFree(S->dev);
   delete S->arena;
   delete S;
@@ -538,8 +652,11 @@ int tgmm_server_read_lineage(TgmmServer* S, int32_t id, TgmmGaussian* gm) {
 
 int tgmm_server_submit(TgmmServer* S, const TgmmServeRequest* r) {
   if (!S || !r) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: null argument");
-  if (!r->query || !r->img || !r->centroids || !r->label_ptr || r->n_vox < 0 || r->n_sv < 1)
+  const bool cpt = is_compact(*r);
+  if ((!cpt && (!r->query || !r->img)) || !r->centroids || !r->label_ptr || r->n_vox < 0 || r->n_sv < 1)
     return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad frame");
+  if (cpt && (r->dims[0] < 1 || r->dims[1] < 1 || r->dims[2] < 1 || !(r->raw_denom != 0.0)))
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad compact frame");
   Request* q = new Request();
   q->r = *r;
   {
@@ -586,6 +703,7 @@ int tgmm_server_stats(TgmmServer* S, TgmmServerStats* o) {
   o->hbm_budget = S->arena->capacity();
   o->hbm_in_use = S->arena->used();
   o->hbm_peak = S->arena->peak();
+  o->h2d_bytes = S->h2d_bytes;
   o->queued = S->queued;
   o->in_flight = S->in_flight;
   return TGMM_OK;
@@ -610,7 +728,9 @@ int tgmm_server_selftest(void) {
   check(a.alloc(10 * kGranule) == 0);
   check(a.peak() == 10 * kGranule);
   const FrameLayout lay(1000, 10);
-  check(lay.total % kGranule == 0 && lay.img >= 12 * 1000 && lay.ind + 4 * 5 * 10 <= lay.total);
+  check(lay.total % kGranule == 0 && lay.img >= 12 * 1000 && lay.ind + 4 * 5 * 10 <= lay.total && lay.lin < 0);
+  const FrameLayout cl(1000, 10, true);
+  check(cl.lin > cl.ind && cl.raw >= cl.lin + 4000 && cl.raw + 2000 <= cl.total);
   return bad;
 }
 

@@ -492,6 +492,10 @@ void tgmm_synth_copy(const TgmmSynthFrame* F, float* query, float* img, float* c
   if (sv_nucleus) memcpy(sv_nucleus, F->sv_nucleus, sizeof(int32_t) * F->n_sv);
 }
 
+void tgmm_synth_copy_raw(const TgmmSynthFrame* F, uint16_t* raw) {
+  if (F && raw) memcpy(raw, F->raw, sizeof(uint16_t) * F->n_vox);
+}
+
 void tgmm_synth_free(TgmmSynthFrame* F) {
   if (!F) return;
   free(F->query);

@@ -195,6 +195,9 @@ void launch_kill_prep(const DevPlan& P, cudaStream_t st);
 void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st);
 void launch_assign(const DevPlan& P, cudaStream_t st);
 cudaError_t configure_kernels(DevPlan& P, int device);
+// bytes from host memory to 16-byte aligned device memory through kernel launch
+// parameters (the tail up to the next 16 bytes is written with zeros)
+cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 void launch_export(const DevPlan& P, cudaStream_t st);
 
 // standalone kNN (tgmm_knn): brute force over refs in shared memory tiles

@@ -40,6 +40,9 @@ float tgmm_synth_max_fg(const TgmmSynthFrame* f);
 /* Copy out: query[3N] SoA, img[N], cent[3S] SoA, lptr[S+1], sv_nucleus[S] (any may be NULL). */
 void tgmm_synth_copy(const TgmmSynthFrame* f, float* query, float* img, float* cent, int64_t* lptr,
                      int32_t* sv_nucleus);
+/* Raw uint16 foreground values in the order of query (img = (raw - threshold) / (max_fg -
+ * threshold), evaluated in double and rounded to float). */
+void tgmm_synth_copy_raw(const TgmmSynthFrame* f, uint16_t* raw);
 void tgmm_synth_free(TgmmSynthFrame* f);
 /* First-frame Gaussians; returns K (out may be NULL to count). */
 int32_t tgmm_synth_init_gaussians(const TgmmSynthFrame* f, const TgmmSynthConfig* c, int32_t n_nuclei,

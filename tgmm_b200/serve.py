@@ -122,26 +122,49 @@ class Server:
         L.check(L.gmem().tgmm_server_read_lineage(self.h, lineage, g.ctypes.data), "tgmm_server_read_lineage")
         return g
 
-    def submit(self, lineage: int, frame, tag: int, want_rnk: bool = True, want_gauss: bool = True) -> None:
+    def submit(self, lineage: int, frame, tag: int, want_rnk: bool = True, want_gauss: bool = True,
+               compact: bool = False, out=None) -> None:
         """frame: an object with query, img, centroids, label_ptr (host arrays of the
-        reference layout), e.g. synth.Frame.  The arrays are used in place."""
+        reference layout), e.g. synth.Frame.  With compact=True the voxels go as
+        (lin, raw, dims, raw_offset, raw_denom): taken from the frame's attributes of those
+        names when present, else from frame.compact().  The arrays are used in place.
+        out: optional (rnk, ind, gauss) arrays to receive the outputs (page-locked ones are
+        written by the device directly)."""
         if tag in self._pending:
             raise ValueError(f"tag {tag} is already pending")
-        arrs = [np.ascontiguousarray(frame.query, np.float32), np.ascontiguousarray(frame.img, np.float32),
-                np.ascontiguousarray(frame.centroids, np.float32), np.ascontiguousarray(frame.label_ptr, np.int64)]
-        q, im, ce, lp = arrs
+        ce = np.ascontiguousarray(frame.centroids, np.float32)
+        lp = np.ascontiguousarray(frame.label_ptr, np.int64)
         S = lp.shape[0] - 1
-        pend = _Pending(keep=arrs)
         r = L.TgmmServeRequest()
         r.lineage, r.tag = lineage, tag
-        r.query, r.img, r.centroids, r.label_ptr = q.ctypes.data, im.ctypes.data, ce.ctypes.data, lp.ctypes.data
-        r.n_vox, r.n_sv = im.shape[0], S
+        r.centroids, r.label_ptr = ce.ctypes.data, lp.ctypes.data
+        if compact:
+            if hasattr(frame, "lin"):
+                lin, raw, dims, off, den = frame.lin, frame.raw, frame.dims, frame.raw_offset, frame.raw_denom
+            else:
+                lin, raw, dims, off, den = frame.compact()
+            lin = np.ascontiguousarray(lin, np.uint32)
+            raw = np.ascontiguousarray(raw, np.uint16)
+            arrs = [lin, raw, ce, lp]
+            r.lin, r.raw = lin.ctypes.data, raw.ctypes.data
+            r.dims[:] = list(dims)
+            r.raw_offset, r.raw_denom = off, den
+            r.n_vox = lin.shape[0]
+        else:
+            q = np.ascontiguousarray(frame.query, np.float32)
+            im = np.ascontiguousarray(frame.img, np.float32)
+            arrs = [q, im, ce, lp]
+            r.query, r.img = q.ctypes.data, im.ctypes.data
+            r.n_vox = im.shape[0]
+        r.n_sv = S
+        pend = _Pending(keep=arrs)
         if want_rnk:
-            pend.rnk = np.zeros(5 * S, np.float32)
-            pend.ind = np.zeros(5 * S, np.int32)
+            pend.rnk = out[0][:5 * S] if out is not None else np.zeros(5 * S, np.float32)
+            pend.ind = out[1][:5 * S] if out is not None else np.zeros(5 * S, np.int32)
             r.rnk_out, r.ind_out = pend.rnk.ctypes.data, pend.ind.ctypes.data
         if want_gauss and lineage in self._n_gauss:  # (an unknown lineage is answered with an error)
-            pend.gauss = np.zeros(self._n_gauss[lineage], L.GAUSS_DTYPE)
+            K = self._n_gauss[lineage]
+            pend.gauss = out[2][:K] if out is not None else np.zeros(K, L.GAUSS_DTYPE)
             r.gm_out = pend.gauss.ctypes.data
         self._pending[tag] = pend
         rc = L.gmem().tgmm_server_submit(self.h, C.byref(r))

@@ -96,6 +96,18 @@ class Frame:
     gauss: np.ndarray = None            # (K,) GAUSS_DTYPE
     gauss_nucleus: np.ndarray = None    # (K,) int32
     meta: dict = field(default_factory=dict)
+    raw: np.ndarray = None              # (N,) uint16 foreground values (img = (raw - thr)/(max_fg - thr))
+
+    def compact(self):
+        """The frame's voxels as (linear index uint32, raw uint16, dims, offset, denominator):
+        6 bytes per voxel that expand exactly into query and img (x = lin % X, y = lin / X
+        % Y, z = lin / (X Y); img = float((raw - offset) / denominator) in double)."""
+        X, Y, Z = self.spec.dims
+        n = self.n_vox
+        q = self.query
+        lin = (q[:n].astype(np.int64) + X * (q[n:2 * n].astype(np.int64) + Y * q[2 * n:].astype(np.int64)))
+        thr = float(np.float32(self.spec.threshold))
+        return lin.astype(np.uint32), self.raw, (X, Y, Z), thr, float(self.max_fg) - thr
 
     @property
     def n_vox(self):
@@ -124,10 +136,13 @@ def make_frame(spec: VolumeSpec, nuclei: Nuclei, seed: int) -> Frame:
         lptr = np.empty(s + 1, np.int64)
         svn = np.empty(s, np.int32)
         lib.tgmm_synth_copy(h, L.ptr(q), L.ptr(img), L.ptr(cent), L.ptr(lptr), L.ptr(svn))
+        raw = np.empty(n, np.uint16)
+        lib.tgmm_synth_copy_raw(h, L.ptr(raw))
         mx = lib.tgmm_synth_max_fg(h)
     finally:
         pass
     f = Frame(q, img, cent, lptr, svn, float(mx), spec=spec, nuclei=nuclei)
+    f.raw = raw
     f.meta["handle"] = h
     return f
 
