@@ -143,6 +143,22 @@ def dist_setup(backend):
     return world, rank, local
 
 
+def reduce_job(total_ms, n_vox, steps, world, device):
+    """Whole-job figures from every rank's device time: the slowest rank's time, the voxels
+    of all ranks (each rank runs its own frame).  Returns (frames/s, voxel-iterations/s,
+    max ms, total voxels)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+    nv = torch.tensor([float(n_vox)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(nv, op=dist.ReduceOp.SUM)
+    max_ms = float(t.item())
+    total_vox = float(nv.item())
+    return world * steps / (max_ms / 1e3), total_vox * EM_ITERS * steps / (max_ms / 1e3), max_ms, total_vox
+
+
 def cpu_baseline(frame, threads=None):
     """The reference's FP32 kernel arithmetic (oracle REF32 port) on the host cores, one EM
     iteration of the workload frame as the bounded sample, scaled to 20 iterations."""
@@ -229,15 +245,7 @@ def run_ours(args):
         dist.barrier()
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    nv = torch.tensor([float(N)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(nv, op=dist.ReduceOp.SUM)
-    max_ms = float(t.item())
-    total_vox = float(nv.item())
-    value = world * args.steps / (max_ms / 1e3)
-    voxel_iters = total_vox * EM_ITERS * args.steps / (max_ms / 1e3)
+    value, voxel_iters, max_ms, total_vox = reduce_job(total_ms, N, args.steps, world, dev)
 
     # roofline of the per-iteration voxel pass (timed alone on this stream, same workload)
     ms_ll = plan_time(plan, L.TGMM_KERNEL_LL_PASS, 20, stream)
