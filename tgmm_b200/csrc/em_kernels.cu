@@ -591,11 +591,12 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 }
 
 // ===========================================================================
-// knn_estep: warp per supervoxel.  Exact 5-NN of the centroid among the frame's
-// Gaussian centres: the lanes split each ring of grid cells, keep private top-5 lists
-// pruned by the warp's current fifth distance, and after each ring the lists are merged
-// by five rounds of a warp-wide (distance, index) arg-min.  Then the E-step from the
-// supervoxel's moments, candidate j on lane j:
+// knn_estep: a group of kKnnGroup lanes per supervoxel (kKnnGroups supervoxels per warp).
+// Exact 5-NN of the centroid among the frame's Gaussian centres: the group's lanes split
+// each ring of grid cells, keep private top-5 lists pruned by the group's current fifth
+// distance, and after each ring the lists are merged by five rounds of a group-wide
+// (distance, index) arg-min.  Then the E-step from the supervoxel's moments, candidate j
+// on lane j of the group:
 //   L_j = sum_v [-1/2 (3/beta + nu d'Wd) + E ln pi + 1/2 E ln|Lambda|]
 //       = -1/2 (3 n/beta + nu tr(W D)) + n (psi(alpha) - psi(sum alpha) + 1/2 E ln|Lambda|),
 //   D = sum_v (x_v - m)(x_v - m)' = G2 - G1 u' - u G1' + n u u',  u = m - c_s,
@@ -603,14 +604,17 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 // candidate or |L| beyond float range -> -inf) and rnk_j = 1 / sum_i exp(L_i - L_j).
 // Pairs with rnk > 1e-3 go to the Gaussian's M-step bucket.
 // ===========================================================================
-constexpr int kKnnWarps = 4;
+constexpr int kKnnGroup = 8;                 // lanes per supervoxel
+constexpr int kKnnGroups = 32 / kKnnGroup;   // supervoxels per warp
+constexpr int kKnnWarps = 4;                 // warps per block
+constexpr int kKnnSvPerBlock = kKnnWarps * kKnnGroups;
 
-// warp-wide lexicographic arg-min of (d, i); every lane gets the winner
-__device__ __forceinline__ void warp_min_pair(float& d, int& i) {
+// group-wide lexicographic arg-min of (d, i); every lane of the group gets the winner
+__device__ __forceinline__ void group_min_pair(float& d, int& i, unsigned gmask) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const float od = __shfl_xor_sync(0xffffffffu, d, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+  for (int o = kKnnGroup / 2; o > 0; o >>= 1) {
+    const float od = __shfl_xor_sync(gmask, d, o);
+    const int oi = __shfl_xor_sync(gmask, i, o);
     if (before(od, oi, d, i)) {
       d = od;
       i = oi;
@@ -618,13 +622,13 @@ __device__ __forceinline__ void warp_min_pair(float& d, int& i) {
   }
 }
 
-// merge the 32 lanes' sorted lists into the warp's top-5 (identical in every lane)
-__device__ __forceinline__ void warp_merge_top5(Top5& mine, Top5& out) {
+// merge the group's sorted lists into its top-5 (identical in every lane of the group)
+__device__ __forceinline__ void group_merge_top5(Top5& mine, Top5& out, unsigned gmask) {
 #pragma unroll
   for (int r = 0; r < kJ; r++) {
     float d = mine.d[0];
     int i = mine.i[0];
-    warp_min_pair(d, i);
+    group_min_pair(d, i, gmask);
     out.d[r] = d;
     out.i[r] = i;
     if (mine.i[0] == i && mine.d[0] == d && i != 0x7fffffff) {  // pop the front of the winner
@@ -639,9 +643,25 @@ __device__ __forceinline__ void warp_merge_top5(Top5& mine, Top5& out) {
   }
 }
 
-__device__ void knn_warp_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
-                                const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, Top5& best) {
-  const int lane = threadIdx.x & 31;
+// group-wide lexicographic arg-max of (d, i)
+__device__ __forceinline__ void group_max_pair(float& d, int& i, unsigned gmask) {
+#pragma unroll
+  for (int o = kKnnGroup / 2; o > 0; o >>= 1) {
+    const float od = __shfl_xor_sync(gmask, d, o);
+    const int oi = __shfl_xor_sync(gmask, i, o);
+    if (before(d, i, od, oi)) {
+      d = od;
+      i = oi;
+    }
+  }
+}
+
+// (td0, ti0): a (distance, index) no smaller than the true fifth neighbour's (the fifth of
+// five known Gaussians), or +inf; refs after it in (distance, index) order cannot be among
+// the five and are rejected without an insertion.
+__device__ void knn_group_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
+                                 const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, Top5& best,
+                                 unsigned gmask, int gl, float td0, int ti0) {
   const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
   int c[3];
   float delta = kInfF;
@@ -655,55 +675,71 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
   delta = fmaxf(delta, 0.0f);
   top5_init(best);
   const int maxr = max(1, max(g.dims[0], max(g.dims[1], g.dims[2])));
-  // the first pass covers rings 0 and 1 (27 cells, one per lane), later passes one ring
+  // the first pass covers rings 0 and 1 (27 cells), later passes one ring
   for (int r = 1; r <= maxr; ++r) {
     Top5 t;
     top5_init(t);
-    // prune with the warp's current fifth: a ref must beat it to matter
-    const float td = best.d[kJ - 1];
-    const int ti = best.i[kJ - 1];
-    auto scan_cell = [&](int dx, int dy, int dz) {
-      const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
-      if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) return;
-      const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
-      const int e = min(ccnt[cell], kCellCap);
+    // prune with the group's current fifth (or the starting bound): a ref must not come
+    // after it to matter
+    const bool use_best = before(best.d[kJ - 1], best.i[kJ - 1], td0, ti0);
+    const float td = use_best ? best.d[kJ - 1] : td0;
+    const int ti = use_best ? best.i[kJ - 1] : ti0;
+    auto scan_refs = [&](int cell, int e) {
       const float4* cr = refs + (int64_t)cell * kCellCap;
       for (int k = 0; k < e; ++k) {
         const float4 rr = cr[k];
         const float d = knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s);
         const int id = __float_as_int(rr.w);
-        if (before(d, id, td, ti)) top5_insert(t, d, id);
+        if (!before(td, ti, d, id)) top5_insert(t, d, id);
       }
+    };
+    auto scan_cell = [&](int dx, int dy, int dz) {
+      const int x = c[0] + dx, yy = c[1] + dy, z = c[2] + dz;
+      if (x < 0 || yy < 0 || z < 0 || x >= g.dims[0] || yy >= g.dims[1] || z >= g.dims[2]) return;
+      const int cell = (z * g.dims[1] + yy) * g.dims[0] + x;
+      scan_refs(cell, min(ccnt[cell], kCellCap));
     };
     // the cells of ring r (the whole cube for r = 1), with constant divisors for the
     // rings a search usually needs
     if (r == 1) {
-      if (lane < 27) scan_cell(lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1);
+      // the lane's cells of the 3x3x3 cube: their counts first, as independent loads
+      constexpr int kPer = (27 + kKnnGroup - 1) / kKnnGroup;
+      int cq[kPer], eq[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const int idx = gl + kKnnGroup * q;
+        const int x = c[0] + idx % 3 - 1, yy = c[1] + (idx / 3) % 3 - 1, z = c[2] + idx / 9 - 1;
+        const bool in = idx < 27 && x >= 0 && yy >= 0 && z >= 0 && x < g.dims[0] && yy < g.dims[1] && z < g.dims[2];
+        cq[q] = in ? (z * g.dims[1] + yy) * g.dims[0] + x : 0;
+        eq[q] = in ? min(ccnt[cq[q]], kCellCap) : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < kPer; q++) scan_refs(cq[q], eq[q]);
     } else if (r == 2) {
-      for (int idx = lane; idx < 125; idx += 32) {
+      for (int idx = gl; idx < 125; idx += kKnnGroup) {
         const int dx = idx % 5 - 2, dy = (idx / 5) % 5 - 2, dz = idx / 25 - 2;
         if (max(abs(dx), max(abs(dy), abs(dz))) == 2) scan_cell(dx, dy, dz);
       }
     } else if (r == 3) {
-      for (int idx = lane; idx < 343; idx += 32) {
+      for (int idx = gl; idx < 343; idx += kKnnGroup) {
         const int dx = idx % 7 - 3, dy = (idx / 7) % 7 - 3, dz = idx / 49 - 3;
         if (max(abs(dx), max(abs(dy), abs(dz))) == 3) scan_cell(dx, dy, dz);
       }
     } else {
       const int side = 2 * r + 1;
       const int cube = side * side * side;
-      for (int idx = lane; idx < cube; idx += 32) {
+      for (int idx = gl; idx < cube; idx += kKnnGroup) {
         const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
         if (max(abs(dx), max(abs(dy), abs(dz))) == r) scan_cell(dx, dy, dz);
       }
     }
-    // lane 0 also carries the previous best (disjoint from this ring's refs)
-    if (lane == 0) {
+    // lane 0 of the group also carries the previous best (disjoint from this ring's refs)
+    if (gl == 0) {
 #pragma unroll
       for (int q = 0; q < kJ; q++) top5_insert(t, best.d[q], best.i[q]);
     }
     Top5 merged;
-    warp_merge_top5(t, merged);
+    group_merge_top5(t, merged, gmask);
     best = merged;
     const float lb = r * g.h + delta;
     const float eps = 4e-3f + 1e-6f * lb;
@@ -715,8 +751,11 @@ __device__ void knn_warp_search(float q0, float q1, float q2, const float* s, co
 }
 
 __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = blockIdx.x * kKnnWarps + warp;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & (kKnnGroup - 1), gbase = lane - gl;
+  const unsigned gmask = ((1u << kKnnGroup) - 1u) << gbase;
+  const int s = blockIdx.x * kKnnSvPerBlock + (threadIdx.x >> 5) * kKnnGroups + gbase / kKnnGroup;
+  // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
   const FrameState& S = P.state[f];
@@ -735,32 +774,55 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
   Top5 t;
   top5_init(t);
   const bool grid_ok = !(S.flags & F_CELL_OVERFLOW);
+  // starting bound from the previous iteration's five candidates (their current centres;
+  // a candidate that died is at +inf): the fifth of them in (distance, index) order
+  float td0 = kInfF;
+  int ti0 = 0x7fffffff;
+  if (S.iter > 1) {
+    float dj = -1.0f;  // lanes without a candidate never win the arg-max
+    int ij = -1;
+    if (gl < kJ) {
+      const int kp = P.cand[(int64_t)s * kJ + gl];
+      if (kp >= D.g_base && kp < D.g_base + D.n_gauss) {
+        dj = knn_dist(q0, q1, q2, __double2float_rn(gcomp(P, G_M0, kp)), __double2float_rn(gcomp(P, G_M1, kp)),
+                      __double2float_rn(gcomp(P, G_M2, kp)), D.scale);
+        ij = kp - D.g_base;
+      } else {
+        dj = kInfF;
+        ij = 0x7fffffff;
+      }
+    }
+    group_max_pair(dj, ij, gmask);
+    td0 = dj;
+    ti0 = ij;
+  }
   if (grid_ok)
-    knn_warp_search(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap, t);
+    knn_group_search(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap,
+                     t, gmask, gl, td0, ti0);
   if (!grid_ok || !(t.d[kJ - 1] < kInfF)) {
     // fewer than five finite distances: exact scan of every Gaussian of the frame
     Top5 m;
     top5_init(m);
-    for (int kl = lane; kl < D.n_gauss; kl += 32) {
+    for (int kl = gl; kl < D.n_gauss; kl += kKnnGroup) {
       const int k = D.g_base + kl;
       const float x = __double2float_rn(gcomp(P, G_M0, k));
       const float y = __double2float_rn(gcomp(P, G_M1, k));
       const float z = __double2float_rn(gcomp(P, G_M2, k));
       top5_insert(m, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
     }
-    warp_merge_top5(m, t);
+    group_merge_top5(m, t, gmask);
   }
-  // E-step: candidate j on lane j
+  // E-step: candidate j on lane j of the group
   const int par = S.iter & 1;
   const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
   const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
   int kl = 0;
 #pragma unroll
   for (int j = 0; j < kJ; j++)
-    if (lane == j) kl = t.i[j];
+    if (gl == j) kl = t.i[j];
   const int k = D.g_base + kl;
   double Lj = 0.0;
-  if (lane < kJ && n != 0.0) {
+  if (gl < kJ && n != 0.0) {
     const double* E = P.ec + (int64_t)k * kEcStride;
     const double2 e01 = *(const double2*)(E), e23 = *(const double2*)(E + 2), e45 = *(const double2*)(E + 4);
     const double2 e67 = *(const double2*)(E + 6), e89 = *(const double2*)(E + 8), e10 = *(const double2*)(E + 10);
@@ -787,18 +849,16 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
       if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
     }
   }
-  // rnk_j = 1 / sum_i exp(L_i - L_j): lane 5i + j evaluates exp(L_i - L_j), and the sum
-  // runs over i in increasing order
-  const int ei = lane / kJ, ej = lane - ei * kJ;
-  const double Li = __shfl_sync(0xffffffffu, Lj, ei < kJ ? ei : 0);
-  const double Lk = __shfl_sync(0xffffffffu, Lj, ej);
-  const double ex = lane < kJ * kJ ? exp(Li - Lk) : 0.0;
-  double acc = 0.0;
+  // rnk_j = 1 / sum_i exp(L_i - L_j), the sum over i in increasing order
+  double Li[kJ];
 #pragma unroll
-  for (int i = 0; i < kJ; i++) acc += __shfl_sync(0xffffffffu, ex, i * kJ + (lane < kJ ? lane : 0));
-  if (lane < kJ) {
+  for (int i = 0; i < kJ; i++) Li[i] = __shfl_sync(gmask, Lj, gbase + i);
+  if (gl < kJ) {
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < kJ; i++) acc += exp(Li[i] - Lj);
     const float r = __double2float_rn(1.0 / acc);
-    const int j = lane;
+    const int j = gl;
     const int64_t pos = (int64_t)j * Sf + sl;
     D.rnk_out[pos] = r;
     D.ind_out[pos] = kl;
@@ -1747,7 +1807,7 @@ void launch_moments(const DevPlan& P, cudaStream_t st) {
   k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
-  k_knn_estep<<<div_up(P.max_sv, kKnnWarps), kKnnWarps * 32, 0, st>>>(P);
+  k_knn_estep<<<div_up(P.max_sv, kKnnSvPerBlock), kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
   k_mstep_update<<<2 * P.max_gchunks, kMChunk, 0, st>>>(P);
