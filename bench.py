@@ -220,6 +220,8 @@ def run_ours(args):
     ind = torch.empty(5 * S, dtype=torch.int32, device=dev)
     plan = E.Plan(N, S, K, device=local)
     stream = torch.cuda.current_stream(dev)
+    # the autotuner picks the kNN/E-step width on this frame (untimed; results do not depend on it)
+    knn_lanes = plan.autotune([df], [gm], [rnk], [ind], params, reps=3)
 
     def step():
         gm.copy_(gm0, non_blocking=True)
@@ -277,6 +279,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_vox": N, "n_sv": S, "n_gauss": K, "em_iterations": EM_ITERS,
+                           "knn_lanes_per_supervoxel": knn_lanes,
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (16 B x n_vox)",
                            "ll_precision": "mixed", "ll_mode": "as_reference"},
                 "voxel_iters_per_s": voxel_iters,
@@ -383,6 +386,10 @@ def run_batch64(args):
     tv, ts, tg = sum(f.n_vox for f in frames), sum(f.n_sv for f in frames), sum(f.n_gauss for f in frames)
     batch_plan = E.Plan(tv, ts, tg, max_frames=len(frames))
     one_plan = E.Plan(max(f.n_vox for f in frames), max(f.n_sv for f in frames), max(f.n_gauss for f in frames))
+    # widths tuned on the batch, and on its largest volume for the one-at-a-time plan (untimed)
+    lanes_b = batch_plan.autotune(dfs, gms, rnks, inds, prm, reps=3)
+    big = max(range(len(frames)), key=lambda i: frames[i].n_vox)
+    lanes_p = one_plan.autotune([dfs[big]], [gms[big]], [rnks[big]], [inds[big]], prm, reps=3)
 
     def batched():
         for g, g0 in zip(gms, gm0):
@@ -420,6 +427,7 @@ def run_batch64(args):
                        "total_vox": tv, "total_sv": ts, "total_gauss": tg},
             "plain": {"value": n / (ms_p / 1e3), "ms_per_sweep": ms_p, "path": "tgmm_em_run_device, one at a time"},
             "batched_over_plain": ms_p / ms_b, "voxel_iters_per_s": tv * EM_ITERS / (ms_b / 1e3),
+            "knn_lanes_per_supervoxel": {"batched": lanes_b, "plain": lanes_p},
             "rnk_ind_identical_to_alone": bool(same)}
     print(json.dumps(line), flush=True)
 

@@ -222,6 +222,20 @@ enum {
 };
 int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* ms_per_launch, void* stream);
 
+/* Lanes per supervoxel of the kNN/E-step kernel (8, 16 or 32; default 8).  Every width
+ * computes the same bits; only the speed differs with the batch (supervoxel count, cells
+ * per ring, candidates per cell).  No reference counterpart: the reference runs one fixed
+ * launch shape (knnCuda.cu:781-817, GMEMupdateCUDA.cu:3120-3141). */
+int tgmm_plan_set_knn_group(TgmmPlan* plan, int32_t lanes);
+
+/* Autotuner: stages the batch (the arguments of tgmm_em_run_batch, whose Gaussians are
+ * only read), runs its first iteration up to the kNN/E-step, times that kernel `reps`
+ * times at each width and keeps the fastest in the plan (returned in *lanes_out).  rnk_dev
+ * and ind_dev are overwritten; the results of later calls do not depend on the choice. */
+int tgmm_plan_autotune(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
+                       TgmmGaussian* const* gm_dev, float* const* rnk_dev, int32_t* const* ind_dev,
+                       const TgmmEmParams* params, int32_t reps, int32_t* lanes_out, void* stream);
+
 /* Last CUDA error string recorded by this library on the calling thread. */
 const char* tgmm_last_error(void);
 /* Library version string. */

@@ -170,3 +170,9 @@ def test_lineage_shard_covers_every_lineage_once():
         flat = sorted(x for p in parts for x in p)
         assert flat == list(range(n))
         assert max(map(len, parts)) - min(map(len, parts)) <= 1
+
+
+def test_width_setter_refuses_bad_arguments_without_a_gpu():
+    lib = L.gmem()
+    assert lib.tgmm_plan_set_knn_group(None, 8) == L.TGMM_ERR_INVALID_ARG
+    assert lib.tgmm_plan_autotune(None, 1, None, None, None, None, None, 1, None, None) == L.TGMM_ERR_INVALID_ARG

@@ -159,6 +159,9 @@ GMEM_FUNCS = {
     "tgmm_assign_supervoxels": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_int32]),
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
+    "tgmm_plan_set_knn_group": (C.c_int, [_VP, C.c_int32]),
+    "tgmm_plan_autotune": (C.c_int, [_VP, C.c_int32, C.POINTER(TgmmFrame), C.POINTER(_VP), C.POINTER(_VP),
+                                     C.POINTER(_VP), C.POINTER(TgmmEmParams), C.c_int32, C.POINTER(C.c_int32), _VP]),
     "tgmm_server_default_desc": (None, [C.POINTER(TgmmServerDesc)]),
     "tgmm_server_create": (C.c_int, [C.POINTER(TgmmServerDesc), C.POINTER(_VP)]),
     "tgmm_server_destroy": (C.c_int, [_VP]),

@@ -186,6 +186,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.ec = (double*)(b + P->L.ec);
   D.llc = (double*)(b + P->L.llc);
   D.work = (int32_t*)(b + P->L.work);
+  D.knn_group = 8;
   e = configure_kernels(D, d->device);
   if (e != cudaSuccess) {
     tgmm_plan_destroy(P);
@@ -477,6 +478,81 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
     if (rc) return rc;
     return flags_to_status(fo);
   }
+  return TGMM_OK;
+}
+
+int tgmm_plan_set_knn_group(TgmmPlan* P, int32_t lanes) {
+  if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_group: null plan");
+  if (lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_group: lanes per supervoxel must be 8, 16 or 32");
+  std::lock_guard<std::mutex> lock(P->mu);
+  if (P->dev.knn_group == lanes) return TGMM_OK;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  if (P->used) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // captured with the old launch shape
+  P->graphs.clear();
+  P->dev.knn_group = lanes;
+  return TGMM_OK;
+}
+
+int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
+                       float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params, int32_t reps,
+                       int32_t* lanes_out, void* stream) {
+  if (!P || !frames || !gm_dev || !rnk_dev || !ind_dev || reps < 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_autotune");
+  int rc = validate_params(params);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(P->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  rc = stage_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params);
+  if (rc) return rc;
+  rc = order_after_previous(P, st);
+  if (rc) return rc;
+  rc = stage_tables(P, st);
+  if (rc) return rc;
+  // the batch's first iteration up to the kNN/E-step; that kernel is then timed at each
+  // width with its only lasting effect, the M-step bucket counts, cleared in between
+  const DevPlan& D = P->dev;
+  launch_build_maps(D, st);
+  launch_import(D, st);
+  launch_moments(D, st);
+  TG_CUDA(cudaGetLastError(), "kernel launch");
+  const int widths[3] = {8, 16, 32};
+  float best_ms = 0.0f;
+  int best = P->dev.knn_group;
+  std::vector<cudaEvent_t> ev(2 * reps);
+  for (auto& e : ev) TG_CUDA(cudaEventCreate(&e), "event");
+  for (int w : widths) {
+    P->dev.knn_group = w;
+    launch_knn_estep(P->dev, st);  // warm-up
+    TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
+    for (int r = 0; r < reps; r++) {
+      TG_CUDA(cudaEventRecord(ev[2 * r], st), "record");
+      launch_knn_estep(P->dev, st);
+      TG_CUDA(cudaEventRecord(ev[2 * r + 1], st), "record");
+      TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
+    }
+    TG_CUDA(cudaGetLastError(), "kernel launch");
+    TG_CUDA(cudaStreamSynchronize(st), "synchronize");
+    float total = 0.0f;
+    for (int r = 0; r < reps; r++) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]);
+      total += ms;
+    }
+    if (w == widths[0] || total < best_ms) {
+      best_ms = total;
+      best = w;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // recaptured with the chosen width
+  P->graphs.clear();
+  P->dev.knn_group = best;
+  TG_CUDA(cudaEventRecord(P->done_ev, st), "record");
+  P->used = true;
+  P->last_stream = st;
+  if (lanes_out) *lanes_out = best;
   return TGMM_OK;
 }
 

@@ -591,7 +591,9 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 }
 
 // ===========================================================================
-// knn_estep: a group of kKnnGroup lanes per supervoxel (kKnnGroups supervoxels per warp).
+// knn_estep: a group of G lanes per supervoxel (32 / G supervoxels per warp; G = 8, 16
+// or 32, chosen per plan, by tgmm_plan_autotune or tgmm_plan_set_knn_group; every G gives
+// the same bits).
 // Exact 5-NN of the centroid among the frame's Gaussian centres: the group's lanes split
 // each ring of grid cells, keep private top-5 lists pruned by the group's current fifth
 // distance, and after each ring the lists are merged by five rounds of a group-wide
@@ -604,15 +606,13 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 // candidate or |L| beyond float range -> -inf) and rnk_j = 1 / sum_i exp(L_i - L_j).
 // Pairs with rnk > 1e-3 go to the Gaussian's M-step bucket.
 // ===========================================================================
-constexpr int kKnnGroup = 8;                 // lanes per supervoxel
-constexpr int kKnnGroups = 32 / kKnnGroup;   // supervoxels per warp
-constexpr int kKnnWarps = 4;                 // warps per block
-constexpr int kKnnSvPerBlock = kKnnWarps * kKnnGroups;
+constexpr int kKnnWarps = 4;  // warps per block; the lanes per supervoxel (G) come from the plan
 
 // group-wide lexicographic arg-min of (d, i); every lane of the group gets the winner
+template <int G>
 __device__ __forceinline__ void group_min_pair(float& d, int& i, unsigned gmask) {
 #pragma unroll
-  for (int o = kKnnGroup / 2; o > 0; o >>= 1) {
+  for (int o = G / 2; o > 0; o >>= 1) {
     const float od = __shfl_xor_sync(gmask, d, o);
     const int oi = __shfl_xor_sync(gmask, i, o);
     if (before(od, oi, d, i)) {
@@ -623,12 +623,13 @@ __device__ __forceinline__ void group_min_pair(float& d, int& i, unsigned gmask)
 }
 
 // merge the group's sorted lists into its top-5 (identical in every lane of the group)
+template <int G>
 __device__ __forceinline__ void group_merge_top5(Top5& mine, Top5& out, unsigned gmask) {
 #pragma unroll
   for (int r = 0; r < kJ; r++) {
     float d = mine.d[0];
     int i = mine.i[0];
-    group_min_pair(d, i, gmask);
+    group_min_pair<G>(d, i, gmask);
     out.d[r] = d;
     out.i[r] = i;
     if (mine.i[0] == i && mine.d[0] == d && i != 0x7fffffff) {  // pop the front of the winner
@@ -644,9 +645,10 @@ __device__ __forceinline__ void group_merge_top5(Top5& mine, Top5& out, unsigned
 }
 
 // group-wide lexicographic arg-max of (d, i)
+template <int G>
 __device__ __forceinline__ void group_max_pair(float& d, int& i, unsigned gmask) {
 #pragma unroll
-  for (int o = kKnnGroup / 2; o > 0; o >>= 1) {
+  for (int o = G / 2; o > 0; o >>= 1) {
     const float od = __shfl_xor_sync(gmask, d, o);
     const int oi = __shfl_xor_sync(gmask, i, o);
     if (before(d, i, od, oi)) {
@@ -659,6 +661,7 @@ __device__ __forceinline__ void group_max_pair(float& d, int& i, unsigned gmask)
 // (td0, ti0): a (distance, index) no smaller than the true fifth neighbour's (the fifth of
 // five known Gaussians), or +inf; refs after it in (distance, index) order cannot be among
 // the five and are rejected without an insertion.
+template <int G>
 __device__ void knn_group_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
                                  const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, Top5& best,
                                  unsigned gmask, int gl, float td0, int ti0) {
@@ -703,11 +706,11 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
     // rings a search usually needs
     if (r == 1) {
       // the lane's cells of the 3x3x3 cube: their counts first, as independent loads
-      constexpr int kPer = (27 + kKnnGroup - 1) / kKnnGroup;
+      constexpr int kPer = (27 + G - 1) / G;
       int cq[kPer], eq[kPer];
 #pragma unroll
       for (int q = 0; q < kPer; q++) {
-        const int idx = gl + kKnnGroup * q;
+        const int idx = gl + G * q;
         const int x = c[0] + idx % 3 - 1, yy = c[1] + (idx / 3) % 3 - 1, z = c[2] + idx / 9 - 1;
         const bool in = idx < 27 && x >= 0 && yy >= 0 && z >= 0 && x < g.dims[0] && yy < g.dims[1] && z < g.dims[2];
         cq[q] = in ? (z * g.dims[1] + yy) * g.dims[0] + x : 0;
@@ -716,19 +719,19 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
 #pragma unroll
       for (int q = 0; q < kPer; q++) scan_refs(cq[q], eq[q]);
     } else if (r == 2) {
-      for (int idx = gl; idx < 125; idx += kKnnGroup) {
+      for (int idx = gl; idx < 125; idx += G) {
         const int dx = idx % 5 - 2, dy = (idx / 5) % 5 - 2, dz = idx / 25 - 2;
         if (max(abs(dx), max(abs(dy), abs(dz))) == 2) scan_cell(dx, dy, dz);
       }
     } else if (r == 3) {
-      for (int idx = gl; idx < 343; idx += kKnnGroup) {
+      for (int idx = gl; idx < 343; idx += G) {
         const int dx = idx % 7 - 3, dy = (idx / 7) % 7 - 3, dz = idx / 49 - 3;
         if (max(abs(dx), max(abs(dy), abs(dz))) == 3) scan_cell(dx, dy, dz);
       }
     } else {
       const int side = 2 * r + 1;
       const int cube = side * side * side;
-      for (int idx = gl; idx < cube; idx += kKnnGroup) {
+      for (int idx = gl; idx < cube; idx += G) {
         const int dx = idx % side - r, dy = (idx / side) % side - r, dz = idx / (side * side) - r;
         if (max(abs(dx), max(abs(dy), abs(dz))) == r) scan_cell(dx, dy, dz);
       }
@@ -739,7 +742,7 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
       for (int q = 0; q < kJ; q++) top5_insert(t, best.d[q], best.i[q]);
     }
     Top5 merged;
-    group_merge_top5(t, merged, gmask);
+    group_merge_top5<G>(t, merged, gmask);
     best = merged;
     const float lb = r * g.h + delta;
     const float eps = 4e-3f + 1e-6f * lb;
@@ -750,11 +753,13 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
   }
 }
 
+template <int G>
 __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
+  static_assert(G >= kJ && G <= 32 && (G & (G - 1)) == 0, "a group holds the five candidates");
   const int lane = threadIdx.x & 31;
-  const int gl = lane & (kKnnGroup - 1), gbase = lane - gl;
-  const unsigned gmask = ((1u << kKnnGroup) - 1u) << gbase;
-  const int s = blockIdx.x * kKnnSvPerBlock + (threadIdx.x >> 5) * kKnnGroups + gbase / kKnnGroup;
+  const int gl = lane & (G - 1), gbase = lane - gl;
+  const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
+  const int s = blockIdx.x * (kKnnWarps * 32 / G) + (threadIdx.x >> 5) * (32 / G) + gbase / G;
   // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
@@ -792,25 +797,25 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
         ij = 0x7fffffff;
       }
     }
-    group_max_pair(dj, ij, gmask);
+    group_max_pair<G>(dj, ij, gmask);
     td0 = dj;
     ti0 = ij;
   }
   if (grid_ok)
-    knn_group_search(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap,
+    knn_group_search<G>(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap,
                      t, gmask, gl, td0, ti0);
   if (!grid_ok || !(t.d[kJ - 1] < kInfF)) {
     // fewer than five finite distances: exact scan of every Gaussian of the frame
     Top5 m;
     top5_init(m);
-    for (int kl = gl; kl < D.n_gauss; kl += kKnnGroup) {
+    for (int kl = gl; kl < D.n_gauss; kl += G) {
       const int k = D.g_base + kl;
       const float x = __double2float_rn(gcomp(P, G_M0, k));
       const float y = __double2float_rn(gcomp(P, G_M1, k));
       const float z = __double2float_rn(gcomp(P, G_M2, k));
       top5_insert(m, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
     }
-    group_merge_top5(m, t, gmask);
+    group_merge_top5<G>(m, t, gmask);
   }
   // E-step: candidate j on lane j of the group
   const int par = S.iter & 1;
@@ -1807,7 +1812,14 @@ void launch_moments(const DevPlan& P, cudaStream_t st) {
   k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
-  k_knn_estep<<<div_up(P.max_sv, kKnnSvPerBlock), kKnnWarps * 32, 0, st>>>(P);
+  const int G = P.knn_group;
+  const int grid = div_up(P.max_sv, kKnnWarps * 32 / G);
+  if (G == 32)
+    k_knn_estep<32><<<grid, kKnnWarps * 32, 0, st>>>(P);
+  else if (G == 16)
+    k_knn_estep<16><<<grid, kKnnWarps * 32, 0, st>>>(P);
+  else
+    k_knn_estep<8><<<grid, kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
   k_mstep_update<<<2 * P.max_gchunks, kMChunk, 0, st>>>(P);

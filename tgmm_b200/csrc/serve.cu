@@ -144,6 +144,7 @@ struct Lane {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
   bool busy = false;
+  bool tuned = false;  // the plan's kNN/E-step width tuned on the lane's first batch
   int launch_rc = TGMM_OK;
   int32_t batch_id = 0;
   std::vector<Request*> reqs;
@@ -288,6 +289,11 @@ void TgmmServer::launch(Lane& L) {
     L.g_off[i] = go;
     so += TGMM_J * S;
     go += L.n_gauss[i];
+  }
+  if (rc == TGMM_OK && !L.tuned) {
+    int32_t lanes = 0;
+    rc = tgmm_plan_autotune(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, 2, &lanes, L.st);
+    L.tuned = true;
   }
   if (rc == TGMM_OK)
     rc = tgmm_em_run_batch(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, nullptr, L.st);

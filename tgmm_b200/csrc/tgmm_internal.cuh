@@ -157,6 +157,7 @@ struct DevPlan {
   int32_t* dead_part;
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
   int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
+  int32_t knn_group;  // lanes per supervoxel of the kNN/E-step (8, 16 or 32)
   double* ec;   // per Gaussian E-step record, kEcStride doubles: nu W [6], m [3], 3/beta, psi(alpha)+eLD/2
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel

@@ -135,6 +135,23 @@ class Plan:
         return [stats_dict(x) for x in st] if st is not None else None
 
 
+    def set_knn_group(self, lanes: int):
+        L.check(self.lib.tgmm_plan_set_knn_group(self.h, lanes), "tgmm_plan_set_knn_group")
+
+    def autotune(self, frames, gms, rnks, inds, params: L.TgmmEmParams, reps: int = 3, stream=None) -> int:
+        """Times the kNN/E-step widths on this batch and keeps the fastest; returns it."""
+        n = len(frames)
+        cfs = (L.TgmmFrame * n)(*[f.cframe() for f in frames])
+        gp = (C.c_void_p * n)(*[g.data_ptr() for g in gms])
+        rp = (C.c_void_p * n)(*[r.data_ptr() for r in rnks])
+        ip = (C.c_void_p * n)(*[i.data_ptr() for i in inds])
+        out = C.c_int32()
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        L.check(self.lib.tgmm_plan_autotune(self.h, n, cfs, gp, rp, ip, C.byref(params), reps, C.byref(out), s),
+                "tgmm_plan_autotune")
+        return out.value
+
+
 def knn(query: torch.Tensor, ref_xyz: torch.Tensor, scale=(1.0, 1.0, 2.0), stream=None) -> torch.Tensor:
     """Exact 5-NN (scaled squared distance, ties to the lower index); ind[j*nq + q]."""
     nq = query.numel() // 3
