@@ -280,6 +280,7 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_vox": N, "n_sv": S, "n_gauss": K, "em_iterations": EM_ITERS,
                            "knn_lanes_per_supervoxel": knn_lanes,
+                           "knn_grid_searches_after_iteration_1": check["knn_searches"],
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (16 B x n_vox)",
                            "ll_precision": "mixed", "ll_mode": "as_reference"},
                 "voxel_iters_per_s": voxel_iters,

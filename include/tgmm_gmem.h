@@ -126,6 +126,10 @@ typedef struct TgmmEmStats {
   double total_alpha;       /* sum of alpha_k after the last kill step */
   int32_t n_dead;           /* dead Gaussians after the call */
   int32_t device_flags;     /* bit mask of device-side anomaly flags (0 = none) */
+  int32_t knn_searches;     /* supervoxel kNN grid searches after the first iteration: the
+                               later iterations take each supervoxel's five candidates from
+                               its list of 8 nearest unless its Gaussians moved too far */
+  int32_t reserved;
 } TgmmEmStats;
 
 /* ---- plans: all device workspace, sized once, reused by every call ---- */
@@ -229,9 +233,12 @@ int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* m
 int tgmm_plan_set_knn_group(TgmmPlan* plan, int32_t lanes);
 
 /* Autotuner: stages the batch (the arguments of tgmm_em_run_batch, whose Gaussians are
- * only read), runs its first iteration up to the kNN/E-step, times that kernel `reps`
- * times at each width and keeps the fastest in the plan (returned in *lanes_out).  rnk_dev
- * and ind_dev are overwritten; the results of later calls do not depend on the choice. */
+ * only read), runs its first iteration up to the kNN/E-step and times that kernel `reps`
+ * times at each width, both as in the first iteration (grid search) and as in a later one
+ * (candidates from the supervoxels' neighbour lists); the width with the least time for a
+ * call of min(max_iter_em, 20) iterations is kept in the plan (returned in *lanes_out).
+ * rnk_dev and ind_dev are overwritten; the results of later calls do not depend on the
+ * choice. */
 int tgmm_plan_autotune(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
                        TgmmGaussian* const* gm_dev, float* const* rnk_dev, int32_t* const* ind_dev,
                        const TgmmEmParams* params, int32_t reps, int32_t* lanes_out, void* stream);

@@ -41,6 +41,19 @@ def _perturb(frame, seed):
     return frame
 
 
+def _displace(frame, seed, sigma=3.0):
+    """Every Gaussian (mean and prior mean) starts sigma voxels off its nucleus: the first
+    iterations move them by voxels, so the supervoxels' kNN neighbour lists go stale and
+    are searched again."""
+    rng = np.random.default_rng(seed)
+    g = frame.gauss.copy()
+    shift = rng.normal(0, sigma, size=(g.shape[0], 3))
+    g["m_k"] += shift
+    g["m_o"] += shift
+    frame.gauss = g
+    return frame
+
+
 @functools.lru_cache(maxsize=None)
 def frame(name: str):
     if name == "tiny":
@@ -53,6 +66,8 @@ def frame(name: str):
         return _perturb(synth.generate(SPEC_HARD, seed=11), 11)
     if name == "big":
         return synth.generate(SPEC_BIG, seed=5)
+    if name == "moved":
+        return _displace(synth.generate(SPEC_SMALL, seed=21), 21)
     raise KeyError(name)
 
 

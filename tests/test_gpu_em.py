@@ -13,7 +13,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["tiny", "small", "c1", "hard", "big"]
+CASES = ["tiny", "small", "c1", "hard", "big", "moved"]
 RNK_TOL = 1e-5
 M_TOL = 1e-3
 W_RTOL = 1e-4
@@ -65,6 +65,17 @@ def compare(g, o, ll_rtol=1e-6):
 @pytest.mark.parametrize("iters", [1, 2, 20])
 def test_em_matches_fp64_oracle(cuda_ok, name, iters):
     compare(gpu_run(name, iters), oracle_run(name, iters))
+
+
+def test_knn_lists_and_searches(cuda_ok):
+    """After the first iteration a supervoxel's five candidates come from its list of the
+    eight nearest Gaussians unless they moved too far, when it searches the grid again;
+    the candidates match the oracle's either way (test_em_matches_fp64_oracle), and both
+    ways run on these frames."""
+    c1 = gpu_run("c1", 20)
+    assert 0 <= c1["knn_searches"] < F.frame("c1").n_sv  # most supervoxels never search again
+    moved = gpu_run("moved", 20)
+    assert moved["knn_searches"] > 0
 
 
 @pytest.mark.parametrize("name", ["tiny", "hard", "big"])

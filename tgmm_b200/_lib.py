@@ -85,7 +85,7 @@ class TgmmEmStats(C.Structure):
     _fields_ = [
         ("iterations", C.c_int32), ("converged", C.c_int32), ("ll", C.c_double), ("ll_true", C.c_double),
         ("ll_as_reference", C.c_double), ("total_alpha", C.c_double), ("n_dead", C.c_int32),
-        ("device_flags", C.c_int32),
+        ("device_flags", C.c_int32), ("knn_searches", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

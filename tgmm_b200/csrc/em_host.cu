@@ -39,7 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, work, sv_frame, sv_rec, mom, cand, rnk, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -69,12 +69,15 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.dead = take(4 * (int64_t)max_gchunks);
   L.ec = take(8 * kEcStride * G);
   L.llc = take(8 * 10 * G);
+  L.kpos = take(16 * G);
   L.work = take(64);
   L.sv_frame = take(4 * S);
   L.sv_rec = take((int64_t)sizeof(SvRec) * S);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(4 * S * kJ);
   L.rnk = take(4 * S * kJ);
+  L.nbr = take(4 * S * kNbr);
+  L.nbr_b = take(8 * S);
   L.llp = take(8 * 2 * S);
   L.gm_scratch = take((int64_t)sizeof(TgmmGaussian) * G);
   L.total = o;
@@ -185,6 +188,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.dead_part = (int32_t*)(b + P->L.dead);
   D.ec = (double*)(b + P->L.ec);
   D.llc = (double*)(b + P->L.llc);
+  D.kpos = (float4*)(b + P->L.kpos);
   D.work = (int32_t*)(b + P->L.work);
   D.knn_group = 8;
   e = configure_kernels(D, d->device);
@@ -197,6 +201,8 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);
   D.rnk = (float*)(b + P->L.rnk);
+  D.nbr = (int32_t*)(b + P->L.nbr);
+  D.nbr_b = (double*)(b + P->L.nbr_b);
   D.ll_part = (double*)(b + P->L.llp);
   *out = P;
   return TGMM_OK;
@@ -394,6 +400,8 @@ int collect_stats(TgmmPlan* P, int32_t n, TgmmEmStats* stats, cudaStream_t st, i
     o.total_alpha = S.total_alpha;
     o.n_dead = S.n_dead;
     o.device_flags = S.flags;
+    o.knn_searches = S.knn_searches;
+    o.reserved = 0;
   }
   if (flags_or) *flags_or = fo;
   return TGMM_OK;
@@ -422,6 +430,8 @@ int frame_state_to_stats(const void* state, TgmmEmStats* o) {
     o->total_alpha = S.total_alpha;
     o->n_dead = S.n_dead;
     o->device_flags = S.flags;
+    o->knn_searches = S.knn_searches;
+    o->reserved = 0;
   }
   int rc = TGMM_OK;
   if (S.flags & F_BAD_CSR)
@@ -511,22 +521,35 @@ int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, T
   rc = stage_tables(P, st);
   if (rc) return rc;
   // the batch's first iteration up to the kNN/E-step; that kernel is then timed at each
-  // width with its only lasting effect, the M-step bucket counts, cleared in between
+  // width with its only lasting effects, the M-step bucket counts (cleared in between) and
+  // the supervoxels' neighbour lists.  It is timed twice: as in the first iteration (the
+  // grid search, which builds the lists) and as in a later one (the frames' iteration
+  // counter set to 2: candidates from the lists).  A width scores as a call of
+  // min(max_iter, 20) iterations: one search and the rest from the lists.
   const DevPlan& D = P->dev;
   launch_build_maps(D, st);
   launch_import(D, st);
   launch_moments(D, st);
   TG_CUDA(cudaGetLastError(), "kernel launch");
+  const int nf = P->s_info.n_frames;
+  const std::vector<int32_t> iter_one(nf, 1), iter_two(nf, 2);
+  auto set_iter = [&](const std::vector<int32_t>& v) {
+    return cudaMemcpy2DAsync(&P->dev.state[0].iter, sizeof(FrameState), v.data(), sizeof(int32_t), sizeof(int32_t),
+                             nf, cudaMemcpyHostToDevice, st);
+  };
+  const double later = (double)std::max(0, std::min(params->max_iter_em, 20) - 1);
   const int widths[3] = {8, 16, 32};
-  float best_ms = 0.0f;
+  double best_score = 0.0;
   int best = P->dev.knn_group;
-  std::vector<cudaEvent_t> ev(2 * reps);
+  std::vector<cudaEvent_t> ev(4 * reps);
   for (auto& e : ev) TG_CUDA(cudaEventCreate(&e), "event");
   for (int w : widths) {
     P->dev.knn_group = w;
+    TG_CUDA(set_iter(iter_one), "set iteration");
     launch_knn_estep(P->dev, st);  // warm-up
     TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
-    for (int r = 0; r < reps; r++) {
+    for (int r = 0; r < 2 * reps; r++) {
+      if (r == reps) TG_CUDA(set_iter(iter_two), "set iteration");
       TG_CUDA(cudaEventRecord(ev[2 * r], st), "record");
       launch_knn_estep(P->dev, st);
       TG_CUDA(cudaEventRecord(ev[2 * r + 1], st), "record");
@@ -534,14 +557,15 @@ int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, T
     }
     TG_CUDA(cudaGetLastError(), "kernel launch");
     TG_CUDA(cudaStreamSynchronize(st), "synchronize");
-    float total = 0.0f;
-    for (int r = 0; r < reps; r++) {
+    double search = 0.0, listed = 0.0;
+    for (int r = 0; r < 2 * reps; r++) {
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]);
-      total += ms;
+      (r < reps ? search : listed) += ms;
     }
-    if (w == widths[0] || total < best_ms) {
-      best_ms = total;
+    const double score = search + later * listed;
+    if (w == widths[0] || score < best_score) {
+      best_score = score;
       best = w;
     }
   }

@@ -90,29 +90,35 @@ __device__ __forceinline__ int block_sum_gchunk_i(int v, int* sh) {
 //   a = (q0 - r0) * s0;  d = a*a;  b = (q1 - r1) * s1;  d = fma(b, b, d);  c = ...; d = fma(c, c, d)
 // Order: (d, index) ascending, NaN as +inf -> ties go to the lower index.
 // ---------------------------------------------------------------------------
-struct Top5 {
-  float d[kJ];
-  int i[kJ];
+// The N nearest found so far, sorted in (d, index) order; unused slots hold (+inf, INT_MAX).
+template <int N>
+struct TopN {
+  float d[N];
+  int i[N];
 };
+using Top5 = TopN<kJ>;
 
-__device__ __forceinline__ void top5_init(Top5& t) {
+template <int N>
+__device__ __forceinline__ void topn_init(TopN<N>& t) {
 #pragma unroll
-  for (int j = 0; j < kJ; j++) {
+  for (int j = 0; j < N; j++) {
     t.d[j] = kInfF;
     t.i[j] = 0x7fffffff;
   }
 }
+__device__ __forceinline__ void top5_init(Top5& t) { topn_init<kJ>(t); }
 
 __device__ __forceinline__ bool before(float da, int ia, float db, int ib) {
   return da < db || (da == db && ia < ib);
 }
 
-__device__ __forceinline__ void top5_insert(Top5& t, float d, int idx) {
-  if (!before(d, idx, t.d[kJ - 1], t.i[kJ - 1])) return;
-  t.d[kJ - 1] = d;
-  t.i[kJ - 1] = idx;
+template <int N>
+__device__ __forceinline__ void topn_insert(TopN<N>& t, float d, int idx) {
+  if (!before(d, idx, t.d[N - 1], t.i[N - 1])) return;
+  t.d[N - 1] = d;
+  t.i[N - 1] = idx;
 #pragma unroll
-  for (int p = kJ - 1; p > 0; --p) {
+  for (int p = N - 1; p > 0; --p) {
     if (before(t.d[p], t.i[p], t.d[p - 1], t.i[p - 1])) {
       float td = t.d[p];
       t.d[p] = t.d[p - 1];
@@ -123,6 +129,7 @@ __device__ __forceinline__ void top5_insert(Top5& t, float d, int idx) {
     }
   }
 }
+__device__ __forceinline__ void top5_insert(Top5& t, float d, int idx) { topn_insert<kJ>(t, d, idx); }
 
 __device__ __forceinline__ float knn_dist(float q0, float q1, float q2, float r0, float r1,
                                           float r2, const float* s) {
@@ -314,6 +321,9 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
     if (D.n_gauss < kJ) flags |= F_FEW_GAUSS;
     set_geometry(S, lo, hi, D.n_gauss, D.cell_budget);
     S->iter = 1;
+    S->disp_cum = 0.0;
+    S->disp_max = 0u;
+    S->knn_searches = 0;
     S->done = (flags & (F_BAD_CSR | F_FEW_GAUSS)) ? 1 : 0;
     S->converged = 0;
     S->flags = flags;
@@ -352,9 +362,11 @@ __device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc&
 // log-likelihood record (-nu W/2 with doubled off-diagonals, the log weight
 // 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the mean), and the Gaussian's float centre
 // inserted into its grid cell (capacity kCellCap; a full cell flags the frame, whose kNN
-// then scans every Gaussian).
-__device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
-                                              int k, int parity) {
+// then scans every Gaussian).  The float centre is also kept in kpos; with `track`, the
+// return value is how far it moved since the last preparation (scaled distance, 0 unless
+// the Gaussian was live both times), which bounds the kNN neighbour lists.
+__device__ __forceinline__ double prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
+                                                int k, int parity, bool track) {
   const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
   double W[6];
 #pragma unroll
@@ -385,10 +397,21 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
   L[7] = m[0];
   L[8] = m[1];
   L[9] = m[2];
+  const float x = __double2float_rn(m[0]);
+  const float y = __double2float_rn(m[1]);
+  const float z = __double2float_rn(m[2]);
+  double move = 0.0;
+  if (track && !dead) {
+    const float4 o = P.kpos[k];
+    if (o.w != 0.0f) {
+      const double a = ((double)x - (double)o.x) * (double)D.scale[0];
+      const double b = ((double)y - (double)o.y) * (double)D.scale[1];
+      const double c = ((double)z - (double)o.z) * (double)D.scale[2];
+      move = sqrt(a * a + b * b + c * c);
+    }
+  }
+  P.kpos[k] = make_float4(x, y, z, dead ? 0.0f : 1.0f);
   if (!dead) {
-    const float x = __double2float_rn(m[0]);
-    const float y = __double2float_rn(m[1]);
-    const float z = __double2float_rn(m[2]);
     const int cell = ref_cell_of(S, D, x, y, z);
     if (cell >= 0) {
       const int g = D.cell_base + cell;
@@ -399,6 +422,7 @@ __device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc&
         atomicOr(&P.state[D.frame_id].flags, F_CELL_OVERFLOW);
     }
   }
+  return move;
 }
 
 // Run by the last Gaussian chunk of a frame to finish (import or kill step): the alpha
@@ -419,6 +443,8 @@ __device__ void frame_tail(const DevPlan& P, int f, int next_parity) {
       S->psi_total[next_parity] = digamma(a);
       S->n_dead = nd;
       S->blk_done = 0;
+      S->disp_cum += (double)__uint_as_float(S->disp_max);
+      S->disp_max = 0u;
     }
   }
 }
@@ -469,7 +495,7 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
     for (int d = 0; d < 3; d++) bad = bad || isnan(g.m_k[d]);
     for (int e = 0; e < 6; e++) bad = bad || isnan(g.W_k[e]);
     if (bad) atomicOr(&P.state[ch.frame].flags, F_NAN_INPUT);
-    prep_gaussian(P, D, S, k, 1);
+    prep_gaussian(P, D, S, k, 1, false);
     alpha = gcomp(P, G_ALPHA, k);
     dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
   }
@@ -622,11 +648,11 @@ __device__ __forceinline__ void group_min_pair(float& d, int& i, unsigned gmask)
   }
 }
 
-// merge the group's sorted lists into its top-5 (identical in every lane of the group)
-template <int G>
-__device__ __forceinline__ void group_merge_top5(Top5& mine, Top5& out, unsigned gmask) {
+// merge the group's sorted lists into its top-N (identical in every lane of the group)
+template <int G, int N>
+__device__ __forceinline__ void group_merge_topn(TopN<N>& mine, TopN<N>& out, unsigned gmask) {
 #pragma unroll
-  for (int r = 0; r < kJ; r++) {
+  for (int r = 0; r < N; r++) {
     float d = mine.d[0];
     int i = mine.i[0];
     group_min_pair<G>(d, i, gmask);
@@ -634,12 +660,12 @@ __device__ __forceinline__ void group_merge_top5(Top5& mine, Top5& out, unsigned
     out.i[r] = i;
     if (mine.i[0] == i && mine.d[0] == d && i != 0x7fffffff) {  // pop the front of the winner
 #pragma unroll
-      for (int q = 0; q < kJ - 1; q++) {
+      for (int q = 0; q < N - 1; q++) {
         mine.d[q] = mine.d[q + 1];
         mine.i[q] = mine.i[q + 1];
       }
-      mine.d[kJ - 1] = kInfF;
-      mine.i[kJ - 1] = 0x7fffffff;
+      mine.d[N - 1] = kInfF;
+      mine.i[N - 1] = 0x7fffffff;
     }
   }
 }
@@ -658,12 +684,12 @@ __device__ __forceinline__ void group_max_pair(float& d, int& i, unsigned gmask)
   }
 }
 
-// (td0, ti0): a (distance, index) no smaller than the true fifth neighbour's (the fifth of
-// five known Gaussians), or +inf; refs after it in (distance, index) order cannot be among
-// the five and are rejected without an insertion.
-template <int G>
+// Exact N nearest over the grid rings.  (td0, ti0): a (distance, index) no smaller than
+// the true N-th neighbour's (the N-th of N known Gaussians), or +inf; refs after it in
+// (distance, index) order cannot be among the N and are rejected without an insertion.
+template <int G, int N>
 __device__ void knn_group_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
-                                 const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, Top5& best,
+                                 const int32_t* __restrict__ ccnt, const float4* __restrict__ refs, TopN<N>& best,
                                  unsigned gmask, int gl, float td0, int ti0) {
   const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
   int c[3];
@@ -676,24 +702,24 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
     delta = fminf(delta, fminf(f0, f1));
   }
   delta = fmaxf(delta, 0.0f);
-  top5_init(best);
+  topn_init<N>(best);
   const int maxr = max(1, max(g.dims[0], max(g.dims[1], g.dims[2])));
   // the first pass covers rings 0 and 1 (27 cells), later passes one ring
   for (int r = 1; r <= maxr; ++r) {
-    Top5 t;
-    top5_init(t);
-    // prune with the group's current fifth (or the starting bound): a ref must not come
+    TopN<N> t;
+    topn_init<N>(t);
+    // prune with the group's current N-th (or the starting bound): a ref must not come
     // after it to matter
-    const bool use_best = before(best.d[kJ - 1], best.i[kJ - 1], td0, ti0);
-    const float td = use_best ? best.d[kJ - 1] : td0;
-    const int ti = use_best ? best.i[kJ - 1] : ti0;
+    const bool use_best = before(best.d[N - 1], best.i[N - 1], td0, ti0);
+    const float td = use_best ? best.d[N - 1] : td0;
+    const int ti = use_best ? best.i[N - 1] : ti0;
     auto scan_refs = [&](int cell, int e) {
       const float4* cr = refs + (int64_t)cell * kCellCap;
       for (int k = 0; k < e; ++k) {
         const float4 rr = cr[k];
         const float d = knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s);
         const int id = __float_as_int(rr.w);
-        if (!before(td, ti, d, id)) top5_insert(t, d, id);
+        if (!before(td, ti, d, id)) topn_insert<N>(t, d, id);
       }
     };
     auto scan_cell = [&](int dx, int dy, int dz) {
@@ -739,16 +765,16 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
     // lane 0 of the group also carries the previous best (disjoint from this ring's refs)
     if (gl == 0) {
 #pragma unroll
-      for (int q = 0; q < kJ; q++) top5_insert(t, best.d[q], best.i[q]);
+      for (int q = 0; q < N; q++) topn_insert<N>(t, best.d[q], best.i[q]);
     }
-    Top5 merged;
-    group_merge_top5<G>(t, merged, gmask);
+    TopN<N> merged;
+    group_merge_topn<G, N>(t, merged, gmask);
     best = merged;
     const float lb = r * g.h + delta;
     const float eps = 4e-3f + 1e-6f * lb;
     if (lb > eps) {
       const float bound = (lb - eps) * (lb - eps);
-      if (best.d[kJ - 1] < bound) break;
+      if (best.d[N - 1] < bound) break;
     }
   }
 }
@@ -776,46 +802,77 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
   }
   g.h = S.h;
   g.inv_h = S.inv_h;
-  Top5 t;
-  top5_init(t);
   const bool grid_ok = !(S.flags & F_CELL_OVERFLOW);
-  // starting bound from the previous iteration's five candidates (their current centres;
-  // a candidate that died is at +inf): the fifth of them in (distance, index) order
-  float td0 = kInfF;
-  int ti0 = 0x7fffffff;
+  const double disp = S.disp_cum;
+  Top5 t;
+  // After the first iteration: the supervoxel's neighbour list, the kNbr nearest Gaussians
+  // when it was last searched (at displacement bound disp_b), member i on lane i.  A
+  // Gaussian outside the list was then at scaled distance >= rho from the centroid and has
+  // since moved at most disp - disp_b, so the five nearest members (current centres, the
+  // same FP32 distances and (distance, index) order) are the exact five nearest whenever
+  //   sqrt(d5) (1 + 1e-6) + disp < nbr_b = rho (1 - 1e-6) - 4e-3 + disp_b;
+  // the margins cover the FP32 rounding of the distances.  Otherwise the supervoxel runs
+  // the exact search for the kNbr nearest and keeps them as its new list.
+  int lk = 0x7fffffff;
+  float ld = kInfF;
+  bool have = false;
   if (S.iter > 1) {
-    float dj = -1.0f;  // lanes without a candidate never win the arg-max
-    int ij = -1;
-    if (gl < kJ) {
-      const int kp = P.cand[(int64_t)s * kJ + gl];
-      if (kp >= D.g_base && kp < D.g_base + D.n_gauss) {
-        dj = knn_dist(q0, q1, q2, __double2float_rn(gcomp(P, G_M0, kp)), __double2float_rn(gcomp(P, G_M1, kp)),
-                      __double2float_rn(gcomp(P, G_M2, kp)), D.scale);
-        ij = kp - D.g_base;
-      } else {
-        dj = kInfF;
-        ij = 0x7fffffff;
+    if (gl < kNbr) {
+      lk = P.nbr[(int64_t)s * kNbr + gl];
+      if (lk != 0x7fffffff) {
+        const float4 r = P.kpos[D.g_base + lk];
+        ld = knn_dist(q0, q1, q2, r.x, r.y, r.z, D.scale);
       }
     }
-    group_max_pair<G>(dj, ij, gmask);
-    td0 = dj;
-    ti0 = ij;
+    Top5 mine;
+    top5_init(mine);
+    mine.d[0] = ld;
+    mine.i[0] = lk;
+    group_merge_topn<G, kJ>(mine, t, gmask);
+    have = t.d[kJ - 1] < kInfF && sqrt((double)t.d[kJ - 1]) * (1.0 + 1e-6) + disp < P.nbr_b[s];
   }
-  if (grid_ok)
-    knn_group_search<G>(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base, P.cell_refs + (int64_t)D.cell_base * kCellCap,
-                     t, gmask, gl, td0, ti0);
-  if (!grid_ok || !(t.d[kJ - 1] < kInfF)) {
-    // fewer than five finite distances: exact scan of every Gaussian of the frame
-    Top5 m;
-    top5_init(m);
-    for (int kl = gl; kl < D.n_gauss; kl += G) {
-      const int k = D.g_base + kl;
-      const float x = __double2float_rn(gcomp(P, G_M0, k));
-      const float y = __double2float_rn(gcomp(P, G_M1, k));
-      const float z = __double2float_rn(gcomp(P, G_M2, k));
-      top5_insert(m, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
+  if (!have) {
+    // starting bound: the kNbr-th of the list members at their current centres
+    float td0 = kInfF;
+    int ti0 = 0x7fffffff;
+    if (S.iter > 1) {
+      float dj = gl < kNbr ? ld : -1.0f;  // lanes without a member never win the arg-max
+      int ij = gl < kNbr ? lk : -1;
+      group_max_pair<G>(dj, ij, gmask);
+      td0 = dj;
+      ti0 = ij;
+      if (gl == 0) atomicAdd(&P.state[f].knn_searches, 1);
     }
-    group_merge_top5<G>(m, t, gmask);
+    TopN<kNbr> nb;
+    topn_init<kNbr>(nb);
+    if (grid_ok)
+      knn_group_search<G, kNbr>(q0, q1, q2, D.scale, g, P.cell_cnt + D.cell_base,
+                                P.cell_refs + (int64_t)D.cell_base * kCellCap, nb, gmask, gl, td0, ti0);
+    if (!grid_ok || !(nb.d[kJ - 1] < kInfF)) {
+      // fewer than five finite distances: exact scan of every Gaussian of the frame
+      TopN<kNbr> m;
+      topn_init<kNbr>(m);
+      for (int kl = gl; kl < D.n_gauss; kl += G) {
+        const int k = D.g_base + kl;
+        const float x = __double2float_rn(gcomp(P, G_M0, k));
+        const float y = __double2float_rn(gcomp(P, G_M1, k));
+        const float z = __double2float_rn(gcomp(P, G_M2, k));
+        topn_insert<kNbr>(m, knn_dist(q0, q1, q2, x, y, z, D.scale), kl);
+      }
+      group_merge_topn<G, kNbr>(m, nb, gmask);
+    }
+#pragma unroll
+    for (int j = 0; j < kJ; j++) {
+      t.d[j] = nb.d[j];
+      t.i[j] = nb.i[j];
+    }
+    int mi = 0x7fffffff;
+#pragma unroll
+    for (int q = 0; q < kNbr; q++)
+      if (gl == q) mi = nb.i[q];
+    if (gl < kNbr) P.nbr[(int64_t)s * kNbr + gl] = mi;
+    if (gl == 0)
+      P.nbr_b[s] = nb.d[kNbr - 1] < kInfF ? sqrt((double)nb.d[kNbr - 1]) * (1.0 - 1e-6) - 4e-3 + disp : (double)kInfF;
   }
   // E-step: candidate j on lane j of the group
   const int par = S.iter & 1;
@@ -1088,7 +1145,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   const double total = s_total;
   const int cur = S.iter & 1, nxt = (S.iter + 1) & 1;
   const int k = ch.g_begin + threadIdx.x;
-  double alpha = 0.0;
+  double alpha = 0.0, move = 0.0;
   int dead = 0;
   if (k < ch.g_end) {
     bool nanw = isnan(gcomp(P, G_ELD0 + cur, k));
@@ -1103,12 +1160,17 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
       const double I6[6] = {1, 0, 0, 1, 0, 1};
       for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = I6[e];
     }
-    prep_gaussian(P, D, S, k, nxt);
+    move = prep_gaussian(P, D, S, k, nxt, true);
     alpha = gcomp(P, G_ALPHA, k);
     dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
   }
   const double at = block_sum_gchunk(alpha, shd);
   const int nd = block_sum_gchunk_i(dead, shi);
+  // the chunk's largest move, rounded up to a float: non-negative floats order as their bits
+  float mv = __double2float_ru(move);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+  if ((threadIdx.x & 31) == 0 && mv > 0.0f) atomicMax(&P.state[ch.frame].disp_max, __float_as_uint(mv));
   if (threadIdx.x == 0) {
     P.alpha_part_f[c] = at;
     P.dead_part[c] = nd;

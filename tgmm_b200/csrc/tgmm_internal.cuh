@@ -33,6 +33,7 @@ constexpr int kSvPerBlockV = kWarpsPerBlockV * kSvPerWarpV;
 constexpr int kNumMoments = 19;
 constexpr int kFrameThreads = 1024;
 constexpr int kCellCap = 32;   // Gaussian centres per kNN grid cell
+constexpr int kNbr = 8;        // Gaussians kept per supervoxel in its kNN neighbour list
 constexpr int kEcStride = 12;  // doubles per E-step record
 
 // moment component indices
@@ -97,6 +98,12 @@ struct FrameState {
   unsigned long long ll_frac[2];
   int32_t sv_done;   // supervoxels finished in this iteration's voxel pass
   int32_t blk_done;  // Gaussian chunks finished in this iteration's kill step
+  // kNN neighbour lists: disp_cum bounds how far any live Gaussian's float centre has moved
+  // (scaled units) since the call began, as the sum over iterations of the largest move of
+  // one iteration; disp_max is the current iteration's largest move (float bits, rounded up)
+  double disp_cum;
+  uint32_t disp_max;
+  int32_t knn_searches;  // supervoxel grid searches after the first iteration (list misses)
 };
 
 // Voxel tiles of the per-iteration voxel pass: kVoxTile voxels of a supervoxel per copy.
@@ -158,6 +165,7 @@ struct DevPlan {
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
   int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
   int32_t knn_group;  // lanes per supervoxel of the kNN/E-step (8, 16 or 32)
+  float4* kpos;  // per Gaussian: the float centre the kNN sees (x, y, z; w = 1 live, 0 dead)
   double* ec;   // per Gaussian E-step record, kEcStride doubles: nu W [6], m [3], 3/beta, psi(alpha)+eLD/2
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
@@ -166,6 +174,8 @@ struct DevPlan {
   double* mom;
   int32_t* cand;
   float* rnk;
+  int32_t* nbr;    // [max_sv][kNbr]: the supervoxel's kNbr nearest Gaussians when last searched
+  double* nbr_b;   // validity bound of that list (see k_knn_estep)
   double* ll_part;  // [2][max_sv]
 };
 

@@ -61,7 +61,7 @@ def gauss_from_device(t: torch.Tensor) -> np.ndarray:
 def stats_dict(st: L.TgmmEmStats) -> dict:
     return dict(iterations=st.iterations, converged=st.converged, ll=st.ll, ll_true=st.ll_true,
                 ll_as_reference=st.ll_as_reference, total_alpha=st.total_alpha, n_dead=st.n_dead,
-                device_flags=st.device_flags)
+                device_flags=st.device_flags, knn_searches=st.knn_searches)
 
 
 class Plan:
