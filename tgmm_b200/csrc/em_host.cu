@@ -39,7 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_order, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -72,6 +72,7 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.kpos = take(16 * G);
   L.work = take(64);
   L.sv_frame = take(4 * S);
+  L.sv_order = take(4 * S);
   L.sv_rec = take((int64_t)sizeof(SvRec) * S);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(4 * S * kJ);
@@ -197,6 +198,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
     return fail(TGMM_ERR_CUDA, "tgmm_plan_create: kernel configuration", e);
   }
   D.sv_frame = (int32_t*)(b + P->L.sv_frame);
+  D.sv_order = (int32_t*)(b + P->L.sv_order);
   D.sv_rec = (SvRec*)(b + P->L.sv_rec);
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);
@@ -340,6 +342,7 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
   const DevPlan& D = P->dev;
   launch_build_maps(D, st);
   launch_import(D, st);
+  launch_order(D, st);
   launch_moments(D, st);
   for (int it = 0; it < max_iter; it++) {
     launch_knn_estep(D, st);
@@ -529,6 +532,7 @@ int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, T
   const DevPlan& D = P->dev;
   launch_build_maps(D, st);
   launch_import(D, st);
+  launch_order(D, st);
   launch_moments(D, st);
   TG_CUDA(cudaGetLastError(), "kernel launch");
   const int nf = P->s_info.n_frames;

@@ -509,6 +509,47 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
 }
 
 // ===========================================================================
+// order: once per call.  The supervoxels of each frame by descending tile count (counting
+// sort, ties in any order), frames in batch order.  The per-iteration voxel pass takes
+// supervoxels in this order, so a frame's last supervoxels are its smallest and no warp is
+// left with a large one after the others ran out of work.  Its sums do not depend on the
+// order.  (The once-per-call moment pass keeps the memory order: neighbouring warps read
+// neighbouring voxels.)
+// ===========================================================================
+constexpr int kOrderBuckets = 64;  // tile counts 0..62, and 63 or more
+
+__device__ __forceinline__ int order_bucket(const FrameDesc& D, int sl) {
+  const int64_t a = D.lptr[sl], b = D.lptr[sl + 1];
+  const int64_t nv = (a < 0 || b < a || b > D.n_vox) ? 0 : b - a;
+  const int64_t nt = (nv + kVoxTile - 1) / kVoxTile;
+  return nt < kOrderBuckets - 1 ? (int)nt : kOrderBuckets - 1;
+}
+
+__global__ void __launch_bounds__(1024) k_order(DevPlan P) {
+  __shared__ int base[kOrderBuckets];
+  const int nf = P.info->n_frames;
+  for (int f = 0; f < nf; f++) {
+    const FrameDesc D = load_desc(P, f);
+    if (threadIdx.x < kOrderBuckets) base[threadIdx.x] = 0;
+    __syncthreads();
+    for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x) atomicAdd(&base[order_bucket(D, sl)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int b = kOrderBuckets - 1; b >= 0; b--) {
+        const int c = base[b];
+        base[b] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x)
+      P.sv_order[D.sv_base + atomicAdd(&base[order_bucket(D, sl)], 1)] = D.sv_base + sl;
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
 // moments: once per call.  Warp per supervoxel; centred at the supervoxel centroid
 // c_s: per-voxel differences e = x - c_s in FP32, accumulation in FP64 (B200 runs
 // FP64 at half the FP32 rate, cheaper here than compensated FP32).  19 moments:
@@ -1294,8 +1335,15 @@ __device__ __forceinline__ double voxel_ll_fp64(const LLShared64& C, float x0, f
 }
 
 // --- TMA bulk staging --------------------------------------------------------
-constexpr int kLLTile = kVoxTile;             // voxels per tile (8 per lane)
-constexpr int kLLStages = 3;                  // tile slots per warp
+#ifndef TGMM_LL_STAGES
+#define TGMM_LL_STAGES 3
+#endif
+#ifndef TGMM_LL_BLOCKS
+#define TGMM_LL_BLOCKS 2
+#endif
+constexpr int kLLTile = kVoxTile;             // voxels per tile (kVoxTile / 32 per lane)
+constexpr int kLLStages = TGMM_LL_STAGES;     // tile slots per warp
+constexpr int kLLBlocks = TGMM_LL_BLOCKS;     // resident blocks per SM the pass is compiled for
 constexpr int kLLSpan = kLLTile + 4;          // floats per component in a slot (16-byte slack)
 constexpr int kLLSlotFloats = 4 * kLLSpan;    // x, y, z, I
 constexpr unsigned long long kLLWaitNs = 1000000000ull;  // a slot not filled within 1 s counts as lost
@@ -1391,7 +1439,7 @@ constexpr int kLLWarpBytes = (kLLCandOff + (int)sizeof(CandF) + 15) / 16 * 16;
 constexpr size_t kLLSmemBytes = (size_t)kLLWarpBytes * kWarpsPerBlockV;
 static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOff % 16 == 0 && kLLCandOff % 16 == 0,
               "slots and records stay 16-byte aligned");
-static_assert(2 * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "two blocks of the voxel pass fit an SM");
+static_assert(kLLBlocks * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "the voxel pass's blocks fit an SM");
 
 // Stage A: the record and candidate ids of supervoxel s.
 __device__ __forceinline__ void ll_fetch_a(const DevPlan& P, LLRec& X, int s) {
@@ -1475,7 +1523,7 @@ __device__ __forceinline__ double ll_walk_back(const Eval& eval, const SvRec& R,
   return 0.0;
 }
 
-// The kept tiles (bit t - (nt - 4) of `mask`) that hold voxels of zero density, after the
+// The kept tiles (bit t - (nt - kKeptTiles) of `mask`) that hold voxels of zero density, after the
 // supervoxel's tiles: their voxels are read again from global memory and each one of zero
 // density adds the walk-back value.  Rare.
 template <class Eval>
@@ -1486,9 +1534,9 @@ __device__ __forceinline__ double ll_fixup(const Eval& eval, const SvRec& R, uns
 #pragma unroll
   for (int c = 0; c < 4; c++) v[c] = reinterpret_cast<const float*>(R.lo0[c]) + ((R.nf[c] >> 16) & 3);
   double add = 0.0;
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < kKeptTiles; k++) {
     if (!(mask & (1u << k))) continue;
-    const int t = R.ntiles - 4 + k;
+    const int t = R.ntiles - kKeptTiles + k;
     const int start = t == 0 ? 0 : R.r0 + (t - 1) * kLLTile;
     const int rem = t == 0 ? R.r0 : kLLTile;
     for (int o = lane; o < rem; o += 32) {
@@ -1501,7 +1549,7 @@ __device__ __forceinline__ double ll_fixup(const Eval& eval, const SvRec& R, uns
 }
 
 // Tile t (landed in `slot`) of the current supervoxel: its sum goes to lt, and to lr when
-// the tile is one of the last four (the reference's kept window of 1024 voxels).  A kept
+// the tile is one of the last kKeptTiles (the reference's kept window of 1024 voxels).  A kept
 // tile of a supervoxel above 1024 voxels with a voxel of zero density is marked in fix.
 template <class Eval>
 __device__ __forceinline__ void ll_consume(const Eval& eval, const float* slot, const int* pk, int t, int nt, int nv,
@@ -1518,9 +1566,9 @@ __device__ __forceinline__ void ll_consume(const Eval& eval, const float* slot, 
   else
     ll_tile<Eval, false>(eval, slot, sht, rem, c0, c1, c2, tsum, allok);
   lt += (double)tsum;
-  if (t >= nt - 4) {
+  if (t >= nt - kKeptTiles) {
     lr += (double)tsum;
-    if (nv > 1024 && __any_sync(0xffffffffu, !allok)) fix |= 1u << (t - (nt - 4));
+    if (nv > 1024 && __any_sync(0xffffffffu, !allok)) fix |= 1u << (t - (nt - kKeptTiles));
   }
 }
 
@@ -1572,7 +1620,7 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // them (with the count of supervoxels) when its frame changes and when it leaves; the
 // warp that completes a frame's count runs the convergence test.
 template <bool kFp64>
-__global__ void __launch_bounds__(kWarpsPerBlockV * 32, 2) k_ll_pass(DevPlan P) {
+__global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ LLShared64 sh64[kFp64 ? kWarpsPerBlockV : 1];
@@ -1616,12 +1664,17 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, 2) k_ll_pass(DevPlan P) 
   FrameState* S = nullptr;
   bool failed = false;
   // tickets: the current, the next, and (lane 0) the one after
+  // a ticket t is the supervoxel sv_order[t] (each frame's largest first), total at the end
+  auto take = [&]() {
+    const int t = atomicAdd(&P.work[0], 1);
+    return t < total ? P.sv_order[t] : total;
+  };
   int tk = 0;
-  if (lane == 0) tk = atomicAdd(&P.work[0], 1);
+  if (lane == 0) tk = take();
   int sc = __shfl_sync(0xffffffffu, tk, 0);
-  if (lane == 0 && sc < total) tk = atomicAdd(&P.work[0], 1);
+  if (lane == 0 && sc < total) tk = take();
   int sn = sc < total ? __shfl_sync(0xffffffffu, tk, 0) : total;
-  if (lane == 0 && sn < total) tk = atomicAdd(&P.work[0], 1);
+  if (lane == 0 && sn < total) tk = take();
   if (sc < total) {
     ll_fetch_a(P, RA[0], sc);
     if (sn < total) ll_fetch_a(P, RA[1], sn);
@@ -1639,7 +1692,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, 2) k_ll_pass(DevPlan P) 
     const LLConst& CB = RB[i & 1];
     const LLRec& NA = RA[(i + 1) % 3];
     const int s2 = __shfl_sync(0xffffffffu, tk, 0);
-    if (lane == 0 && s2 < total) tk = atomicAdd(&P.work[0], 1);
+    if (lane == 0 && s2 < total) tk = take();
     if (sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
     if (s2 < total) ll_fetch_a(P, RA[(i + 2) % 3], s2);
     cp_commit();
@@ -1870,6 +1923,7 @@ void launch_build_maps(const DevPlan& P, cudaStream_t st) {
   k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
 }
 void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
+void launch_order(const DevPlan& P, cudaStream_t st) { k_order<<<1, 1024, 0, st>>>(P); }
 void launch_moments(const DevPlan& P, cudaStream_t st) {
   k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
 }

@@ -106,13 +106,19 @@ struct FrameState {
   int32_t knn_searches;  // supervoxel grid searches after the first iteration (list misses)
 };
 
-// Voxel tiles of the per-iteration voxel pass: kVoxTile voxels of a supervoxel per copy.
-constexpr int kVoxTile = 256;
+// Voxel tiles of the per-iteration voxel pass: kVoxTile voxels of a supervoxel per copy;
+// the reference's kept window of a supervoxel's last 1024 voxels is its last kKeptTiles.
+#ifndef TGMM_VOX_TILE
+#define TGMM_VOX_TILE 256
+#endif
+constexpr int kVoxTile = TGMM_VOX_TILE;
+constexpr int kKeptTiles = 1024 / kVoxTile;
+static_assert(kVoxTile >= 32 && kVoxTile % 32 == 0 && 1024 % kVoxTile == 0, "tiles split the kept window evenly");
 
 // Per-supervoxel stream record of the voxel pass, built once per call (k_moments).
 // Tiles are aligned to the END of the supervoxel: tile 0 holds its first r0 voxels
 // (1 <= r0 <= kVoxTile) and every later tile kVoxTile voxels, so the reference's kept
-// window of the last 1024 voxels is exactly the last four tiles.  Component c (x, y, z,
+// window of the last 1024 voxels is exactly the last kKeptTiles tiles.  Component c (x, y, z,
 // I) of tile 0 is the 16-byte aligned span [lo0[c], + n0[c]); of tile t >= 1 the span
 // [lo1[c] + 4 kVoxTile (t - 1), + (nf[c] & 0xffff)).  The first voxel of tile 0 sits
 // (nf[c] >> 16) & 3 floats into its span, that of the later tiles (nf[c] >> 20) & 3.
@@ -170,6 +176,7 @@ struct DevPlan {
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
   int32_t* sv_frame;
+  int32_t* sv_order;  // the order in which the voxel passes take supervoxels (k_order)
   SvRec* sv_rec;
   double* mom;
   int32_t* cand;
@@ -199,6 +206,7 @@ __device__ __forceinline__ double& gcomp(const DevPlan& P, int c, int k) {
 // ---- kernel launchers (em_kernels.cu) ----
 void launch_build_maps(const DevPlan& P, cudaStream_t st);
 void launch_import(const DevPlan& P, cudaStream_t st);
+void launch_order(const DevPlan& P, cudaStream_t st);
 void launch_moments(const DevPlan& P, cudaStream_t st);
 void launch_knn_estep(const DevPlan& P, cudaStream_t st);
 void launch_mstep_update(const DevPlan& P, cudaStream_t st);
