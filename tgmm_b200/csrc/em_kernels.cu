@@ -357,23 +357,16 @@ __device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc&
   return (cz * S.dims[1] + cy) * S.dims[0] + cx;
 }
 
-// Per-Gaussian preparation for the next iteration: psi(alpha), E[ln|Lambda|], the E-step
-// record (nu W, m, 3/beta, psi(alpha) + E[ln|Lambda|]/2, or -inf for a dead Gaussian), the
-// log-likelihood record (-nu W/2 with doubled off-diagonals, the log weight
-// 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the mean), and the Gaussian's float centre
-// inserted into its grid cell (capacity kCellCap; a full cell flags the frame, whose kNN
-// then scans every Gaussian).  The float centre is also kept in kpos; with `track`, the
-// return value is how far it moved since the last preparation (scaled distance, 0 unless
-// the Gaussian was live both times), which bounds the kNN neighbour lists.
-__device__ __forceinline__ double prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S,
-                                                int k, int parity, bool track) {
-  const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
-  double W[6];
-#pragma unroll
-  for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
-  const double nu = gcomp(P, G_NU, k);
-  const double alpha = gcomp(P, G_ALPHA, k);
-  const double m[3] = {gcomp(P, G_M0, k), gcomp(P, G_M1, k), gcomp(P, G_M2, k)};
+// The next iteration's records of Gaussian k from its parameters: psi(alpha) and
+// E[ln|Lambda|] (in the parity slot), the E-step record (nu W, m, 3/beta, psi(alpha) +
+// E[ln|Lambda|]/2, or -inf for a dead Gaussian), the log-likelihood record (-nu W/2 with
+// doubled off-diagonals, the log weight 1/2 ln(det W nu^3) - 3/2 ln(2 pi) + ln(alpha), the
+// mean) and the float centre the kNN sees (kpos).  With `track`, returns how far that
+// centre moved since the previous record (scaled distance, 0 unless live both times),
+// which bounds the kNN neighbour lists.
+__device__ __forceinline__ double write_records(const DevPlan& P, const FrameDesc& D, int k, int parity, bool dead,
+                                                const double* W, double nu, double alpha, double beta,
+                                                const double* m, bool track) {
   const double psa = digamma(alpha);
   const double eld = dead ? -1e32 : expected_log_det(W, nu);
   gcomp(P, G_PSIA0 + parity, k) = psa;
@@ -384,7 +377,7 @@ __device__ __forceinline__ double prep_gaussian(const DevPlan& P, const FrameDes
   E[6] = m[0];
   E[7] = m[1];
   E[8] = m[2];
-  E[9] = 3.0 / gcomp(P, G_BETA, k);
+  E[9] = 3.0 / beta;
   E[10] = dead ? -(double)kInfF : psa + 0.5 * eld;
   double* L = P.llc + (int64_t)k * 10;
   L[0] = -0.5 * nu * W[0];
@@ -411,18 +404,34 @@ __device__ __forceinline__ double prep_gaussian(const DevPlan& P, const FrameDes
     }
   }
   P.kpos[k] = make_float4(x, y, z, dead ? 0.0f : 1.0f);
-  if (!dead) {
-    const int cell = ref_cell_of(S, D, x, y, z);
-    if (cell >= 0) {
-      const int g = D.cell_base + cell;
-      const int pos = atomicAdd(&P.cell_cnt[g], 1);
-      if (pos < kCellCap)
-        P.cell_refs[(int64_t)g * kCellCap + pos] = make_float4(x, y, z, __int_as_float(k - D.g_base));
-      else
-        atomicOr(&P.state[D.frame_id].flags, F_CELL_OVERFLOW);
-    }
-  }
   return move;
+}
+
+// A live Gaussian's float centre (kpos) into its grid cell (capacity kCellCap; a full cell
+// flags the frame, whose kNN then scans every Gaussian).
+__device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k) {
+  const float4 c4 = P.kpos[k];
+  const int cell = ref_cell_of(S, D, c4.x, c4.y, c4.z);
+  if (cell >= 0) {
+    const int g = D.cell_base + cell;
+    const int pos = atomicAdd(&P.cell_cnt[g], 1);
+    if (pos < kCellCap)
+      P.cell_refs[(int64_t)g * kCellCap + pos] = make_float4(c4.x, c4.y, c4.z, __int_as_float(k - D.g_base));
+    else
+      atomicOr(&P.state[D.frame_id].flags, F_CELL_OVERFLOW);
+  }
+}
+
+// Records and grid entry of Gaussian k from its parameters in memory (first iteration).
+__device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k,
+                                              int parity) {
+  const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
+  double W[6];
+#pragma unroll
+  for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
+  const double m[3] = {gcomp(P, G_M0, k), gcomp(P, G_M1, k), gcomp(P, G_M2, k)};
+  write_records(P, D, k, parity, dead, W, gcomp(P, G_NU, k), gcomp(P, G_ALPHA, k), gcomp(P, G_BETA, k), m, false);
+  if (!dead) grid_insert(P, D, S, k);
 }
 
 // Run by the last Gaussian chunk of a frame to finish (import or kill step): the alpha
@@ -495,7 +504,7 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
     for (int d = 0; d < 3; d++) bad = bad || isnan(g.m_k[d]);
     for (int e = 0; e < 6; e++) bad = bad || isnan(g.W_k[e]);
     if (bad) atomicOr(&P.state[ch.frame].flags, F_NAN_INPUT);
-    prep_gaussian(P, D, S, k, 1, false);
+    prep_gaussian(P, D, S, k, 1);
     alpha = gcomp(P, G_ALPHA, k);
     dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
   }
@@ -1114,26 +1123,32 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   }
   if (ovf)
     for (int i = 0; i < 10; i++) A[i] = s_ovf_acc[threadIdx.x][i];
-  double alpha = 0.0;
+  double alpha = 0.0, move = 0.0;
+  const int cur = P.state[ch.frame].iter & 1, nxt = cur ^ 1;
   if (valid) {
     const bool alive = !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k];
     if (alive) {
       const double N = A[0];
       double xb[3] = {0, 0, 0}, Sk[6] = {0, 0, 0, 0, 0, 0};
       if (N > 0.0) {
-        for (int d = 0; d < 3; d++) xb[d] = mref[d] + A[1 + d] / N;
+        const double iN = 1.0 / N;
+        for (int d = 0; d < 3; d++) xb[d] = mref[d] + A[1 + d] * iN;
         const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
-        for (int e = 0; e < 6; e++) Sk[e] = A[4 + e] - A[1 + ia[e]] * A[1 + ib[e]] / N;
+        for (int e = 0; e < 6; e++) Sk[e] = A[4 + e] - A[1 + ia[e]] * A[1 + ib[e]] * iN;
       }
       const double bo = gcomp(P, G_BETAO, k);
       const double beta = bo + N;
+      const double ib_ = 1.0 / beta;
+      const double nu = gcomp(P, G_NUO, k) + N;
+      const double alpha_n = fmax(gcomp(P, G_ALPHAO, k) + N, 0.0);
       gcomp(P, G_BETA, k) = beta;
-      gcomp(P, G_NU, k) = gcomp(P, G_NUO, k) + N;
-      gcomp(P, G_ALPHA, k) = fmax(gcomp(P, G_ALPHAO, k) + N, 0.0);
-      double mo[3];
+      gcomp(P, G_NU, k) = nu;
+      gcomp(P, G_ALPHA, k) = alpha_n;
+      double mo[3], mn[3];
       for (int d = 0; d < 3; d++) {
         mo[d] = gcomp(P, G_MO0 + d, k);
-        gcomp(P, G_M0 + d, k) = (bo * mo[d] + N * xb[d]) / beta;
+        mn[d] = (bo * mo[d] + N * xb[d]) * ib_;
+        gcomp(P, G_M0 + d, k) = mn[d];
       }
       double Wo[6];
       for (int e = 0; e < 6; e++) Wo[e] = gcomp(P, G_WO0 + e, k);
@@ -1144,7 +1159,7 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
       double Winv[6];
       inv3(Wo, Winv);
       const double dx[3] = {xb[0] - mo[0], xb[1] - mo[1], xb[2] - mo[2]};
-      const double fct = N * (bo / (bo + N));
+      const double fct = N * (bo * ib_);
       const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
       for (int e = 0; e < 6; e++) Winv[e] += Sk[e] + fct * dx[ia[e]] * dx[ib[e]];
       double W[6];
@@ -1155,13 +1170,27 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
       rc.lambda_min = D.lambda_min;
       rc.lambda_max = D.lambda_max;
       rc.max_exc = D.max_exc;
-      regularize_W(W, gcomp(P, G_NU, k), rc);
+      regularize_W(W, nu, rc);
       for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = W[e];
+      // the next iteration's records, as if the Gaussian survives the kill step (which
+      // rewrites them for the Gaussians it kills)
+      move = write_records(P, D, k, nxt, false, W, nu, alpha_n, beta, mn, true);
+    } else {
+      // fixed or dead: unchanged parameters, unchanged records; psi and E[ln|Lambda|] go
+      // on to the next iteration's slot
+      gcomp(P, G_PSIA0 + nxt, k) = gcomp(P, G_PSIA0 + cur, k);
+      gcomp(P, G_ELD0 + nxt, k) = gcomp(P, G_ELD0 + cur, k);
     }
     alpha = gcomp(P, G_ALPHA, k);
   }
   const double a = block_sum_n<kMChunk>(alpha, shd);
   if (threadIdx.x == 0) P.alpha_part_e[blockIdx.x] = a;
+  // the block's largest move of a kNN centre, rounded up to a float (non-negative floats
+  // order as their bits)
+  float mv = __double2float_ru(move);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+  if ((threadIdx.x & 31) == 0 && mv > 0.0f) atomicMax(&P.state[ch.frame].disp_max, __float_as_uint(mv));
 }
 
 // ===========================================================================
@@ -1186,32 +1215,32 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   const double total = s_total;
   const int cur = S.iter & 1, nxt = (S.iter + 1) & 1;
   const int k = ch.g_begin + threadIdx.x;
-  double alpha = 0.0, move = 0.0;
+  double alpha = 0.0;
   int dead = 0;
   if (k < ch.g_end) {
     bool nanw = isnan(gcomp(P, G_ELD0 + cur, k));
     for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
     const double a = gcomp(P, G_ALPHA, k);
-    if (nanw || (a / total < TGMM_MIN_PI_FOR_DEAD && !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k])) {
+    const bool was_dead = is_dead_prior(gcomp(P, G_MO0, k));
+    if (nanw || (a / total < TGMM_MIN_PI_FOR_DEAD && !was_dead && !P.fixed[k])) {
       gcomp(P, G_ALPHA, k) = 0.0;
+      const double mdead[3] = {-1e32, -1e32, -1e32};
       for (int d = 0; d < 3; d++) {
         gcomp(P, G_MO0 + d, k) = -1e32;
         gcomp(P, G_M0 + d, k) = -1e32;
       }
       const double I6[6] = {1, 0, 0, 1, 0, 1};
       for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = I6[e];
+      write_records(P, D, k, nxt, true, I6, gcomp(P, G_NU, k), 0.0, gcomp(P, G_BETA, k), mdead, false);
+      dead = 1;
+    } else {
+      alpha = a;
+      dead = was_dead ? 1 : 0;
+      if (!was_dead) grid_insert(P, D, S, k);
     }
-    move = prep_gaussian(P, D, S, k, nxt, true);
-    alpha = gcomp(P, G_ALPHA, k);
-    dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
   }
   const double at = block_sum_gchunk(alpha, shd);
   const int nd = block_sum_gchunk_i(dead, shi);
-  // the chunk's largest move, rounded up to a float: non-negative floats order as their bits
-  float mv = __double2float_ru(move);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mv = fmaxf(mv, __shfl_xor_sync(0xffffffffu, mv, o));
-  if ((threadIdx.x & 31) == 0 && mv > 0.0f) atomicMax(&P.state[ch.frame].disp_max, __float_as_uint(mv));
   if (threadIdx.x == 0) {
     P.alpha_part_f[c] = at;
     P.dead_part[c] = nd;
