@@ -32,10 +32,14 @@ METRIC = "EM frames/s & voxel-iters/s at 1 Gvox/20k nuclei; p50/p99 frame latenc
 UNIT = "frames/s"
 WORKLOAD = "2048x1024x512 uint16 volume, 20000 nuclei (semi-axes 4-8, anisotropy 2), 5-NN, 20 EM iterations"
 EM_ITERS = 20
-# kernels the engine launches per EM call: build_maps, import, moments,
-# 4 per iteration (knn_estep, mstep_update, kill_prep, ll_pass),
-# assign, export
-KERNELS_PER_CALL = 3 + 4 * EM_ITERS + 2
+
+
+def kernels_per_call(knn_fused: bool) -> int:
+    """Kernels the engine launches per EM call: 3 table stagings (k_stage), build_maps,
+    import, order, moments, the first iteration's knn_estep, 3 per iteration (mstep_update,
+    kill_prep, ll_pass), the later iterations' knn_estep unless the voxel pass runs them,
+    assign, export."""
+    return 3 + 5 + 3 * EM_ITERS + (0 if knn_fused else EM_ITERS - 1) + 2
 
 
 def parse():
@@ -70,14 +74,15 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes (read + write) per launch of the voxel pass from the committed ncu summary,
-    with the voxel count of the captured frame, or None.  The pass streams each voxel once,
-    so its traffic scales with the voxel count."""
+def committed_traffic(kernel):
+    """DRAM bytes (read + write) per launch of the voxel pass (the form named `kernel`) from
+    the committed ncu summary, with the voxel count of the captured frame, or None.  The pass
+    streams each voxel once, so its traffic scales with the voxel count."""
     p = os.path.join(ROOT, "profiles", "ll_pass_traffic.json")
     try:
         with open(p) as f:
-            return json.load(f)
+            t = json.load(f)
+        return t if t.get("kernel") == kernel else None
     except Exception:
         return None
 
@@ -222,6 +227,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     # the autotuner picks the kNN/E-step width on this frame (untimed; results do not depend on it)
     knn_lanes = plan.autotune([df], [gm], [rnk], [ind], params, reps=3)
+    knn_fused = plan.tuning()["knn_fused"]
 
     def step():
         gm.copy_(gm0, non_blocking=True)
@@ -249,20 +255,35 @@ def run_ours(args):
     total_ms = ev[0].elapsed_time(ev[-1])
     value, voxel_iters, max_ms, total_vox = reduce_job(total_ms, N, args.steps, world, dev)
 
-    # roofline of the per-iteration voxel pass (timed alone on this stream, same workload)
+    # roofline of the dominant kernel, timed alone on this stream on the same workload: the
+    # per-iteration voxel pass, or, when the autotuner made it run the next iteration's
+    # kNN/E-step, that form.  Algorithmic bytes: 16 B per voxel (x, y, z, I); the kNN/E-step
+    # adds 164 B per supervoxel (centroid, CSR bounds, 9 moments, neighbour list, candidates
+    # and responsibilities out) and 104 B per Gaussian (E-step record, float centre).
+    ms_llk = plan_time(plan, L.TGMM_KERNEL_LL_PASS_KNN, 20, stream)
     ms_ll = plan_time(plan, L.TGMM_KERNEL_LL_PASS, 20, stream)
     ms_mom = plan_time(plan, L.TGMM_KERNEL_MOMENTS, 10, stream)
     peak, peak_kind = measured_peaks()
-    alg_bytes = 16.0 * N
-    achieved = alg_bytes / (ms_ll * 1e-3) / 1e9
-    traffic = committed_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_ll_pass (log-likelihood voxel pass, per iteration)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+    vox_bytes = 16.0 * N
+    knn_bytes = 164.0 * S + 104.0 * K
+    alone = {"kernel": "k_ll_pass<0, 0> (the voxel pass alone)", "ms_per_launch": ms_ll,
+             "algorithmic_bytes_per_launch": vox_bytes, "achieved": vox_bytes / (ms_ll * 1e-3) / 1e9,
+             "frac": vox_bytes / (ms_ll * 1e-3) / 1e9 / peak}
+    fused = {"kernel": f"k_ll_pass<0, {knn_lanes}> (the voxel pass running the next iteration's kNN/E-step)",
+             "ms_per_launch": ms_llk, "algorithmic_bytes_per_launch": vox_bytes + knn_bytes,
+             "achieved": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9,
+             "frac": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9 / peak}
+    top, other = (fused, alone) if knn_fused else (alone, fused)
+    traffic = committed_traffic(top["kernel"].split(" ")[0] + " " + top["kernel"].split(" ")[1])
+    roofline = {"bound": "hbm", "kernel": top["kernel"] + ", per iteration",
+                "achieved": top["achieved"], "peak": peak, "unit": "GB/s", "frac": top["frac"],
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
-                "fallback 6650 GB/s", "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms_ll,
+                "fallback 6650 GB/s", "algorithmic_bytes_per_launch": top["algorithmic_bytes_per_launch"],
+                "ms_per_launch": top["ms_per_launch"],
                 "traffic": (traffic["bytes_per_launch"] * N / traffic["n_vox"]) if traffic else None,
-                "moments_pass": {"ms_per_launch": ms_mom, "achieved": alg_bytes / (ms_mom * 1e-3) / 1e9,
-                                 "frac": alg_bytes / (ms_mom * 1e-3) / 1e9 / peak}}
+                "other_form": other,
+                "moments_pass": {"ms_per_launch": ms_mom, "achieved": vox_bytes / (ms_mom * 1e-3) / 1e9,
+                                 "frac": vox_bytes / (ms_mom * 1e-3) / 1e9 / peak}}
 
     # end to end through the C ABI with host buffers: H2D of the frame, Gaussians H2D/D2H
     # inside tgmm_em_run, D2H of rnk/ind, every step
@@ -279,13 +300,13 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_vox": N, "n_sv": S, "n_gauss": K, "em_iterations": EM_ITERS,
-                           "knn_lanes_per_supervoxel": knn_lanes,
+                           "knn_lanes_per_supervoxel": knn_lanes, "knn_in_voxel_pass": knn_fused,
                            "knn_grid_searches_after_iteration_1": check["knn_searches"],
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (16 B x n_vox)",
                            "ll_precision": "mixed", "ll_mode": "as_reference"},
                 "voxel_iters_per_s": voxel_iters,
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
-                "gpu_launches": KERNELS_PER_CALL * args.steps,
+                "gpu_launches": kernels_per_call(knn_fused) * args.steps,
                 "roofline": roofline, "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     plan.close()
@@ -387,10 +408,12 @@ def run_batch64(args):
     tv, ts, tg = sum(f.n_vox for f in frames), sum(f.n_sv for f in frames), sum(f.n_gauss for f in frames)
     batch_plan = E.Plan(tv, ts, tg, max_frames=len(frames))
     one_plan = E.Plan(max(f.n_vox for f in frames), max(f.n_sv for f in frames), max(f.n_gauss for f in frames))
-    # widths tuned on the batch, and on its largest volume for the one-at-a-time plan (untimed)
-    lanes_b = batch_plan.autotune(dfs, gms, rnks, inds, prm, reps=3)
-    big = max(range(len(frames)), key=lambda i: frames[i].n_vox)
-    lanes_p = one_plan.autotune([dfs[big]], [gms[big]], [rnks[big]], [inds[big]], prm, reps=3)
+    # tuned on the batch, and on its median volume for the one-at-a-time plan (untimed)
+    lanes_b = batch_plan.autotune(dfs, gms, rnks, inds, prm, reps=2)
+    fused_b = batch_plan.tuning()["knn_fused"]
+    mid = sorted(range(len(frames)), key=lambda i: frames[i].n_vox)[len(frames) // 2]
+    lanes_p = one_plan.autotune([dfs[mid]], [gms[mid]], [rnks[mid]], [inds[mid]], prm, reps=3)
+    fused_p = one_plan.tuning()["knn_fused"]
 
     def batched():
         for g, g0 in zip(gms, gm0):
@@ -429,6 +452,7 @@ def run_batch64(args):
             "plain": {"value": n / (ms_p / 1e3), "ms_per_sweep": ms_p, "path": "tgmm_em_run_device, one at a time"},
             "batched_over_plain": ms_p / ms_b, "voxel_iters_per_s": tv * EM_ITERS / (ms_b / 1e3),
             "knn_lanes_per_supervoxel": {"batched": lanes_b, "plain": lanes_p},
+            "knn_in_voxel_pass": {"batched": fused_b, "plain": fused_p},
             "rnk_ind_identical_to_alone": bool(same)}
     print(json.dumps(line), flush=True)
 

@@ -219,10 +219,11 @@ int tgmm_write_rnk_file(const char* path, const float* rnk_host, const int32_t* 
 /* Measurement hook (no reference counterpart): launch one kernel of the EM `reps` times
  * back to back on `stream` between two CUDA events, on the batch last run through this
  * plan, and return the average milliseconds per launch.  The plan's per-frame EM state
- * is restored afterwards.  Only kernels without lasting side effects are accepted. */
+ * is restored afterwards; the results of the last call stay as they were returned. */
 enum {
-  TGMM_KERNEL_MOMENTS = 0, /* per-supervoxel moment pass (once per call) */
-  TGMM_KERNEL_LL_PASS = 2  /* log-likelihood voxel pass (per iteration) */
+  TGMM_KERNEL_MOMENTS = 0,    /* per-supervoxel moment pass (once per call) */
+  TGMM_KERNEL_LL_PASS = 2,    /* log-likelihood voxel pass alone */
+  TGMM_KERNEL_LL_PASS_KNN = 3 /* the voxel pass running the next iteration's kNN/E-step */
 };
 int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* ms_per_launch, void* stream);
 
@@ -232,13 +233,20 @@ int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* m
  * launch shape (knnCuda.cu:781-817, GMEMupdateCUDA.cu:3120-3141). */
 int tgmm_plan_set_knn_group(TgmmPlan* plan, int32_t lanes);
 
-/* Autotuner: stages the batch (the arguments of tgmm_em_run_batch, whose Gaussians are
- * only read), runs its first iteration up to the kNN/E-step and times that kernel `reps`
- * times at each width, both as in the first iteration (grid search) and as in a later one
- * (candidates from the supervoxels' neighbour lists); the width with the least time for a
- * call of min(max_iter_em, 20) iterations is kept in the plan (returned in *lanes_out).
- * rnk_dev and ind_dev are overwritten; the results of later calls do not depend on the
- * choice. */
+/* Whether the log-likelihood voxel pass of each iteration also runs the next iteration's
+ * kNN/E-step (1) or that kernel follows the pass (0, the default).  Both give the same
+ * bits; running them together pays off when the voxel pass leaves the SMs idle (small
+ * frames), apart when the batch is large.  No reference counterpart. */
+int tgmm_plan_set_knn_fusion(TgmmPlan* plan, int32_t on);
+/* The plan's current kNN/E-step width and arrangement (either pointer may be NULL). */
+int tgmm_plan_tuning(TgmmPlan* plan, int32_t* lanes, int32_t* fused);
+
+/* Autotuner (no reference counterpart): runs the whole EM call of the batch (the
+ * arguments of tgmm_em_run_batch; at most 20 iterations) `reps` times for every kNN/E-step
+ * width and arrangement, after a first run that warms up, and keeps the fastest pair in
+ * the plan (the width is returned in *lanes_out, tgmm_plan_tuning reads both).  The runs
+ * work on a copy of the Gaussians in the plan: gm_dev is only read.  rnk_dev and ind_dev
+ * are overwritten; the results of later calls do not depend on the choices. */
 int tgmm_plan_autotune(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
                        TgmmGaussian* const* gm_dev, float* const* rnk_dev, int32_t* const* ind_dev,
                        const TgmmEmParams* params, int32_t reps, int32_t* lanes_out, void* stream);

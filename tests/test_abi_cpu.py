@@ -176,3 +176,5 @@ def test_width_setter_refuses_bad_arguments_without_a_gpu():
     lib = L.gmem()
     assert lib.tgmm_plan_set_knn_group(None, 8) == L.TGMM_ERR_INVALID_ARG
     assert lib.tgmm_plan_autotune(None, 1, None, None, None, None, None, 1, None, None) == L.TGMM_ERR_INVALID_ARG
+    assert lib.tgmm_plan_set_knn_fusion(None, 1) == L.TGMM_ERR_INVALID_ARG
+    assert lib.tgmm_plan_tuning(None, None, None) == L.TGMM_ERR_INVALID_ARG

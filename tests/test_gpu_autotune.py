@@ -1,5 +1,6 @@
-"""The kNN/E-step width (lanes per supervoxel) only changes speed: every width gives the
-same bits, and the autotuner's choice leaves the results as they are."""
+"""The kNN/E-step width (lanes per supervoxel) and whether the voxel pass runs the next
+iteration's kNN/E-step only change speed: every choice gives the same bits, and the
+autotuner's choices leave the results as they are."""
 import numpy as np
 import pytest
 
@@ -81,3 +82,56 @@ def test_bad_width_is_refused(cuda_ok):
             plan.set_knn_group(4)
     finally:
         plan.close()
+
+
+@pytest.mark.parametrize("name,tol", [("c1", -1.0), ("hard", -1.0), ("moved", -1.0), ("c1", 1e-6), ("hard", 0.0),
+                                      ("moved", 1e-6)])
+def test_knn_in_voxel_pass_gives_the_same_bits(cuda_ok, name, tol):
+    """The voxel pass running the next iteration's kNN/E-step gives the bits of the two
+    kernels one after the other, also when a frame converges and the kNN/E-step it ran
+    ahead is dropped (tol >= 0), at every width."""
+    from tgmm_b200 import engine as E
+    f = F.frame(name)
+    df = E.to_device(f)
+    plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
+    try:
+        runs = {}
+        for lanes in (8, 32):
+            plan.set_knn_group(lanes)
+            for fused in (False, True, False):
+                plan.set_knn_fusion(fused)
+                runs.setdefault((lanes, fused), []).append(plan.run_host(df, f.gauss, F.params(30, tol)))
+        assert plan.tuning() == {"knn_lanes": 32, "knn_fused": False}
+    finally:
+        plan.close()
+    ref = runs[(8, False)][0]
+    if tol >= 0:
+        assert ref["converged"] == 1 and ref["iterations"] < 30  # the dropped run-ahead is exercised
+    for rs in runs.values():
+        for r in rs:
+            same(ref, r)
+
+
+def test_autotune_reads_the_gaussians_only_and_keeps_the_results(cuda_ok):
+    import torch
+    from tgmm_b200 import engine as E
+    f = F.frame("c1")
+    df = E.to_device(f)
+    gm = E.gauss_to_device(f.gauss)
+    before = gm.clone()
+    rnk = torch.empty(5 * f.n_sv, device="cuda")
+    ind = torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda")
+    plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
+    try:
+        lanes = plan.autotune([df], [gm], [rnk], [ind], F.params(20, -1.0), reps=1)
+        torch.cuda.synchronize()
+        assert torch.equal(gm, before)
+        t = plan.tuning()
+        assert t["knn_lanes"] == lanes and isinstance(t["knn_fused"], bool)
+        got = plan.run_host(df, f.gauss, F.params(20, -1.0))
+        plan.set_knn_group(8)
+        plan.set_knn_fusion(False)
+        want = plan.run_host(df, f.gauss, F.params(20, -1.0))
+    finally:
+        plan.close()
+    same(got, want)

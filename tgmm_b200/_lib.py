@@ -37,6 +37,7 @@ TGMM_LLPREC_FP64 = 1
 
 TGMM_KERNEL_MOMENTS = 0
 TGMM_KERNEL_LL_PASS = 2
+TGMM_KERNEL_LL_PASS_KNN = 3
 
 
 class TgmmGaussian(C.Structure):
@@ -160,6 +161,8 @@ GMEM_FUNCS = {
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
     "tgmm_plan_set_knn_group": (C.c_int, [_VP, C.c_int32]),
+    "tgmm_plan_set_knn_fusion": (C.c_int, [_VP, C.c_int32]),
+    "tgmm_plan_tuning": (C.c_int, [_VP, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "tgmm_plan_autotune": (C.c_int, [_VP, C.c_int32, C.POINTER(TgmmFrame), C.POINTER(_VP), C.POINTER(_VP),
                                      C.POINTER(_VP), C.POINTER(TgmmEmParams), C.c_int32, C.POINTER(C.c_int32), _VP]),
     "tgmm_server_default_desc": (None, [C.POINTER(TgmmServerDesc)]),

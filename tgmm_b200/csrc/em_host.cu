@@ -75,8 +75,8 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.sv_order = take(4 * S);
   L.sv_rec = take((int64_t)sizeof(SvRec) * S);
   L.mom = take(8 * S * kNumMoments);
-  L.cand = take(4 * S * kJ);
-  L.rnk = take(4 * S * kJ);
+  L.cand = take(2 * 4 * S * kJ);
+  L.rnk = take(2 * 4 * S * kJ);
   L.nbr = take(4 * S * kNbr);
   L.nbr_b = take(8 * S);
   L.llp = take(8 * 2 * S);
@@ -104,6 +104,7 @@ struct TgmmPlan {
   cudaEvent_t done_ev = nullptr;       // end of the last call
   cudaStream_t last_stream = nullptr;  // its stream
   bool used = false;
+  bool fuse_knn = false;  // the voxel pass runs the next iteration's kNN/E-step (autotuned)
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (max_iter, ll_prec) -> exec
   // host copy of the tables of the last staged batch
   BatchInfo s_info{};
@@ -338,17 +339,30 @@ int stage_tables(TgmmPlan* P, cudaStream_t st) {
 }
 
 // The whole EM (after the tables are staged) as a stream of async operations on `st`.
+// Each launch carries its iteration number.  With fuse_knn the voxel pass of iteration t
+// also runs the kNN/E-step of iteration t + 1 (mixed-precision voxel terms only); else that
+// kernel follows the pass.
 int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
-  const DevPlan& D = P->dev;
+  DevPlan D = P->dev;
+  D.iter = 1;
   launch_build_maps(D, st);
   launch_import(D, st);
   launch_order(D, st);
   launch_moments(D, st);
-  for (int it = 0; it < max_iter; it++) {
-    launch_knn_estep(D, st);
+  const bool fp64 = ll_prec == TGMM_LLPREC_FP64;
+  const bool fuse = P->fuse_knn && !fp64;
+  if (max_iter >= 1) launch_knn_estep(D, st);
+  for (int it = 1; it <= max_iter; it++) {
+    D.iter = it;
     launch_mstep_update(D, st);
     launch_kill_prep(D, st);
-    launch_ll_pass(D, ll_prec == TGMM_LLPREC_FP64, st);
+    const bool more = it < max_iter;
+    launch_ll_pass(D, fp64, more && fuse ? D.knn_group : 0, st);
+    if (more && !fuse) {
+      DevPlan N = D;
+      N.iter = it + 1;
+      launch_knn_estep(N, st);
+    }
   }
   launch_assign(D, st);
   launch_export(D, st);
@@ -508,85 +522,114 @@ int tgmm_plan_set_knn_group(TgmmPlan* P, int32_t lanes) {
   return TGMM_OK;
 }
 
+int tgmm_plan_set_knn_fusion(TgmmPlan* P, int32_t on) {
+  if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_fusion: null plan");
+  if (on != 0 && on != 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_fusion: on must be 0 or 1");
+  std::lock_guard<std::mutex> lock(P->mu);
+  if (P->fuse_knn == (on == 1)) return TGMM_OK;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  if (P->used) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // captured with the other arrangement
+  P->graphs.clear();
+  P->fuse_knn = on == 1;
+  return TGMM_OK;
+}
+
+int tgmm_plan_tuning(TgmmPlan* P, int32_t* lanes, int32_t* fused) {
+  if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_tuning: null plan");
+  std::lock_guard<std::mutex> lock(P->mu);
+  if (lanes) *lanes = P->dev.knn_group;
+  if (fused) *fused = P->fuse_knn ? 1 : 0;
+  return TGMM_OK;
+}
+
+// The autotuner runs the whole EM call of the batch (its CUDA graph, at most 20
+// iterations) for every kNN/E-step width and arrangement and keeps the fastest: the
+// kernels' costs interact (the width changes the kNN/E-step's occupancy, running it inside
+// the voxel pass changes what hides whose latency), so only the call shows the best pair.
+// The runs work on the plan's scratch copy of the Gaussians, refreshed before each run.
 int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
                        float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params, int32_t reps,
                        int32_t* lanes_out, void* stream) {
-  if (!P || !frames || !gm_dev || !rnk_dev || !ind_dev || reps < 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_autotune");
+  if (!P || !frames || !gm_dev || !rnk_dev || !ind_dev || reps < 1 || n_frames < 1)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_autotune");
   int rc = validate_params(params);
   if (rc) return rc;
   std::lock_guard<std::mutex> lock(P->mu);
   cudaStream_t st = (cudaStream_t)stream;
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
-  rc = stage_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params);
+  if (n_frames > P->desc.max_frames) return fail(TGMM_ERR_BAD_SIZE, "frame count beyond plan capacity");
+  int64_t tg = 0;
+  for (int32_t f = 0; f < n_frames; f++) {
+    if (!gm_dev[f] || frames[f].n_gauss < 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_autotune: bad frame");
+    tg += frames[f].n_gauss;
+  }
+  if (tg > P->desc.max_gauss) return fail(TGMM_ERR_BAD_SIZE, "batch exceeds plan capacity");
+  TgmmGaussian* scratch = (TgmmGaussian*)(P->base + P->L.gm_scratch);
+  std::vector<TgmmGaussian*> work(n_frames);
+  for (int32_t f = 0, off = 0; f < n_frames; off += frames[f].n_gauss, f++) work[f] = scratch + off;
+  TgmmEmParams tp = *params;
+  tp.max_iter_em = std::min(tp.max_iter_em, 20);
+  rc = stage_batch(P, n_frames, frames, work.data(), rnk_dev, ind_dev, &tp);
   if (rc) return rc;
-  rc = order_after_previous(P, st);
+  rc = order_after_previous(P, st);  // the scratch Gaussians may still be in use
   if (rc) return rc;
-  rc = stage_tables(P, st);
-  if (rc) return rc;
-  // the batch's first iteration up to the kNN/E-step; that kernel is then timed at each
-  // width with its only lasting effects, the M-step bucket counts (cleared in between) and
-  // the supervoxels' neighbour lists.  It is timed twice: as in the first iteration (the
-  // grid search, which builds the lists) and as in a later one (the frames' iteration
-  // counter set to 2: candidates from the lists).  A width scores as a call of
-  // min(max_iter, 20) iterations: one search and the rest from the lists.
-  const DevPlan& D = P->dev;
-  launch_build_maps(D, st);
-  launch_import(D, st);
-  launch_order(D, st);
-  launch_moments(D, st);
-  TG_CUDA(cudaGetLastError(), "kernel launch");
-  const int nf = P->s_info.n_frames;
-  const std::vector<int32_t> iter_one(nf, 1), iter_two(nf, 2);
-  auto set_iter = [&](const std::vector<int32_t>& v) {
-    return cudaMemcpy2DAsync(&P->dev.state[0].iter, sizeof(FrameState), v.data(), sizeof(int32_t), sizeof(int32_t),
-                             nf, cudaMemcpyHostToDevice, st);
-  };
-  const double later = (double)std::max(0, std::min(params->max_iter_em, 20) - 1);
+  const bool can_fuse = tp.ll_precision != TGMM_LLPREC_FP64 && tp.max_iter_em > 1;
+  cudaEvent_t ev[2];
+  TG_CUDA(cudaEventCreate(&ev[0]), "event");
+  TG_CUDA(cudaEventCreate(&ev[1]), "event");
   const int widths[3] = {8, 16, 32};
-  double best_score = 0.0;
-  int best = P->dev.knn_group;
-  std::vector<cudaEvent_t> ev(4 * reps);
-  for (auto& e : ev) TG_CUDA(cudaEventCreate(&e), "event");
+  float best_ms = 0.0f;
+  int best_w = P->dev.knn_group;
+  bool best_f = P->fuse_knn, have = false;
   for (int w : widths) {
-    P->dev.knn_group = w;
-    TG_CUDA(set_iter(iter_one), "set iteration");
-    launch_knn_estep(P->dev, st);  // warm-up
-    TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
-    for (int r = 0; r < 2 * reps; r++) {
-      if (r == reps) TG_CUDA(set_iter(iter_two), "set iteration");
-      TG_CUDA(cudaEventRecord(ev[2 * r], st), "record");
-      launch_knn_estep(P->dev, st);
-      TG_CUDA(cudaEventRecord(ev[2 * r + 1], st), "record");
-      TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
-    }
-    TG_CUDA(cudaGetLastError(), "kernel launch");
-    TG_CUDA(cudaStreamSynchronize(st), "synchronize");
-    double search = 0.0, listed = 0.0;
-    for (int r = 0; r < 2 * reps; r++) {
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]);
-      (r < reps ? search : listed) += ms;
-    }
-    const double score = search + later * listed;
-    if (w == widths[0] || score < best_score) {
-      best_score = score;
-      best = w;
+    for (int fu = 0; fu < (can_fuse ? 2 : 1); fu++) {
+      for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
+      P->graphs.clear();
+      P->dev.knn_group = w;
+      P->fuse_knn = fu == 1;
+      float best_here = 0.0f;
+      for (int r = 0; r <= reps && rc == TGMM_OK; r++) {  // run 0 captures the graph and warms up
+        for (int32_t f = 0; f < n_frames && rc == TGMM_OK; f++)
+          if (cudaMemcpyAsync(work[f], gm_dev[f], sizeof(TgmmGaussian) * (size_t)frames[f].n_gauss,
+                              cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            rc = fail(TGMM_ERR_CUDA, "tgmm_plan_autotune: copy Gaussians", cudaGetLastError());
+        if (rc == TGMM_OK) rc = stage_tables(P, st);
+        if (rc == TGMM_OK && cudaEventRecord(ev[0], st) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "record");
+        if (rc == TGMM_OK) rc = run_batch(P, tp.max_iter_em, tp.ll_precision, st);
+        if (rc == TGMM_OK && cudaEventRecord(ev[1], st) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "record");
+        if (rc == TGMM_OK && cudaEventSynchronize(ev[1]) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "synchronize");
+        float ms = 0.0f;
+        if (rc == TGMM_OK && r > 0) {
+          cudaEventElapsedTime(&ms, ev[0], ev[1]);
+          if (r == 1 || ms < best_here) best_here = ms;
+        }
+      }
+      if (rc == TGMM_OK && (!have || best_here < best_ms)) {
+        have = true;
+        best_ms = best_here;
+        best_w = w;
+        best_f = fu == 1;
+      }
     }
   }
-  for (auto& e : ev) cudaEventDestroy(e);
-  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // recaptured with the chosen width
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // recaptured with the chosen tuning
   P->graphs.clear();
-  P->dev.knn_group = best;
+  P->dev.knn_group = best_w;
+  P->fuse_knn = best_f;
   TG_CUDA(cudaEventRecord(P->done_ev, st), "record");
   P->used = true;
   P->last_stream = st;
-  if (lanes_out) *lanes_out = best;
+  if (rc) return rc;
+  if (lanes_out) *lanes_out = best_w;
   return TGMM_OK;
 }
 
 int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, void* stream) {
   if (!P || !ms || reps < 1) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_time_kernel");
-  if (kernel != TGMM_KERNEL_MOMENTS && kernel != TGMM_KERNEL_LL_PASS)
+  if (kernel != TGMM_KERNEL_MOMENTS && kernel != TGMM_KERNEL_LL_PASS && kernel != TGMM_KERNEL_LL_PASS_KNN)
     return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_time_kernel: only the moment and log-likelihood passes");
   std::lock_guard<std::mutex> lock(P->mu);
   cudaStream_t st = (cudaStream_t)stream;
@@ -610,12 +653,21 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   cudaEvent_t a, b;
   TG_CUDA(cudaEventCreate(&a), "event");
   TG_CUDA(cudaEventCreate(&b), "event");
+  // as the last iteration of frame 0 ran; the kNN/E-step form writes the buffers of the
+  // iteration after it, which the returned results do not use, and M-step bucket counts,
+  // cleared below
+  DevPlan D = P->dev;
+  D.iter = backup[0].iter > 1 ? backup[0].iter - 1 : 1;
+  const int fp64 = P->s_frames[0].ll_prec == TGMM_LLPREC_FP64;
   TG_CUDA(cudaEventRecord(a, st), "record");
   for (int r = 0; r < reps; r++) {
-    if (kernel == TGMM_KERNEL_MOMENTS) launch_moments(P->dev, st);
-    if (kernel == TGMM_KERNEL_LL_PASS) launch_ll_pass(P->dev, P->s_frames[0].ll_prec == TGMM_LLPREC_FP64, st);
+    if (kernel == TGMM_KERNEL_MOMENTS) launch_moments(D, st);
+    if (kernel == TGMM_KERNEL_LL_PASS) launch_ll_pass(D, fp64, 0, st);
+    if (kernel == TGMM_KERNEL_LL_PASS_KNN) launch_ll_pass(D, fp64, fp64 ? 0 : D.knn_group, st);
   }
   TG_CUDA(cudaEventRecord(b, st), "record");
+  if (kernel == TGMM_KERNEL_LL_PASS_KNN)
+    TG_CUDA(cudaMemsetAsync(D.bcnt, 0, 4 * (size_t)P->s_info.total_gauss, st), "clear buckets");
   TG_CUDA(cudaEventSynchronize(b), "synchronize");
   float t = 0;
   cudaEventElapsedTime(&t, a, b);

@@ -829,18 +829,20 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
   }
 }
 
+// The kNN/E-step of supervoxel s for iteration `it` by the G lanes of one group (lane gl
+// of the group whose first lane is gbase).  Its candidates and responsibilities go to the
+// buffers of the iteration's parity.  It reads the frame state the kill step of iteration
+// it - 1 left (grid, neighbour-list bound, psi of the alpha total) and the done flag:
+// when it runs inside the voxel pass of iteration it - 1 (k_ll_pass), that pass may end
+// the frame meanwhile, and the results of an iteration that does not run are never read.
 template <int G>
-__global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
+__device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, int gl, int gbase, unsigned gmask) {
   static_assert(G >= kJ && G <= 32 && (G & (G - 1)) == 0, "a group holds the five candidates");
-  const int lane = threadIdx.x & 31;
-  const int gl = lane & (G - 1), gbase = lane - gl;
-  const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
-  const int s = blockIdx.x * (kKnnWarps * 32 / G) + (threadIdx.x >> 5) * (32 / G) + gbase / G;
   // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
   const FrameState& S = P.state[f];
-  if (S.done) return;
+  if (*(volatile const int32_t*)&S.done) return;
   const FrameDesc D = load_desc(P, f);
   const int sl = s - D.sv_base;
   const int Sf = D.n_sv;
@@ -866,7 +868,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
   int lk = 0x7fffffff;
   float ld = kInfF;
   bool have = false;
-  if (S.iter > 1) {
+  if (it > 1) {
     if (gl < kNbr) {
       lk = P.nbr[(int64_t)s * kNbr + gl];
       if (lk != 0x7fffffff) {
@@ -885,7 +887,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
     // starting bound: the kNbr-th of the list members at their current centres
     float td0 = kInfF;
     int ti0 = 0x7fffffff;
-    if (S.iter > 1) {
+    if (it > 1) {
       float dj = gl < kNbr ? ld : -1.0f;  // lanes without a member never win the arg-max
       int ij = gl < kNbr ? lk : -1;
       group_max_pair<G>(dj, ij, gmask);
@@ -925,7 +927,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
       P.nbr_b[s] = nb.d[kNbr - 1] < kInfF ? sqrt((double)nb.d[kNbr - 1]) * (1.0 - 1e-6) - 4e-3 + disp : (double)kInfF;
   }
   // E-step: candidate j on lane j of the group
-  const int par = S.iter & 1;
+  const int par = it & 1;
   const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
   const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
   int kl = 0;
@@ -972,15 +974,22 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
     const float r = __double2float_rn(1.0 / acc);
     const int j = gl;
     const int64_t pos = (int64_t)j * Sf + sl;
-    D.rnk_out[pos] = r;
-    D.ind_out[pos] = kl;
-    P.cand[(int64_t)s * kJ + j] = k;
-    P.rnk[(int64_t)s * kJ + j] = r;
+    cand_buf(P, it)[(int64_t)s * kJ + j] = k;
+    rnk_buf(P, it)[(int64_t)s * kJ + j] = r;
     if ((double)r > 1e-3) {
       const int b = atomicAdd(&P.bcnt[k], 1);
       if (b < kBucketCap) P.bucket[(int64_t)k * kBucketCap + b] = (int)pos;
     }
   }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & (G - 1), gbase = lane - gl;
+  const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
+  const int s = blockIdx.x * (kKnnWarps * 32 / G) + (threadIdx.x >> 5) * (32 / G) + gbase / G;
+  knn_estep_sv<G>(P, s, P.iter, gl, gbase, gmask);
 }
 
 // M-step contribution of one (supervoxel, slot) pair to Gaussian k, moments re-centred
@@ -993,7 +1002,7 @@ __device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, 
   const int Sf = D.n_sv;
   const int j = p / Sf, sl = p - j * Sf;
   const int s = D.sv_base + sl;
-  const double r = (double)P.rnk[(int64_t)s * kJ + j];
+  const double r = (double)rnk_buf(P, P.iter)[(int64_t)s * kJ + j];
   const double d0 = (double)D.cent[sl] - mref[0];
   const double d1 = (double)D.cent[(int64_t)Sf + sl] - mref[1];
   const double d2 = (double)D.cent[2 * (int64_t)Sf + sl] - mref[2];
@@ -1018,8 +1027,10 @@ __device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, 
 // position p = j*S + s of the frame in increasing order, keep those whose candidate is k
 // and whose rnk exceeds `thr`; `visit(p)` is called by thread 0 in increasing p order.
 template <typename F>
-__device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int k, double thr, int* sh_list,
+__device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int it, int k, double thr, int* sh_list,
                              int* sh_cnt, F visit) {
+  const int32_t* cand = cand_buf(P, it);
+  const float* rnk = rnk_buf(P, it);
   const int64_t total = (int64_t)kJ * D.n_sv;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int64_t base = 0; base < total; base += blockDim.x) {
@@ -1028,7 +1039,7 @@ __device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int k, double
     if (p < total) {
       const int j = (int)(p / D.n_sv), sl = (int)(p - (int64_t)j * D.n_sv);
       const int64_t idx = (int64_t)(D.sv_base + sl) * kJ + j;
-      pred = (P.cand[idx] == k) && ((double)P.rnk[idx] > thr);
+      pred = (cand[idx] == k) && ((double)rnk[idx] > thr);
     }
     const unsigned m = __ballot_sync(0xffffffffu, pred);
     if (lane == 0) sh_cnt[w] = __popc(m);
@@ -1116,7 +1127,7 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
     double mr[3] = {gcomp(P, G_MO0, kk), gcomp(P, G_MO1, kk), gcomp(P, G_MO2, kk)};
     double acc[10];
     for (int i = 0; i < 10; i++) acc[i] = 0.0;
-    ordered_scan(P, D, kk, 1e-3, s_list, s_cnt, [&](int p) { mstep_add(P, D, p, mr, acc); });
+    ordered_scan(P, D, P.iter, kk, 1e-3, s_list, s_cnt, [&](int p) { mstep_add(P, D, p, mr, acc); });
     if (threadIdx.x == 0)
       for (int i = 0; i < 10; i++) s_ovf_acc[tk][i] = acc[i];
     __syncthreads();
@@ -1124,7 +1135,7 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   if (ovf)
     for (int i = 0; i < 10; i++) A[i] = s_ovf_acc[threadIdx.x][i];
   double alpha = 0.0, move = 0.0;
-  const int cur = P.state[ch.frame].iter & 1, nxt = cur ^ 1;
+  const int cur = P.iter & 1, nxt = cur ^ 1;
   if (valid) {
     const bool alive = !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k];
     if (alive) {
@@ -1477,7 +1488,7 @@ __device__ __forceinline__ void ll_fetch_a(const DevPlan& P, LLRec& X, int s) {
   if (lane < kRecChunks)
     cp_async16(reinterpret_cast<char*>(&X.rec) + 16 * lane, reinterpret_cast<const char*>(P.sv_rec + s) + 16 * lane);
   else if (lane < kRecChunks + kJ)
-    cp_async4(&X.cand[lane - kRecChunks], P.cand + (int64_t)s * kJ + (lane - kRecChunks));
+    cp_async4(&X.cand[lane - kRecChunks], cand_buf(P, P.iter) + (int64_t)s * kJ + (lane - kRecChunks));
 }
 // Stage B (after A landed): the candidates' constants and the frame scalars.
 __device__ __forceinline__ void ll_fetch_b(const DevPlan& P, const LLRec& A, LLConst& X) {
@@ -1648,7 +1659,13 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // earlier.  A warp adds its supervoxels' sums into fixed-point registers and publishes
 // them (with the count of supervoxels) when its frame changes and when it leaves; the
 // warp that completes a frame's count runs the convergence test.
-template <bool kFp64>
+// With G > 0 the warps also run the kNN/E-step of the next iteration (G lanes per
+// supervoxel, 32/G supervoxels an item, from a second work counter): one item after each
+// supervoxel's look-ahead copies are issued, and the rest once the voxel work has run out.
+// It needs only what the kill step left, and its results go to the next iteration's
+// buffers, so it runs ahead of the convergence test; a frame that converges here never
+// reads them.
+template <bool kFp64, int G>
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1713,6 +1730,25 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     ll_fetch_b(P, RA[0], RB[0]);
     cp_commit();
   }
+  // the next iteration's kNN/E-step items
+  constexpr int kPerItem = G > 0 ? 32 / G : 1;
+  const int knn_items = G > 0 ? (total + kPerItem - 1) / kPerItem : 0;
+  bool knn_more = G > 0;
+  auto knn_step = [&]() {
+    if constexpr (G > 0) {
+      int item = 0;
+      if (lane == 0) item = atomicAdd(&P.work[2], 1);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if (item < knn_items) {
+        const int gl = lane & (G - 1), gbase = lane - gl;
+        const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
+        knn_estep_sv<G>(P, item * kPerItem + gbase / G, P.iter + 1, gl, gbase, gmask);
+        __syncwarp();
+      } else {
+        knn_more = false;
+      }
+    }
+  };
   for (unsigned i = 0; sc < total; i++) {
     // everything fetched so far was issued at least a supervoxel ago
     cp_wait_all();
@@ -1725,6 +1761,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     if (sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
     if (s2 < total) ll_fetch_a(P, RA[(i + 2) % 3], s2);
     cp_commit();
+    if (knn_more) knn_step();  // while this supervoxel's tiles and records land
     int in = 0;
     const int n_nt = sn < total ? NA.rec.ntiles : 0;  // the next one's tiles may start early
     const int nv = CA.rec.nv, nt = CA.rec.ntiles, f = CA.rec.frame, nsv = CA.rec.frame_nsv;
@@ -1839,9 +1876,11 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
   }
   cp_wait_all();
   publish();
+  while (knn_more) knn_step();
   if (lane == 0 && atomicAdd(&P.work[1], 1) == (int)(gridDim.x * kWarpsPerBlockV) - 1) {
     P.work[0] = 0;
     P.work[1] = 0;
+    P.work[2] = 0;
   }
 }
 
@@ -1854,13 +1893,23 @@ __global__ void __launch_bounds__(kSvPerBlockT) k_assign(DevPlan P) {
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
   const FrameDesc D = load_desc(P, f);
-  if (P.state[f].flags & (F_BAD_CSR | F_FEW_GAUSS)) return;
+  const FrameState& S = P.state[f];
+  if (S.flags & (F_BAD_CSR | F_FEW_GAUSS)) return;
   const int sl = s - D.sv_base;
+  // the last E-step that ran (a kNN/E-step run ahead of a converged frame is ignored); its
+  // responsibilities and candidates are the call's outputs
+  const int last = S.iter - 1;
+  const float* rnk = rnk_buf(P, last);
+  const int32_t* cand = cand_buf(P, last);
 #pragma unroll
   for (int j = 0; j < kJ; j++) {
-    const float r = P.rnk[(int64_t)s * kJ + j];
+    const float r = rnk[(int64_t)s * kJ + j];
+    const int k = cand[(int64_t)s * kJ + j];
+    if (last >= 1) {
+      D.rnk_out[(int64_t)j * D.n_sv + sl] = r;
+      D.ind_out[(int64_t)j * D.n_sv + sl] = k - D.g_base;
+    }
     if ((double)r > 0.5) {
-      const int k = P.cand[(int64_t)s * kJ + j];
       const int b = atomicAdd(&P.acnt[k], 1);
       if (b < kBucketCap) P.abucket[(int64_t)k * kBucketCap + b] = j * D.n_sv + sl;
     }
@@ -1910,7 +1959,7 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
     const int tk = s_ovf[o];
     int taken = 0;
     int* dst = s_first[tk];
-    ordered_scan(P, D, ch.g_begin + tk, 0.5, s_list, s_cnt, [&](int p) {
+    ordered_scan(P, D, S.iter - 1, ch.g_begin + tk, 0.5, s_list, s_cnt, [&](int p) {
       if (taken < TGMM_MAX_SV_PER_GAUSSIAN) dst[taken++] = p;
     });
     if (threadIdx.x == 0) dst[TGMM_MAX_SV_PER_GAUSSIAN] = taken;
@@ -1972,12 +2021,19 @@ void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
 void launch_kill_prep(const DevPlan& P, cudaStream_t st) {
   k_kill_prep<<<P.max_gchunks, kGChunk, 0, st>>>(P);
 }
-void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st) {
+void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) {
   const int grid = P.ll_blocks;
+  const int bs = kWarpsPerBlockV * 32;
   if (fp64)
-    k_ll_pass<true><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
+    k_ll_pass<true, 0><<<grid, bs, kLLSmemBytes, st>>>(P);
+  else if (knn_group == 8)
+    k_ll_pass<false, 8><<<grid, bs, kLLSmemBytes, st>>>(P);
+  else if (knn_group == 16)
+    k_ll_pass<false, 16><<<grid, bs, kLLSmemBytes, st>>>(P);
+  else if (knn_group == 32)
+    k_ll_pass<false, 32><<<grid, bs, kLLSmemBytes, st>>>(P);
   else
-    k_ll_pass<false><<<grid, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
+    k_ll_pass<false, 0><<<grid, bs, kLLSmemBytes, st>>>(P);
 }
 
 // Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging
@@ -2010,14 +2066,20 @@ cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStr
 }
 
 cudaError_t configure_kernels(DevPlan& P, int device) {
-  cudaError_t e = cudaFuncSetAttribute(k_ll_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_ll_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
-  int sms = 0, per = 0;
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ll_pass<false>, kWarpsPerBlockV * 32, kLLSmemBytes);
-  P.ll_blocks = sms * (per > 0 ? per : 1);
+  // every form of the voxel pass: its dynamic shared memory, and the blocks per SM the
+  // persistent grid is sized for (the fewest of the forms)
+  const void* forms[5] = {(const void*)k_ll_pass<true, 0>, (const void*)k_ll_pass<false, 0>,
+                          (const void*)k_ll_pass<false, 8>, (const void*)k_ll_pass<false, 16>,
+                          (const void*)k_ll_pass<false, 32>};
+  int sms = 0, per = 1 << 30;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  for (const void* fn : forms) {
+    int p = 0;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, fn, kWarpsPerBlockV * 32, kLLSmemBytes);
+    per = p < per ? p : per;
+  }
+  P.ll_blocks = sms * (per > 0 && per < (1 << 30) ? per : 1);
   return e;
 }
 void launch_assign(const DevPlan& P, cudaStream_t st) {

@@ -171,6 +171,7 @@ struct DevPlan {
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
   int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
   int32_t knn_group;  // lanes per supervoxel of the kNN/E-step (8, 16 or 32)
+  int32_t iter;       // the EM iteration a launch belongs to (1-based; set per launch)
   float4* kpos;  // per Gaussian: the float centre the kNN sees (x, y, z; w = 1 live, 0 dead)
   double* ec;   // per Gaussian E-step record, kEcStride doubles: nu W [6], m [3], 3/beta, psi(alpha)+eLD/2
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
@@ -179,8 +180,8 @@ struct DevPlan {
   int32_t* sv_order;  // the order in which the voxel passes take supervoxels (k_order)
   SvRec* sv_rec;
   double* mom;
-  int32_t* cand;
-  float* rnk;
+  int32_t* cand;  // [2][max_sv][kJ]: candidates of the odd / even iterations' E-steps
+  float* rnk;     // [2][max_sv][kJ]: their responsibilities
   int32_t* nbr;    // [max_sv][kNbr]: the supervoxel's kNbr nearest Gaussians when last searched
   double* nbr_b;   // validity bound of that list (see k_knn_estep)
   double* ll_part;  // [2][max_sv]
@@ -203,6 +204,15 @@ __device__ __forceinline__ double& gcomp(const DevPlan& P, int c, int k) {
   return P.gd[(int64_t)c * P.max_gauss + k];
 }
 
+// The E-step buffers of iteration `it` (two, by parity: the kNN/E-step of the next
+// iteration may run while the voxel pass still reads this one's candidates).
+__device__ __forceinline__ int32_t* cand_buf(const DevPlan& P, int it) {
+  return P.cand + (int64_t)(it & 1) * P.max_sv * kJ;
+}
+__device__ __forceinline__ float* rnk_buf(const DevPlan& P, int it) {
+  return P.rnk + (int64_t)(it & 1) * P.max_sv * kJ;
+}
+
 // ---- kernel launchers (em_kernels.cu) ----
 void launch_build_maps(const DevPlan& P, cudaStream_t st);
 void launch_import(const DevPlan& P, cudaStream_t st);
@@ -211,7 +221,7 @@ void launch_moments(const DevPlan& P, cudaStream_t st);
 void launch_knn_estep(const DevPlan& P, cudaStream_t st);
 void launch_mstep_update(const DevPlan& P, cudaStream_t st);
 void launch_kill_prep(const DevPlan& P, cudaStream_t st);
-void launch_ll_pass(const DevPlan& P, int fp64, cudaStream_t st);
+void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st);
 void launch_assign(const DevPlan& P, cudaStream_t st);
 cudaError_t configure_kernels(DevPlan& P, int device);
 // bytes from host memory to 16-byte aligned device memory through kernel launch

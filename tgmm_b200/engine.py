@@ -138,8 +138,19 @@ class Plan:
     def set_knn_group(self, lanes: int):
         L.check(self.lib.tgmm_plan_set_knn_group(self.h, lanes), "tgmm_plan_set_knn_group")
 
+    def set_knn_fusion(self, on: bool):
+        L.check(self.lib.tgmm_plan_set_knn_fusion(self.h, 1 if on else 0), "tgmm_plan_set_knn_fusion")
+
+    def tuning(self) -> dict:
+        """The kNN/E-step width and whether the voxel pass runs it (autotuned or set)."""
+        lanes, fused = C.c_int32(), C.c_int32()
+        L.check(self.lib.tgmm_plan_tuning(self.h, C.byref(lanes), C.byref(fused)), "tgmm_plan_tuning")
+        return {"knn_lanes": lanes.value, "knn_fused": bool(fused.value)}
+
     def autotune(self, frames, gms, rnks, inds, params: L.TgmmEmParams, reps: int = 3, stream=None) -> int:
-        """Times the kNN/E-step widths on this batch and keeps the fastest; returns it."""
+        """Runs the batch's EM call at every kNN/E-step width and arrangement and keeps the
+        fastest pair (the Gaussians in gms are only read); returns the width (tuning() gives
+        both)."""
         n = len(frames)
         cfs = (L.TgmmFrame * n)(*[f.cframe() for f in frames])
         gp = (C.c_void_p * n)(*[g.data_ptr() for g in gms])
