@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2000)
+    ap.add_argument("--knn-lanes", type=int, choices=[8, 16, 32], default=0,
+                    help="fix the kNN/E-step width instead of autotuning (with --knn-fused; for profiling)")
+    ap.add_argument("--knn-fused", type=int, choices=[0, 1], default=0,
+                    help="with --knn-lanes: 1 = the voxel pass runs the next iteration's kNN/E-step")
     return ap.parse_args()
 
 
@@ -226,7 +230,12 @@ def run_ours(args):
     plan = E.Plan(N, S, K, device=local)
     stream = torch.cuda.current_stream(dev)
     # the autotuner picks the kNN/E-step width on this frame (untimed; results do not depend on it)
-    knn_lanes = plan.autotune([df], [gm], [rnk], [ind], params, reps=3)
+    if args.knn_lanes:
+        plan.set_knn_group(args.knn_lanes)
+        plan.set_knn_fusion(bool(args.knn_fused))
+        knn_lanes = args.knn_lanes
+    else:
+        knn_lanes = plan.autotune([df], [gm], [rnk], [ind], params, reps=3)
     knn_fused = plan.tuning()["knn_fused"]
 
     def step():

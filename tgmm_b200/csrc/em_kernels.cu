@@ -840,13 +840,24 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   static_assert(G >= kJ && G <= 32 && (G & (G - 1)) == 0, "a group holds the five candidates");
   // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
+  // what needs only s goes out first, ahead of the frame's state and descriptor: the list
+  // member of this lane and the list's bound, and (into L1) the moments the E-step reads
   const int f = P.sv_frame[s];
+  int lk = 0x7fffffff;
+  double nbr_bound = 0.0;
+  if (it > 1) {
+    if (gl < kNbr) lk = P.nbr[(int64_t)s * kNbr + gl];
+    nbr_bound = P.nbr_b[s];
+  }
+  if (gl < 9) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)(M_E0 + gl) * P.max_sv + s));
+  if (G == 8 && gl == 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)M_EE22 * P.max_sv + s));
   const FrameState& S = P.state[f];
   if (*(volatile const int32_t*)&S.done) return;
   const FrameDesc D = load_desc(P, f);
   const int sl = s - D.sv_base;
   const int Sf = D.n_sv;
   const float q0 = D.cent[sl], q1 = D.cent[(int64_t)Sf + sl], q2 = D.cent[2 * (int64_t)Sf + sl];
+  const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
   GridGeom g;
   for (int d = 0; d < 3; d++) {
     g.lo[d] = S.lo[d];
@@ -865,23 +876,19 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   //   sqrt(d5) (1 + 1e-6) + disp < nbr_b = rho (1 - 1e-6) - 4e-3 + disp_b;
   // the margins cover the FP32 rounding of the distances.  Otherwise the supervoxel runs
   // the exact search for the kNbr nearest and keeps them as its new list.
-  int lk = 0x7fffffff;
   float ld = kInfF;
   bool have = false;
   if (it > 1) {
-    if (gl < kNbr) {
-      lk = P.nbr[(int64_t)s * kNbr + gl];
-      if (lk != 0x7fffffff) {
-        const float4 r = P.kpos[D.g_base + lk];
-        ld = knn_dist(q0, q1, q2, r.x, r.y, r.z, D.scale);
-      }
+    if (gl < kNbr && lk != 0x7fffffff) {
+      const float4 r = P.kpos[D.g_base + lk];
+      ld = knn_dist(q0, q1, q2, r.x, r.y, r.z, D.scale);
     }
     Top5 mine;
     top5_init(mine);
     mine.d[0] = ld;
     mine.i[0] = lk;
     group_merge_topn<G, kJ>(mine, t, gmask);
-    have = t.d[kJ - 1] < kInfF && sqrt((double)t.d[kJ - 1]) * (1.0 + 1e-6) + disp < P.nbr_b[s];
+    have = t.d[kJ - 1] < kInfF && sqrt((double)t.d[kJ - 1]) * (1.0 + 1e-6) + disp < nbr_bound;
   }
   if (!have) {
     // starting bound: the kNbr-th of the list members at their current centres
@@ -928,7 +935,6 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   }
   // E-step: candidate j on lane j of the group
   const int par = it & 1;
-  const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
   const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
   int kl = 0;
 #pragma unroll
@@ -997,21 +1003,38 @@ __global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
 // during a call, so responsibilities that repeat bit for bit give parameters that repeat
 // bit for bit -- the exact fixed point the reference's tol = 0 stopping rule looks for:
 //   A0 += r H0;  A1 += r (H1 + H0 d);  A2 += r (H2 + H1 d' + d H1' + H0 d d'),  d = c_s - m_ref.
-__device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, int p, const double* mref,
-                                          double* A) {
+// The inputs of one (supervoxel, slot) pair, loaded apart from their use so that the loads
+// of several pairs can be in flight together.
+struct MEntry {
+  float r, c[3];
+  double h0, h1[3], h2[6];
+};
+
+__device__ __forceinline__ MEntry mentry_load(const DevPlan& P, const FrameDesc& D, int p) {
   const int Sf = D.n_sv;
   const int j = p / Sf, sl = p - j * Sf;
   const int s = D.sv_base + sl;
-  const double r = (double)rnk_buf(P, P.iter)[(int64_t)s * kJ + j];
-  const double d0 = (double)D.cent[sl] - mref[0];
-  const double d1 = (double)D.cent[(int64_t)Sf + sl] - mref[1];
-  const double d2 = (double)D.cent[2 * (int64_t)Sf + sl] - mref[2];
-  const double h0 = P.mom[(int64_t)M_I * P.max_sv + s];
-  const double h1[3] = {P.mom[(int64_t)M_IE0 * P.max_sv + s], P.mom[(int64_t)M_IE1 * P.max_sv + s],
-                        P.mom[(int64_t)M_IE2 * P.max_sv + s]};
-  const double h2[6] = {P.mom[(int64_t)M_IEE00 * P.max_sv + s], P.mom[(int64_t)M_IEE01 * P.max_sv + s],
-                        P.mom[(int64_t)M_IEE02 * P.max_sv + s], P.mom[(int64_t)M_IEE11 * P.max_sv + s],
-                        P.mom[(int64_t)M_IEE12 * P.max_sv + s], P.mom[(int64_t)M_IEE22 * P.max_sv + s]};
+  MEntry e;
+  e.r = rnk_buf(P, P.iter)[(int64_t)s * kJ + j];
+  e.c[0] = D.cent[sl];
+  e.c[1] = D.cent[(int64_t)Sf + sl];
+  e.c[2] = D.cent[2 * (int64_t)Sf + sl];
+  e.h0 = P.mom[(int64_t)M_I * P.max_sv + s];
+#pragma unroll
+  for (int i = 0; i < 3; i++) e.h1[i] = P.mom[(int64_t)(M_IE0 + i) * P.max_sv + s];
+#pragma unroll
+  for (int i = 0; i < 6; i++) e.h2[i] = P.mom[(int64_t)(M_IEE00 + i) * P.max_sv + s];
+  return e;
+}
+
+__device__ __forceinline__ void mentry_add(const MEntry& e, const double* mref, double* A) {
+  const double r = (double)e.r;
+  const double d0 = (double)e.c[0] - mref[0];
+  const double d1 = (double)e.c[1] - mref[1];
+  const double d2 = (double)e.c[2] - mref[2];
+  const double h0 = e.h0;
+  const double* h1 = e.h1;
+  const double* h2 = e.h2;
   const double d[3] = {d0, d1, d2};
   A[0] += r * h0;
   A[1] += r * (h1[0] + h0 * d0);
@@ -1021,6 +1044,11 @@ __device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, 
 #pragma unroll
   for (int e = 0; e < 6; e++)
     A[4 + e] += r * (h2[e] + h1[ia[e]] * d[ib[e]] + d[ia[e]] * h1[ib[e]] + h0 * d[ia[e]] * d[ib[e]]);
+}
+
+__device__ __forceinline__ void mstep_add(const DevPlan& P, const FrameDesc& D, int p, const double* mref,
+                                          double* A) {
+  mentry_add(mentry_load(P, D, p), mref, A);
 }
 
 // Block-cooperative ordered scan for Gaussians whose bucket overflowed: visit every
@@ -1080,6 +1108,7 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   __shared__ int s_list[kMChunk];
   __shared__ int s_cnt[kMChunk / 32 + 1];
   __shared__ double shd[kMChunk / 32];
+  __shared__ int s_bk[kBucketCap][kMChunk];  // each thread's bucket, one column per thread
   if (threadIdx.x == 0) s_novf = 0;
   __syncthreads();
   {
@@ -1106,17 +1135,29 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
       s_ovf[o] = threadIdx.x;
       atomicOr(&P.state[ch.frame].flags, F_BUCKET_OVERFLOW);
     } else {
-      int* bk = P.bucket + (int64_t)k * kBucketCap;  // this Gaussian's own bucket
-      for (int i = 1; i < n; i++) {                  // insertion sort by position
-        const int v = bk[i];
+      // this Gaussian's bucket into shared memory, sorted there by position
+      const int* bk = P.bucket + (int64_t)k * kBucketCap;
+      const int t = threadIdx.x;
+#pragma unroll 4
+      for (int i = 0; i < n; i++) s_bk[i][t] = bk[i];
+      for (int i = 1; i < n; i++) {
+        const int v = s_bk[i][t];
         int q = i;
-        while (q > 0 && bk[q - 1] > v) {
-          bk[q] = bk[q - 1];
+        while (q > 0 && s_bk[q - 1][t] > v) {
+          s_bk[q][t] = s_bk[q - 1][t];
           q--;
         }
-        bk[q] = v;
+        s_bk[q][t] = v;
       }
-      for (int i = 0; i < n; i++) mstep_add(P, D, bk[i], mref, A);
+      // in that order, two pairs' inputs in flight at a time
+      int i = 0;
+      for (; i + 1 < n; i += 2) {
+        const MEntry e0 = mentry_load(P, D, s_bk[i][t]);
+        const MEntry e1 = mentry_load(P, D, s_bk[i + 1][t]);
+        mentry_add(e0, mref, A);
+        mentry_add(e1, mref, A);
+      }
+      if (i < n) mstep_add(P, D, s_bk[i][t], mref, A);
     }
   }
   __syncthreads();
@@ -1212,28 +1253,35 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   const int c = blockIdx.x;
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
-  const FrameState S = P.state[ch.frame];
+  const FrameState& S = P.state[ch.frame];
   if (S.done) return;
   const FrameDesc D = load_desc(P, ch.frame);
   __shared__ double s_total;
   __shared__ double shd[kGChunk / 32];
   __shared__ int shi[kGChunk / 32];
+  const int cur = P.iter & 1, nxt = cur ^ 1;
+  const int k = ch.g_begin + threadIdx.x;
+  const bool valid = k < ch.g_end;
+  // this Gaussian's inputs are on their way while warp 0 sums the frame's alpha partials
+  bool nanw = false, was_dead = true, fixed = true;
+  double a = 0.0;
+  if (valid) {
+    nanw = isnan(gcomp(P, G_ELD0 + cur, k));
+    for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
+    a = gcomp(P, G_ALPHA, k);
+    was_dead = is_dead_prior(gcomp(P, G_MO0, k));
+    fixed = P.fixed[k] != 0;
+  }
   if (threadIdx.x < 32) {
     const double tot = warp_sum_range(P.alpha_part_e, 2 * D.gchunk_base, 2 * D.n_gchunks);
     if (threadIdx.x == 0) s_total = tot;
   }
   __syncthreads();
   const double total = s_total;
-  const int cur = S.iter & 1, nxt = (S.iter + 1) & 1;
-  const int k = ch.g_begin + threadIdx.x;
   double alpha = 0.0;
   int dead = 0;
-  if (k < ch.g_end) {
-    bool nanw = isnan(gcomp(P, G_ELD0 + cur, k));
-    for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
-    const double a = gcomp(P, G_ALPHA, k);
-    const bool was_dead = is_dead_prior(gcomp(P, G_MO0, k));
-    if (nanw || (a / total < TGMM_MIN_PI_FOR_DEAD && !was_dead && !P.fixed[k])) {
+  if (valid) {
+    if (nanw || (a / total < TGMM_MIN_PI_FOR_DEAD && !was_dead && !fixed)) {
       gcomp(P, G_ALPHA, k) = 0.0;
       const double mdead[3] = {-1e32, -1e32, -1e32};
       for (int d = 0; d < 3; d++) {
@@ -1250,11 +1298,26 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
       if (!was_dead) grid_insert(P, D, S, k);
     }
   }
-  const double at = block_sum_gchunk(alpha, shd);
-  const int nd = block_sum_gchunk_i(dead, shi);
-  if (threadIdx.x == 0) {
-    P.alpha_part_f[c] = at;
-    P.dead_part[c] = nd;
+  // the chunk's alpha (fixed order) and dead count, in one reduction
+  {
+    const double wa = warp_sum(alpha);
+    const int wd = warp_sum_i(dead);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      shd[w] = wa;
+      shi[w] = wd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double at = 0.0;
+      int nd = 0;
+      for (int i = 0; i < kGChunk / 32; i++) {
+        at += shd[i];
+        nd += shi[i];
+      }
+      P.alpha_part_f[c] = at;
+      P.dead_part[c] = nd;
+    }
   }
   chunk_done(P, ch.frame, D.n_gchunks, nxt);
 }
