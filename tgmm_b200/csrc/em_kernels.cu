@@ -60,29 +60,28 @@ __device__ __forceinline__ double block_sum_n(double v, double* sh) {
   return t;
 }
 
-// Block (kGChunk threads) fixed-order sum; result valid in thread 0.
-__device__ __forceinline__ double block_sum_gchunk(double v, double* sh) {
-  v = warp_sum(v);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// A chunk's alpha (fixed-order sum, kGChunk threads) and dead count, in one reduction,
+// written to the chunk's partials by thread 0.
+__device__ __forceinline__ void chunk_partials(double alpha, int dead, double* shd, int* shi, double* alpha_part,
+                                               int32_t* dead_part, int c) {
+  const double wa = warp_sum(alpha);
+  const int wd = warp_sum_i(dead);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    shd[w] = wa;
+    shi[w] = wd;
+  }
   __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < kGChunk / 32; i++) t += sh[i];
-  return t;
-}
-
-__device__ __forceinline__ int block_sum_gchunk_i(int v, int* sh) {
-  v = warp_sum_i(v);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  int t = 0;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < kGChunk / 32; i++) t += sh[i];
-  return t;
+  if (threadIdx.x == 0) {
+    double at = 0.0;
+    int nd = 0;
+    for (int i = 0; i < kGChunk / 32; i++) {
+      at += shd[i];
+      nd += shi[i];
+    }
+    alpha_part[c] = at;
+    dead_part[c] = nd;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -265,6 +264,7 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
   if (threadIdx.x == 0) sbad = 0;
   __syncthreads();
   for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) P.sv_frame[D.sv_base + i] = f;
+#pragma unroll 4
   for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) {
     P.g_frame[D.g_base + i] = f;
     P.bcnt[D.g_base + i] = 0;  // M-step and assignment buckets start empty
@@ -273,6 +273,8 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
   for (int i = threadIdx.x; i < D.cell_budget; i += blockDim.x) P.cell_cnt[D.cell_base + i] = 0;
   int bad = 0;
   float lo[3] = {kInfF, kInfF, kInfF}, hi[3] = {-kInfF, -kInfF, -kInfF};
+  // unrolled so that several supervoxels' loads are in flight at once
+#pragma unroll 4
   for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) {
     const int64_t a = D.lptr[i], b = D.lptr[i + 1];
     if (a < 0 || b < a || b > D.n_vox) bad = 1;
@@ -422,17 +424,6 @@ __device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D
   }
 }
 
-// Records and grid entry of Gaussian k from its parameters in memory (first iteration).
-__device__ __forceinline__ void prep_gaussian(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k,
-                                              int parity) {
-  const bool dead = is_dead_prior(gcomp(P, G_MO0, k));
-  double W[6];
-#pragma unroll
-  for (int e = 0; e < 6; e++) W[e] = gcomp(P, G_W0 + e, k);
-  const double m[3] = {gcomp(P, G_M0, k), gcomp(P, G_M1, k), gcomp(P, G_M2, k)};
-  write_records(P, D, k, parity, dead, W, gcomp(P, G_NU, k), gcomp(P, G_ALPHA, k), gcomp(P, G_BETA, k), m, false);
-  if (!dead) grid_insert(P, D, S, k);
-}
 
 // Run by the last Gaussian chunk of a frame to finish (import or kill step): the alpha
 // total as a fixed-order sum of the chunk partials, psi and ln of it for the next
@@ -480,7 +471,7 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
   const FrameDesc D = load_desc(P, ch.frame);
-  const FrameState S = P.state[ch.frame];
+  const FrameState& S = P.state[ch.frame];
   __shared__ double shd[kGChunk / 32];
   __shared__ int shi[kGChunk / 32];
   const int k = ch.g_begin + threadIdx.x;
@@ -504,16 +495,14 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
     for (int d = 0; d < 3; d++) bad = bad || isnan(g.m_k[d]);
     for (int e = 0; e < 6; e++) bad = bad || isnan(g.W_k[e]);
     if (bad) atomicOr(&P.state[ch.frame].flags, F_NAN_INPUT);
-    prep_gaussian(P, D, S, k, 1);
-    alpha = gcomp(P, G_ALPHA, k);
-    dead = is_dead_prior(gcomp(P, G_MO0, k)) ? 1 : 0;
+    // the first iteration's records and grid entry from the values just read
+    const bool is_dead = is_dead_prior(g.m_o[0]);
+    write_records(P, D, k, 1, is_dead, g.W_k, g.nu_k, g.alpha_k, g.beta_k, g.m_k, false);
+    if (!is_dead) grid_insert(P, D, S, k);
+    alpha = g.alpha_k;
+    dead = is_dead ? 1 : 0;
   }
-  const double a = block_sum_gchunk(alpha, shd);
-  const int nd = block_sum_gchunk_i(dead, shi);
-  if (threadIdx.x == 0) {
-    P.alpha_part_f[c] = a;
-    P.dead_part[c] = nd;
-  }
+  chunk_partials(alpha, dead, shd, shi, P.alpha_part_f, P.dead_part, c);
   chunk_done(P, ch.frame, D.n_gchunks, 1);
 }
 
@@ -541,6 +530,7 @@ __global__ void __launch_bounds__(1024) k_order(DevPlan P) {
     const FrameDesc D = load_desc(P, f);
     if (threadIdx.x < kOrderBuckets) base[threadIdx.x] = 0;
     __syncthreads();
+#pragma unroll 4
     for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x) atomicAdd(&base[order_bucket(D, sl)], 1);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -552,6 +542,7 @@ __global__ void __launch_bounds__(1024) k_order(DevPlan P) {
       }
     }
     __syncthreads();
+#pragma unroll 4
     for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x)
       P.sv_order[D.sv_base + atomicAdd(&base[order_bucket(D, sl)], 1)] = D.sv_base + sl;
     __syncthreads();
@@ -1298,27 +1289,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
       if (!was_dead) grid_insert(P, D, S, k);
     }
   }
-  // the chunk's alpha (fixed order) and dead count, in one reduction
-  {
-    const double wa = warp_sum(alpha);
-    const int wd = warp_sum_i(dead);
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-      shd[w] = wa;
-      shi[w] = wd;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double at = 0.0;
-      int nd = 0;
-      for (int i = 0; i < kGChunk / 32; i++) {
-        at += shd[i];
-        nd += shi[i];
-      }
-      P.alpha_part_f[c] = at;
-      P.dead_part[c] = nd;
-    }
-  }
+  chunk_partials(alpha, dead, shd, shi, P.alpha_part_f, P.dead_part, c);
   chunk_done(P, ch.frame, D.n_gchunks, nxt);
 }
 
