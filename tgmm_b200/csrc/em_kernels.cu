@@ -524,27 +524,56 @@ __device__ __forceinline__ int order_bucket(const FrameDesc& D, int sl) {
 }
 
 __global__ void __launch_bounds__(1024) k_order(DevPlan P) {
+  // per-warp bucket counts (lanes with the same bucket counted once, by their lowest lane),
+  // so that the hot buckets see no contended atomics; a supervoxel's place is fixed by its
+  // bucket, warp, loop trip and lane: the order is the same on every run
+  constexpr int kW = 1024 / 32;
+  __shared__ int hist[kW][kOrderBuckets];
   __shared__ int base[kOrderBuckets];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
   const int nf = P.info->n_frames;
   for (int f = 0; f < nf; f++) {
     const FrameDesc D = load_desc(P, f);
-    if (threadIdx.x < kOrderBuckets) base[threadIdx.x] = 0;
+    for (int i = threadIdx.x; i < kW * kOrderBuckets; i += blockDim.x) (&hist[0][0])[i] = 0;
     __syncthreads();
-#pragma unroll 4
-    for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x) atomicAdd(&base[order_bucket(D, sl)], 1);
+    const int trips = (D.n_sv + (int)blockDim.x - 1) / (int)blockDim.x;
+    for (int t = 0; t < trips; t++) {
+      const int sl = t * blockDim.x + threadIdx.x;
+      const int b = sl < D.n_sv ? order_bucket(D, sl) : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, b);
+      if (b >= 0 && (m & below) == 0) hist[w][b] += __popc(m);
+    }
     __syncthreads();
+    // bucket bases (largest tile counts first), then each warp's start inside its bucket
     if (threadIdx.x == 0) {
       int run = 0;
       for (int b = kOrderBuckets - 1; b >= 0; b--) {
-        const int c = base[b];
         base[b] = run;
+        for (int v = 0; v < kW; v++) run += hist[v][b];
+      }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) {
+      int run = base[b];
+      for (int v = 0; v < kW; v++) {
+        const int c = hist[v][b];
+        hist[v][b] = run;
         run += c;
       }
     }
     __syncthreads();
-#pragma unroll 4
-    for (int sl = threadIdx.x; sl < D.n_sv; sl += blockDim.x)
-      P.sv_order[D.sv_base + atomicAdd(&base[order_bucket(D, sl)], 1)] = D.sv_base + sl;
+    for (int t = 0; t < trips; t++) {
+      const int sl = t * blockDim.x + threadIdx.x;
+      const int b = sl < D.n_sv ? order_bucket(D, sl) : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, b);
+      if (b >= 0) {
+        P.sv_order[D.sv_base + hist[w][b] + __popc(m & below)] = D.sv_base + sl;
+        __syncwarp(m);
+        if ((m & below) == 0) hist[w][b] += __popc(m);
+      }
+      __syncwarp();
+    }
     __syncthreads();
   }
 }
@@ -674,6 +703,10 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
 // Pairs with rnk > 1e-3 go to the Gaussian's M-step bucket.
 // ===========================================================================
 constexpr int kKnnWarps = 4;  // warps per block; the lanes per supervoxel (G) come from the plan
+#ifndef TGMM_KNN_BLOCKS
+#define TGMM_KNN_BLOCKS 5  // 102 registers: the list path fits more warps; the rare grid search spills a little
+#endif
+constexpr int kKnnBlocks = TGMM_KNN_BLOCKS;  // resident blocks per SM the kNN/E-step is compiled for
 
 // group-wide lexicographic arg-min of (d, i); every lane of the group gets the winner
 template <int G>
@@ -981,7 +1014,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
 }
 
 template <int G>
-__global__ void __launch_bounds__(kKnnWarps * 32) k_knn_estep(DevPlan P) {
+__global__ void __launch_bounds__(kKnnWarps * 32, kKnnBlocks) k_knn_estep(DevPlan P) {
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1), gbase = lane - gl;
   const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
