@@ -39,7 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_order, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_order, ord_hist, ord_cur, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -73,6 +73,8 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.work = take(64);
   L.sv_frame = take(4 * S);
   L.sv_order = take(4 * S);
+  L.ord_hist = take(4 * 64 * (int64_t)d.max_frames);
+  L.ord_cur = take(4 * 64 * (int64_t)d.max_frames);
   L.sv_rec = take((int64_t)sizeof(SvRec) * S);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(2 * 4 * S * kJ);
@@ -200,6 +202,8 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   }
   D.sv_frame = (int32_t*)(b + P->L.sv_frame);
   D.sv_order = (int32_t*)(b + P->L.sv_order);
+  D.ord_hist = (int32_t*)(b + P->L.ord_hist);
+  D.ord_cur = (int32_t*)(b + P->L.ord_cur);
   D.sv_rec = (SvRec*)(b + P->L.sv_rec);
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);

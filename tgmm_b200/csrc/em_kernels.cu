@@ -226,10 +226,10 @@ __device__ void set_geometry(FrameState* S, const float* lo, const float* hi, in
     ext[d] = fmaxf(hi[d] - lo[d], 1.0f);
     vol *= ext[d];
   }
-  // about three references per cell: the fifth neighbour then usually lies within the
-  // first ring of cells around the query
+  // about kRefsPerCell references per cell: the neighbours a supervoxel keeps then usually
+  // lie within the first ring of cells around the query
   const int budget = max(cell_budget - 1, 1);
-  const int target = max(1, min(budget, n_ref / 3));
+  const int target = max(1, min(budget, n_ref / kRefsPerCell));
   float h = (float)cbrt(vol / target);
   int dims[3] = {1, 1, 1};
   for (int guard = 0; guard < 400; guard++) {
@@ -250,6 +250,36 @@ __device__ void set_geometry(FrameState* S, const float* lo, const float* hi, in
   S->n_cells = dims[0] * dims[1] * dims[2];
 }
 
+// The stream record (SvRec) of supervoxel s (frame-local sl) for the voxel pass.
+__device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s, int sl) {
+  const int64_t a = D.lptr[sl], b = D.lptr[sl + 1];
+  const bool ok = !(a < 0 || b < a || b > D.n_vox || b - a >= (1 << 30));
+  const int nv = ok ? (int)(b - a) : 0;
+  const int nt = (nv + kVoxTile - 1) / kVoxTile;
+  const int r0 = nt ? nv - (nt - 1) * kVoxTile : 0;
+  SvRec r;
+  const float* comp[4] = {D.query, D.query + D.n_vox, D.query + 2 * D.n_vox, D.img};
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const uintptr_t a0 = nt ? (uintptr_t)(comp[c] + a) : 0;
+    const uintptr_t a1 = a0 + 4u * (unsigned)r0;  // first voxel of tile 1
+    r.lo0[c] = a0 & ~(uintptr_t)15;
+    r.lo1[c] = a1 & ~(uintptr_t)15;
+    r.n0[c] = nt ? (unsigned)(((a1 + 15) & ~(uintptr_t)15) - r.lo0[c]) : 0u;
+    r.nf[c] = (4u * kVoxTile + ((a1 & 15) ? 16u : 0u)) | ((unsigned)((a0 & 15) >> 2) << 16) |
+              ((unsigned)((a1 & 15) >> 2) << 20);
+  }
+  r.ntiles = nt;
+  r.nv = nv;
+  r.frame = f;
+  r.frame_nsv = D.n_sv;
+  r.c0 = D.cent[sl];
+  r.c1 = D.cent[(int64_t)D.n_sv + sl];
+  r.c2 = D.cent[2 * (int64_t)D.n_sv + sl];
+  r.r0 = r0;
+  P.sv_rec[s] = r;
+}
+
 // ===========================================================================
 // build_maps: per frame -- supervoxel/Gaussian -> frame maps, CSR validation,
 // centroid bounding box and grid geometry, EM state reset.
@@ -264,6 +294,10 @@ __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
   if (threadIdx.x == 0) sbad = 0;
   __syncthreads();
   for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) P.sv_frame[D.sv_base + i] = f;
+  if (threadIdx.x < kOrderBuckets) {  // the supervoxel order's bucket counts and cursors
+    P.ord_hist[f * kOrderBuckets + threadIdx.x] = 0;
+    P.ord_cur[f * kOrderBuckets + threadIdx.x] = 0;
+  }
 #pragma unroll 4
   for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) {
     P.g_frame[D.g_base + i] = f;
@@ -507,14 +541,12 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
 }
 
 // ===========================================================================
-// order: once per call.  The supervoxels of each frame by descending tile count (counting
-// sort, ties in any order), frames in batch order.  The per-iteration voxel pass takes
-// supervoxels in this order, so a frame's last supervoxels are its smallest and no warp is
-// left with a large one after the others ran out of work.  Its sums do not depend on the
-// order.  (The once-per-call moment pass keeps the memory order: neighbouring warps read
-// neighbouring voxels.)
+// order: once per call.  The supervoxels' stream records, and the supervoxels of each
+// frame by descending tile count (counting sort, ties in any order), frames in batch order.
+// The voxel passes take supervoxels in this order, so a frame's last supervoxels are its
+// smallest and no warp is left with a large one after the others ran out of work.  Their
+// sums do not depend on the order.
 // ===========================================================================
-constexpr int kOrderBuckets = 64;  // tile counts 0..62, and 63 or more
 
 __device__ __forceinline__ int order_bucket(const FrameDesc& D, int sl) {
   const int64_t a = D.lptr[sl], b = D.lptr[sl + 1];
@@ -523,168 +555,56 @@ __device__ __forceinline__ int order_bucket(const FrameDesc& D, int sl) {
   return nt < kOrderBuckets - 1 ? (int)nt : kOrderBuckets - 1;
 }
 
-__global__ void __launch_bounds__(1024) k_order(DevPlan P) {
-  // per-warp bucket counts (lanes with the same bucket counted once, by their lowest lane),
-  // so that the hot buckets see no contended atomics; a supervoxel's place is fixed by its
-  // bucket, warp, loop trip and lane: the order is the same on every run
-  constexpr int kW = 1024 / 32;
-  __shared__ int hist[kW][kOrderBuckets];
-  __shared__ int base[kOrderBuckets];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned below = (1u << lane) - 1u;
-  const int nf = P.info->n_frames;
-  for (int f = 0; f < nf; f++) {
-    const FrameDesc D = load_desc(P, f);
-    for (int i = threadIdx.x; i < kW * kOrderBuckets; i += blockDim.x) (&hist[0][0])[i] = 0;
-    __syncthreads();
-    const int trips = (D.n_sv + (int)blockDim.x - 1) / (int)blockDim.x;
-    for (int t = 0; t < trips; t++) {
-      const int sl = t * blockDim.x + threadIdx.x;
-      const int b = sl < D.n_sv ? order_bucket(D, sl) : -1;
-      const unsigned m = __match_any_sync(0xffffffffu, b);
-      if (b >= 0 && (m & below) == 0) hist[w][b] += __popc(m);
-    }
-    __syncthreads();
-    // bucket bases (largest tile counts first), then each warp's start inside its bucket
-    if (threadIdx.x == 0) {
-      int run = 0;
-      for (int b = kOrderBuckets - 1; b >= 0; b--) {
-        base[b] = run;
-        for (int v = 0; v < kW; v++) run += hist[v][b];
-      }
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) {
-      int run = base[b];
-      for (int v = 0; v < kW; v++) {
-        const int c = hist[v][b];
-        hist[v][b] = run;
-        run += c;
-      }
-    }
-    __syncthreads();
-    for (int t = 0; t < trips; t++) {
-      const int sl = t * blockDim.x + threadIdx.x;
-      const int b = sl < D.n_sv ? order_bucket(D, sl) : -1;
-      const unsigned m = __match_any_sync(0xffffffffu, b);
-      if (b >= 0) {
-        P.sv_order[D.sv_base + hist[w][b] + __popc(m & below)] = D.sv_base + sl;
-        __syncwarp(m);
-        if ((m & below) == 0) hist[w][b] += __popc(m);
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-  }
-}
-
-// ===========================================================================
-// moments: once per call.  Warp per supervoxel; centred at the supervoxel centroid
-// c_s: per-voxel differences e = x - c_s in FP32, accumulation in FP64 (B200 runs
-// FP64 at half the FP32 rate, cheaper here than compensated FP32).  19 moments:
-// sum e, sum e e', sum I, sum I e, sum I e e'.
-// ===========================================================================
-// The stream record (SvRec) of supervoxel s (frame-local sl) for the voxel pass.
-__device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s, int sl) {
-  const int64_t a = D.lptr[sl], b = D.lptr[sl + 1];
-  const bool ok = !(a < 0 || b < a || b > D.n_vox || b - a >= (1 << 30));
-  const int nv = ok ? (int)(b - a) : 0;
-  const int nt = (nv + kVoxTile - 1) / kVoxTile;
-  const int r0 = nt ? nv - (nt - 1) * kVoxTile : 0;
-  SvRec r;
-  const float* comp[4] = {D.query, D.query + D.n_vox, D.query + 2 * D.n_vox, D.img};
-#pragma unroll
-  for (int c = 0; c < 4; c++) {
-    const uintptr_t a0 = nt ? (uintptr_t)(comp[c] + a) : 0;
-    const uintptr_t a1 = a0 + 4u * (unsigned)r0;  // first voxel of tile 1
-    r.lo0[c] = a0 & ~(uintptr_t)15;
-    r.lo1[c] = a1 & ~(uintptr_t)15;
-    r.n0[c] = nt ? (unsigned)(((a1 + 15) & ~(uintptr_t)15) - r.lo0[c]) : 0u;
-    r.nf[c] = (4u * kVoxTile + ((a1 & 15) ? 16u : 0u)) | ((unsigned)((a0 & 15) >> 2) << 16) |
-              ((unsigned)((a1 & 15) >> 2) << 20);
-  }
-  r.ntiles = nt;
-  r.nv = nv;
-  r.frame = f;
-  r.frame_nsv = D.n_sv;
-  r.c0 = D.cent[sl];
-  r.c1 = D.cent[(int64_t)D.n_sv + sl];
-  r.c2 = D.cent[2 * (int64_t)D.n_sv + sl];
-  r.r0 = r0;
-  P.sv_rec[s] = r;
-}
-
-__global__ void __launch_bounds__(kWarpsPerBlockV * 32) k_moments(DevPlan P) {
-  const int total = P.info->total_sv;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = 0; q < kSvPerWarpV; q++) {
-    const int s = blockIdx.x * kSvPerBlockV + q * kWarpsPerBlockV + warp;
-    if (s >= total) return;
+// k_sv_records: thread per supervoxel -- its stream record, and its bucket counted in its
+// frame's histogram (lanes of a warp with the same frame and bucket add once).
+__global__ void __launch_bounds__(256) k_sv_records(DevPlan P) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = s < P.info->total_sv;
+  int key = -1;
+  if (in) {
     const int f = P.sv_frame[s];
     const FrameDesc D = load_desc(P, f);
     const int sl = s - D.sv_base;
-    if (lane == 0) write_sv_rec(P, D, f, s, sl);
-    int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
-    if (p0 < 0 || p1 < p0 || p1 > D.n_vox) p0 = p1 = 0;  // flagged by build_maps
-    const float c0 = D.cent[sl], c1 = D.cent[(int64_t)D.n_sv + sl], c2 = D.cent[2 * (int64_t)D.n_sv + sl];
-    const float* __restrict__ qx = D.query;
-    const float* __restrict__ qy = D.query + D.n_vox;
-    const float* __restrict__ qz = D.query + 2 * D.n_vox;
-    const float* __restrict__ im = D.img;
-    double m[kNumMoments];
-#pragma unroll
-    for (int i = 0; i < kNumMoments; i++) m[i] = 0.0;
-    bool nan_seen = false;
-    constexpr int U = 4;  // voxels in flight per lane
-    for (int64_t v0 = p0 + lane; v0 < p1; v0 += 32 * U) {
-      float xs[U], ys[U], zs[U], ws[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int64_t v = v0 + 32 * u;
-        const bool in = v < p1;
-        xs[u] = in ? __ldcs(qx + v) : c0;
-        ys[u] = in ? __ldcs(qy + v) : c1;
-        zs[u] = in ? __ldcs(qz + v) : c2;
-        ws[u] = in ? __ldcs(im + v) : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-      if (v0 + 32 * u >= p1) break;
-      const float x = xs[u], y = ys[u], z = zs[u], I = ws[u];
-      nan_seen |= isnan(x) || isnan(y) || isnan(z) || isnan(I);
-      const double e0 = (double)(x - c0), e1 = (double)(y - c1), e2 = (double)(z - c2);
-      const double wI = (double)I;
-      m[M_E0] += e0;
-      m[M_E1] += e1;
-      m[M_E2] += e2;
-      m[M_EE00] = fma(e0, e0, m[M_EE00]);
-      m[M_EE01] = fma(e0, e1, m[M_EE01]);
-      m[M_EE02] = fma(e0, e2, m[M_EE02]);
-      m[M_EE11] = fma(e1, e1, m[M_EE11]);
-      m[M_EE12] = fma(e1, e2, m[M_EE12]);
-      m[M_EE22] = fma(e2, e2, m[M_EE22]);
-      m[M_I] += wI;
-      const double i0 = wI * e0, i1 = wI * e1, i2 = wI * e2;
-      m[M_IE0] += i0;
-      m[M_IE1] += i1;
-      m[M_IE2] += i2;
-      m[M_IEE00] = fma(i0, e0, m[M_IEE00]);
-      m[M_IEE01] = fma(i0, e1, m[M_IEE01]);
-      m[M_IEE02] = fma(i0, e2, m[M_IEE02]);
-      m[M_IEE11] = fma(i1, e1, m[M_IEE11]);
-      m[M_IEE12] = fma(i1, e2, m[M_IEE12]);
-      m[M_IEE22] = fma(i2, e2, m[M_IEE22]);
-      }
-    }
-    if (__any_sync(0xffffffffu, nan_seen) && lane == 0) atomicOr(&P.state[f].flags, F_NAN_INPUT);
-#pragma unroll
-    for (int i = 0; i < kNumMoments; i++) m[i] = warp_sum(m[i]);
-    // lane i writes component i
-#pragma unroll
-    for (int i = 0; i < kNumMoments; i++)
-      if (lane == i) P.mom[(int64_t)i * P.max_sv + s] = m[i];
+    write_sv_rec(P, D, f, s, sl);
+    key = f * kOrderBuckets + order_bucket(D, sl);
+  }
+  const unsigned m = __match_any_sync(0xffffffffu, key);
+  if (in && (m & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(&P.ord_hist[key], __popc(m));
+}
+
+// k_order_base: one warp per frame -- the buckets' first places, largest tile counts first.
+__global__ void __launch_bounds__(32) k_order_base(DevPlan P) {
+  const int f = blockIdx.x;
+  if (f >= P.info->n_frames || threadIdx.x != 0) return;
+  int run = 0;
+  for (int b = kOrderBuckets - 1; b >= 0; b--) {
+    const int c = P.ord_hist[f * kOrderBuckets + b];
+    P.ord_hist[f * kOrderBuckets + b] = run;  // from here on: the bucket's base
+    run += c;
   }
 }
+
+// k_order_scatter: thread per supervoxel -- its place, its bucket's base plus a cursor
+// (one atomic per warp and bucket).  Places within a bucket depend on the run; the voxel
+// pass's sums do not.
+__global__ void __launch_bounds__(256) k_order_scatter(DevPlan P) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = s < P.info->total_sv;
+  int key = -1, base = 0;
+  if (in) {
+    const int f = P.sv_frame[s];
+    const FrameDesc D = load_desc(P, f);
+    key = f * kOrderBuckets + order_bucket(D, s - D.sv_base);
+    base = D.sv_base + P.ord_hist[key];
+  }
+  const unsigned m = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+  int start = 0;
+  if (in && lane == lead) start = atomicAdd(&P.ord_cur[key], __popc(m));
+  start = __shfl_sync(m, start, lead);
+  if (in) P.sv_order[base + start + __popc(m & ((1u << lane) - 1u))] = s;
+}
+
 
 // ===========================================================================
 // knn_estep: a group of G lanes per supervoxel (32 / G supervoxels per warp; G = 8, 16
@@ -1549,12 +1469,13 @@ static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOf
 static_assert(kLLBlocks * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "the voxel pass's blocks fit an SM");
 
 // Stage A: the record and candidate ids of supervoxel s.
+template <bool kCand>
 __device__ __forceinline__ void ll_fetch_a(const DevPlan& P, LLRec& X, int s) {
   const int lane = threadIdx.x & 31;
   constexpr int kRecChunks = (int)sizeof(SvRec) / 16;
   if (lane < kRecChunks)
     cp_async16(reinterpret_cast<char*>(&X.rec) + 16 * lane, reinterpret_cast<const char*>(P.sv_rec + s) + 16 * lane);
-  else if (lane < kRecChunks + kJ)
+  else if (kCand && lane < kRecChunks + kJ)
     cp_async4(&X.cand[lane - kRecChunks], cand_buf(P, P.iter) + (int64_t)s * kJ + (lane - kRecChunks));
 }
 // Stage B (after A landed): the candidates' constants and the frame scalars.
@@ -1655,6 +1576,59 @@ __device__ __forceinline__ double ll_fixup(const Eval& eval, const SvRec& R, uns
   return add;
 }
 
+// The moment pass's tile t (landed in `slot`): the 19 sums e, ee', I, Ie, Iee' (e = x - c in
+// FP32, FP64 accumulation) of the lane's voxels o = u*32 + lane; nan_seen turns true on a
+// NaN coordinate or intensity.
+template <bool kFull>
+__device__ __forceinline__ void mom_tile(const float* __restrict__ slot, const int* sht, int rem, float c0, float c1,
+                                         float c2, double* m, bool& nan_seen) {
+  const int lane = threadIdx.x & 31;
+  const float* bx = slot + sht[0] + lane;
+  const float* by = slot + kLLSpan + sht[1] + lane;
+  const float* bz = slot + 2 * kLLSpan + sht[2] + lane;
+  const float* bi = slot + 3 * kLLSpan + sht[3] + lane;
+#pragma unroll
+  for (int u = 0; u < kLLTile / 32; u++) {
+    if (!kFull && u * 32 >= rem) break;
+    if (!kFull && u * 32 + lane >= rem) continue;
+    const float x = bx[32 * u], y = by[32 * u], z = bz[32 * u], I = bi[32 * u];
+    nan_seen |= isnan(x) || isnan(y) || isnan(z) || isnan(I);
+    const double e0 = (double)(x - c0), e1 = (double)(y - c1), e2 = (double)(z - c2);
+    const double wI = (double)I;
+    m[M_E0] += e0;
+    m[M_E1] += e1;
+    m[M_E2] += e2;
+    m[M_EE00] = fma(e0, e0, m[M_EE00]);
+    m[M_EE01] = fma(e0, e1, m[M_EE01]);
+    m[M_EE02] = fma(e0, e2, m[M_EE02]);
+    m[M_EE11] = fma(e1, e1, m[M_EE11]);
+    m[M_EE12] = fma(e1, e2, m[M_EE12]);
+    m[M_EE22] = fma(e2, e2, m[M_EE22]);
+    m[M_I] += wI;
+    const double i0 = wI * e0, i1 = wI * e1, i2 = wI * e2;
+    m[M_IE0] += i0;
+    m[M_IE1] += i1;
+    m[M_IE2] += i2;
+    m[M_IEE00] = fma(i0, e0, m[M_IEE00]);
+    m[M_IEE01] = fma(i0, e1, m[M_IEE01]);
+    m[M_IEE02] = fma(i0, e2, m[M_IEE02]);
+    m[M_IEE11] = fma(i1, e1, m[M_IEE11]);
+    m[M_IEE12] = fma(i1, e2, m[M_IEE12]);
+    m[M_IEE22] = fma(i2, e2, m[M_IEE22]);
+  }
+}
+
+__device__ __forceinline__ void mom_consume(const float* slot, const int* pk, int t, int r0, float c0, float c1,
+                                            float c2, double* m, bool& nan_seen) {
+  const int sft = t == 0 ? 0 : 4;
+  const int sht[4] = {(pk[0] >> sft) & 3, (pk[1] >> sft) & 3, (pk[2] >> sft) & 3, (pk[3] >> sft) & 3};
+  const int rem = t == 0 ? r0 : kLLTile;
+  if (rem == kLLTile)
+    mom_tile<true>(slot, sht, rem, c0, c1, c2, m, nan_seen);
+  else
+    mom_tile<false>(slot, sht, rem, c0, c1, c2, m, nan_seen);
+}
+
 // Tile t (landed in `slot`) of the current supervoxel: its sum goes to lt, and to lr when
 // the tile is one of the last kKeptTiles (the reference's kept window of 1024 voxels).  A kept
 // tile of a supervoxel above 1024 voxels with a voxel of zero density is marked in fix.
@@ -1732,7 +1706,7 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // It needs only what the kill step left, and its results go to the next iteration's
 // buffers, so it runs ahead of the convergence test; a frame that converges here never
 // reads them.
-template <bool kFp64, int G>
+template <bool kFp64, int G, bool kMom>
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1789,12 +1763,12 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
   int sn = sc < total ? __shfl_sync(0xffffffffu, tk, 0) : total;
   if (lane == 0 && sn < total) tk = take();
   if (sc < total) {
-    ll_fetch_a(P, RA[0], sc);
-    if (sn < total) ll_fetch_a(P, RA[1], sn);
+    ll_fetch_a<!kMom>(P, RA[0], sc);
+    if (sn < total) ll_fetch_a<!kMom>(P, RA[1], sn);
     cp_commit();
     cp_wait_all();
     __syncwarp();
-    ll_fetch_b(P, RA[0], RB[0]);
+    if (!kMom) ll_fetch_b(P, RA[0], RB[0]);
     cp_commit();
   }
   // the next iteration's kNN/E-step items
@@ -1825,16 +1799,61 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     const LLRec& NA = RA[(i + 1) % 3];
     const int s2 = __shfl_sync(0xffffffffu, tk, 0);
     if (lane == 0 && s2 < total) tk = take();
-    if (sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
-    if (s2 < total) ll_fetch_a(P, RA[(i + 2) % 3], s2);
+    if (!kMom && sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
+    if (s2 < total) ll_fetch_a<!kMom>(P, RA[(i + 2) % 3], s2);
     cp_commit();
     if (knn_more) knn_step();  // while this supervoxel's tiles and records land
     int in = 0;
     const int n_nt = sn < total ? NA.rec.ntiles : 0;  // the next one's tiles may start early
     const int nv = CA.rec.nv, nt = CA.rec.ntiles, f = CA.rec.frame, nsv = CA.rec.frame_nsv;
     const float c0 = CA.rec.c0, c1 = CA.rec.c1, c2 = CA.rec.c2;
-    const bool run = CB.done == 0;
     S = &P.state[f];
+    int pk[4];  // slot offsets of the components: tile 0 in bits 0-1, later tiles in bits 4-5
+#pragma unroll
+    for (int c = 0; c < 4; c++) pk[c] = (int)(CA.rec.nf[c] >> 16);
+    const int r0 = CA.rec.r0;
+    // the next staged tile of the supervoxel (of ntr): the ring is refilled first, with the
+    // current supervoxel's tiles and then the next one's; nullptr if the tile never arrived
+    auto ring_next = [&](int ntr) -> const float* {
+      __syncwarp();  // every lane is done with the slots refilled below
+      while (gi < gc + kLLStages) {
+        const bool mine = ic < ntr;
+        if (!mine && in >= n_nt) break;
+        const int tt = mine ? ic++ : in++;
+        if (lane == 0) {
+          const unsigned q = gi % kLLStages;
+          ll_issue(mine ? CA.rec : NA.rec, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
+        }
+        gi++;
+      }
+      const unsigned q = gc % kLLStages;
+      if (!__all_sync(0xffffffffu, mbar_wait(bar0 + 8 * q, (gc / kLLStages) & 1))) return nullptr;
+      return wbuf + q * kLLSlotFloats;
+    };
+    if constexpr (kMom) {
+      // the moment pass: 19 sums per lane over its voxels of every tile, then per supervoxel
+      double m[kNumMoments];
+#pragma unroll
+      for (int j = 0; j < kNumMoments; j++) m[j] = 0.0;
+      bool nan_seen = false;
+      for (int t = 0; t < nt; t++) {
+        const float* slot = ring_next(nt);
+        if (!slot) {
+          failed = true;
+          break;
+        }
+        mom_consume(slot, pk, t, r0, c0, c1, c2, m, nan_seen);
+        gc++;
+      }
+      if (failed) break;
+      if (__any_sync(0xffffffffu, nan_seen) && lane == 0) atomicOr(&S->flags, F_NAN_INPUT);
+#pragma unroll
+      for (int j = 0; j < kNumMoments; j++) m[j] = warp_sum(m[j]);
+#pragma unroll
+      for (int j = 0; j < kNumMoments; j++)  // lane j writes moment j
+        if (lane == j) P.mom[(int64_t)j * P.max_sv + sc] = m[j];
+    } else {
+    const bool run = CB.done == 0;
     // candidate j on lane j: u = m - c, weight b = ln(w) - ln(A), -nu W/2
     double u[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, b = 0.0;
     if (lane < kJ) {
@@ -1872,33 +1891,16 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     }
     __syncwarp();
     const CandF cf = *cs;
-    int pk[4];  // slot offsets of the components: tile 0 in bits 0-1, later tiles in bits 4-5
-#pragma unroll
-    for (int c = 0; c < 4; c++) pk[c] = (int)(CA.rec.nf[c] >> 16);
-    const int r0 = CA.rec.r0;
     double lt = 0.0, lr = 0.0;
     unsigned fix = 0;  // kept tiles with voxels of zero density
     // a finished frame issues no more tiles; those issued early are consumed unread
     const int ntr = run ? nt : ic;
     for (int t = 0; t < ntr; t++) {
-      __syncwarp();  // every lane is done with the slots refilled below
-      // refill the ring: the current supervoxel's tiles, then the next one's
-      while (gi < gc + kLLStages) {
-        const bool mine = ic < ntr;
-        if (!mine && in >= n_nt) break;
-        const int tt = mine ? ic++ : in++;
-        if (lane == 0) {
-          const unsigned q = gi % kLLStages;
-          ll_issue(mine ? CA.rec : NA.rec, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
-        }
-        gi++;
-      }
-      const unsigned q = gc % kLLStages;
-      if (!__all_sync(0xffffffffu, mbar_wait(bar0 + 8 * q, (gc / kLLStages) & 1))) {
+      const float* slot = ring_next(ntr);
+      if (!slot) {
         failed = true;
         break;
       }
-      const float* slot = wbuf + q * kLLSlotFloats;
       if (compute) {
         if (kFp64)
           ll_consume(VoxelEval<2>{sh64[warp]}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
@@ -1932,6 +1934,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
         acc_n++;
       }
     }
+    }  // the log-likelihood pass
     __syncwarp();  // the records of this supervoxel are refilled from the next iteration on
     sc = sn;
     sn = s2;
@@ -2068,9 +2071,13 @@ void launch_build_maps(const DevPlan& P, cudaStream_t st) {
   k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
 }
 void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
-void launch_order(const DevPlan& P, cudaStream_t st) { k_order<<<1, 1024, 0, st>>>(P); }
+void launch_order(const DevPlan& P, cudaStream_t st) {
+  k_sv_records<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
+  k_order_base<<<P.max_frames, 32, 0, st>>>(P);
+  k_order_scatter<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
+}
 void launch_moments(const DevPlan& P, cudaStream_t st) {
-  k_moments<<<div_up(P.max_sv, kSvPerBlockV), kWarpsPerBlockV * 32, 0, st>>>(P);
+  k_ll_pass<false, 0, true><<<P.ll_blocks, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
   const int G = P.knn_group;
@@ -2092,15 +2099,15 @@ void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) 
   const int grid = P.ll_blocks;
   const int bs = kWarpsPerBlockV * 32;
   if (fp64)
-    k_ll_pass<true, 0><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<true, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 8)
-    k_ll_pass<false, 8><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<false, 8, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 16)
-    k_ll_pass<false, 16><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<false, 16, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 32)
-    k_ll_pass<false, 32><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<false, 32, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else
-    k_ll_pass<false, 0><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<false, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
 }
 
 // Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging
@@ -2135,9 +2142,9 @@ cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStr
 cudaError_t configure_kernels(DevPlan& P, int device) {
   // every form of the voxel pass: its dynamic shared memory, and the blocks per SM the
   // persistent grid is sized for (the fewest of the forms)
-  const void* forms[5] = {(const void*)k_ll_pass<true, 0>, (const void*)k_ll_pass<false, 0>,
-                          (const void*)k_ll_pass<false, 8>, (const void*)k_ll_pass<false, 16>,
-                          (const void*)k_ll_pass<false, 32>};
+  const void* forms[6] = {(const void*)k_ll_pass<true, 0, false>,  (const void*)k_ll_pass<false, 0, false>,
+                          (const void*)k_ll_pass<false, 8, false>, (const void*)k_ll_pass<false, 16, false>,
+                          (const void*)k_ll_pass<false, 32, false>, (const void*)k_ll_pass<false, 0, true>};
   int sms = 0, per = 1 << 30;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   for (const void* fn : forms) {

@@ -33,7 +33,15 @@ constexpr int kSvPerBlockV = kWarpsPerBlockV * kSvPerWarpV;
 constexpr int kNumMoments = 19;
 constexpr int kFrameThreads = 1024;
 constexpr int kCellCap = 32;   // Gaussian centres per kNN grid cell
-constexpr int kNbr = 8;        // Gaussians kept per supervoxel in its kNN neighbour list
+#ifndef TGMM_NBR
+#define TGMM_NBR 8
+#endif
+#ifndef TGMM_REFS_PER_CELL
+#define TGMM_REFS_PER_CELL 3
+#endif
+constexpr int kNbr = TGMM_NBR;  // Gaussians kept per supervoxel in its kNN neighbour list
+constexpr int kRefsPerCell = TGMM_REFS_PER_CELL;  // kNN grid resolution: references per cell
+static_assert(kNbr >= TGMM_J && kNbr <= 8, "a list holds the five candidates, one member per lane of 8");
 constexpr int kEcStride = 12;  // doubles per E-step record
 
 // moment component indices
@@ -113,6 +121,7 @@ struct FrameState {
 #endif
 constexpr int kVoxTile = TGMM_VOX_TILE;
 constexpr int kKeptTiles = 1024 / kVoxTile;
+constexpr int kOrderBuckets = 64;  // supervoxel order: tile counts 0..62, and 63 or more
 static_assert(kVoxTile >= 32 && kVoxTile % 32 == 0 && 1024 % kVoxTile == 0, "tiles split the kept window evenly");
 
 // Per-supervoxel stream record of the voxel pass, built once per call (k_moments).
@@ -177,7 +186,9 @@ struct DevPlan {
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]
   // per supervoxel
   int32_t* sv_frame;
-  int32_t* sv_order;  // the order in which the voxel passes take supervoxels (k_order)
+  int32_t* sv_order;  // the order in which the voxel passes take supervoxels (k_order_*)
+  int32_t* ord_hist;  // [max_frames][64]: per frame, supervoxels per tile-count bucket, then bases
+  int32_t* ord_cur;   // [max_frames][64]: cursors of the scatter
   SvRec* sv_rec;
   double* mom;
   int32_t* cand;  // [2][max_sv][kJ]: candidates of the odd / even iterations' E-steps
