@@ -445,8 +445,8 @@ __device__ __forceinline__ double write_records(const DevPlan& P, const FrameDes
 
 // A live Gaussian's float centre (kpos) into its grid cell (capacity kCellCap; a full cell
 // flags the frame, whose kNN then scans every Gaussian).
-__device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k) {
-  const float4 c4 = P.kpos[k];
+__device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k,
+                                            float4 c4) {
   const int cell = ref_cell_of(S, D, c4.x, c4.y, c4.z);
   if (cell >= 0) {
     const int g = D.cell_base + cell;
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
     // the first iteration's records and grid entry from the values just read
     const bool is_dead = is_dead_prior(g.m_o[0]);
     write_records(P, D, k, 1, is_dead, g.W_k, g.nu_k, g.alpha_k, g.beta_k, g.m_k, false);
-    if (!is_dead) grid_insert(P, D, S, k);
+    if (!is_dead) grid_insert(P, D, S, k, P.kpos[k]);
     alpha = g.alpha_k;
     dead = is_dead ? 1 : 0;
   }
@@ -1209,7 +1209,9 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   // this Gaussian's inputs are on their way while warp 0 sums the frame's alpha partials
   bool nanw = false, was_dead = true, fixed = true;
   double a = 0.0;
+  float4 centre = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (valid) {
+    centre = P.kpos[k];
     nanw = isnan(gcomp(P, G_ELD0 + cur, k));
     for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
     a = gcomp(P, G_ALPHA, k);
@@ -1239,7 +1241,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     } else {
       alpha = a;
       dead = was_dead ? 1 : 0;
-      if (!was_dead) grid_insert(P, D, S, k);
+      if (!was_dead) grid_insert(P, D, S, k, centre);
     }
   }
   chunk_partials(alpha, dead, shd, shi, P.alpha_part_f, P.dead_part, c);
