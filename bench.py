@@ -36,10 +36,10 @@ EM_ITERS = 20
 
 def kernels_per_call(knn_fused: bool) -> int:
     """Kernels the engine launches per EM call: 3 table stagings (k_stage), build_maps,
-    import, order, moments, the first iteration's knn_estep, 3 per iteration (mstep_update,
-    kill_prep, ll_pass), the later iterations' knn_estep unless the voxel pass runs them,
-    assign, export."""
-    return 3 + 5 + 3 * EM_ITERS + (0 if knn_fused else EM_ITERS - 1) + 2
+    import, the 3 order kernels (sv_records, order_base, order_scatter), the moment pass,
+    the first iteration's knn_estep, 3 per iteration (mstep_update, kill_prep, ll_pass), the
+    later iterations' knn_estep unless the voxel pass runs them, assign, export."""
+    return 3 + 7 + 3 * EM_ITERS + (0 if knn_fused else EM_ITERS - 1) + 2
 
 
 def parse():
@@ -275,15 +275,15 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     vox_bytes = 16.0 * N
     knn_bytes = 164.0 * S + 104.0 * K
-    alone = {"kernel": "k_ll_pass<0, 0> (the voxel pass alone)", "ms_per_launch": ms_ll,
+    alone = {"kernel": "k_ll_pass<0, 0, 0> (the voxel pass alone)", "ms_per_launch": ms_ll,
              "algorithmic_bytes_per_launch": vox_bytes, "achieved": vox_bytes / (ms_ll * 1e-3) / 1e9,
              "frac": vox_bytes / (ms_ll * 1e-3) / 1e9 / peak}
-    fused = {"kernel": f"k_ll_pass<0, {knn_lanes}> (the voxel pass running the next iteration's kNN/E-step)",
+    fused = {"kernel": f"k_ll_pass<0, {knn_lanes}, 0> (the voxel pass running the next iteration's kNN/E-step)",
              "ms_per_launch": ms_llk, "algorithmic_bytes_per_launch": vox_bytes + knn_bytes,
              "achieved": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9,
              "frac": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9 / peak}
     top, other = (fused, alone) if knn_fused else (alone, fused)
-    traffic = committed_traffic(top["kernel"].split(" ")[0] + " " + top["kernel"].split(" ")[1])
+    traffic = committed_traffic(top["kernel"].split(" (")[0])
     roofline = {"bound": "hbm", "kernel": top["kernel"] + ", per iteration",
                 "achieved": top["achieved"], "peak": peak, "unit": "GB/s", "frac": top["frac"],
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
