@@ -31,6 +31,8 @@ sys.path.insert(0, ROOT)
 METRIC = "EM frames/s & voxel-iters/s at 1 Gvox/20k nuclei; p50/p99 frame latency"
 UNIT = "frames/s"
 WORKLOAD = "2048x1024x512 uint16 volume, 20000 nuclei (semi-axes 4-8, anisotropy 2), 5-NN, 20 EM iterations"
+WORKLOADS = {"c2": WORKLOAD,
+             "c1": "256x256x64 uint16 volume, 300 nuclei (semi-axes 3-6, anisotropy 2), 5-NN, 20 EM iterations"}
 EM_ITERS = 20
 
 
@@ -168,19 +170,71 @@ def reduce_job(total_ms, n_vox, steps, world, device):
     return world * steps / (max_ms / 1e3), total_vox * EM_ITERS * steps / (max_ms / 1e3), max_ms, total_vox
 
 
-def cpu_baseline(frame, threads=None):
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(frame, threads=None, single=False):
     """The reference's FP32 kernel arithmetic (oracle REF32 port) on the host cores, one EM
-    iteration of the workload frame as the bounded sample, scaled to 20 iterations."""
+    iteration of the workload frame as the bounded sample (repeated until half a second has
+    passed, for small frames), scaled to 20 iterations; with `single`, the same sample on one
+    thread too, for context."""
     from oracle import oracle as O
     n = threads or os.cpu_count() or 1
-    O.lib().or_set_num_threads(n)
     p = O.params(max_iter=1, tol=-1.0, mode=O.MODE_REF32)
-    t0 = time.perf_counter()
-    O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, p)
-    dt = time.perf_counter() - t0
-    return {"value": 1.0 / (EM_ITERS * dt), "unit": UNIT, "cores": n, "kind": "port",
+
+    def sample(t):
+        O.lib().or_set_num_threads(t)
+        reps, t0 = 0, time.perf_counter()
+        while True:
+            O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, p)
+            reps += 1
+            el = time.perf_counter() - t0
+            if el >= 0.5:
+                return el / reps
+    dt = sample(n)
+    info = {"value": 1.0 / (EM_ITERS * dt), "unit": UNIT, "cores": n, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"1 of {EM_ITERS} EM iterations of the workload frame with the FP32 OpenMP port of the "
-                      f"reference kernels ({dt:.2f} s), scaled to {EM_ITERS} iterations"}, dt
+                      f"reference kernels ({dt:.2f} s), scaled to {EM_ITERS} iterations"}
+    if single:
+        d1 = sample(1)
+        O.lib().or_set_num_threads(n)
+        info["single_thread"] = {"value": 1.0 / (EM_ITERS * d1), "unit": UNIT, "cores": 1,
+                                 "sample": f"the same iteration on one thread ({d1:.2f} s)"}
+    return info, dt
+
+
+def reference_gpu(frame, reps=3):
+    """The reference's own GPU path (GMEMvariationalInferenceCUDAWithSupervoxels compiled from
+    its sources for sm_100a) on the workload frame, per synchronous call with host arrays in
+    and out as its callers use it (its context creation, allocations and copies included).
+    Only for frames of at most 1024 supervoxels: its kNN kernel returns early for surplus
+    threads before a __syncthreads(), well-defined only when no thread of a block leaves."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref/libtgmm_ref.so not built (the reference sources were absent)"}
+    if frame.n_sv > 1024:
+        return {"unavailable": f"{frame.n_sv} supervoxels: the reference's kNN kernel is only well-defined "
+                               f"up to 1024 (early return before __syncthreads, knnCuda.cu:69,106)"}
+    try:
+        O.ref_em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, max_iter=EM_ITERS)  # warm
+    except (OSError, RuntimeError) as e:
+        return {"unavailable": f"the reference's GPU path did not run: {str(e).splitlines()[0]}"}
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.ref_em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, max_iter=EM_ITERS)
+        ts.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.median(ts))
+    return {"value": 1e3 / ms, "unit": UNIT, "ms_per_call": ms, "calls": reps,
+            "path": "the reference's GPU path compiled from its sources, host arrays in and out, per call"}
 
 
 def run_reference(args):
@@ -199,11 +253,13 @@ def run_reference(args):
     per_frame = EM_ITERS * float(np.sum(times)) / len(times)
     value = 1.0 / per_frame
     info["value"] = value
+    gpu_ref = reference_gpu(frame)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_frame * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_vox": frame.n_vox, "n_sv": frame.n_sv, "n_gauss": frame.n_gauss},
-            "cpu_baseline": info,
+            "config": {"workload": WORKLOADS[args.workload], "n_vox": frame.n_vox, "n_sv": frame.n_sv,
+                       "n_gauss": frame.n_gauss},
+            "cpu_baseline": info, "reference_gpu": gpu_ref,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -302,13 +358,14 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = cpu_baseline(frame)
+        cpu, _ = cpu_baseline(frame, single=True)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "n_vox": N, "n_sv": S, "n_gauss": K, "em_iterations": EM_ITERS,
+                "config": {"workload": WORKLOADS[args.workload], "n_vox": N, "n_sv": S, "n_gauss": K,
+                           "em_iterations": EM_ITERS,
                            "knn_lanes_per_supervoxel": knn_lanes, "knn_in_voxel_pass": knn_fused,
                            "knn_grid_searches_after_iteration_1": check["knn_searches"],
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (16 B x n_vox)",
