@@ -19,6 +19,7 @@
  *   tgmm_frame_release       <- GMEMreleaseMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:140-144
  *   tgmm_assign_supervoxels  <- post-loop rnk>0.5 assignment, GMEMupdateCUDA.cu:4310-4350
  *   tgmm_write_rnk_file      <- rnk/ind debug dump, GMEMupdateCUDA.cu:4364-4384
+ *   tgmm_write_gmm_xml       <- GMM XML document, GMEMupdateCUDA.cu:4679-4716 (+ :3841-3844)
  */
 #ifndef TGMM_GMEM_H_
 #define TGMM_GMEM_H_
@@ -211,6 +212,12 @@ int tgmm_frame_release(TgmmFrame* frame);
  * rnk[j*n_sv+s] > 0.5, append s to gm[ind].supervoxelIdx (at most 16). */
 int tgmm_assign_supervoxels(const float* rnk_host, const int32_t* ind_host, int32_t n_sv,
                             TgmmGaussian* gm_host, int32_t n_gauss);
+
+/* Reference GMM XML document of n Gaussians (host records): the header, one
+ * <GaussianMixtureModel> element per Gaussian with its index as id, the footer -- the text
+ * the reference's writeXMLheader / writeXML / writeXMLfooter produce
+ * (GMEMupdateCUDA.h:43-52, GMEMupdateCUDA.cu:4679-4716, as called at :3841-3844). */
+int tgmm_write_gmm_xml(const char* path, const TgmmGaussian* gm_host, int32_t n);
 
 /* Reference rnk dump: int n_sv, int 5, float rnk[5*n_sv], int ind[5*n_sv]. */
 int tgmm_write_rnk_file(const char* path, const float* rnk_host, const int32_t* ind_host,

@@ -128,6 +128,8 @@ def ref_lib():
         _ref.ref_em_run.restype = C.c_int
         _ref.ref_knn.argtypes = [vp, C.c_longlong, vp, C.c_int, vp, vp]
         _ref.ref_knn.restype = C.c_int
+        _ref.ref_write_gmm_xml.argtypes = [C.c_char_p, vp, C.c_int]
+        _ref.ref_write_gmm_xml.restype = C.c_int
     return _ref
 
 
@@ -162,3 +164,11 @@ def ref_knn(query, ref_xyz, scale=(1.0, 1.0, 2.0)):
     if rc != 0:
         raise RuntimeError(f"reference kNN failed ({rc})")
     return ind
+
+
+def ref_write_gmm_xml(path, gauss):
+    """The reference's own GMM XML writer on host records (gauss: 288-byte structured array)."""
+    g = np.ascontiguousarray(gauss).copy()
+    rc = ref_lib().ref_write_gmm_xml(str(path).encode(), _p(g), g.shape[0])
+    if rc != 0:
+        raise RuntimeError(f"reference XML writer failed ({rc})")

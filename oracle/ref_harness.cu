@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include <fstream>
 #include <string>
 
 #include "GMEMupdateCUDA.h"
@@ -47,4 +48,16 @@ extern "C" int ref_knn(float* query, long long nq, float* ref, int nref, float* 
   cudaFree(rd);
   cudaFree(id);
   return e == cudaSuccess ? 0 : 2;
+}
+
+// The reference's GMM XML document of n Gaussians (its writeXMLheader, writeXML(os, i) per
+// record, writeXMLfooter), to compare the library's writer with byte for byte.
+extern "C" int ref_write_gmm_xml(const char* path, void* gauss, int n) {
+  std::ofstream os(path);
+  if (!os) return 1;
+  GaussianMixtureModelCUDA* g = (GaussianMixtureModelCUDA*)gauss;
+  GaussianMixtureModelCUDA::writeXMLheader(os);
+  for (int i = 0; i < n; i++) g[i].writeXML(os, i);
+  GaussianMixtureModelCUDA::writeXMLfooter(os);
+  return os.good() ? 0 : 2;
 }

@@ -178,3 +178,24 @@ def test_width_setter_refuses_bad_arguments_without_a_gpu():
     assert lib.tgmm_plan_autotune(None, 1, None, None, None, None, None, 1, None, None) == L.TGMM_ERR_INVALID_ARG
     assert lib.tgmm_plan_set_knn_fusion(None, 1) == L.TGMM_ERR_INVALID_ARG
     assert lib.tgmm_plan_tuning(None, None, None) == L.TGMM_ERR_INVALID_ARG
+
+
+def test_gmm_xml_document_parses_and_carries_each_gaussian(tmp_path):
+    """The GMM XML writer (the reference's writeXML format) needs no GPU: a document with one
+    element per Gaussian, ids in order, means and precision matrices as written."""
+    import xml.etree.ElementTree as ET
+    import _fixtures as F
+    g = np.ascontiguousarray(F.frame("hard").gauss)
+    path = tmp_path / "gmm.xml"
+    assert L.gmem().tgmm_write_gmm_xml(str(path).encode(), g.ctypes.data, g.shape[0]) == L.TGMM_OK
+    root = ET.parse(path).getroot()
+    els = root.findall("GaussianMixtureModel")
+    assert len(els) == g.shape[0]
+    for i, e in enumerate(els):
+        assert int(e.get("id")) == i
+        m = [float(v) for v in e.get("m").split()]
+        np.testing.assert_allclose(m, g["m_k"][i], rtol=1e-5, atol=1e-5)
+        W = np.array([float(v) for v in e.get("W").split()]).reshape(3, 3)
+        np.testing.assert_allclose(W, W.T)
+        np.testing.assert_allclose(W[0], g["W_k"][i][[0, 1, 2]], rtol=1e-5, atol=1e-12)
+    assert L.gmem().tgmm_write_gmm_xml(None, g.ctypes.data, 1) == L.TGMM_ERR_INVALID_ARG

@@ -54,3 +54,24 @@ def test_reference_knn_sets_equal_canonical(cuda_ok, name):
     S = f.n_sv
     np.testing.assert_array_equal(canon_sets(got, S), canon_sets(O.knn(f.centroids, ref_xyz), S))
     np.testing.assert_array_equal(got, O.knn(f.centroids, ref_xyz, reference_rule=True))
+
+
+def test_gmm_xml_is_the_references(cuda_ok, tmp_path):
+    """The library's GMM XML document is byte for byte the one the reference's own writer
+    (compiled from its sources) makes for the same records: live, dead, fixed and twin
+    Gaussians, before and after an EM run."""
+    needs_ref()
+    from tgmm_b200 import _lib as L
+    from tgmm_b200 import engine as E
+    f = F.frame("hard")
+    g0 = np.ascontiguousarray(f.gauss)
+    plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
+    try:
+        g1 = plan.run_host(E.to_device(f), f.gauss, F.params(20, -1.0))["gauss"]
+    finally:
+        plan.close()
+    for i, g in enumerate([g0, np.ascontiguousarray(g1)]):
+        ours, ref = tmp_path / f"ours{i}.xml", tmp_path / f"ref{i}.xml"
+        assert L.gmem().tgmm_write_gmm_xml(str(ours).encode(), g.ctypes.data, g.shape[0]) == L.TGMM_OK
+        O.ref_write_gmm_xml(ref, g)
+        assert ours.read_bytes() == ref.read_bytes()

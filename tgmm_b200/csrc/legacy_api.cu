@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <fstream>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -231,4 +232,19 @@ int selectCUDAdeviceMaxMemory() {
     }
   }
   return device;
+}
+
+extern "C" int tgmm_write_gmm_xml(const char* path, const TgmmGaussian* gm, int32_t n) {
+  static_assert(sizeof(TgmmGaussian) == sizeof(GaussianMixtureModelCUDA), "one 288-byte record layout");
+  if (!path || (!gm && n > 0) || n < 0) return TGMM_ERR_INVALID_ARG;
+  std::ofstream os(path);
+  if (!os) return TGMM_ERR_INVALID_ARG;
+  GaussianMixtureModelCUDA::writeXMLheader(os);
+  for (int32_t i = 0; i < n; i++) {
+    GaussianMixtureModelCUDA g;
+    memcpy((void*)&g, gm + i, sizeof(g));
+    g.writeXML(os, i);
+  }
+  GaussianMixtureModelCUDA::writeXMLfooter(os);
+  return os.good() ? TGMM_OK : TGMM_ERR_INVALID_ARG;
 }
