@@ -13,6 +13,7 @@
  *   tgmm_em_run              <- GMEMvariationalInferenceCUDAWithSupervoxels,
  *                               UtilsCUDA/GMEMupdateCUDA.h:92-98 (body GMEMupdateCUDA.cu:3985-4421)
  *   tgmm_knn                 <- knnCUDAinPlace, UtilsCUDA/knnCuda.h:225-226 (knnCuda.cu:781-817)
+ *   tgmm_knn_k               <- knnCUDA_, temporalLogicalRules/knnCUDA/knnCuda.h:48-58
  *   tgmm_update_priors       <- GaussianMixtureModel::updatePriors, GaussianMixtureModel.cpp:892-910,
  *                               plus the nu_k*=2, W_k/=2 step of mainTrackingGaussianMixtureModel.cpp:961-969
  *   tgmm_frame_upload        <- GMEMinitializeMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:132-137
@@ -178,6 +179,17 @@ int tgmm_em_run_batch(TgmmPlan* plan, int32_t n_frames, const TgmmFrame* frames,
  * (scaled squared distance, index); ind_dev[j*n_query+q].  Exact. */
 int tgmm_knn(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
              int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
+
+/* The tracking graph's supervoxel kNN (knnCUDA_, temporalLogicalRules/knnCUDA/knnCuda.h:48-58,
+ * body knnCuda.cu:56-140): the k nearest (1 <= k <= 11) of n_query points (SoA, dev) among
+ * n_ref points (SoA: x block, y block, z block, dev) by the same scaled squared distance, with
+ * the distances: ind_dev[j*n_query+q] and, if dist_dev is not NULL, dist_dev[j*n_query+q],
+ * ordered by (distance, index).  A slot with no point closer than 1e32 holds index -1 and
+ * distance 1e32 (the reference leaves such indices unset).  Exact; ties go to the lower
+ * index (the reference's replacement rule lets the later one win and leaves the slots
+ * unsorted). */
+int tgmm_knn_k(const float* query_dev, int64_t n_query, const float* ref_dev, int32_t n_ref,
+               int32_t k, const float scale[3], int32_t* ind_dev, float* dist_dev, void* stream);
 
 /* No counterpart in the reference.  The same exact kNN as tgmm_knn for callers that may not
  * allocate device memory -- code whose device memory belongs to another allocator (a

@@ -11,7 +11,7 @@
  *   GMEMreleaseMemoryWithSupervoxels               <- UtilsCUDA/GMEMupdateCUDA.h:140-144
  *   GMEMvariationalInferenceCUDAWithSupervoxels    <- UtilsCUDA/GMEMupdateCUDA.h:92-98
  *   copyScaleToDvice                               <- UtilsCUDA/GMEMupdateCUDA.h:82
- *   knnCUDAinPlace, setDeviceCUDA, uploadScaleCUDA,
+ *   knnCUDAinPlace, setDeviceCUDA, uploadScaleCUDA, knnCUDA_ (temporalLogicalRules/knnCUDA),
  *   selectCUDAdeviceMaxMemory                      <- UtilsCUDA/knnCuda.h:225-231
  *   regularizePrecisionMatrixConstants             <- constants.h:19-45 (the library carries
  *       weak definitions of the three statics; a program's own definitions take precedence)
@@ -82,6 +82,10 @@ void GMEMvariationalInferenceCUDAWithSupervoxels(float* queryCUDA, float* imgDat
                                                  std::string debugPath = "");
 void copyScaleToDvice(float* scale);
 void knnCUDAinPlace(int* indCUDA, float* queryCUDA, float* refTemp, long long int query_nb, int ref_nb);
+/* The tracking graph's supervoxel kNN (temporalLogicalRules/knnCUDA/knnCuda.h:48-58): host
+ * query (SoA) and ref (SoA) in, ind (and dist, if not NULL) out, KNN <= 11; over tgmm_knn_k. */
+int knnCUDA_(int* ind, float* dist, float* query, float* ref, long long int query_nb, int ref_nb, int KNN,
+             float* scale, int devCUDA);
 void setDeviceCUDA(int devCUDA);
 void uploadScaleCUDA(float* scale);
 int selectCUDAdeviceMaxMemory();

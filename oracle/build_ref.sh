@@ -19,5 +19,11 @@ g++ -O2 -fPIC -c "$REF/constants.cpp" -o "$OUT/constants.o"
 $NVCC $FLAGS -I"$REF/UtilsCUDA" -I"$REF" -c "$HERE/ref_harness.cu" -o "$OUT/ref_harness.o"
 $NVCC -gencode arch=compute_100a,code=sm_100a -shared -o "$OUT/libtgmm_ref.so" \
   "$OUT/GMEMupdateCUDA.o" "$OUT/knnCuda.o" "$OUT/constants.o" "$OUT/ref_harness.o" -lcusparse -lcuda
+# the tracking graph's supervoxel kNN, in a library of its own (its symbols are distinct)
+F3="$REF/temporalLogicalRules/knnCUDA"
+$NVCC $FLAGS -c "$F3/knnCuda.cu" -o "$OUT/f3_knnCuda.o"
+$NVCC $FLAGS -I"$F3" -c "$HERE/ref_f3_harness.cu" -o "$OUT/ref_f3_harness.o"
+$NVCC -gencode arch=compute_100a,code=sm_100a -shared -o "$OUT/libtgmm_ref_f3.so" \
+  "$OUT/f3_knnCuda.o" "$OUT/ref_f3_harness.o" -lcuda
 rm -f "$OUT"/*.o
-echo "built $OUT/libtgmm_ref.so"
+echo "built $OUT/libtgmm_ref.so $OUT/libtgmm_ref_f3.so"

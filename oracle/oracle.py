@@ -48,6 +48,7 @@ def lib():
                                    vp, vp, C.POINTER(OrStats)]
         _lib.or_em_run.restype = C.c_int
         _lib.or_knn_canonical.argtypes = [vp, C.c_int64, vp, C.c_int32, C.POINTER(C.c_float), vp]
+        _lib.or_knn_topk.argtypes = [vp, C.c_int64, vp, C.c_int32, C.c_int32, C.POINTER(C.c_float), vp, vp]
         _lib.or_knn_reference.argtypes = [vp, C.c_int64, vp, C.c_int32, C.POINTER(C.c_float), vp]
         _lib.or_digamma.argtypes = [C.c_double]
         _lib.or_digamma.restype = C.c_double
@@ -105,6 +106,19 @@ def knn(query, ref_xyz, scale=(1.0, 1.0, 2.0), reference_rule=False):
     f = lb.or_knn_reference if reference_rule else lb.or_knn_canonical
     f(_p(query), nq, _p(ref_xyz), ref_xyz.shape[0] // 3, sc, _p(ind))
     return ind
+
+
+def knn_topk(query, ref_soa, k, scale=(1.0, 1.0, 2.0)):
+    """The supervoxel kNN of the tracking graph (k <= 11, distances), canonical order."""
+    lb = lib()
+    q = np.ascontiguousarray(query, np.float32)
+    r = np.ascontiguousarray(ref_soa, np.float32)
+    nq, nref = q.shape[0] // 3, r.shape[0] // 3
+    ind = np.zeros(k * nq, np.int32)
+    dist = np.zeros(k * nq, np.float32)
+    sc = (C.c_float * 3)(*scale)
+    lb.or_knn_topk(_p(q), nq, _p(r), nref, k, sc, _p(ind), _p(dist))
+    return ind, dist
 
 
 # ---------------------------------------------------------------------------
@@ -172,3 +186,32 @@ def ref_write_gmm_xml(path, gauss):
     rc = ref_lib().ref_write_gmm_xml(str(path).encode(), _p(g), g.shape[0])
     if rc != 0:
         raise RuntimeError(f"reference XML writer failed ({rc})")
+
+
+REF_F3_SO = os.path.join(HERE, "_ref", "libtgmm_ref_f3.so")
+_ref_f3 = None
+
+
+def ref_f3_available() -> bool:
+    return os.path.exists(REF_F3_SO)
+
+
+def ref_knn_k(query, ref_soa, k, scale=(1.0, 1.0, 2.0)):
+    """The reference's own supervoxel kNN of the tracking graph (its slot order: replace the
+    current maximum, later index on ties); n_query <= 1024."""
+    global _ref_f3
+    if _ref_f3 is None:
+        _ref_f3 = C.CDLL(REF_F3_SO)
+        vp = C.c_void_p
+        _ref_f3.ref_knn_k.argtypes = [vp, vp, vp, vp, C.c_longlong, C.c_int, C.c_int, vp]
+        _ref_f3.ref_knn_k.restype = C.c_int
+    q = np.ascontiguousarray(query, np.float32).copy()
+    r = np.ascontiguousarray(ref_soa, np.float32).copy()
+    nq, nref = q.shape[0] // 3, r.shape[0] // 3
+    ind = np.zeros(k * nq, np.int32)
+    dist = np.zeros(k * nq, np.float32)
+    sc = np.asarray(scale, np.float32)
+    rc = _ref_f3.ref_knn_k(_p(ind), _p(dist), _p(q), _p(r), nq, nref, k, _p(sc))
+    if rc != 0:
+        raise RuntimeError(f"reference supervoxel kNN failed ({rc})")
+    return ind, dist

@@ -273,6 +273,40 @@ void or_knn_canonical(const float* query, int64_t nq, const float* ref, int32_t 
   }
 }
 
+/* The tracking graph's supervoxel kNN (knnCUDA_, temporalLogicalRules/knnCUDA/knnCuda.cu:
+ * 56-140) restated canonically: the k nearest (k <= OR_MAXK) of each query (SoA) among the
+ * reference points (SoA), the same scaled squared FP32 distance, (distance, index) order;
+ * slots with no point closer than 1e32 get index -1 and distance 1e32. */
+void or_knn_topk(const float* query, int64_t nq, const float* ref, int32_t nref, int32_t k,
+                 const float scale[3], int32_t* ind, float* dist) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < nq; i++) {
+    float q[3] = {query[i], query[nq + i], query[2 * nq + i]};
+    float bd[OR_MAXK];
+    int32_t bi[OR_MAXK];
+    int cnt = 0;
+    for (int32_t r = 0; r < nref; r++) {
+      float rp[3] = {ref[r], ref[(int64_t)nref + r], ref[2 * (int64_t)nref + r]};
+      float d = knn_dist(q, rp, scale);
+      if (isnan(d)) d = INFINITY;
+      if (!(d < 1e32f)) continue; /* never assigned, as in the reference */
+      if (cnt == k && !(d < bd[k - 1])) continue; /* ties keep the lower index */
+      int pos = (cnt < k) ? cnt++ : k - 1;
+      while (pos > 0 && d < bd[pos - 1]) {
+        bd[pos] = bd[pos - 1];
+        bi[pos] = bi[pos - 1];
+        pos--;
+      }
+      bd[pos] = d;
+      bi[pos] = r;
+    }
+    for (int j = 0; j < k; j++) {
+      ind[(int64_t)j * nq + i] = (j < cnt) ? bi[j] : -1;
+      if (dist) dist[(int64_t)j * nq + i] = (j < cnt) ? bd[j] : 1e32f;
+    }
+  }
+}
+
 void or_knn_reference(const float* query, int64_t nq, const float* ref, int32_t nref,
                       const float scale[3], int32_t* ind) {
 #pragma omp parallel for schedule(static)

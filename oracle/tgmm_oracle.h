@@ -78,6 +78,9 @@ void or_eig3(const double* w, double* d, double* v);
  * reference kernel's replace-the-current-maximum rule and slot order. */
 void or_knn_canonical(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
                       const float scale[3], int32_t* ind);
+#define OR_MAXK 11
+void or_knn_topk(const float* query, int64_t nq, const float* ref, int32_t nref, int32_t k,
+                 const float scale[3], int32_t* ind, float* dist);
 void or_knn_reference(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
                       const float scale[3], int32_t* ind);
 double or_total_alpha(const OrGaussian* g, int32_t K, int32_t mode);

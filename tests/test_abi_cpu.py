@@ -18,6 +18,7 @@ INC = os.path.join(ROOT, "include")
 LEGACY_SYMBOLS = [
     "_Z13setDeviceCUDAi",
     "_Z14knnCUDAinPlacePiPfS0_xi",
+    "_Z8knnCUDA_PiPfS0_S0_xiiS0_i",
     "_Z15uploadScaleCUDAPf",
     "_Z16copyScaleToDvicePf",
     "_Z25selectCUDAdeviceMaxMemoryv",

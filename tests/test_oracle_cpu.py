@@ -209,3 +209,20 @@ def test_update_priors_matches_reference_formula():
     np.testing.assert_allclose(g["nu_k"], 2 * ref["nu_k"])
     np.testing.assert_allclose(g["W_k"], ref["W_k"] / 2)
     np.testing.assert_array_equal(g["m_o"], ref["m_k"])
+
+
+def test_supervoxel_knn_topk_restatement():
+    """The tracking graph's supervoxel kNN restated in the oracle (k <= 11, distances): its
+    first five are the canonical 5-NN, shorter lists are prefixes of longer ones, and slots
+    beyond the reference points are -1 / 1e32."""
+    rng = np.random.default_rng(3)
+    q = rng.uniform(0, 100, size=(3, 300)).astype(np.float32).reshape(-1)
+    r = rng.uniform(0, 100, size=(3, 200)).astype(np.float32)
+    ind11, d11 = O.knn_topk(q, r.reshape(-1), 11)
+    ind5, d5 = O.knn_topk(q, r.reshape(-1), 5)
+    np.testing.assert_array_equal(ind5, O.knn(q, np.ascontiguousarray(r.T).reshape(-1)))
+    np.testing.assert_array_equal(ind11.reshape(11, -1)[:5], ind5.reshape(5, -1))
+    np.testing.assert_array_equal(d11.reshape(11, -1)[:5], d5.reshape(5, -1))
+    assert np.all(np.diff(d11.reshape(11, -1), axis=0) >= 0)
+    ind, d = O.knn_topk(q, r[:, :3].reshape(-1), 5)
+    assert np.all(ind.reshape(5, -1)[3:] == -1) and np.all(d.reshape(5, -1)[3:] == np.float32(1e32))

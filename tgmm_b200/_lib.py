@@ -160,6 +160,7 @@ GMEM_FUNCS = {
     "tgmm_assign_supervoxels": (C.c_int, [_VP, _VP, C.c_int32, _VP, C.c_int32]),
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
     "tgmm_write_gmm_xml": (C.c_int, [C.c_char_p, _VP, C.c_int32]),
+    "tgmm_knn_k": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP, _VP, _VP]),
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
     "tgmm_plan_set_knn_group": (C.c_int, [_VP, C.c_int32]),
     "tgmm_plan_set_knn_fusion": (C.c_int, [_VP, C.c_int32]),

@@ -804,6 +804,26 @@ int tgmm_knn(const float* query, int64_t nq, const float* ref, int32_t nref, con
   return TGMM_OK;
 }
 
+int tgmm_knn_k(const float* query, int64_t nq, const float* ref, int32_t nref, int32_t k, const float scale[3],
+               int32_t* ind, float* dist, void* stream) {
+  if (!query || !ref || !scale || !ind || nq < 0 || nref < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_knn_k");
+  if (k < 1 || k > kMaxK) return fail(TGMM_ERR_BAD_SIZE, "tgmm_knn_k: k must be 1..11");
+  if (nq == 0) return TGMM_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nref == 0) {  // nothing to assign: every slot empty
+    TG_CUDA(cudaMemsetAsync(ind, 0xff, sizeof(int32_t) * (size_t)k * nq, st), "tgmm_knn_k");
+    if (dist) {
+      std::vector<float> big((size_t)k * nq, 1e32f);
+      TG_CUDA(cudaMemcpyAsync(dist, big.data(), big.size() * 4, cudaMemcpyHostToDevice, st), "tgmm_knn_k");
+      TG_CUDA(cudaStreamSynchronize(st), "tgmm_knn_k");
+    }
+    return TGMM_OK;
+  }
+  cudaError_t e = knn_grid_topk(query, nq, ref, nref, 1, k, scale, ind, dist, st);
+  if (e != cudaSuccess) return fail(TGMM_ERR_CUDA, "tgmm_knn_k", e);
+  return TGMM_OK;
+}
+
 int tgmm_update_priors(TgmmGaussian* gm, int32_t n, double bp, double np, double ap, double atot, int32_t compute,
                        void* stream) {
   if (!gm || n < 0) return fail(TGMM_ERR_INVALID_ARG, "tgmm_update_priors");

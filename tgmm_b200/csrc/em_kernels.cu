@@ -159,9 +159,10 @@ __device__ __forceinline__ int cell_coord(float y, float lo, float inv_h, int di
 // bound (r*h + delta - eps)^2 of every unvisited cell.  eps absorbs float rounding of
 // the scaled coordinates and of the distance itself.  Refs outside the box sit in the
 // boundary cells, which keeps the bound valid for queries inside the box.
+template <int N>
 __device__ void knn_grid_search(float q0, float q1, float q2, const float* s, const GridGeom& g,
                                 const int32_t* __restrict__ cstart, const float4* __restrict__ refs,
-                                Top5& t) {
+                                TopN<N>& t) {
   const float y[3] = {q0 * s[0], q1 * s[1], q2 * s[2]};
   int c[3];
   float delta = kInfF;
@@ -198,7 +199,7 @@ __device__ void knn_grid_search(float q0, float q1, float q2, const float* s, co
           const int b = cstart[cell], e = cstart[cell + 1];
           for (int k = b; k < e; ++k) {
             const float4 rr = refs[k];
-            top5_insert(t, knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s), __float_as_int(rr.w));
+            topn_insert<N>(t, knn_dist(q0, q1, q2, rr.x, rr.y, rr.z, s), __float_as_int(rr.w));
           }
         }
       }
@@ -207,7 +208,7 @@ __device__ void knn_grid_search(float q0, float q1, float q2, const float* s, co
     const float eps = 4e-3f + 1e-6f * lb;
     if (lb > eps) {
       const float bound = (lb - eps) * (lb - eps);
-      if (t.d[kJ - 1] < bound) break;
+      if (t.d[N - 1] < bound) break;
     }
   }
 }
@@ -2205,11 +2206,14 @@ __global__ void __launch_bounds__(1024) k_sa_geometry(const float* q, int64_t nq
   }
 }
 
-__global__ void k_sa_count(const float* ref, int nref, float s0, float s1, float s2, const FrameState* S, int* cnt,
-                           int* rcell) {
+// Reference point k, coordinate d, sits at ref[k * step + d * comp]: AoS xyz (step 3,
+// comp 1) or SoA x-block, y-block, z-block (step 1, comp nref).
+__global__ void k_sa_count(const float* ref, int nref, int step, int64_t comp, float s0, float s1, float s2,
+                           const FrameState* S, int* cnt, int* rcell) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nref) return;
-  const float ys[3] = {ref[3 * k] * s0, ref[3 * k + 1] * s1, ref[3 * k + 2] * s2};
+  const float* rk = ref + (int64_t)k * step;
+  const float ys[3] = {rk[0] * s0, rk[comp] * s1, rk[2 * comp] * s2};
   int cell = 0;
   for (int d = 0; d < 3; d++)
     if (!isfinite(ys[d]) || fabsf(ys[d]) >= 1e25f) cell = -1;
@@ -2247,11 +2251,13 @@ __global__ void __launch_bounds__(1024) k_sa_scan(const FrameState* S, int* cnt,
   if (threadIdx.x == blockDim.x - 1) start[n] = scan[blockDim.x - 1];
 }
 
-__global__ void k_sa_fill(const float* ref, int nref, const int* rcell, int* cur, float4* refs) {
+__global__ void k_sa_fill(const float* ref, int nref, int step, int64_t comp, const int* rcell, int* cur,
+                          float4* refs) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nref || rcell[k] < 0) return;
   const int pos = atomicAdd(&cur[rcell[k]], 1);
-  refs[pos] = make_float4(ref[3 * k], ref[3 * k + 1], ref[3 * k + 2], __int_as_float(k));
+  const float* rk = ref + (int64_t)k * step;
+  refs[pos] = make_float4(rk[0], rk[comp], rk[2 * comp], __int_as_float(k));
 }
 
 __global__ void k_sa_query(const float* q, int64_t nq, const float* ref, int nref, float s0, float s1, float s2,
@@ -2269,12 +2275,49 @@ __global__ void k_sa_query(const float* q, int64_t nq, const float* ref, int nre
   g.inv_h = S->inv_h;
   Top5 t;
   top5_init(t);
-  knn_grid_search(q0, q1, q2, sc, g, start, refs, t);
+  knn_grid_search<kJ>(q0, q1, q2, sc, g, start, refs, t);
   if (!(t.d[kJ - 1] < kInfF)) {
     top5_init(t);
     for (int k = 0; k < nref; k++) top5_insert(t, knn_dist(q0, q1, q2, ref[3 * k], ref[3 * k + 1], ref[3 * k + 2], sc), k);
   }
   for (int j = 0; j < kJ; j++) ind[(int64_t)j * nq + i] = t.i[j];
+}
+
+// The K nearest (K <= kMaxK) of each query with their squared scaled distances, for the
+// tracking graph's supervoxel kNN: the same grid search, the same exact fallback scan when
+// fewer than K finite distances were found, (distance, index) order; a slot with no
+// reference point closer than 1e32 (squared) gets index -1 and distance 1e32.
+template <int K>
+__global__ void k_sa_query_k(const float* q, int64_t nq, const float* ref, int nref, int step, int64_t comp,
+                             float s0, float s1, float s2, const FrameState* S, const int* start, const float4* refs,
+                             int32_t* ind, float* dist) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  const float sc[3] = {s0, s1, s2};
+  const float q0 = q[i], q1 = q[nq + i], q2 = q[2 * nq + i];
+  GridGeom g;
+  for (int d = 0; d < 3; d++) {
+    g.lo[d] = S->lo[d];
+    g.dims[d] = S->dims[d];
+  }
+  g.h = S->h;
+  g.inv_h = S->inv_h;
+  TopN<K> t;
+  topn_init<K>(t);
+  knn_grid_search<K>(q0, q1, q2, sc, g, start, refs, t);
+  if (!(t.d[K - 1] < kInfF)) {
+    topn_init<K>(t);
+    for (int k = 0; k < nref; k++) {
+      const float* rk = ref + (int64_t)k * step;
+      topn_insert<K>(t, knn_dist(q0, q1, q2, rk[0], rk[comp], rk[2 * comp], sc), k);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    const bool real = t.i[j] != 0x7fffffff && t.d[j] < 1e32f;
+    ind[(int64_t)j * nq + i] = real ? t.i[j] : -1;
+    if (dist) dist[(int64_t)j * nq + i] = real ? t.d[j] : 1e32f;
+  }
 }
 
 cudaError_t knn_grid_standalone(const float* q, int64_t nq, const float* ref, int32_t nref, const float scale[3],
@@ -2295,11 +2338,54 @@ cudaError_t knn_grid_standalone(const float* q, int64_t nq, const float* ref, in
   cudaMemsetAsync(cnt, 0, 4 * (size_t)budget, st);
   k_sa_geometry<<<1, 1024, 0, st>>>(q, nq, scale[0], scale[1], scale[2], nref, budget, S);
   const int gb = (nref + 255) / 256;
-  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, scale[0], scale[1], scale[2], S, cnt, rc);
+  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, 3, 1, scale[0], scale[1], scale[2], S, cnt, rc);
   k_sa_scan<<<1, 1024, 0, st>>>(S, cnt, start, cur);
-  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, rc, cur, refs);
+  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, 3, 1, rc, cur, refs);
   k_sa_query<<<(unsigned)((nq + 127) / 128), 128, 0, st>>>(q, nq, ref, nref, scale[0], scale[1], scale[2], S, start,
                                                           refs, ind);
+  e = cudaGetLastError();
+  cudaFreeAsync(buf, st);
+  return e;
+}
+
+// The K-nearest grid search (1 <= K <= kMaxK) over reference points in AoS or SoA layout
+// (see k_sa_count), with distances; scratch from the stream-ordered allocator.
+cudaError_t knn_grid_topk(const float* q, int64_t nq, const float* ref, int32_t nref, int soa, int K,
+                          const float scale[3], int32_t* ind, float* dist, cudaStream_t st) {
+  const int step = soa ? 1 : 3;
+  const int64_t comp = soa ? nref : 1;
+  const int budget = 2 * nref + 2;
+  char* buf = nullptr;
+  const size_t off_state = 0, off_cnt = 256, off_start = off_cnt + 4 * (size_t)budget,
+               off_cur = off_start + 4 * ((size_t)budget + 1), off_rc = off_cur + 4 * (size_t)budget,
+               off_refs = (off_rc + 4 * (size_t)nref + 255) / 256 * 256, total = off_refs + 16 * (size_t)nref;
+  cudaError_t e = cudaMallocAsync((void**)&buf, total, st);
+  if (e != cudaSuccess) return e;
+  FrameState* S = (FrameState*)(buf + off_state);
+  int* cnt = (int*)(buf + off_cnt);
+  int* start = (int*)(buf + off_start);
+  int* cur = (int*)(buf + off_cur);
+  int* rc = (int*)(buf + off_rc);
+  float4* refs = (float4*)(buf + off_refs);
+  cudaMemsetAsync(cnt, 0, 4 * (size_t)budget, st);
+  k_sa_geometry<<<1, 1024, 0, st>>>(q, nq, scale[0], scale[1], scale[2], nref, budget, S);
+  const int gb = (nref + 255) / 256;
+  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, step, comp, scale[0], scale[1], scale[2], S, cnt, rc);
+  k_sa_scan<<<1, 1024, 0, st>>>(S, cnt, start, cur);
+  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, step, comp, rc, cur, refs);
+  const unsigned grid = (unsigned)((nq + 127) / 128);
+  switch (K) {
+#define TGMM_TOPK_CASE(KK)                                                                                     \
+  case KK:                                                                                                   \
+    k_sa_query_k<KK><<<grid, 128, 0, st>>>(q, nq, ref, nref, step, comp, scale[0], scale[1], scale[2], S, start, \
+                                           refs, ind, dist);                                                 \
+    break;
+    TGMM_TOPK_CASE(1) TGMM_TOPK_CASE(2) TGMM_TOPK_CASE(3) TGMM_TOPK_CASE(4) TGMM_TOPK_CASE(5) TGMM_TOPK_CASE(6)
+    TGMM_TOPK_CASE(7) TGMM_TOPK_CASE(8) TGMM_TOPK_CASE(9) TGMM_TOPK_CASE(10) TGMM_TOPK_CASE(11)
+#undef TGMM_TOPK_CASE
+    default:
+      break;
+  }
   e = cudaGetLastError();
   cudaFreeAsync(buf, st);
   return e;
@@ -2331,9 +2417,9 @@ cudaError_t knn_grid_in_scratch(const float* q, int64_t nq, const float* ref, in
   if (e != cudaSuccess) return e;
   k_sa_geometry<<<1, 1024, 0, st>>>(q, nq, scale[0], scale[1], scale[2], nref, budget, S);
   const int gb = (nref + 255) / 256;
-  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, scale[0], scale[1], scale[2], S, cnt, rc);
+  k_sa_count<<<gb, 256, 0, st>>>(ref, nref, 3, 1, scale[0], scale[1], scale[2], S, cnt, rc);
   k_sa_scan<<<1, 1024, 0, st>>>(S, cnt, start, cur);
-  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, rc, cur, refs);
+  k_sa_fill<<<gb, 256, 0, st>>>(ref, nref, 3, 1, rc, cur, refs);
   k_sa_query<<<(unsigned)((nq + 127) / 128), 128, 0, st>>>(q, nq, ref, nref, scale[0], scale[1], scale[2], S, start,
                                                           refs, ind);
   return cudaGetLastError();

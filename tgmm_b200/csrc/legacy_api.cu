@@ -219,6 +219,36 @@ void knnCUDAinPlace(int* indCUDA, float* queryCUDA, float* refTemp, long long in
   if (tgmm_knn(queryCUDA, query_nb, refTemp, ref_nb, S.knn_scale, indCUDA, nullptr) != TGMM_OK) die("knnCUDAinPlace");
 }
 
+// Host arrays in and out, like the reference's (which allocates and copies per call too);
+// failures print and exit as the reference's HANDLE_ERROR does.
+int knnCUDA_(int* ind, float* dist, float* query, float* ref, long long int query_nb, int ref_nb, int KNN,
+             float* scale, int devCUDA) {
+  if (KNN < 1 || KNN > 11) die("knnCUDA_: KNN must be 1..11");
+  if (ref_nb <= 0) {  // nothing to assign (the reference's early return)
+    if (dist)
+      for (long long i = 0; i < query_nb * KNN; i++) dist[i] = 1e32f;
+    return 0;
+  }
+  check_cuda(cudaSetDevice(devCUDA), "knnCUDA_: cudaSetDevice");
+  float *qd = nullptr, *rd = nullptr, *dd = nullptr;
+  int* id = nullptr;
+  const size_t nq = (size_t)query_nb, nr = (size_t)ref_nb, no = nq * (size_t)KNN;
+  check_cuda(cudaMalloc((void**)&qd, 3 * nq * sizeof(float)), "knnCUDA_: cudaMalloc");
+  check_cuda(cudaMalloc((void**)&rd, 3 * nr * sizeof(float)), "knnCUDA_: cudaMalloc");
+  check_cuda(cudaMalloc((void**)&id, no * sizeof(int)), "knnCUDA_: cudaMalloc");
+  if (dist) check_cuda(cudaMalloc((void**)&dd, no * sizeof(float)), "knnCUDA_: cudaMalloc");
+  check_cuda(cudaMemcpy(qd, query, 3 * nq * sizeof(float), cudaMemcpyHostToDevice), "knnCUDA_: copy");
+  check_cuda(cudaMemcpy(rd, ref, 3 * nr * sizeof(float), cudaMemcpyHostToDevice), "knnCUDA_: copy");
+  if (tgmm_knn_k(qd, query_nb, rd, ref_nb, KNN, scale, id, dd, nullptr) != TGMM_OK) die("knnCUDA_");
+  check_cuda(cudaMemcpy(ind, id, no * sizeof(int), cudaMemcpyDeviceToHost), "knnCUDA_: copy");
+  if (dist) check_cuda(cudaMemcpy(dist, dd, no * sizeof(float), cudaMemcpyDeviceToHost), "knnCUDA_: copy");
+  cudaFree(qd);
+  cudaFree(rd);
+  cudaFree(id);
+  if (dd) cudaFree(dd);
+  return 0;
+}
+
 int selectCUDAdeviceMaxMemory() {
   int count = 0, device = -1;
   size_t best = 0;

@@ -250,6 +250,9 @@ cudaError_t knn_grid_standalone(const float* query, int64_t nq, const float* ref
 
 // grid kNN on caller-provided scratch (no allocation)
 size_t knn_grid_scratch_bytes(int32_t nref);
+constexpr int kMaxK = 11;  // neighbours of the tracking graph's supervoxel kNN (maxKNN)
+cudaError_t knn_grid_topk(const float* q, int64_t nq, const float* ref, int32_t nref, int soa, int K,
+                          const float scale[3], int32_t* ind, float* dist, cudaStream_t st);
 cudaError_t knn_grid_in_scratch(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
                                 const float scale[3], int32_t* ind, cudaStream_t st, void* scratch);
 // records a failure for tgmm_last_error() and returns code
