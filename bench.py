@@ -50,10 +50,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "c1", "batch64", "series", "mixed"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c1", "batch64", "series", "mixed", "frames"], default="c2",
                     help="c2: the 1-Gvoxel frame (default, the headline); c1: 256x256x64; batch64: 64 uneven "
                          "volumes in one batched call vs one at a time; series: one served time series of "
-                         "1024x1024x256 frames; mixed: four served time series of four sizes vs the plain form")
+                         "1024x1024x256 frames; mixed: four served time series of four sizes vs the plain form; "
+                         "frames: frame preparation (trimming, centroids, rescale, SoA/CSR) of the c2 volume "
+                         "from its raw image and label volume")
+    ap.add_argument("--fb-dims", default="", help="frames: X,Y,Z of a smaller volume (profiling)")
+    ap.add_argument("--fb-nuclei", type=int, default=0, help="frames: nuclei of the --fb-dims volume")
     ap.add_argument("--frames", type=int, default=0, help="frames per time series (series/mixed; 0 = default sample)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -660,6 +664,152 @@ def run_served(args):
     print(json.dumps(line), flush=True)
 
 
+FB_STAGES = ["clear+init", "k_fb_scan", "k_fb_ptr", "k_fb_group", "k_fb_trim", "k_fb_order", "k_fb_csr", "k_fb_emit"]
+
+
+def fb_volume(spec, seed, device):
+    """A synthetic frame's supervoxels scattered into full volumes on the device: the raw
+    image (background 100-129, the frame's foreground values) and the label volume (its
+    supervoxels, 1-based).  Returns (raw int16, label int32, n_labels, labelled voxels,
+    summed bounding-box voxels)."""
+    import torch
+    from tgmm_b200 import synth
+    fr = synth.make_frame(spec, synth.random_nuclei(spec, seed), seed)
+    synth.release(fr)
+    X, Y, Z = spec.dims
+    nvol, N, S = X * Y * Z, fr.n_vox, fr.n_sv
+    q = fr.query.reshape(3, N)
+    lp = fr.label_ptr
+    lo = np.minimum.reduceat(q, lp[:-1], axis=1) if N else np.zeros((3, S))
+    hi = np.maximum.reduceat(q, lp[:-1], axis=1) if N else np.zeros((3, S))
+    box = int(np.prod(hi - lo + 1, axis=0).sum())
+    qd = torch.from_numpy(fr.query).to(device).view(3, N).long()
+    lin = qd[0] + X * (qd[1] + Y * qd[2])
+    del qd
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    raw = torch.randint(100, 130, (nvol,), device=device, generator=g, dtype=torch.int32)
+    raw[lin] = torch.from_numpy(fr.raw.astype(np.int32)).to(device)
+    raw = raw.to(torch.int16)
+    lab = torch.zeros(nvol, dtype=torch.int32, device=device)
+    lab[lin] = torch.repeat_interleave(torch.arange(1, S + 1, device=device, dtype=torch.int32),
+                                       torch.from_numpy(np.diff(lp)).to(device))
+    return raw, lab, S, N, box
+
+
+def run_frames(args):
+    """Frame preparation (tgmm_frame_build) of one volume per rank: value = volumes per second
+    over all ranks, with the raw and label volumes resident; e2e adds their upload from pinned
+    host memory every step."""
+    import torch
+    import torch.distributed as dist
+    from tgmm_b200 import engine as E
+    from tgmm_b200 import synth
+    world, rank, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if args.fb_dims:
+        dims = tuple(int(x) for x in args.fb_dims.split(","))
+        spec = synth.VolumeSpec(dims=dims, n_nuclei=args.fb_nuclei or max(1, dims[0] * dims[1] * dims[2] // 53687),
+                                axis_min=4.0, axis_max=8.0)
+    else:
+        spec = synth.C2
+    raw, lab, S, Nfg, box = fb_volume(spec, args.seed + rank, dev)
+    X, Y, Z = spec.dims
+    nvol = X * Y * Z
+    b = E.FrameBuilder((X, Y, Z), S, device=dev, max_vox=Nfg)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        b.build(raw, lab, read_thr=False)
+    stages = []
+    for _ in range(3):
+        ms = []
+        b.build(raw, lab, stage_ms=ms, read_thr=False)
+        stages.append(ms)
+    stage = np.mean(np.array(stages), axis=0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            f, _ = b.build(raw, lab, read_thr=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        raw_h, lab_h = raw.cpu().pin_memory(), lab.cpu().pin_memory()
+        for _ in range(2):
+            raw.copy_(raw_h, non_blocking=True)
+            lab.copy_(lab_h, non_blocking=True)
+            b.build(raw, lab, read_thr=False)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            raw.copy_(raw_h, non_blocking=True)
+            lab.copy_(lab_h, non_blocking=True)
+            b.build(raw, lab, read_thr=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * args.steps / (float(te.item()) / 1e3), "unit": "volumes/s",
+               "h2d_bytes_per_step": 6 * nvol, "d2h_bytes_per_step": 64,
+               "path": "pinned raw + label upload, then tgmm_frame_build (reads its sizes back)"}
+    # roofline of the dominant step, from the events between the steps
+    algo = {"k_fb_scan": 4 * nvol, "k_fb_group": 4 * box + 8 * Nfg,
+            "k_fb_emit": 6 * Nfg + 16 * f.n_vox}
+    top = int(np.argmax(stage))
+    name = FB_STAGES[top]
+    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")))["hbm_gbs"]
+    if name in algo:
+        ach = algo[name] / (stage[top] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "algorithmic_bytes": algo[name]}
+    else:
+        roof = {"bound": "latency", "kernel": name, "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                "traffic": None}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        raw_n = raw.cpu().numpy().view(np.uint16).reshape(Z, Y, X)
+        lab_n = lab.cpu().numpy().view(np.uint32).reshape(Z, Y, X)
+        t0 = time.perf_counter()
+        rc, o = O.frame_build(raw_n, lab_n, S, max_vox=Nfg)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / dt, "unit": "volumes/s", "cores": 1, "kind": "port", "cpu_model": cpu_model(),
+               "sample": f"the whole volume once through the oracle's single-thread C restatement of the "
+                         f"reference's host build ({dt:.2f} s)",
+               "same_outputs": bool(rc == 0 and o["n_vox"] == f.n_vox and
+                                    np.array_equal(o["img"], f.img.cpu().numpy()) and
+                                    np.array_equal(o["query"], f.query.cpu().numpy()))}
+    if rank == 0:
+        line = {"metric": "frame preparations/s", "value": value, "unit": "volumes/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/u32 -> f32",
+                "data": "synthetic (seeded nuclei volume; labels = its supervoxels)",
+                "config": {"workload": f"frame preparation of a {X}x{Y}x{Z} uint16 volume with {S} labelled "
+                                       f"supervoxels ({Nfg} labelled voxels): trim, erase, centroids, "
+                                       f"background, [0,1] rescale, SoA/CSR",
+                           "n_vox_out": f.n_vox, "n_sv_out": f.n_sv, "l2": "inputs larger than L2"},
+                "stage_ms": dict(zip(FB_STAGES, [round(float(x), 4) for x in stage])),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+                "gpu_launches": 8 * args.steps}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -668,6 +818,8 @@ def main():
         run_batch64(args)
     elif args.workload in ("series", "mixed"):
         run_served(args)
+    elif args.workload == "frames":
+        run_frames(args)
     else:
         run_ours(args)
 

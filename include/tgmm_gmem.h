@@ -50,7 +50,8 @@ enum {
   TGMM_ERR_OOM = 6,           /* device allocation failed */
   TGMM_ERR_DEVICE_FLAG = 7,   /* a kernel reported an internal inconsistency */
   TGMM_ERR_NOT_SET = 8,       /* regularisation constants not set (reference exit(3)) */
-  TGMM_ERR_ADMISSION = 9      /* served form: request does not fit in free HBM */
+  TGMM_ERR_ADMISSION = 9,     /* served form: request does not fit in free HBM */
+  TGMM_ERR_NO_SUPERVOXEL = 10 /* frame preparation erased every supervoxel (reference exit(5)) */
 };
 
 /* Per-Gaussian record.  Byte-for-byte the reference's 288-byte
@@ -213,6 +214,52 @@ int tgmm_knn_noalloc(const float* query_dev, int64_t n_query, const float* ref_x
 int tgmm_update_priors(TgmmGaussian* gm_dev, int32_t n_gauss, double beta_pct,
                        double nu_pct, double alpha_pct, double alpha_total,
                        int32_t compute_alpha_total, void* stream);
+
+/* Frame preparation on the device: the EM's input arrays from the raw 16-bit image and the
+ * label volume of the segmentation at tau (mainTrackingGaussianMixtureModel.cpp:553-651 and
+ * 774-870; supervoxel.cpp:1410-1450, 1556-1747).  Each supervoxel is trimmed as the
+ * reference's trimSupervoxel does -- threshold = the largest of its (n - max_nuclei_size)-th
+ * value, its (1 - max_percentile) percentile and Otsu's threshold, then the voxels above it
+ * connected to its brightest voxel through the conn3d neighbourhood (linear-index offsets, as
+ * the reference builds them) -- supervoxels left with fewer than min_nuclei_size voxels are
+ * erased in the reference's order (each erased index trades places with the current last
+ * supervoxel), the centroids are the FP32 raw-intensity-weighted means of the kept voxels,
+ * each kept supervoxel's threshold is subtracted from its voxels (16-bit), every other voxel
+ * counts as 0, and the volume is rescaled to [0,1] as mylib's Scale_Array_To_Range does.
+ *
+ * raw, label: X*Y*Z device arrays (x fastest; label 16-byte aligned); label l in
+ * 1..n_labels puts a voxel in supervoxel l-1 (0: none); X*Y*Z < 2^32.  workspace: device memory of at least
+ * tgmm_frame_build_bytes(dims, n_labels) bytes (no other allocation is made).  Outputs
+ * (device): query[3*max_vox] (SoA with stride *n_vox), img[max_vox],
+ * centroids[3*max_sv] (SoA with stride *n_sv), label_ptr[max_sv+1], and, if thr is not
+ * NULL, thr[max_sv] (each output supervoxel's threshold).  *n_vox and *n_sv are set on
+ * TGMM_OK and on TGMM_ERR_BAD_SIZE (outputs too small; nothing written).  Synchronises
+ * `stream`.  The reference's deltaZ split of tall supervoxels (main:566-592) needs the
+ * segmentation hierarchy and is not part of this step. */
+typedef struct TgmmFrameBuildParams {
+  int32_t max_nuclei_size; /* 3000 */
+  float max_percentile;    /* 0.4 */
+  int32_t conn3d;          /* 4, 6, 8, 26 or 74 (6) */
+  int32_t min_nuclei_size; /* 50 */
+} TgmmFrameBuildParams;
+void tgmm_frame_build_default_params(TgmmFrameBuildParams* p);
+/* Measurement hook (no reference counterpart): tgmm_frame_build with CUDA events between its
+ * steps; stage_ms[TGMM_FRAME_BUILD_STAGES] receives each step's milliseconds: clear + init,
+ * volume scan, supervoxel CSR, grouping, trimming, erase order, output CSR, emission. */
+#define TGMM_FRAME_BUILD_STAGES 8
+int64_t tgmm_frame_build_bytes(const int32_t dims[3], int32_t n_labels);
+int tgmm_frame_build(const uint16_t* raw_dev, const uint32_t* label_dev, const int32_t dims[3],
+                     int32_t n_labels, const TgmmFrameBuildParams* p, void* workspace_dev,
+                     int64_t workspace_bytes, float* query_dev, float* img_dev,
+                     float* centroids_dev, int64_t* label_ptr_dev, uint16_t* thr_dev,
+                     int64_t max_vox, int32_t max_sv, int64_t* n_vox, int32_t* n_sv,
+                     void* stream);
+int tgmm_frame_build_timed(const uint16_t* raw_dev, const uint32_t* label_dev,
+                           const int32_t dims[3], int32_t n_labels, const TgmmFrameBuildParams* p,
+                           void* workspace_dev, int64_t workspace_bytes, float* query_dev,
+                           float* img_dev, float* centroids_dev, int64_t* label_ptr_dev,
+                           uint16_t* thr_dev, int64_t max_vox, int32_t max_sv, int64_t* n_vox,
+                           int32_t* n_sv, void* stream, float* stage_ms);
 
 /* Allocate device buffers and upload one frame from host arrays (legacy ownership model). */
 int tgmm_frame_upload(const float* query_host, const float* img_host,

@@ -215,3 +215,99 @@ def ref_knn_k(query, ref_soa, k, scale=(1.0, 1.0, 2.0)):
     if rc != 0:
         raise RuntimeError(f"reference supervoxel kNN failed ({rc})")
     return ind, dist
+
+
+# ---------------------------------------------------------------------------
+# Frame preparation from a supervoxel label volume (frame_oracle.c).
+# ---------------------------------------------------------------------------
+class OrFrameParams(C.Structure):
+    _fields_ = [("max_size", C.c_int32), ("max_pct", C.c_float), ("conn", C.c_int32), ("min_size", C.c_int32)]
+
+
+def frame_params(max_size=3000, max_pct=0.4, conn=6, min_size=50) -> OrFrameParams:
+    return OrFrameParams(max_size, max_pct, conn, min_size)
+
+
+def frame_build(raw, label, n_labels, p: OrFrameParams | None = None, max_vox=None):
+    """The EM's input arrays from a raw 16-bit volume and a supervoxel label volume (shape
+    (Z, Y, X), labels 1..n_labels, 0 = none).  Returns (rc, dict)."""
+    p = p or frame_params()
+    raw = np.ascontiguousarray(raw, np.uint16)
+    label = np.ascontiguousarray(label, np.uint32)
+    Z, Y, X = raw.shape
+    dims = np.array([X, Y, Z], np.int32)
+    nvol = raw.size if max_vox is None else int(max_vox)
+    query = np.zeros(3 * nvol, np.float32)
+    img = np.zeros(nvol, np.float32)
+    cent = np.zeros(3 * n_labels, np.float32)
+    lptr = np.zeros(n_labels + 1, np.int64)
+    thr = np.zeros(n_labels, np.uint16)
+    n_vox = C.c_int64(0)
+    n_sv = C.c_int32(0)
+    L = lib()
+    vp = C.c_void_p
+    L.or_frame_build.argtypes = [vp, vp, vp, C.c_int32, C.POINTER(OrFrameParams), vp, vp, vp, vp, vp, C.c_int64,
+                                 C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    L.or_frame_build.restype = C.c_int
+    rc = L.or_frame_build(_p(raw), _p(label), _p(dims), n_labels, C.byref(p), _p(query), _p(img), _p(cent), _p(lptr),
+                          _p(thr), nvol, n_labels, C.byref(n_vox), C.byref(n_sv))
+    N, S = n_vox.value, n_sv.value
+    out = dict(n_vox=N, n_sv=S)
+    if rc == 0:
+        out.update(query=query[:3 * N].copy(), img=img[:N].copy(), cent=cent[:3 * S].copy(),
+                   lptr=lptr[:S + 1].copy(), thr=thr[:S].copy())
+    return rc, out
+
+
+def erase_order(erased):
+    e = np.ascontiguousarray(erased, np.uint8)
+    order = np.zeros(e.shape[0], np.int32)
+    L = lib()
+    L.or_erase_order.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.or_erase_order(_p(e), e.shape[0], _p(order))
+    return order[:e.shape[0] - int((e != 0).sum())]
+
+
+def supervoxel_lists(label, n_labels):
+    """Per label, its voxels' linear indices in ascending order (CSR)."""
+    flat = np.ascontiguousarray(label, np.uint32).reshape(-1)
+    idx = np.nonzero(flat)[0]
+    lab = flat[idx].astype(np.int64) - 1
+    order = np.argsort(lab, kind="stable")
+    lin = idx[order].astype(np.uint64)
+    ptr = np.zeros(n_labels + 1, np.int64)
+    np.add.at(ptr, lab + 1, 1)
+    return np.cumsum(ptr), lin
+
+
+REF_F1_SO = os.path.join(HERE, "_ref", "libtgmm_ref_f1.so")
+
+
+def ref_f1_available() -> bool:
+    return os.path.exists(REF_F1_SO)
+
+
+def ref_trim_stats(raw, ptr, lin, max_size=3000, max_pct=0.4, conn=6):
+    """The reference's own trimSupervoxel<uint16>() and weightedGaussianStatistics<uint16>(true)
+    (temporalLogicalRules/supervoxel.cpp) on each supervoxel of the CSR (ptr, lin)."""
+    ref = C.CDLL(REF_F1_SO)
+    vp = C.c_void_p
+    ref.ref_trim_stats.argtypes = [vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_float, C.c_int32, vp, vp, vp, vp, vp]
+    ref.ref_trim_stats.restype = C.c_int
+    raw = np.ascontiguousarray(raw, np.uint16)
+    Z, Y, X = raw.shape
+    dims = np.array([X, Y, Z], np.int32)
+    n = ptr.shape[0] - 1
+    ptr = np.ascontiguousarray(ptr, np.int64)
+    lin = np.ascontiguousarray(lin, np.uint64)
+    thr = np.zeros(n, np.uint16)
+    cnt = np.zeros(n, np.int64)
+    lin_out = np.zeros(max(1, lin.shape[0]), np.uint64)
+    cent = np.zeros(3 * n, np.float32)
+    inten = np.zeros(n, np.float32)
+    rc = ref.ref_trim_stats(_p(raw), _p(dims), _p(ptr), _p(lin), n, max_size, max_pct, conn, _p(thr), _p(cnt),
+                            _p(lin_out), _p(cent), _p(inten))
+    if rc != 0:
+        raise RuntimeError(f"reference trimming failed ({rc})")
+    kept = [lin_out[ptr[s]:ptr[s] + cnt[s]].copy() for s in range(n)]
+    return dict(thr=thr, cnt=cnt, lists=kept, cent=cent.reshape(n, 3), intensity=inten)

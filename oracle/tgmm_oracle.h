@@ -109,6 +109,26 @@ int or_em_run(const float* query, const float* img, const float* centroids,
               const int64_t* lptr, int64_t N, int32_t S, OrGaussian* g, int32_t K,
               const OrParams* p, float* rnk, int32_t* ind, double* ll_hist, OrStats* st);
 
+/* Frame preparation from a supervoxel label volume (frame_oracle.c): trimming, size
+ * filter, centroids, background subtraction, [0,1] rescale, SoA/CSR arrays. */
+typedef struct OrFrameParams {
+  int32_t max_size;  /* maxNucleiSize (3000) */
+  float max_pct;     /* maxPercentileTrimSV (0.4) */
+  int32_t conn;      /* conn3DsvTrim (6) */
+  int32_t min_size;  /* minNucleiSize (50) */
+} OrFrameParams;
+int or_conn_offsets(int32_t conn, const int32_t dims[3], int64_t* off);
+float or_otsu(const float* v, int32_t n);
+uint16_t or_trim_threshold(const uint16_t* val, int32_t n, int32_t max_size, float max_pct, int32_t* seed);
+int64_t or_trim_flood(const uint32_t* lin, const uint16_t* val, int64_t n, int32_t seed, uint16_t thr,
+                      const int64_t* off, int32_t noff, int64_t nvol, uint8_t* keep);
+void or_erase_order(const uint8_t* erased, int32_t n, int32_t* order);
+/* 0 ok, 1 bad argument (label above n_labels, unknown neighbourhood), 2 outputs too small
+ * (n_vox/n_sv still set), 5 every supervoxel erased. */
+int or_frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3], int32_t n_labels,
+                   const OrFrameParams* p, float* query, float* img, float* cent, int64_t* lptr, uint16_t* thr_out,
+                   int64_t max_vox, int32_t max_sv, int64_t* n_vox, int32_t* n_sv);
+
 int or_num_threads(void);
 void or_set_num_threads(int n);
 

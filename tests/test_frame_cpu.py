@@ -1,0 +1,146 @@
+"""Frame preparation without a GPU: the oracle's restatement of the tracking program's input
+build (trimming, size filter, erase order, centroids, background subtraction, rescale, SoA
+arrays) checked against the reference's own trimSupervoxel / weightedGaussianStatistics
+compiled from its sources, the device's closed form of the erase order checked against the
+reference's swap loop, and the C ABI's argument checks."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import _volumes as V
+from oracle import oracle as O
+from tgmm_b200 import _lib as L
+
+CASES = [
+    dict(seed=1),
+    dict(seed=2, conn=26),
+    dict(seed=3, max_size=60),            # the size rank sets the threshold
+    dict(seed=4, max_pct=0.15, conn=8),   # the percentile sets it
+    dict(seed=5, conn=4, min_size=20),
+    dict(seed=6, conn=74, max_size=200),
+]
+
+
+def _coords(lin, X, Y):
+    lin = lin.astype(np.int64)
+    return np.stack([lin % X, (lin // X) % Y, lin // (X * Y)]).astype(np.float32)
+
+
+@pytest.mark.skipif(not O.ref_f1_available(), reason="reference trimming harness not built")
+@pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
+def test_oracle_matches_reference_trimming_and_centroids(case):
+    c = dict(max_size=3000, max_pct=0.4, conn=6, min_size=50)
+    c.update({k: v for k, v in case.items() if k != "seed"})
+    raw, lab, n = V.make(seed=case["seed"])
+    Z, Y, X = raw.shape
+    rc, o = O.frame_build(raw, lab, n, O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"]))
+    assert rc == 0
+    ptr, lin = O.supervoxel_lists(lab, n)
+    r = O.ref_trim_stats(raw, ptr, lin, c["max_size"], c["max_pct"], c["conn"])
+    erased = (r["cnt"] < c["min_size"]).astype(np.uint8)
+    assert erased.any() and not erased.all()
+    order = O.erase_order(erased)
+    N, S = o["n_vox"], o["n_sv"]
+    assert S == len(order) and N == int(sum(r["cnt"][s] for s in order))
+    q = o["query"].reshape(3, N)
+    cent = o["cent"].reshape(3, S)
+    for p, s in enumerate(order):
+        a, b = o["lptr"][p], o["lptr"][p + 1]
+        assert o["thr"][p] == r["thr"][s]
+        assert b - a == r["cnt"][s]
+        np.testing.assert_array_equal(q[:, a:b], _coords(r["lists"][s], X, Y))
+        np.testing.assert_array_equal(cent[:, p].view(np.uint32), r["cent"][s].view(np.uint32))
+
+
+def test_oracle_rescale_and_background():
+    """img is the kept voxels' raw - thr, with every other voxel 0, rescaled to [0,1] as mylib's
+    Scale_Array_To_Range does: (float)(f * (v + shift)), f = 1 / (max - min), shift = -min."""
+    raw, lab, n = V.make(seed=7)
+    Z, Y, X = raw.shape
+    rc, o = O.frame_build(raw, lab, n)
+    assert rc == 0
+    N = o["n_vox"]
+    q = o["query"].reshape(3, N).astype(np.int64)
+    lin = q[0] + X * (q[1] + Y * q[2])
+    thr = np.repeat(o["thr"].astype(np.int64), np.diff(o["lptr"]))
+    sub = (raw.reshape(-1)[lin].astype(np.int64) - thr) & 0xFFFF
+    assert (sub > 0).all()
+    f = 1.0 / float(sub.max())
+    np.testing.assert_array_equal(o["img"], (f * (sub.astype(np.float32).astype(np.float64) + 0.0)).astype(np.float32))
+    assert o["img"].max() == 1.0 and o["img"].min() > 0
+
+
+def _closed_form(erased):
+    """The device's erase order: output p is p when kept, else the end of the chain from
+    n-m+rank(p), each erased tail position q stepping to n-m+rank(q)."""
+    e = np.asarray(erased, bool)
+    n, m = len(e), int(e.sum())
+    S = n - m
+    rank = np.concatenate([[0], np.cumsum(e)[:-1]])
+    nxt = np.arange(n)
+    nxt[S:] = np.where(e[S:], S + rank[S:], np.arange(S, n))
+    for _ in range(64):  # pointer jumping
+        nxt[S:] = nxt[nxt[S:]]
+    return np.array([nxt[S + rank[p]] if e[p] else p for p in range(S)], np.int32)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_erase_order_closed_form_is_the_reference_swap_loop(seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 400))
+    erased = rng.random(n) < rng.choice([0.05, 0.3, 0.7, 0.95])
+    if erased.all():
+        erased[rng.integers(0, n)] = False
+    np.testing.assert_array_equal(_closed_form(erased), O.erase_order(erased.astype(np.uint8)))
+
+
+def test_erase_order_examples():
+    # erase {1, 3} of 5: 3 trades with 4, then 1 with the new last (the old 4)
+    np.testing.assert_array_equal(O.erase_order(np.array([0, 1, 0, 1, 0], np.uint8)), [0, 4, 2])
+    np.testing.assert_array_equal(O.erase_order(np.array([0, 1, 0, 0, 1], np.uint8)), [0, 3, 2])
+
+
+def test_oracle_reports_errors_like_the_reference():
+    raw, lab, n = V.make(seed=8, n_nuclei=4)
+    assert O.frame_build(raw, lab, n, O.frame_params(min_size=10 ** 6))[0] == 5  # every supervoxel erased
+    bad = lab.copy()
+    bad[0, 0, 0] = n + 1
+    assert O.frame_build(raw, bad, n)[0] == 1
+    assert O.frame_build(raw, lab, n, O.frame_params(conn=75))[0] == 1
+
+
+def test_otsu_threshold_cases():
+    lib = O.lib()
+    lib.or_otsu.argtypes = [C.c_void_p, C.c_int32]
+    lib.or_otsu.restype = C.c_float
+    flat = np.full(10, 7.0, np.float32)
+    assert lib.or_otsu(flat.ctypes.data, 10) == -np.finfo(np.float32).max
+    two = np.array([10.0] * 5 + [200.0] * 5, np.float32)
+    t = lib.or_otsu(two.ctypes.data, 10)
+    assert 10.0 <= t < 200.0
+
+
+def test_abi_frame_build_checks_arguments_without_a_gpu():
+    lib = L.gmem()
+    dims = (C.c_int32 * 3)(64, 48, 16)
+    assert lib.tgmm_frame_build_bytes(dims, 0) == -1
+    b1, b2 = lib.tgmm_frame_build_bytes(dims, 10), lib.tgmm_frame_build_bytes(dims, 1000)
+    assert 0 < b1 < b2
+    assert b1 >= 10 * 64 * 48 * 16  # lists, values, queues, flood bits
+    p = L.TgmmFrameBuildParams()
+    lib.tgmm_frame_build_default_params(C.byref(p))
+    assert (p.max_nuclei_size, round(p.max_percentile, 6), p.conn3d, p.min_nuclei_size) == (3000, 0.4, 6, 50)
+    nv, ns = C.c_int64(0), C.c_int32(0)
+    rc = lib.tgmm_frame_build(None, None, dims, 10, C.byref(p), None, 0, None, None, None, None, None, 0, 0,
+                              C.byref(nv), C.byref(ns), None)
+    assert rc == L.TGMM_ERR_INVALID_ARG
+    fake = C.c_void_p(256)  # never dereferenced: the checks below fail first
+    p.conn3d = 75
+    rc = lib.tgmm_frame_build(fake, fake, dims, 10, C.byref(p), fake, b1, fake, fake, fake, fake, None, 1, 1,
+                              C.byref(nv), C.byref(ns), None)
+    assert rc == L.TGMM_ERR_INVALID_ARG and b"conn3d" in lib.tgmm_last_error()
+    p.conn3d = 6
+    rc = lib.tgmm_frame_build(fake, fake, dims, 10, C.byref(p), fake, b1 - 1, fake, fake, fake, fake, None, 1, 1,
+                              C.byref(nv), C.byref(ns), None)
+    assert rc == L.TGMM_ERR_BAD_SIZE

@@ -29,6 +29,8 @@ TGMM_ERR_OOM = 6
 TGMM_ERR_DEVICE_FLAG = 7
 TGMM_ERR_NOT_SET = 8
 TGMM_ERR_ADMISSION = 9
+TGMM_ERR_NO_SUPERVOXEL = 10
+TGMM_FRAME_BUILD_STAGES = 8
 
 TGMM_LL_AS_REFERENCE = 0
 TGMM_LL_TRUE = 1
@@ -105,6 +107,11 @@ class TgmmSynthConfig(C.Structure):
     ]
 
 
+class TgmmFrameBuildParams(C.Structure):
+    _fields_ = [("max_nuclei_size", C.c_int32), ("max_percentile", C.c_float), ("conn3d", C.c_int32),
+                ("min_nuclei_size", C.c_int32)]
+
+
 class TgmmServerDesc(C.Structure):
     _fields_ = [
         ("device", C.c_int32), ("hbm_budget", C.c_int64), ("lanes", C.c_int32), ("max_batch_frames", C.c_int32),
@@ -161,6 +168,14 @@ GMEM_FUNCS = {
     "tgmm_write_rnk_file": (C.c_int, [C.c_char_p, _VP, _VP, C.c_int32]),
     "tgmm_write_gmm_xml": (C.c_int, [C.c_char_p, _VP, C.c_int32]),
     "tgmm_knn_k": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP, _VP, _VP]),
+    "tgmm_frame_build_default_params": (None, [C.POINTER(TgmmFrameBuildParams)]),
+    "tgmm_frame_build_bytes": (C.c_int64, [_VP, C.c_int32]),
+    "tgmm_frame_build": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.POINTER(TgmmFrameBuildParams), _VP, C.c_int64, _VP,
+                                   _VP, _VP, _VP, _VP, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int32), _VP]),
+    "tgmm_frame_build_timed": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.POINTER(TgmmFrameBuildParams), _VP, C.c_int64,
+                                         _VP, _VP, _VP, _VP, _VP, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int32), _VP, _VP]),
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
     "tgmm_plan_set_knn_group": (C.c_int, [_VP, C.c_int32]),
     "tgmm_plan_set_knn_fusion": (C.c_int, [_VP, C.c_int32]),

@@ -1,0 +1,730 @@
+// frame_build.cu -- frame preparation on the device: the EM's input arrays (coordinates SoA,
+// intensities, CSR, centroids) from the raw 16-bit image and the label volume of the
+// segmentation at tau, as the tracking program builds them on the host
+// (mainTrackingGaussianMixtureModel.cpp:553-651, 774-870; supervoxel.cpp:1410-1450,
+// 1556-1747; hierarchicalSegmentation.cpp:1064-1092; mylib/array.p:2769-2822).
+//
+//   k_fb_scan    one pass over the label volume (16-byte loads, all-background groups
+//                skipped): voxels and bounding box per supervoxel (lanes of a warp with the
+//                same label add once);
+//   k_fb_ptr     the supervoxels' CSR (one block);
+//   k_fb_group   a warp per supervoxel walks its box in raster order and lists its voxels
+//                in ascending linear index (ballot + popcount: no sort), with their values;
+//   k_fb_trim    a block per supervoxel: the trimming threshold (two order statistics by a
+//                two-pass radix select, Otsu's threshold from a 256-bin histogram), the
+//                flood from the brightest voxel (level-synchronous, a bit per voxel claimed
+//                with atomicOr), and for kept supervoxels the FP32 centroid in the
+//                reference's summation order and the range of the background-subtracted
+//                values;
+//   k_fb_order   one block: the reference's erase order (a closed form of its
+//                swap-to-the-back loop, resolved by pointer jumping), the output CSR, the
+//                [0,1] rescale factors;
+//   k_fb_emit    a warp per output supervoxel writes its kept voxels in ascending order.
+// Every rounding step is written with explicit _rn intrinsics so that no multiply-add is
+// contracted: the results are the host build's bits.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "tgmm_internal.cuh"
+
+namespace tgmm {
+namespace {
+
+constexpr int kFbMaxOff = 74;
+constexpr int kFbTrimThreads = 256;
+
+struct FbBox {
+  int32_t lo[3], hi[3];
+};
+
+struct FbOffsets {
+  int64_t off[kFbMaxOff];
+  int32_t n;
+};
+
+// per-call scalars shared by the kernels
+struct FbStat {
+  uint32_t flags;        // 1: a label above n_labels; 2: every supervoxel erased; 4: lists inconsistent
+  uint32_t sub_min;      // range of the background-subtracted values of kept voxels
+  uint32_t sub_max;
+  uint32_t pad;
+  unsigned long long kept_vox;
+  int64_t n_vox;         // output sizes
+  int32_t n_sv;
+  int32_t scaled;        // the rescale applies (the volume is not constant)
+  double fct, shift;     // img = (float)(fct * ((double)v + shift))
+};
+
+struct FbWork {
+  int32_t* cnt;     // [n] voxels per supervoxel (untrimmed)
+  FbBox* box;       // [n]
+  int64_t* uptr;    // [n+1] CSR of the untrimmed lists
+  uint32_t* ulin;   // [nvol] lists: linear indices, ascending within a supervoxel
+  uint16_t* uval;   // [nvol] their raw values
+  uint32_t* queue;  // [nvol] flood queues (a supervoxel's at its list offset)
+  uint32_t* bits;   // [nvol/32] flood: reached voxels
+  int32_t* tcnt;    // [n] voxels kept by trimming
+  uint32_t* thr;    // [n] trimming thresholds
+  float* tcent;     // [3n] centroids (AoS)
+  int32_t* rank;    // [n] erased supervoxels before each index
+  int32_t* order;   // [n] output supervoxel -> supervoxel
+  int32_t* nxt;     // [n] pointer jumping over the tail positions
+  FbStat* stat;
+};
+
+size_t align_up(size_t x) { return (x + 255) / 256 * 256; }
+
+// Carves the workspace; returns its size (base may be null to measure).
+size_t carve(char* base, int64_t nvol, int32_t n, FbWork* w) {
+  size_t at = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + at : nullptr;
+    at += align_up(bytes);
+    return p;
+  };
+  w->cnt = (int32_t*)take(4 * (size_t)n);
+  w->box = (FbBox*)take(sizeof(FbBox) * (size_t)n);
+  w->uptr = (int64_t*)take(8 * ((size_t)n + 1));
+  w->ulin = (uint32_t*)take(4 * (size_t)nvol);
+  w->uval = (uint16_t*)take(2 * (size_t)nvol);
+  w->queue = (uint32_t*)take(4 * (size_t)nvol);
+  w->bits = (uint32_t*)take(4 * (size_t)((nvol + 31) / 32));
+  w->tcnt = (int32_t*)take(4 * (size_t)n);
+  w->thr = (uint32_t*)take(4 * (size_t)n);
+  w->tcent = (float*)take(12 * (size_t)n);
+  w->rank = (int32_t*)take(4 * (size_t)n);
+  w->order = (int32_t*)take(4 * (size_t)n);
+  w->nxt = (int32_t*)take(4 * (size_t)n);
+  w->stat = (FbStat*)take(sizeof(FbStat));
+  return at;
+}
+
+__global__ void __launch_bounds__(256) k_fb_init(int32_t n, FbWork w) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) {
+    FbStat* st = w.stat;
+    st->flags = 0;
+    st->sub_min = 0xffffffffu;
+    st->sub_max = 0;
+    st->kept_vox = 0;
+    st->n_vox = 0;
+    st->n_sv = 0;
+  }
+  if (s >= n) return;
+  w.cnt[s] = 0;
+  for (int d = 0; d < 3; d++) {
+    w.box[s].lo[d] = 0x7fffffff;
+    w.box[s].hi[d] = -1;
+  }
+}
+
+// One label of the scan: its lanes (those that matched) add their count and extent once.
+__device__ __forceinline__ void scan_label(uint32_t l, uint32_t v, uint32_t X, uint32_t XY, int32_t n, int lane,
+                                           FbWork& w) {
+  if (l > (uint32_t)n) {
+    atomicOr(&w.stat->flags, 1u);
+    l = 0;
+  }
+  const unsigned m = __match_any_sync(0xffffffffu, l);
+  const uint32_t z = v / XY, r = v - z * XY, y = r / X, x = r - y * X;
+  const int32_t x0 = (int32_t)__reduce_min_sync(m, x), x1 = (int32_t)__reduce_max_sync(m, x);
+  const int32_t y0 = (int32_t)__reduce_min_sync(m, y), y1 = (int32_t)__reduce_max_sync(m, y);
+  const int32_t z0 = (int32_t)__reduce_min_sync(m, z), z1 = (int32_t)__reduce_max_sync(m, z);
+  if (l != 0 && (m & ((1u << lane) - 1u)) == 0) {
+    const int s = (int)l - 1;
+    FbBox* b = &w.box[s];
+    atomicAdd(&w.cnt[s], __popc(m));
+    atomicMin(&b->lo[0], x0);
+    atomicMax(&b->hi[0], x1);
+    atomicMin(&b->lo[1], y0);
+    atomicMax(&b->hi[1], y1);
+    atomicMin(&b->lo[2], z0);
+    atomicMax(&b->hi[2], z1);
+  }
+}
+
+// One pass over the label volume, four labels per lane (16-byte loads); warps whose 128
+// labels are all 0 (most of a volume) do nothing more.  Coordinates in 32-bit arithmetic
+// (X*Y*Z < 2^32).
+__global__ void __launch_bounds__(256) k_fb_scan(const uint32_t* __restrict__ label, int64_t nvol, int32_t X,
+                                                 int32_t Y, int32_t n, FbWork w) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t XY = (uint32_t)X * (uint32_t)Y;
+  const int64_t nq = nvol / 4;  // whole 16-byte groups
+  const uint4* l4 = reinterpret_cast<const uint4*>(label);
+  const int64_t G = (int64_t)gridDim.x * blockDim.x;
+  // two groups in flight per lane
+  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)); base < nq; base += 2 * G) {
+    uint4 q[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t i = base + u * G + lane;
+      q[u] = i < nq ? __ldcs(l4 + i) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      if (__ballot_sync(0xffffffffu, (q[u].x | q[u].y | q[u].z | q[u].w) != 0) == 0) continue;
+      const uint32_t v = (uint32_t)(4 * (base + u * G + lane));
+      scan_label(q[u].x, v, X, XY, n, lane, w);
+      scan_label(q[u].y, v + 1, X, XY, n, lane, w);
+      scan_label(q[u].z, v + 2, X, XY, n, lane, w);
+      scan_label(q[u].w, v + 3, X, XY, n, lane, w);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) {  // the last nvol % 4 labels
+    const int64_t v = 4 * nq + lane;
+    scan_label(v < nvol ? label[v] : 0u, (uint32_t)v, X, XY, n, lane, w);
+  }
+}
+
+// Exclusive scan of `count(i)` over i < n by one block of 1024 threads (contiguous chunks per
+// thread); out[i] = sum of the counts before i, returns the total to every thread.
+template <typename T, typename F>
+__device__ T block_scan_1024(int32_t n, F count, T* out) {
+  __shared__ T part[1024];
+  const int t = threadIdx.x;
+  const int per = (n + 1023) / 1024;
+  const int a = min(n, t * per), b = min(n, a + per);
+  T sum = 0;
+  for (int i = a; i < b; i++) sum += count(i);
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const T v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  T run = part[t] - sum;
+  for (int i = a; i < b; i++) {
+    out[i] = run;
+    run += count(i);
+  }
+  const T total = part[1023];
+  __syncthreads();
+  return total;
+}
+
+__global__ void __launch_bounds__(1024) k_fb_ptr(int32_t n, FbWork w) {
+  const int64_t total = block_scan_1024<int64_t>(n, [&](int i) { return (int64_t)w.cnt[i]; }, w.uptr);
+  if (threadIdx.x == 0) w.uptr[n] = total;
+}
+
+__global__ void __launch_bounds__(256) k_fb_group(const uint32_t* __restrict__ label, const uint16_t* __restrict__ raw,
+                                                  int32_t X, int32_t Y, int32_t n, FbWork w) {
+  const int lane = threadIdx.x & 31;
+  const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  if (s >= n) return;
+  const FbBox bx = w.box[s];
+  const uint32_t want = (uint32_t)s + 1u;
+  int64_t at = w.uptr[s];
+  const unsigned below = (1u << lane) - 1u;
+  for (int32_t z = bx.lo[2]; z <= bx.hi[2]; z++)
+    for (int32_t y = bx.lo[1]; y <= bx.hi[1]; y++) {
+      const int64_t row = ((int64_t)z * Y + y) * X;
+      for (int32_t x0 = bx.lo[0]; x0 <= bx.hi[0]; x0 += 32) {
+        const int32_t x = x0 + lane;
+        const bool in = x <= bx.hi[0] && label[row + x] == want;
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+          const int64_t p = at + __popc(m & below);
+          w.ulin[p] = (uint32_t)(row + x);
+          w.uval[p] = raw[row + x];
+        }
+        at += __popc(m);
+      }
+    }
+  if (lane == 0 && at != w.uptr[s + 1]) atomicOr(&w.stat->flags, 4u);  // box and count disagree
+}
+
+// The k-th smallest value (0-based) from a histogram of 256 bins: bucket and rank within it.
+__device__ void hist_select(const int32_t* h, int32_t k, int32_t* bucket, int32_t* rest) {
+  int32_t run = 0;
+  for (int b = 0; b < 256; b++) {
+    if (run + h[b] > k) {
+      *bucket = b;
+      *rest = k - run;
+      return;
+    }
+    run += h[b];
+  }
+  *bucket = 255;
+  *rest = 0;
+}
+
+__global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __restrict__ label,
+                                                            const uint16_t* __restrict__ raw, int64_t nvol,
+                                                            int32_t X, int32_t Y, int32_t n, int32_t max_size,
+                                                            float max_pct, int32_t min_size, FbOffsets off,
+                                                            FbWork w) {
+  __shared__ int32_t h_hi[256], h_lo1[256], h_lo2[256], h_ot[256];
+  __shared__ float s_sumb[256];
+  __shared__ float s_var[256];
+  __shared__ int32_t s_wb[256];
+  __shared__ uint32_t s_min, s_max, s_seed, s_tail;
+  __shared__ int32_t s_b1, s_r1, s_b2, s_r2, s_v1, s_v2;
+  __shared__ float s_mm;
+  __shared__ int32_t s_best;
+  __shared__ float st_v[32], st_x[32], st_y[32], st_z[32];
+  const int s = blockIdx.x, t = threadIdx.x;
+  if (w.stat->flags) return;
+  const int64_t a = w.uptr[s];
+  const int32_t N = (int32_t)(w.uptr[s + 1] - a);
+  const uint32_t* lin = w.ulin + a;
+  const uint16_t* val = w.uval + a;
+  if (N == 0) {
+    if (t == 0) {
+      w.tcnt[s] = 0;
+      w.thr[s] = 0;
+    }
+    return;
+  }
+  h_hi[t] = 0;
+  h_lo1[t] = 0;
+  h_lo2[t] = 0;
+  h_ot[t] = 0;
+  if (t == 0) {
+    s_min = 0xffffffffu;
+    s_max = 0;
+    s_seed = 0xffffffffu;
+    s_tail = 0;
+  }
+  __syncthreads();
+  // pass 1: range and the high bytes
+  uint32_t mn = 0xffffffffu, mx = 0;
+  for (int32_t i = t; i < N; i += kFbTrimThreads) {
+    const uint32_t v = val[i];
+    mn = min(mn, v);
+    mx = max(mx, v);
+    atomicAdd(&h_hi[v >> 8], 1);
+  }
+  atomicMin(&s_min, mn);
+  atomicMax(&s_max, mx);
+  __syncthreads();
+  const int32_t k1 = max(0, N - max_size);
+  int32_t k2 = __float2int_rz(__fmul_rn(__fsub_rn(1.0f, max_pct), (float)N));
+  k2 = min(max(k2, 0), N - 1);  // the reference reads past the end only for max_pct < 1/N
+  if (t == 0) {
+    hist_select(h_hi, k1, &s_b1, &s_r1);
+    hist_select(h_hi, k2, &s_b2, &s_r2);
+    const float fmin = (float)s_min, fmax = (float)s_max;
+    s_mm = __fdiv_rn(255.0f, __fsub_rn(fmax, fmin));
+  }
+  __syncthreads();
+  const float fmin = (float)s_min, mm = s_mm;
+  const bool otsu = isfinite(mm);
+  // pass 2: low bytes inside the two buckets, Otsu's histogram, the first brightest voxel
+  for (int32_t i = t; i < N; i += kFbTrimThreads) {
+    const uint32_t v = val[i];
+    if ((int32_t)(v >> 8) == s_b1) atomicAdd(&h_lo1[v & 255], 1);
+    if ((int32_t)(v >> 8) == s_b2) atomicAdd(&h_lo2[v & 255], 1);
+    if (otsu) {
+      const int b = __float2int_rz(__fmul_rn(__fsub_rn((float)v, fmin), mm));
+      atomicAdd(&h_ot[min(b, 255)], 1);
+    }
+    if (v == s_max) atomicMin(&s_seed, (uint32_t)i);
+  }
+  __syncthreads();
+  if (t == 0) {
+    int32_t l1, l2, r;
+    hist_select(h_lo1, s_r1, &l1, &r);
+    hist_select(h_lo2, s_r2, &l2, &r);
+    s_v1 = (s_b1 << 8) | l1;
+    s_v2 = (s_b2 << 8) | l2;
+    // Otsu: the between-class sums in the reference's order
+    float sum_b = 0.0f;
+    int32_t wb = 0;
+    for (int b = 0; b < 256; b++) {
+      wb += h_ot[b];
+      sum_b = __fadd_rn(sum_b, (float)(b * h_ot[b]));
+      s_wb[b] = wb;
+      s_sumb[b] = sum_b;
+    }
+  }
+  __syncthreads();
+  if (otsu) {
+    const int32_t wb = s_wb[t], wf = N - wb;
+    float var = 0.0f;
+    if (wb > 0 && wf > 0) {
+      const float sum = s_sumb[255], sb = s_sumb[t];
+      const float m_b = __fdiv_rn(sb, (float)wb), m_f = __fdiv_rn(__fsub_rn(sum, sb), (float)wf);
+      const float d = __fsub_rn(m_b, m_f);
+      var = __fmul_rn(__fmul_rn(__fmul_rn((float)wb, (float)wf), d), d);
+    }
+    s_var[t] = var;
+  }
+  __syncthreads();
+  if (t == 0) {
+    float t3 = -FLT_MAX;
+    if (otsu) {
+      float vmax = 0.0f;
+      int32_t best = 0;
+      for (int b = 0; b < 256; b++)
+        if (s_var[b] > vmax) {
+          vmax = s_var[b];
+          best = b;
+        }
+      t3 = __fadd_rn(__fdiv_rn((float)best, mm), fmin);
+    }
+    float thr = (float)s_v1;
+    if ((float)s_v2 > thr) thr = (float)s_v2;
+    if (t3 > thr) thr = t3;
+    const uint32_t th = (uint32_t)(uint16_t)__float2uint_rz(thr);
+    w.thr[s] = th;
+    s_best = (int32_t)th;
+    const uint32_t seed = s_seed;
+    if (val[seed] > th) {
+      const uint32_t v = lin[seed];
+      atomicOr(&w.bits[v >> 5], 1u << (v & 31));
+      w.queue[a] = v;
+      s_tail = 1;
+    }
+  }
+  __syncthreads();
+  // the flood, level by level: a voxel joins when it carries this label, is brighter than the
+  // threshold and its bit was not yet set
+  const uint32_t want = (uint32_t)s + 1u, th = (uint32_t)s_best;
+  uint32_t* q = w.queue + a;
+  uint32_t head = 0;
+  for (;;) {
+    const uint32_t tail = s_tail;
+    __syncthreads();
+    if (head == tail) break;
+    for (uint32_t i = head + t; i < tail; i += kFbTrimThreads) {
+      const int64_t v = q[i];
+      for (int j = 0; j < off.n; j++) {
+        const int64_t nb = v + off.off[j];
+        if (nb < 0 || nb >= nvol) continue;
+        if (label[nb] != want || raw[nb] <= th) continue;
+        const uint32_t bit = 1u << (nb & 31);
+        if (atomicOr(&w.bits[nb >> 5], bit) & bit) continue;
+        q[atomicAdd(&s_tail, 1u)] = (uint32_t)nb;
+      }
+    }
+    head = tail;
+    __syncthreads();
+  }
+  const int32_t kept = (int32_t)s_tail;
+  if (t == 0) w.tcnt[s] = kept;
+  if (kept < min_size || t >= 32) return;
+  // warp 0: the centroid in list order (FP32, as the reference sums it) and the range of the
+  // background-subtracted values
+  const int lane = t;
+  const unsigned below = (1u << lane) - 1u;
+  float sw = 0.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+  uint32_t smin = 0xffffffffu, smax = 0;
+  for (int32_t i0 = 0; i0 < N; i0 += 32) {
+    const int32_t i = i0 + lane;
+    bool in = false;
+    uint32_t v = 0, r = 0;
+    if (i < N) {
+      v = lin[i];
+      r = val[i];
+      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (in) {
+      const int p = __popc(m & below);
+      st_v[p] = (float)r;
+      st_x[p] = (float)(v % (uint32_t)X);
+      st_y[p] = (float)((v / (uint32_t)X) % (uint32_t)Y);
+      st_z[p] = (float)(v / ((uint32_t)X * (uint32_t)Y));
+      const uint32_t sub = (uint16_t)(r - th);
+      smin = min(smin, sub);
+      smax = max(smax, sub);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const int c = __popc(m);
+      for (int p = 0; p < c; p++) {
+        const float I = st_v[p];
+        sw = __fadd_rn(sw, I);
+        c0 = __fadd_rn(c0, __fmul_rn(I, st_x[p]));
+        c1 = __fadd_rn(c1, __fmul_rn(I, st_y[p]));
+        c2 = __fadd_rn(c2, __fmul_rn(I, st_z[p]));
+      }
+    }
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+    smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+  }
+  if (lane == 0) {
+    const bool zero = (double)sw < 1e-5;
+    w.tcent[3 * s] = zero ? 0.0f : __fdiv_rn(c0, sw);
+    w.tcent[3 * s + 1] = zero ? 0.0f : __fdiv_rn(c1, sw);
+    w.tcent[3 * s + 2] = zero ? 0.0f : __fdiv_rn(c2, sw);
+    atomicMin(&w.stat->sub_min, smin);
+    atomicMax(&w.stat->sub_max, smax);
+    atomicAdd(&w.stat->kept_vox, (unsigned long long)kept);
+  }
+}
+
+// The reference erases each index of the ascending list E (m of n), from the last, by trading
+// places with the current last supervoxel.  Step i (erasing E[i]) swaps with position n-m+i,
+// whose content is then: the supervoxel at n-m+i if that index is kept, else -- it was itself
+// erased, as E[j] for some j > i, and received position n-m+j's content -- the content of
+// n-m+j.  These chains only climb, so output p is p when kept, else the end of the chain from
+// n-m+rank(p).
+__global__ void __launch_bounds__(1024) k_fb_order(int32_t n, int64_t nvol, int32_t min_size, FbWork w) {
+  __shared__ int s_changed;
+  const int t = threadIdx.x;
+  if (w.stat->flags) return;
+  const int32_t m = block_scan_1024<int32_t>(n, [&](int i) { return (int32_t)(w.tcnt[i] < min_size); }, w.rank);
+  FbStat* st = w.stat;
+  if (m >= n) {
+    if (t == 0) {
+      st->flags |= 2u;
+      st->n_sv = 0;
+      st->n_vox = 0;
+    }
+    return;
+  }
+  const int32_t S = n - m;
+  for (int32_t q = S + t; q < n; q += 1024) w.nxt[q] = w.tcnt[q] < min_size ? S + w.rank[q] : q;
+  __syncthreads();
+  for (int round = 0; round < 40; round++) {
+    if (t == 0) s_changed = 0;
+    __syncthreads();
+    int changed = 0;
+    for (int32_t q = S + t; q < n; q += 1024) {
+      const int32_t j = w.nxt[q], k = w.nxt[j];
+      if (k != j) {
+        w.nxt[q] = k;
+        changed = 1;
+      }
+    }
+    if (changed) s_changed = 1;
+    __syncthreads();
+    if (!s_changed) break;
+    __syncthreads();
+  }
+  for (int32_t p = t; p < S; p += 1024) w.order[p] = w.tcnt[p] < min_size ? w.nxt[S + w.rank[p]] : p;
+  if (t == 0) {
+    const int64_t N = (int64_t)st->kept_vox;
+    double lo = (double)st->sub_min, hi = (double)st->sub_max;
+    if (N < nvol) {
+      lo = lo < 0.0 ? lo : 0.0;
+      hi = hi > 0.0 ? hi : 0.0;
+    }
+    double f = 1.0;
+    f /= hi - lo;
+    st->fct = f;
+    st->shift = 0.0 / f - lo;
+    st->scaled = hi != lo;
+    st->n_sv = S;
+    st->n_vox = N;
+  }
+}
+
+// Output CSR (one block) over the output order.
+__global__ void __launch_bounds__(1024) k_fb_csr(int64_t max_vox, int32_t max_sv, FbWork w, int64_t* lptr) {
+  const FbStat* st = w.stat;
+  if (st->flags) return;
+  const int32_t S = st->n_sv;
+  if (S > max_sv || st->n_vox > max_vox) return;
+  const int64_t total = block_scan_1024<int64_t>(S, [&](int p) { return (int64_t)w.tcnt[w.order[p]]; }, lptr);
+  if (threadIdx.x == 0) lptr[S] = total;
+}
+
+__global__ void __launch_bounds__(256) k_fb_emit(int32_t X, int32_t Y, int64_t max_vox, int32_t max_sv, FbWork w,
+                                                 const int64_t* __restrict__ lptr, float* query, float* img,
+                                                 float* cent, uint16_t* thr_out) {
+  const FbStat* st = w.stat;
+  const int lane = threadIdx.x & 31;
+  const int p = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  if (st->flags) return;
+  const int32_t S = st->n_sv;
+  const int64_t N = st->n_vox;
+  if (p >= S || S > max_sv || N > max_vox) return;
+  const int s = w.order[p];
+  const uint32_t th = w.thr[s];
+  const bool scaled = st->scaled;
+  const double f = st->fct, sh = st->shift;
+  const int64_t a = w.uptr[s];
+  const int32_t n = (int32_t)(w.uptr[s + 1] - a);
+  int64_t at = lptr[p];
+  const unsigned below = (1u << lane) - 1u;
+  for (int32_t i0 = 0; i0 < n; i0 += 32) {
+    const int32_t i = i0 + lane;
+    bool in = false;
+    uint32_t v = 0;
+    if (i < n) {
+      v = w.ulin[a + i];
+      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (in) {
+      const int64_t o = at + __popc(m & below);
+      query[o] = (float)(v % (uint32_t)X);
+      query[N + o] = (float)((v / (uint32_t)X) % (uint32_t)Y);
+      query[2 * N + o] = (float)(v / ((uint32_t)X * (uint32_t)Y));
+      const float sub = (float)(uint16_t)(w.uval[a + i] - th);
+      img[o] = scaled ? (float)__dmul_rn(f, __dadd_rn((double)sub, sh)) : sub;
+    }
+    at += __popc(m);
+  }
+  if (lane == 0) {
+    for (int d = 0; d < 3; d++) cent[(int64_t)d * S + p] = w.tcent[3 * s + d];
+    if (thr_out) thr_out[p] = (uint16_t)th;
+  }
+}
+
+int fb_offsets(int32_t conn, const int32_t dims[3], FbOffsets* o) {
+  const int64_t X = dims[0], XY = (int64_t)dims[0] * dims[1];
+  int n = 0;
+  switch (conn) {
+    case 4:
+    case 6:
+      if (conn == 6) o->off[n++] = -XY;
+      o->off[n++] = -X;
+      o->off[n++] = -1;
+      o->off[n++] = 1;
+      o->off[n++] = X;
+      if (conn == 6) o->off[n++] = XY;
+      break;
+    case 8:
+    case 26:
+    case 74: {
+      const int rz = conn == 8 ? 0 : 1, rxy = conn == 74 ? 2 : 1;
+      for (int z = -rz; z <= rz; z++)
+        for (int y = -rxy; y <= rxy; y++)
+          for (int x = -rxy; x <= rxy; x++)
+            if (x || y || z) o->off[n++] = x + X * y + XY * z;
+      break;
+    }
+    default:
+      return 0;
+  }
+  o->n = n;
+  return n;
+}
+
+}  // namespace
+}  // namespace tgmm
+
+using namespace tgmm;
+
+extern "C" void tgmm_frame_build_default_params(TgmmFrameBuildParams* p) {
+  if (!p) return;
+  p->max_nuclei_size = 3000;
+  p->max_percentile = 0.4f;
+  p->conn3d = 6;
+  p->min_nuclei_size = 50;
+}
+
+extern "C" int64_t tgmm_frame_build_bytes(const int32_t dims[3], int32_t n_labels) {
+  if (!dims || dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || n_labels < 1) return -1;
+  const int64_t nvol = (int64_t)dims[0] * dims[1] * dims[2];
+  FbWork w;
+  return (int64_t)carve(nullptr, nvol, n_labels, &w);
+}
+
+namespace {
+// The build; with `ev` (TGMM_FRAME_BUILD_STAGES + 1 events) an event is recorded before the
+// first step and after each.
+int frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3], int32_t n_labels,
+                const TgmmFrameBuildParams* p, void* workspace, int64_t workspace_bytes, float* query, float* img,
+                float* cent, int64_t* lptr, uint16_t* thr, int64_t max_vox, int32_t max_sv, int64_t* n_vox_out,
+                int32_t* n_sv_out, cudaStream_t st, cudaEvent_t* ev) {
+  static const char* kWhat = "tgmm_frame_build";
+  if (!raw || !label || !dims || !p || !workspace || !query || !img || !cent || !lptr || !n_vox_out || !n_sv_out ||
+      n_labels < 1 || max_vox < 0 || max_sv < 0)
+    return report_error(TGMM_ERR_INVALID_ARG, kWhat, cudaSuccess);
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1)
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build: dimensions", cudaSuccess);
+  const int64_t nvol = (int64_t)dims[0] * dims[1] * dims[2];
+  if (nvol >= ((int64_t)1 << 32) || n_labels > (1 << 24))
+    return report_error(TGMM_ERR_BAD_SIZE, "tgmm_frame_build: more than 2^32 voxels or 2^24 labels", cudaSuccess);
+  if (p->max_nuclei_size < 0 || !(p->max_percentile >= 0.0f && p->max_percentile <= 1.0f))
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build: trimming parameters", cudaSuccess);
+  if (((uintptr_t)label & 15) != 0)
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build: label volume not 16-byte aligned", cudaSuccess);
+  FbOffsets off;
+  if (!fb_offsets(p->conn3d, dims, &off))
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build: conn3d must be 4, 6, 8, 26 or 74", cudaSuccess);
+  FbWork w;
+  if ((int64_t)carve(nullptr, nvol, n_labels, &w) > workspace_bytes)
+    return report_error(TGMM_ERR_BAD_SIZE, "tgmm_frame_build: workspace smaller than tgmm_frame_build_bytes",
+                        cudaSuccess);
+  carve((char*)workspace, nvol, n_labels, &w);
+  const int32_t X = dims[0], Y = dims[1], n = n_labels;
+  int stage = 0;
+  auto mark = [&]() {
+    if (ev) cudaEventRecord(ev[stage++], st);
+  };
+  mark();
+  cudaError_t e = cudaMemsetAsync(w.bits, 0, 4 * (size_t)((nvol + 31) / 32), st);
+  if (e != cudaSuccess) return report_error(TGMM_ERR_CUDA, kWhat, e);
+  const unsigned warp_blocks = (unsigned)(((int64_t)n * 32 + 255) / 256);
+  k_fb_init<<<(n + 255) / 256, 256, 0, st>>>(n, w);
+  mark();
+  const int64_t span = (nvol / 4 + 511) / 512;
+  k_fb_scan<<<(unsigned)(span < 1 ? 1 : span < 148 * 8 ? span : 148 * 8), 256, 0, st>>>(label, nvol, X, Y, n, w);
+  mark();
+  k_fb_ptr<<<1, 1024, 0, st>>>(n, w);
+  mark();
+  k_fb_group<<<warp_blocks, 256, 0, st>>>(label, raw, X, Y, n, w);
+  mark();
+  k_fb_trim<<<n, kFbTrimThreads, 0, st>>>(label, raw, nvol, X, Y, n, p->max_nuclei_size, p->max_percentile,
+                                          p->min_nuclei_size, off, w);
+  mark();
+  k_fb_order<<<1, 1024, 0, st>>>(n, nvol, p->min_nuclei_size, w);
+  mark();
+  k_fb_csr<<<1, 1024, 0, st>>>(max_vox, max_sv, w, lptr);
+  mark();
+  k_fb_emit<<<warp_blocks, 256, 0, st>>>(X, Y, max_vox, max_sv, w, lptr, query, img, cent, thr);
+  mark();
+  FbStat h;
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, w.stat, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return report_error(TGMM_ERR_CUDA, kWhat, e);
+  if (h.flags & 1u) return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build: a label above n_labels", cudaSuccess);
+  if (h.flags & 4u)
+    return report_error(TGMM_ERR_DEVICE_FLAG, "tgmm_frame_build: supervoxel lists inconsistent", cudaSuccess);
+  *n_vox_out = h.n_vox;
+  *n_sv_out = h.n_sv;
+  if (h.flags & 2u)
+    return report_error(TGMM_ERR_NO_SUPERVOXEL, "tgmm_frame_build: every supervoxel was erased", cudaSuccess);
+  if (h.n_vox > max_vox || h.n_sv > max_sv)
+    return report_error(TGMM_ERR_BAD_SIZE, "tgmm_frame_build: more voxels or supervoxels than the outputs hold",
+                        cudaSuccess);
+  return TGMM_OK;
+}
+}  // namespace
+
+extern "C" int tgmm_frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3], int32_t n_labels,
+                                const TgmmFrameBuildParams* p, void* workspace, int64_t workspace_bytes, float* query,
+                                float* img, float* cent, int64_t* lptr, uint16_t* thr, int64_t max_vox, int32_t max_sv,
+                                int64_t* n_vox_out, int32_t* n_sv_out, void* stream) {
+  return frame_build(raw, label, dims, n_labels, p, workspace, workspace_bytes, query, img, cent, lptr, thr, max_vox,
+                     max_sv, n_vox_out, n_sv_out, (cudaStream_t)stream, nullptr);
+}
+
+extern "C" int tgmm_frame_build_timed(const uint16_t* raw, const uint32_t* label, const int32_t dims[3],
+                                      int32_t n_labels, const TgmmFrameBuildParams* p, void* workspace,
+                                      int64_t workspace_bytes, float* query, float* img, float* cent, int64_t* lptr,
+                                      uint16_t* thr, int64_t max_vox, int32_t max_sv, int64_t* n_vox_out,
+                                      int32_t* n_sv_out, void* stream, float* stage_ms) {
+  if (!stage_ms) return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build_timed", cudaSuccess);
+  cudaEvent_t ev[TGMM_FRAME_BUILD_STAGES + 1] = {};
+  int created = 0, rc = TGMM_OK;
+  for (; created <= TGMM_FRAME_BUILD_STAGES; created++)
+    if (cudaEventCreate(&ev[created]) != cudaSuccess) {
+      rc = report_error(TGMM_ERR_CUDA, "tgmm_frame_build_timed: events", cudaGetLastError());
+      break;
+    }
+  if (rc == TGMM_OK)
+    rc = frame_build(raw, label, dims, n_labels, p, workspace, workspace_bytes, query, img, cent, lptr, thr, max_vox,
+                     max_sv, n_vox_out, n_sv_out, (cudaStream_t)stream, ev);
+  for (int i = 0; i < TGMM_FRAME_BUILD_STAGES; i++) {
+    stage_ms[i] = 0.0f;
+    if (rc == TGMM_OK || rc == TGMM_ERR_BAD_SIZE || rc == TGMM_ERR_NO_SUPERVOXEL)
+      cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+  }
+  for (int i = 0; i < created; i++) cudaEventDestroy(ev[i]);
+  return rc;
+}

@@ -179,3 +179,53 @@ def update_priors(gm_dev: torch.Tensor, n: int, beta_pct=0.01, nu_pct=1.0, alpha
     s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
     L.check(L.gmem().tgmm_update_priors(gm_dev.data_ptr(), n, beta_pct, nu_pct, alpha_pct, alpha_total,
                                         1 if compute_alpha_total else 0, s), "tgmm_update_priors")
+
+
+class FrameBuilder:
+    """Frame preparation on the device (tgmm_frame_build) for volumes of one size: the raw
+    16-bit image and the segmentation's label volume in, the EM's input arrays out.  The
+    workspace and the output buffers are allocated once, for at most max_vox kept voxels
+    (default: every voxel) and no supervoxel erased."""
+
+    def __init__(self, dims, n_labels, device="cuda", max_nuclei_size=3000, max_percentile=0.4, conn3d=6,
+                 min_nuclei_size=50, max_vox=None):
+        self.lib = L.gmem()
+        self.dims = (C.c_int32 * 3)(*dims)
+        self.n_labels = int(n_labels)
+        self.params = L.TgmmFrameBuildParams(max_nuclei_size, max_percentile, conn3d, min_nuclei_size)
+        nbytes = self.lib.tgmm_frame_build_bytes(self.dims, self.n_labels)
+        if nbytes < 0:
+            raise ValueError("tgmm_frame_build_bytes: bad dimensions or label count")
+        nvol = int(dims[0]) * int(dims[1]) * int(dims[2])
+        self.nvol = nvol
+        self.max_vox = nvol if max_vox is None else int(max_vox)
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        self.query = torch.empty(3 * self.max_vox, dtype=torch.float32, device=device)
+        self.img = torch.empty(self.max_vox, dtype=torch.float32, device=device)
+        self.cent = torch.empty(3 * self.n_labels, dtype=torch.float32, device=device)
+        self.lptr = torch.empty(self.n_labels + 1, dtype=torch.int64, device=device)
+        self.thr = torch.empty(self.n_labels, dtype=torch.int16, device=device)  # uint16 bits
+
+    def build(self, raw: torch.Tensor, label: torch.Tensor, n_gauss: int = 0, stream=None, stage_ms=None,
+              read_thr=True):
+        """raw: uint16 bits (any 2-byte dtype), label: 4-byte labels (1..n_labels, 0 none), both
+        X*Y*Z with x fastest.  Returns (DeviceFrame, thresholds as uint16 numpy or None).
+        stage_ms: a list that receives each step's milliseconds (the timed form)."""
+        if raw.numel() != self.nvol or label.numel() != self.nvol or raw.element_size() != 2 or \
+                label.element_size() != 4:
+            raise ValueError("raw must hold X*Y*Z 16-bit values and label X*Y*Z 32-bit labels")
+        n_vox, n_sv = C.c_int64(0), C.c_int32(0)
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        args = (raw.data_ptr(), label.data_ptr(), self.dims, self.n_labels, C.byref(self.params),
+                self.workspace.data_ptr(), self.workspace.numel(), self.query.data_ptr(), self.img.data_ptr(),
+                self.cent.data_ptr(), self.lptr.data_ptr(), self.thr.data_ptr(), self.max_vox, self.n_labels,
+                C.byref(n_vox), C.byref(n_sv), s)
+        if stage_ms is None:
+            L.check(self.lib.tgmm_frame_build(*args), "tgmm_frame_build")
+        else:
+            ms = (C.c_float * L.TGMM_FRAME_BUILD_STAGES)()
+            L.check(self.lib.tgmm_frame_build_timed(*args, ms), "tgmm_frame_build_timed")
+            stage_ms[:] = list(ms)
+        N, S = n_vox.value, n_sv.value
+        f = DeviceFrame(self.query[:3 * N], self.img[:N], self.cent[:3 * S], self.lptr[:S + 1], n_gauss)
+        return f, (self.thr[:S].cpu().numpy().view(np.uint16).copy() if read_thr else None)
