@@ -770,11 +770,19 @@ def run_frames(args):
             "k_fb_emit": 6 * Nfg + 16 * f.n_vox}
     top = int(np.argmax(stage))
     name = FB_STAGES[top]
-    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")))["hbm_gbs"]
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
     if name in algo:
         ach = algo[name] / (stage[top] * 1e-3) / 1e9
+        traffic = None
+        try:  # the committed ncu capture of the scan on a smaller volume, scaled by its voxels
+            with open(os.path.join(ROOT, "profiles", "frame_scan_traffic.json")) as fh:
+                tr = json.load(fh)
+            if name == tr["kernel"]:
+                traffic = (tr["dram_bytes_read_per_launch"] + tr["dram_bytes_write_per_launch"]) / tr["n_voxels"] * nvol
+        except Exception:
+            pass
         roof = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                 "algorithmic_bytes": algo[name]}
     else:
         roof = {"bound": "latency", "kernel": name, "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,

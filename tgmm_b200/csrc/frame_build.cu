@@ -33,13 +33,15 @@ namespace {
 
 constexpr int kFbMaxOff = 74;
 constexpr int kFbTrimThreads = 256;
+constexpr int kFbScanDepth = 4;  // 16-byte label groups each lane of the scan has in flight
 
 struct FbBox {
   int32_t lo[3], hi[3];
 };
 
 struct FbOffsets {
-  int64_t off[kFbMaxOff];
+  int64_t off[kFbMaxOff];    // linear-index offsets, as the reference builds them
+  int8_t d[kFbMaxOff][3];    // their (dx, dy, dz)
   int32_t n;
 };
 
@@ -63,7 +65,8 @@ struct FbWork {
   uint32_t* ulin;   // [nvol] lists: linear indices, ascending within a supervoxel
   uint16_t* uval;   // [nvol] their raw values
   uint32_t* queue;  // [nvol] flood queues (a supervoxel's at its list offset)
-  uint32_t* bits;   // [nvol/32] flood: reached voxels
+  uint32_t* bits;   // [nvol/32] flood: reached voxels (supervoxels whose box exceeds shared memory)
+  uint8_t* ukeep;   // [nvol] 1 where a list entry survived trimming
   int32_t* tcnt;    // [n] voxels kept by trimming
   uint32_t* thr;    // [n] trimming thresholds
   float* tcent;     // [3n] centroids (AoS)
@@ -90,6 +93,7 @@ size_t carve(char* base, int64_t nvol, int32_t n, FbWork* w) {
   w->uval = (uint16_t*)take(2 * (size_t)nvol);
   w->queue = (uint32_t*)take(4 * (size_t)nvol);
   w->bits = (uint32_t*)take(4 * (size_t)((nvol + 31) / 32));
+  w->ukeep = (uint8_t*)take((size_t)nvol);
   w->tcnt = (int32_t*)take(4 * (size_t)n);
   w->thr = (uint32_t*)take(4 * (size_t)n);
   w->tcent = (float*)take(12 * (size_t)n);
@@ -154,16 +158,17 @@ __global__ void __launch_bounds__(256) k_fb_scan(const uint32_t* __restrict__ la
   const int64_t nq = nvol / 4;  // whole 16-byte groups
   const uint4* l4 = reinterpret_cast<const uint4*>(label);
   const int64_t G = (int64_t)gridDim.x * blockDim.x;
-  // two groups in flight per lane
-  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)); base < nq; base += 2 * G) {
-    uint4 q[2];
+  // kFbScanDepth groups in flight per lane
+  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)); base < nq;
+       base += kFbScanDepth * G) {
+    uint4 q[kFbScanDepth];
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < kFbScanDepth; u++) {
       const int64_t i = base + u * G + lane;
       q[u] = i < nq ? __ldcs(l4 + i) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < kFbScanDepth; u++) {
       if (__ballot_sync(0xffffffffu, (q[u].x | q[u].y | q[u].z | q[u].w) != 0) == 0) continue;
       const uint32_t v = (uint32_t)(4 * (base + u * G + lane));
       scan_label(q[u].x, v, X, XY, n, lane, w);
@@ -219,7 +224,32 @@ __global__ void __launch_bounds__(256) k_fb_group(const uint32_t* __restrict__ l
   const FbBox bx = w.box[s];
   const uint32_t want = (uint32_t)s + 1u;
   int64_t at = w.uptr[s];
+  if (at == w.uptr[s + 1]) return;  // no voxels: no box
   const unsigned below = (1u << lane) - 1u;
+  if (bx.hi[0] - bx.lo[0] < 32) {  // one chunk per row: four rows' labels in flight
+    const int32_t x = bx.lo[0] + lane;
+    const bool xin = x <= bx.hi[0];
+    for (int32_t z = bx.lo[2]; z <= bx.hi[2]; z++)
+      for (int32_t y = bx.lo[1]; y <= bx.hi[1]; y += 4) {
+        uint32_t l[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          l[u] = (xin && y + u <= bx.hi[1]) ? label[((int64_t)z * Y + y + u) * X + x] : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const bool in = l[u] == want;
+          const unsigned m = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const int64_t p = at + __popc(m & below), v = ((int64_t)z * Y + y + u) * X + x;
+            w.ulin[p] = (uint32_t)v;
+            w.uval[p] = raw[v];
+          }
+          at += __popc(m);
+        }
+      }
+    if (lane == 0 && at != w.uptr[s + 1]) atomicOr(&w.stat->flags, 4u);  // box and count disagree
+    return;
+  }
   for (int32_t z = bx.lo[2]; z <= bx.hi[2]; z++)
     for (int32_t y = bx.lo[1]; y <= bx.hi[1]; y++) {
       const int64_t row = ((int64_t)z * Y + y) * X;
@@ -238,41 +268,62 @@ __global__ void __launch_bounds__(256) k_fb_group(const uint32_t* __restrict__ l
   if (lane == 0 && at != w.uptr[s + 1]) atomicOr(&w.stat->flags, 4u);  // box and count disagree
 }
 
-// The k-th smallest value (0-based) from a histogram of 256 bins: bucket and rank within it.
-__device__ void hist_select(const int32_t* h, int32_t k, int32_t* bucket, int32_t* rest) {
-  int32_t run = 0;
-  for (int b = 0; b < 256; b++) {
-    if (run + h[b] > k) {
-      *bucket = b;
-      *rest = k - run;
-      return;
-    }
-    run += h[b];
+// The k-th smallest value (0-based) from a 256-bin histogram, by one warp: each lane holds 8
+// bins, a scan over the lanes finds the lane holding it.  0 <= k < the histogram's total.
+__device__ void warp_hist_select(const int32_t* h, int32_t k, int32_t* bucket, int32_t* rest) {
+  const int lane = threadIdx.x & 31;
+  int32_t c[8], sum = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    c[i] = h[lane * 8 + i];
+    sum += c[i];
   }
-  *bucket = 255;
-  *rest = 0;
+  int32_t inc = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  int32_t run = inc - sum;
+  if (run <= k && k < inc) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (run + c[i] > k) {
+        *bucket = lane * 8 + i;
+        *rest = k - run;
+        break;
+      }
+      run += c[i];
+    }
+  }
+}
+
+constexpr int kFbMaskWords = 2048;  // bounding boxes up to 65536 voxels flood in shared memory
+
+__device__ __forceinline__ void decode(uint32_t v, uint32_t X, uint32_t XY, int32_t* x, int32_t* y, int32_t* z) {
+  const uint32_t zz = v / XY, r = v - zz * XY, yy = r / X;
+  *x = (int32_t)(r - yy * X), *y = (int32_t)yy, *z = (int32_t)zz;
 }
 
 __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __restrict__ label,
                                                             const uint16_t* __restrict__ raw, int64_t nvol,
-                                                            int32_t X, int32_t Y, int32_t n, int32_t max_size,
-                                                            float max_pct, int32_t min_size, FbOffsets off,
-                                                            FbWork w) {
+                                                            int32_t X, int32_t Y, int32_t Z, int32_t n,
+                                                            int32_t max_size, float max_pct, int32_t min_size,
+                                                            FbOffsets off, FbWork w) {
   __shared__ int32_t h_hi[256], h_lo1[256], h_lo2[256], h_ot[256];
   __shared__ float s_sumb[256];
-  __shared__ float s_var[256];
   __shared__ int32_t s_wb[256];
   __shared__ uint32_t s_min, s_max, s_seed, s_tail;
-  __shared__ int32_t s_b1, s_r1, s_b2, s_r2, s_v1, s_v2;
+  __shared__ int32_t s_b1, s_r1, s_b2, s_r2, s_l1, s_l2, s_rr, s_best;
   __shared__ float s_mm;
-  __shared__ int32_t s_best;
   __shared__ float st_v[32], st_x[32], st_y[32], st_z[32];
-  const int s = blockIdx.x, t = threadIdx.x;
+  __shared__ uint32_t s_cand[kFbMaskWords], s_reach[kFbMaskWords];
+  const int s = blockIdx.x, t = threadIdx.x, lane = t & 31;
   if (w.stat->flags) return;
   const int64_t a = w.uptr[s];
   const int32_t N = (int32_t)(w.uptr[s + 1] - a);
   const uint32_t* lin = w.ulin + a;
   const uint16_t* val = w.uval + a;
+  uint8_t* keep = w.ukeep + a;
   if (N == 0) {
     if (t == 0) {
       w.tcnt[s] = 0;
@@ -280,6 +331,7 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     }
     return;
   }
+  const uint32_t uX = (uint32_t)X, XY = (uint32_t)X * (uint32_t)Y;
   h_hi[t] = 0;
   h_lo1[t] = 0;
   h_lo2[t] = 0;
@@ -289,6 +341,8 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     s_max = 0;
     s_seed = 0xffffffffu;
     s_tail = 0;
+    s_b1 = s_b2 = 255;
+    s_r1 = s_r2 = s_l1 = s_l2 = s_rr = 0;
   }
   __syncthreads();
   // pass 1: range and the high bytes
@@ -305,20 +359,20 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
   const int32_t k1 = max(0, N - max_size);
   int32_t k2 = __float2int_rz(__fmul_rn(__fsub_rn(1.0f, max_pct), (float)N));
   k2 = min(max(k2, 0), N - 1);  // the reference reads past the end only for max_pct < 1/N
-  if (t == 0) {
-    hist_select(h_hi, k1, &s_b1, &s_r1);
-    hist_select(h_hi, k2, &s_b2, &s_r2);
-    const float fmin = (float)s_min, fmax = (float)s_max;
-    s_mm = __fdiv_rn(255.0f, __fsub_rn(fmax, fmin));
+  if (t < 32) {
+    warp_hist_select(h_hi, k1, &s_b1, &s_r1);
+    warp_hist_select(h_hi, k2, &s_b2, &s_r2);
+    if (t == 0) s_mm = __fdiv_rn(255.0f, __fsub_rn((float)s_max, (float)s_min));
   }
   __syncthreads();
   const float fmin = (float)s_min, mm = s_mm;
   const bool otsu = isfinite(mm);
+  const int32_t b1 = s_b1, b2 = s_b2;
   // pass 2: low bytes inside the two buckets, Otsu's histogram, the first brightest voxel
   for (int32_t i = t; i < N; i += kFbTrimThreads) {
     const uint32_t v = val[i];
-    if ((int32_t)(v >> 8) == s_b1) atomicAdd(&h_lo1[v & 255], 1);
-    if ((int32_t)(v >> 8) == s_b2) atomicAdd(&h_lo2[v & 255], 1);
+    if ((int32_t)(v >> 8) == b1) atomicAdd(&h_lo1[v & 255], 1);
+    if ((int32_t)(v >> 8) == b2) atomicAdd(&h_lo2[v & 255], 1);
     if (otsu) {
       const int b = __float2int_rz(__fmul_rn(__fsub_rn((float)v, fmin), mm));
       atomicAdd(&h_ot[min(b, 255)], 1);
@@ -326,91 +380,162 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     if (v == s_max) atomicMin(&s_seed, (uint32_t)i);
   }
   __syncthreads();
-  if (t == 0) {
-    int32_t l1, l2, r;
-    hist_select(h_lo1, s_r1, &l1, &r);
-    hist_select(h_lo2, s_r2, &l2, &r);
-    s_v1 = (s_b1 << 8) | l1;
-    s_v2 = (s_b2 << 8) | l2;
-    // Otsu: the between-class sums in the reference's order
-    float sum_b = 0.0f;
-    int32_t wb = 0;
-    for (int b = 0; b < 256; b++) {
-      wb += h_ot[b];
-      sum_b = __fadd_rn(sum_b, (float)(b * h_ot[b]));
-      s_wb[b] = wb;
-      s_sumb[b] = sum_b;
+  if (t < 32) {
+    warp_hist_select(h_lo1, s_r1, &s_l1, &s_rr);
+    warp_hist_select(h_lo2, s_r2, &s_l2, &s_rr);
+    if (t == 0) {
+      // Otsu: the between-class sums in the reference's order
+      float sum_b = 0.0f;
+      int32_t wb = 0;
+      for (int bin = 0; bin < 256; bin++) {
+        wb += h_ot[bin];
+        sum_b = __fadd_rn(sum_b, (float)(bin * h_ot[bin]));
+        s_wb[bin] = wb;
+        s_sumb[bin] = sum_b;
+      }
     }
-  }
-  __syncthreads();
-  if (otsu) {
-    const int32_t wb = s_wb[t], wf = N - wb;
-    float var = 0.0f;
-    if (wb > 0 && wf > 0) {
-      const float sum = s_sumb[255], sb = s_sumb[t];
-      const float m_b = __fdiv_rn(sb, (float)wb), m_f = __fdiv_rn(__fsub_rn(sum, sb), (float)wf);
-      const float d = __fsub_rn(m_b, m_f);
-      var = __fmul_rn(__fmul_rn(__fmul_rn((float)wb, (float)wf), d), d);
-    }
-    s_var[t] = var;
-  }
-  __syncthreads();
-  if (t == 0) {
-    float t3 = -FLT_MAX;
+    __syncwarp();
+    // the bin of the largest between-class variance (the first of equals; 0 if none is > 0)
+    float best_v = 0.0f;
+    int32_t best_b = 0x7fffffff;
     if (otsu) {
-      float vmax = 0.0f;
-      int32_t best = 0;
-      for (int b = 0; b < 256; b++)
-        if (s_var[b] > vmax) {
-          vmax = s_var[b];
-          best = b;
+      const float sum = s_sumb[255];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int bin = lane * 8 + i;
+        const int32_t wb = s_wb[bin], wf = N - wb;
+        if (wb > 0 && wf > 0) {
+          const float sb = s_sumb[bin];
+          const float m_b = __fdiv_rn(sb, (float)wb), m_f = __fdiv_rn(__fsub_rn(sum, sb), (float)wf);
+          const float d = __fsub_rn(m_b, m_f);
+          const float var = __fmul_rn(__fmul_rn(__fmul_rn((float)wb, (float)wf), d), d);
+          if (var > best_v) {
+            best_v = var;
+            best_b = bin;
+          }
         }
-      t3 = __fadd_rn(__fdiv_rn((float)best, mm), fmin);
+      }
     }
-    float thr = (float)s_v1;
-    if ((float)s_v2 > thr) thr = (float)s_v2;
-    if (t3 > thr) thr = t3;
-    const uint32_t th = (uint32_t)(uint16_t)__float2uint_rz(thr);
-    w.thr[s] = th;
-    s_best = (int32_t)th;
-    const uint32_t seed = s_seed;
-    if (val[seed] > th) {
-      const uint32_t v = lin[seed];
-      atomicOr(&w.bits[v >> 5], 1u << (v & 31));
-      w.queue[a] = v;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, best_v, o);
+      const int32_t ob = __shfl_xor_sync(0xffffffffu, best_b, o);
+      if (ov > best_v || (ov == best_v && ob < best_b)) {
+        best_v = ov;
+        best_b = ob;
+      }
+    }
+    if (t == 0) {
+      float t3 = -FLT_MAX;
+      if (otsu) t3 = __fadd_rn(__fdiv_rn((float)(best_v > 0.0f ? best_b : 0), mm), fmin);
+      float thr = (float)((b1 << 8) | s_l1);
+      const float v2 = (float)((b2 << 8) | s_l2);
+      if (v2 > thr) thr = v2;
+      if (t3 > thr) thr = t3;
+      const uint32_t th = (uint32_t)(uint16_t)__float2uint_rz(thr);
+      w.thr[s] = th;
+      s_best = (int32_t)th;
+    }
+  }
+  __syncthreads();
+  // the flood from the brightest voxel: a voxel joins when it carries this label, is brighter
+  // than the threshold and was not reached yet.  Neighbours are the reference's linear-index
+  // offsets: inside the volume they are the coordinate steps; across an x or y border they wrap
+  // into the next row or slice, and those are decoded from the linear index.
+  const uint32_t th = (uint32_t)s_best;
+  const FbBox bx = w.box[s];
+  const int32_t bw = bx.hi[0] - bx.lo[0] + 1, bh = bx.hi[1] - bx.lo[1] + 1, bd = bx.hi[2] - bx.lo[2] + 1;
+  const bool shared_path = (int64_t)bw * bh * bd <= 32 * kFbMaskWords;
+  uint32_t* q = w.queue + a;
+  if (shared_path) {
+    const int32_t words = (bw * bh * bd + 31) / 32;
+    for (int i = t; i < words; i += kFbTrimThreads) s_cand[i] = s_reach[i] = 0u;
+    __syncthreads();
+    for (int32_t i = t; i < N; i += kFbTrimThreads)
+      if (val[i] > th) {
+        int32_t x, y, z;
+        decode(lin[i], uX, XY, &x, &y, &z);
+        const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
+        atomicOr(&s_cand[li >> 5], 1u << (li & 31));
+      }
+    __syncthreads();
+    if (t == 0 && val[s_seed] > th) {
+      int32_t x, y, z;
+      decode(lin[s_seed], uX, XY, &x, &y, &z);
+      const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
+      s_reach[li >> 5] |= 1u << (li & 31);
+      q[0] = lin[s_seed];
       s_tail = 1;
     }
+  } else if (t == 0 && val[s_seed] > th) {
+    const uint32_t v = lin[s_seed];
+    atomicOr(&w.bits[v >> 5], 1u << (v & 31));
+    q[0] = v;
+    s_tail = 1;
   }
   __syncthreads();
-  // the flood, level by level: a voxel joins when it carries this label, is brighter than the
-  // threshold and its bit was not yet set
-  const uint32_t want = (uint32_t)s + 1u, th = (uint32_t)s_best;
-  uint32_t* q = w.queue + a;
+  const uint32_t want = (uint32_t)s + 1u;
   uint32_t head = 0;
   for (;;) {
     const uint32_t tail = s_tail;
     __syncthreads();
     if (head == tail) break;
     for (uint32_t i = head + t; i < tail; i += kFbTrimThreads) {
-      const int64_t v = q[i];
-      for (int j = 0; j < off.n; j++) {
-        const int64_t nb = v + off.off[j];
-        if (nb < 0 || nb >= nvol) continue;
-        if (label[nb] != want || raw[nb] <= th) continue;
-        const uint32_t bit = 1u << (nb & 31);
-        if (atomicOr(&w.bits[nb >> 5], bit) & bit) continue;
-        q[atomicAdd(&s_tail, 1u)] = (uint32_t)nb;
+      const uint32_t v = q[i];
+      if (shared_path) {
+        int32_t x, y, z;
+        decode(v, uX, XY, &x, &y, &z);
+        for (int j = 0; j < off.n; j++) {
+          int32_t tx = x + off.d[j][0], ty = y + off.d[j][1], tz = z + off.d[j][2];
+          if (tx < 0 || tx >= X || ty < 0 || ty >= Y) {  // wraps: where the linear offset lands
+            const int64_t nb = (int64_t)v + off.off[j];
+            if (nb < 0 || nb >= nvol) continue;
+            decode((uint32_t)nb, uX, XY, &tx, &ty, &tz);
+          } else if (tz < 0 || tz >= Z) {
+            continue;
+          }
+          const int32_t lx = tx - bx.lo[0], ly = ty - bx.lo[1], lz = tz - bx.lo[2];
+          if (lx < 0 || lx >= bw || ly < 0 || ly >= bh || lz < 0 || lz >= bd) continue;
+          const int32_t li = lx + bw * (ly + bh * lz);
+          const uint32_t bit = 1u << (li & 31);
+          if (!(s_cand[li >> 5] & bit)) continue;
+          if (atomicOr(&s_reach[li >> 5], bit) & bit) continue;
+          q[atomicAdd(&s_tail, 1u)] = (uint32_t)tx + uX * (uint32_t)ty + XY * (uint32_t)tz;
+        }
+      } else {
+        for (int j = 0; j < off.n; j++) {
+          const int64_t nb = (int64_t)v + off.off[j];
+          if (nb < 0 || nb >= nvol) continue;
+          if (label[nb] != want || raw[nb] <= th) continue;
+          const uint32_t bit = 1u << (nb & 31);
+          if (atomicOr(&w.bits[nb >> 5], bit) & bit) continue;
+          q[atomicAdd(&s_tail, 1u)] = (uint32_t)nb;
+        }
       }
     }
     head = tail;
     __syncthreads();
   }
   const int32_t kept = (int32_t)s_tail;
+  // each list entry's verdict, for the centroid and the emission
+  for (int32_t i = t; i < N; i += kFbTrimThreads) {
+    const uint32_t v = lin[i];
+    bool in;
+    if (shared_path) {
+      int32_t x, y, z;
+      decode(v, uX, XY, &x, &y, &z);
+      const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
+      in = (s_reach[li >> 5] >> (li & 31)) & 1u;
+    } else {
+      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+    }
+    keep[i] = in ? 1 : 0;
+  }
   if (t == 0) w.tcnt[s] = kept;
-  if (kept < min_size || t >= 32) return;
+  if (kept < min_size) return;
+  __syncthreads();
+  if (t >= 32) return;
   // warp 0: the centroid in list order (FP32, as the reference sums it) and the range of the
   // background-subtracted values
-  const int lane = t;
   const unsigned below = (1u << lane) - 1u;
   float sw = 0.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
   uint32_t smin = 0xffffffffu, smax = 0;
@@ -421,15 +546,17 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     if (i < N) {
       v = lin[i];
       r = val[i];
-      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+      in = keep[i] != 0;
     }
     const unsigned m = __ballot_sync(0xffffffffu, in);
     if (in) {
       const int p = __popc(m & below);
+      int32_t x, y, z;
+      decode(v, uX, XY, &x, &y, &z);
       st_v[p] = (float)r;
-      st_x[p] = (float)(v % (uint32_t)X);
-      st_y[p] = (float)((v / (uint32_t)X) % (uint32_t)Y);
-      st_z[p] = (float)(v / ((uint32_t)X * (uint32_t)Y));
+      st_x[p] = (float)x;
+      st_y[p] = (float)y;
+      st_z[p] = (float)z;
       const uint32_t sub = (uint16_t)(r - th);
       smin = min(smin, sub);
       smax = max(smax, sub);
@@ -553,7 +680,7 @@ __global__ void __launch_bounds__(256) k_fb_emit(int32_t X, int32_t Y, int64_t m
     uint32_t v = 0;
     if (i < n) {
       v = w.ulin[a + i];
-      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+      in = w.ukeep[a + i] != 0;
     }
     const unsigned m = __ballot_sync(0xffffffffu, in);
     if (in) {
@@ -574,30 +701,32 @@ __global__ void __launch_bounds__(256) k_fb_emit(int32_t X, int32_t Y, int64_t m
 
 int fb_offsets(int32_t conn, const int32_t dims[3], FbOffsets* o) {
   const int64_t X = dims[0], XY = (int64_t)dims[0] * dims[1];
-  int n = 0;
+  int rz, rxy;
   switch (conn) {
     case 4:
-    case 6:
-      if (conn == 6) o->off[n++] = -XY;
-      o->off[n++] = -X;
-      o->off[n++] = -1;
-      o->off[n++] = 1;
-      o->off[n++] = X;
-      if (conn == 6) o->off[n++] = XY;
-      break;
     case 8:
-    case 26:
-    case 74: {
-      const int rz = conn == 8 ? 0 : 1, rxy = conn == 74 ? 2 : 1;
-      for (int z = -rz; z <= rz; z++)
-        for (int y = -rxy; y <= rxy; y++)
-          for (int x = -rxy; x <= rxy; x++)
-            if (x || y || z) o->off[n++] = x + X * y + XY * z;
+      rz = 0, rxy = 1;
       break;
-    }
+    case 6:
+    case 26:
+      rz = 1, rxy = 1;
+      break;
+    case 74:
+      rz = 1, rxy = 2;
+      break;
     default:
       return 0;
   }
+  int n = 0;
+  for (int z = -rz; z <= rz; z++)
+    for (int y = -rxy; y <= rxy; y++)
+      for (int x = -rxy; x <= rxy; x++) {
+        if (!(x || y || z)) continue;
+        if ((conn == 4 || conn == 6) && (x != 0) + (y != 0) + (z != 0) != 1) continue;  // faces only
+        o->off[n] = x + X * y + XY * z;
+        o->d[n][0] = (int8_t)x, o->d[n][1] = (int8_t)y, o->d[n][2] = (int8_t)z;
+        n++;
+      }
   o->n = n;
   return n;
 }
@@ -661,14 +790,20 @@ int frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3
   const unsigned warp_blocks = (unsigned)(((int64_t)n * 32 + 255) / 256);
   k_fb_init<<<(n + 255) / 256, 256, 0, st>>>(n, w);
   mark();
-  const int64_t span = (nvol / 4 + 511) / 512;
-  k_fb_scan<<<(unsigned)(span < 1 ? 1 : span < 148 * 8 ? span : 148 * 8), 256, 0, st>>>(label, nvol, X, Y, n, w);
+  // the scan: as many blocks as fit on the device at once (it strides over the volume)
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fb_scan, 256, 0);
+  const int64_t span = (nvol / 4 + 256 * kFbScanDepth - 1) / (256 * kFbScanDepth);
+  const int64_t full = (int64_t)sms * (occ > 0 ? occ : 1);
+  k_fb_scan<<<(unsigned)(span < 1 ? 1 : span < full ? span : full), 256, 0, st>>>(label, nvol, X, Y, n, w);
   mark();
   k_fb_ptr<<<1, 1024, 0, st>>>(n, w);
   mark();
   k_fb_group<<<warp_blocks, 256, 0, st>>>(label, raw, X, Y, n, w);
   mark();
-  k_fb_trim<<<n, kFbTrimThreads, 0, st>>>(label, raw, nvol, X, Y, n, p->max_nuclei_size, p->max_percentile,
+  k_fb_trim<<<n, kFbTrimThreads, 0, st>>>(label, raw, nvol, X, Y, dims[2], n, p->max_nuclei_size, p->max_percentile,
                                           p->min_nuclei_size, off, w);
   mark();
   k_fb_order<<<1, 1024, 0, st>>>(n, nvol, p->min_nuclei_size, w);
