@@ -241,9 +241,56 @@ def reference_gpu(frame, reps=3):
             "path": "the reference's GPU path compiled from its sources, host arrays in and out, per call"}
 
 
+def fb_spec(args):
+    from tgmm_b200 import synth
+    if args.fb_dims:
+        dims = tuple(int(x) for x in args.fb_dims.split(","))
+        return synth.VolumeSpec(dims=dims, n_nuclei=args.fb_nuclei or max(1, dims[0] * dims[1] * dims[2] // 53687),
+                                axis_min=4.0, axis_max=8.0)
+    return synth.C2
+
+
+def run_reference_frames(args):
+    """The reference arm of the frame-preparation workload: the reference's host build, as the
+    oracle's single-thread C restatement, on the same volume; each step one whole volume."""
+    import torch
+    from oracle import oracle as O
+    spec = fb_spec(args)
+    raw, lab, S, Nfg, _ = fb_volume(spec, args.seed, torch.device("cpu"))
+    X, Y, Z = spec.dims
+    raw_n = raw.numpy().view(np.uint16).reshape(Z, Y, X)
+    lab_n = lab.numpy().view(np.uint32).reshape(Z, Y, X)
+    times = []
+    out = None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        rc, out = O.frame_build(raw_n, lab_n, S, max_vox=Nfg)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+        assert rc == 0
+    per = float(np.mean(times))
+    value = 1.0 / per
+    sample = (f"the whole {X}x{Y}x{Z} volume per step through the oracle's single-thread C restatement of the "
+              f"reference's host build ({per:.2f} s)")
+    line = {"impl": "reference", "metric": "frame preparations/s", "value": value, "unit": "volumes/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/u32 -> f32",
+            "data": "synthetic (seeded nuclei volume; labels = its supervoxels)",
+            "config": {"workload": f"frame preparation of a {X}x{Y}x{Z} uint16 volume with {S} labelled "
+                                   f"supervoxels ({Nfg} labelled voxels): trim, erase, centroids, background, "
+                                   f"[0,1] rescale, SoA/CSR", "n_vox_out": out["n_vox"], "n_sv_out": out["n_sv"]},
+            "cpu_baseline": {"value": value, "unit": "volumes/s", "cores": 1, "kind": "port", "cpu_model": cpu_model(),
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "volumes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     world, rank, local = dist_setup("gloo")
     if rank != 0:
+        return
+    if args.workload == "frames":
+        run_reference_frames(args)
         return
     from tgmm_b200 import synth
     spec = spec_for(args.workload)
@@ -708,12 +755,7 @@ def run_frames(args):
     world, rank, local = dist_setup("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.fb_dims:
-        dims = tuple(int(x) for x in args.fb_dims.split(","))
-        spec = synth.VolumeSpec(dims=dims, n_nuclei=args.fb_nuclei or max(1, dims[0] * dims[1] * dims[2] // 53687),
-                                axis_min=4.0, axis_max=8.0)
-    else:
-        spec = synth.C2
+    spec = fb_spec(args)
     raw, lab, S, Nfg, box = fb_volume(spec, args.seed + rank, dev)
     X, Y, Z = spec.dims
     nvol = X * Y * Z

@@ -11,8 +11,10 @@ from __future__ import annotations
 import numpy as np
 
 
-def make(dims=(96, 80, 24), n_nuclei=24, seed=0, background=100.0, specials=True):
-    """Returns (raw (Z, Y, X) uint16, label (Z, Y, X) uint32, n_labels)."""
+def make(dims=(96, 80, 24), n_nuclei=24, seed=0, background=100.0, specials=True, big=False):
+    """Returns (raw (Z, Y, X) uint16, label (Z, Y, X) uint32, n_labels).  big: one more
+    supervoxel whose bounding box (70 x 60 x 16 voxels) is larger than a trimming block holds in
+    shared memory, around a bright blob (needs dims of at least 72 x 62 x 18)."""
     X, Y, Z = dims
     rng = np.random.default_rng(seed)
     raw = rng.poisson(background, size=(Z, Y, X)).astype(np.float64)
@@ -73,6 +75,13 @@ def make(dims=(96, 80, 24), n_nuclei=24, seed=0, background=100.0, specials=True
             raw[z, y0 + 1:y0 + 7, 0] = 900.0 + rng.integers(0, 40, size=6)
         nxt += 1
         nxt += 2  # label numbers with no voxels
+    if big:
+        blk = (slice(1, 17), slice(1, 61), slice(1, 71))
+        zz, yy, xx = np.meshgrid(np.arange(1, 17), np.arange(1, 61), np.arange(1, 71), indexing="ij")
+        d2 = ((xx - 30.0) / 9.0) ** 2 + ((yy - 25.0) / 8.0) ** 2 + ((zz - 8.0) / 4.0) ** 2
+        raw[blk] += 900.0 * np.exp(-0.5 * d2)
+        label[blk] = nxt
+        nxt += 1
     n_labels = nxt - 1
     # number the supervoxels in an order unrelated to space
     perm = np.concatenate([[0], rng.permutation(n_labels) + 1]).astype(np.uint32)

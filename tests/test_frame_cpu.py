@@ -19,6 +19,7 @@ CASES = [
     dict(seed=4, max_pct=0.15, conn=8),   # the percentile sets it
     dict(seed=5, conn=4, min_size=20),
     dict(seed=6, conn=74, max_size=200),
+    dict(seed=15, big=True, dims=(160, 144, 40), n_nuclei=80),  # a supervoxel of 67,200 voxels
 ]
 
 
@@ -31,8 +32,8 @@ def _coords(lin, X, Y):
 @pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
 def test_oracle_matches_reference_trimming_and_centroids(case):
     c = dict(max_size=3000, max_pct=0.4, conn=6, min_size=50)
-    c.update({k: v for k, v in case.items() if k != "seed"})
-    raw, lab, n = V.make(seed=case["seed"])
+    c.update({k: case[k] for k in c if k in case})
+    raw, lab, n = V.make(seed=case["seed"], **{k: case[k] for k in ("dims", "n_nuclei", "big") if k in case})
     Z, Y, X = raw.shape
     rc, o = O.frame_build(raw, lab, n, O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"]))
     assert rc == 0

@@ -23,6 +23,7 @@ CASES = [
     dict(seed=6, conn=74, max_size=200),
     dict(seed=9, dims=(160, 144, 40), n_nuclei=120),
     dict(seed=10, dims=(512, 512, 64), n_nuclei=1500),  # 16.8M voxels
+    dict(seed=15, big=True, dims=(160, 144, 40), n_nuclei=80),  # a box beyond the shared-memory flood
 ]
 
 
@@ -33,7 +34,7 @@ def _params(case):
 
 
 def _volume(case):
-    kw = {k: case[k] for k in ("dims", "n_nuclei") if k in case}
+    kw = {k: case[k] for k in ("dims", "n_nuclei", "big") if k in case}
     return V.make(seed=case["seed"], **kw)
 
 
