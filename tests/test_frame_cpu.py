@@ -145,3 +145,21 @@ def test_abi_frame_build_checks_arguments_without_a_gpu():
     rc = lib.tgmm_frame_build(fake, fake, dims, 10, C.byref(p), fake, b1 - 1, fake, fake, fake, fake, None, 1, 1,
                               C.byref(nv), C.byref(ns), None)
     assert rc == L.TGMM_ERR_BAD_SIZE
+
+
+def test_bench_frames_reference_arm_runs_on_cpu():
+    """bench.py --impl reference --workload frames: the host build's restatement on a small
+    synthetic volume prints one JSON line of the frames metric (no GPU)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--workload", "frames",
+                        "--fb-dims", "256,128,32", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "frame preparations/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["config"]["n_sv_out"] > 0
