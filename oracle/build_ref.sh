@@ -27,11 +27,13 @@ $NVCC -gencode arch=compute_100a,code=sm_100a -shared -o "$OUT/libtgmm_ref_f3.so
   "$OUT/f3_knnCuda.o" "$OUT/ref_f3_harness.o" -lcuda
 # the frame preparation's supervoxel trimming and statistics (host C++ only: runs without a GPU)
 TLR="$REF/temporalLogicalRules"
-CXXF="-std=c++14 -O2 -fPIC -w -I$REF -I$TLR"
+HSD="$REF/nucleiChSvWshedPBC"
+CXXF="-std=c++14 -O2 -fPIC -w -I$REF -I$TLR -I$HSD"
 g++ $CXXF -c "$TLR/supervoxel.cpp" -o "$OUT/f1_supervoxel.o"
 g++ $CXXF -c "$TLR/localGeometricDescriptor.cpp" -o "$OUT/f1_lgd.o"
+g++ $CXXF -c "$HSD/hierarchicalSegmentation.cpp" -o "$OUT/f1_hs.o"
 g++ $CXXF -c "$HERE/ref_f1_harness.cpp" -o "$OUT/ref_f1_harness.o"
-g++ -shared -o "$OUT/libtgmm_ref_f1.so" "$OUT/f1_supervoxel.o" "$OUT/f1_lgd.o" "$OUT/constants.o" \
-  "$OUT/ref_f1_harness.o"
+g++ -shared -Wl,--no-undefined -o "$OUT/libtgmm_ref_f1.so" "$OUT/f1_supervoxel.o" "$OUT/f1_lgd.o" "$OUT/f1_hs.o" \
+  "$OUT/constants.o" "$OUT/ref_f1_harness.o"
 rm -f "$OUT"/*.o
 echo "built $OUT/libtgmm_ref.so $OUT/libtgmm_ref_f3.so $OUT/libtgmm_ref_f1.so"

@@ -311,3 +311,15 @@ def ref_trim_stats(raw, ptr, lin, max_size=3000, max_pct=0.4, conn=6):
         raise RuntimeError(f"reference trimming failed ({rc})")
     kept = [lin_out[ptr[s]:ptr[s] + cnt[s]].copy() for s in range(n)]
     return dict(thr=thr, cnt=cnt, lists=kept, cent=cent.reshape(n, 3), intensity=inten)
+
+
+def ref_erase_order(erased):
+    """The reference's own eraseSupervoxelFromCurrentSegmentation: the original index of each
+    supervoxel left, in the order it leaves them."""
+    ref = C.CDLL(REF_F1_SO)
+    ref.ref_erase_order.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    ref.ref_erase_order.restype = C.c_int
+    e = np.ascontiguousarray(erased, np.uint8)
+    order = np.zeros(max(1, e.shape[0]), np.int32)
+    left = ref.ref_erase_order(_p(e), e.shape[0], _p(order))
+    return order[:left].copy()

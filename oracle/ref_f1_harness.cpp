@@ -1,9 +1,11 @@
 // TEST INFRASTRUCTURE ONLY.  Runs the reference's own supervoxel trimming and weighted
-// statistics (temporalLogicalRules/supervoxel.cpp, compiled from its sources by
-// oracle/build_ref.sh) on supervoxels given as ascending voxel lists, for the frame
-// preparation of mainTrackingGaussianMixtureModel.cpp:557-621: per supervoxel the
-// threshold trimSupervoxel<uint16>() returns, the voxels it keeps, and the centroid and
-// intensity weightedGaussianStatistics<uint16>(true) computes from the raw image.
+// statistics (temporalLogicalRules/supervoxel.cpp) and its erase of small supervoxels
+// (nucleiChSvWshedPBC/hierarchicalSegmentation.cpp), compiled from their sources by
+// oracle/build_ref.sh, for the frame preparation of mainTrackingGaussianMixtureModel.cpp:
+// 557-634: per supervoxel (given as an ascending voxel list) the threshold
+// trimSupervoxel<uint16>() returns, the voxels it keeps, the centroid and intensity
+// weightedGaussianStatistics<uint16>(true) computes from the raw image; and the order
+// eraseSupervoxelFromCurrentSegmentation leaves the survivors in.
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -11,6 +13,7 @@
 #include <vector>
 
 #include "constants.h"
+#include "hierarchicalSegmentation.h"
 #include "supervoxel.h"
 
 // supervoxel.cpp references the tracking graph's kNN; trimming and statistics never call it
@@ -41,4 +44,21 @@ extern "C" int ref_trim_stats(const uint16_t* raw, const int32_t* dims, const in
   }
   supervoxel::freeTrimParameters();
   return 0;
+}
+
+// order[0..n-m) = the original index of each supervoxel left after erasing those flagged
+// (eraseIdx ascending, as main:598-600 builds it); returns n - m.
+extern "C" int ref_erase_order(const uint8_t* erased, int32_t n, int32_t* order) {
+  hierarchicalSegmentation hs;
+  hs.currentSegmentatioSupervoxel.resize(n);
+  hs.currentSegmentationNodes.assign(n, nullptr);
+  std::vector<int> erase_idx;
+  for (int32_t i = 0; i < n; i++) {
+    hs.currentSegmentatioSupervoxel[i].PixelIdxList.assign(1, (uint64)i);  // the supervoxel's tag
+    if (erased[i]) erase_idx.push_back(i);
+  }
+  hs.eraseSupervoxelFromCurrentSegmentation(erase_idx);
+  const int32_t left = (int32_t)hs.currentSegmentatioSupervoxel.size();
+  for (int32_t i = 0; i < left; i++) order[i] = (int32_t)hs.currentSegmentatioSupervoxel[i].PixelIdxList[0];
+  return left;
 }

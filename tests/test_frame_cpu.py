@@ -1,8 +1,9 @@
 """Frame preparation without a GPU: the oracle's restatement of the tracking program's input
 build (trimming, size filter, erase order, centroids, background subtraction, rescale, SoA
-arrays) checked against the reference's own trimSupervoxel / weightedGaussianStatistics
-compiled from its sources, the device's closed form of the erase order checked against the
-reference's swap loop, and the C ABI's argument checks."""
+arrays) checked against the reference's own trimSupervoxel / weightedGaussianStatistics and
+eraseSupervoxelFromCurrentSegmentation compiled from their sources, the device's closed form
+of the erase order checked against the reference's swap loop, and the C ABI's argument
+checks."""
 import ctypes as C
 
 import numpy as np
@@ -41,7 +42,7 @@ def test_oracle_matches_reference_trimming_and_centroids(case):
     r = O.ref_trim_stats(raw, ptr, lin, c["max_size"], c["max_pct"], c["conn"])
     erased = (r["cnt"] < c["min_size"]).astype(np.uint8)
     assert erased.any() and not erased.all()
-    order = O.erase_order(erased)
+    order = O.ref_erase_order(erased)  # the reference's own erase
     N, S = o["n_vox"], o["n_sv"]
     assert S == len(order) and N == int(sum(r["cnt"][s] for s in order))
     q = o["query"].reshape(3, N)
@@ -94,6 +95,21 @@ def test_erase_order_closed_form_is_the_reference_swap_loop(seed):
     if erased.all():
         erased[rng.integers(0, n)] = False
     np.testing.assert_array_equal(_closed_form(erased), O.erase_order(erased.astype(np.uint8)))
+
+
+@pytest.mark.skipif(not O.ref_f1_available(), reason="reference trimming harness not built")
+@pytest.mark.parametrize("seed", range(8))
+def test_erase_order_is_the_references(seed):
+    """The oracle's restatement and the device's closed form against the reference's own
+    hierarchicalSegmentation::eraseSupervoxelFromCurrentSegmentation."""
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(1, 3000))
+    erased = (rng.random(n) < rng.choice([0.02, 0.2, 0.5, 0.9])).astype(np.uint8)
+    if erased.all():
+        erased[0] = 0
+    ref = O.ref_erase_order(erased)
+    np.testing.assert_array_equal(O.erase_order(erased), ref)
+    np.testing.assert_array_equal(_closed_form(erased.astype(bool)), ref)
 
 
 def test_erase_order_examples():
