@@ -179,3 +179,34 @@ def test_bench_frames_reference_arm_runs_on_cpu():
     assert line["impl"] == "reference" and line["metric"] == "frame preparations/s" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["config"]["n_sv_out"] > 0
+
+
+@pytest.mark.skipif(not O.ref_f1_available(), reason="reference trimming harness not built")
+@pytest.mark.parametrize("seed", range(10))
+def test_trimming_matches_reference_on_random_volumes(seed):
+    """Random small volumes and parameters: every supervoxel's threshold, kept voxels and
+    centroid from the oracle equal the reference's own, through the whole frame build."""
+    rng = np.random.default_rng(1000 + seed)
+    dims = (int(rng.integers(40, 90)), int(rng.integers(30, 70)), int(rng.integers(8, 20)))
+    raw, lab, n = V.make(dims=dims, n_nuclei=int(rng.integers(5, 25)), seed=2000 + seed,
+                         background=float(rng.uniform(50, 300)))
+    c = dict(max_size=int(rng.choice([40, 150, 3000])), max_pct=float(rng.choice([0.1, 0.4, 0.75])),
+             conn=int(rng.choice([4, 6, 8, 26, 74])), min_size=int(rng.choice([1, 20, 50])))
+    rc, o = O.frame_build(raw, lab, n, O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"]))
+    ptr, lin = O.supervoxel_lists(lab, n)
+    r = O.ref_trim_stats(raw, ptr, lin, c["max_size"], c["max_pct"], c["conn"])
+    erased = (r["cnt"] < c["min_size"]).astype(np.uint8)
+    if erased.all():
+        assert rc == 5
+        return
+    assert rc == 0
+    order = O.ref_erase_order(erased)
+    Z, Y, X = raw.shape
+    N, S = o["n_vox"], o["n_sv"]
+    assert S == len(order)
+    q = o["query"].reshape(3, N)
+    for p, s in enumerate(order):
+        a, b = o["lptr"][p], o["lptr"][p + 1]
+        assert o["thr"][p] == r["thr"][s] and b - a == r["cnt"][s]
+        np.testing.assert_array_equal(q[:, a:b], _coords(r["lists"][s], X, Y))
+        np.testing.assert_array_equal(o["cent"].reshape(3, S)[:, p].view(np.uint32), r["cent"][s].view(np.uint32))
