@@ -210,3 +210,32 @@ def test_trimming_matches_reference_on_random_volumes(seed):
         assert o["thr"][p] == r["thr"][s] and b - a == r["cnt"][s]
         np.testing.assert_array_equal(q[:, a:b], _coords(r["lists"][s], X, Y))
         np.testing.assert_array_equal(o["cent"].reshape(3, S)[:, p].view(np.uint32), r["cent"][s].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["frame_default", "frame_conn26", "frame_big"])
+def test_oracle_matches_committed_reference_outputs(name):
+    """The committed outputs of the reference's own trimming, statistics and erase
+    (tests/golden/make_frame_golden.py) against the oracle's frame build: needs neither the
+    reference sources nor a GPU."""
+    import os
+    import sys
+    gold_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, gold_dir)
+    import make_frame_golden as MG
+    with np.load(os.path.join(gold_dir, f"{name}.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    c = MG.FRAME_CASES[name]
+    raw, lab, n = MG.volume(c)
+    assert MG.digest(raw, lab) == str(g["input_sha256"]), "the volume generator changed: regenerate the fixtures"
+    rc, o = O.frame_build(raw, lab, n, O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"]))
+    assert rc == 0
+    Z, Y, X = raw.shape
+    order = g["order"]
+    N, S = o["n_vox"], o["n_sv"]
+    assert S == len(order) and N == int(g["cnt"][order].sum())
+    q = o["query"].reshape(3, N)
+    for p, s in enumerate(order):
+        a, b = o["lptr"][p], o["lptr"][p + 1]
+        assert o["thr"][p] == g["thr"][s] and b - a == g["cnt"][s]
+        np.testing.assert_array_equal(q[:, a:b], _coords(g["kept_lin"][g["kept_ptr"][s]:g["kept_ptr"][s + 1]], X, Y))
+        np.testing.assert_array_equal(o["cent"].reshape(3, S)[:, p].view(np.uint32), g["cent"][s].view(np.uint32))
