@@ -323,3 +323,33 @@ def ref_erase_order(erased):
     order = np.zeros(max(1, e.shape[0]), np.int32)
     left = ref.ref_erase_order(_p(e), e.shape[0], _p(order))
     return order[:left].copy()
+
+
+def ref_frame_build(raw, label, n_labels, p: OrFrameParams | None = None, max_vox=None, lists=None):
+    """The reference's host frame build run with its own trimming, statistics and erase
+    (oracle/ref_f1_harness.cpp); same outputs as frame_build.  lists: (ptr, lin) from
+    supervoxel_lists(label, n_labels), the reference's per-supervoxel pixel lists, if already
+    made.  Returns (rc, dict)."""
+    p = p or frame_params()
+    ref = C.CDLL(REF_F1_SO)
+    vp = C.c_void_p
+    ref.ref_frame_build.argtypes = [vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_float, C.c_int32, C.c_int32, vp, vp, vp,
+                                    vp, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    ref.ref_frame_build.restype = C.c_int
+    raw = np.ascontiguousarray(raw, np.uint16)
+    Z, Y, X = raw.shape
+    dims = np.array([X, Y, Z], np.int32)
+    ptr, lin = lists if lists is not None else supervoxel_lists(label, n_labels)
+    mv = raw.size if max_vox is None else int(max_vox)
+    query = np.zeros(3 * mv, np.float32)
+    img = np.zeros(mv, np.float32)
+    cent = np.zeros(3 * n_labels, np.float32)
+    lptr = np.zeros(n_labels + 1, np.int64)
+    n_vox, n_sv = C.c_int64(0), C.c_int32(0)
+    rc = ref.ref_frame_build(_p(raw), _p(dims), _p(ptr), _p(lin), n_labels, p.max_size, p.max_pct, p.conn, p.min_size,
+                             _p(query), _p(img), _p(cent), _p(lptr), mv, C.byref(n_vox), C.byref(n_sv))
+    N, S = n_vox.value, n_sv.value
+    out = dict(n_vox=N, n_sv=S)
+    if rc == 0:
+        out.update(query=query[:3 * N].copy(), img=img[:N].copy(), cent=cent[:3 * S].copy(), lptr=lptr[:S + 1].copy())
+    return rc, out

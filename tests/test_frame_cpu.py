@@ -177,7 +177,8 @@ def test_bench_frames_reference_arm_runs_on_cpu():
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["metric"] == "frame preparations/s" and line["value"] > 0
-    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == ("reference" if O.ref_f1_available() else "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["config"]["n_sv_out"] > 0
 
 
@@ -239,3 +240,23 @@ def test_oracle_matches_committed_reference_outputs(name):
         assert o["thr"][p] == g["thr"][s] and b - a == g["cnt"][s]
         np.testing.assert_array_equal(q[:, a:b], _coords(g["kept_lin"][g["kept_ptr"][s]:g["kept_ptr"][s + 1]], X, Y))
         np.testing.assert_array_equal(o["cent"].reshape(3, S)[:, p].view(np.uint32), g["cent"][s].view(np.uint32))
+
+
+@pytest.mark.skipif(not O.ref_f1_available(), reason="reference trimming harness not built")
+@pytest.mark.parametrize("case", CASES + [dict(seed=7), dict(seed=8, n_nuclei=6, min_size=120)],
+                         ids=[str(c) for c in CASES] + ["seed7", "seed8-min120"])
+def test_oracle_frame_build_is_the_reference_host_build(case):
+    """The whole build, bit for bit: the oracle against main's loop run with the reference's own
+    trimming, statistics and erase (coordinates, rescaled intensities, centroids, CSR)."""
+    c = dict(max_size=3000, max_pct=0.4, conn=6, min_size=50)
+    c.update({k: case[k] for k in c if k in case})
+    raw, lab, n = V.make(seed=case["seed"], **{k: case[k] for k in ("dims", "n_nuclei", "big") if k in case})
+    p = O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"])
+    rc, o = O.frame_build(raw, lab, n, p)
+    rr, r = O.ref_frame_build(raw, lab, n, p)
+    assert rc == rr
+    if rc:
+        return
+    assert (o["n_vox"], o["n_sv"]) == (r["n_vox"], r["n_sv"])
+    for k in ("query", "img", "cent", "lptr"):
+        np.testing.assert_array_equal(o[k].view(np.uint8), r[k].view(np.uint8), err_msg=k)
