@@ -11,14 +11,16 @@
 //   k_fb_group   a warp per supervoxel walks its box in raster order and lists its voxels
 //                in ascending linear index (ballot + popcount: no sort), with their values;
 //   k_fb_trim    a block per supervoxel: the trimming threshold (two order statistics by a
-//                two-pass radix select, Otsu's threshold from a 256-bin histogram), the
-//                flood from the brightest voxel (level-synchronous, a bit per voxel claimed
-//                with atomicOr), and for kept supervoxels the FP32 centroid in the
-//                reference's summation order and the range of the background-subtracted
-//                values;
+//                two-pass radix select over 256-bin histograms, Otsu's threshold), the
+//                flood from the brightest voxel (level-synchronous; candidate and reached
+//                bits of the supervoxel's box in shared memory, or one bit per volume voxel
+//                in global memory for boxes beyond 65536 voxels), each list entry's verdict,
+//                and for kept supervoxels the FP32 centroid in the reference's summation
+//                order and the range of the background-subtracted values;
 //   k_fb_order   one block: the reference's erase order (a closed form of its
-//                swap-to-the-back loop, resolved by pointer jumping), the output CSR, the
-//                [0,1] rescale factors;
+//                swap-to-the-back loop, resolved by pointer jumping), the [0,1] rescale
+//                factors;
+//   k_fb_csr     one block: the output CSR in that order;
 //   k_fb_emit    a warp per output supervoxel writes its kept voxels in ascending order.
 // Every rounding step is written with explicit _rn intrinsics so that no multiply-add is
 // contracted: the results are the host build's bits.
