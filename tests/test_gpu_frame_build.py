@@ -145,8 +145,11 @@ def test_em_on_the_built_frame_is_the_em_on_the_oracles_arrays(cuda_ok):
     b = plan.run_host(up, g, prm)
     np.testing.assert_array_equal(a["rnk"], b["rnk"])
     np.testing.assert_array_equal(a["ind"], b["ind"])
+    # integer fields exactly; FP64 parameters to 1e-12 relative (the EM's own run-to-run
+    # reproducibility is the subject of other tests; here the inputs are what is compared)
     for name in a["gauss"].dtype.names:
-        x = np.ascontiguousarray(a["gauss"][name]).view(np.uint8).reshape(S, -1)
-        y = np.ascontiguousarray(b["gauss"][name]).view(np.uint8).reshape(S, -1)
-        rows = np.nonzero((x != y).any(1))[0]
-        assert len(rows) == 0, (name, rows.tolist(), a["gauss"][name][rows].tolist(), b["gauss"][name][rows].tolist())
+        x, y = a["gauss"][name], b["gauss"][name]
+        if np.issubdtype(x.dtype, np.floating):
+            np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-300, err_msg=name)
+        else:
+            np.testing.assert_array_equal(x, y, err_msg=name)
