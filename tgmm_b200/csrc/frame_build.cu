@@ -527,8 +527,8 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
       decode(v, uX, XY, &x, &y, &z);
       const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
       in = (s_reach[li >> 5] >> (li & 31)) & 1u;
-    } else {
-      in = (w.bits[v >> 5] >> (v & 31)) & 1u;
+    } else {  // the flood's bits were set by atomics at L2: read them there
+      in = (__ldcg(&w.bits[v >> 5]) >> (v & 31)) & 1u;
     }
     keep[i] = in ? 1 : 0;
   }
