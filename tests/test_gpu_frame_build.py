@@ -132,6 +132,11 @@ def test_em_on_the_built_frame_is_the_em_on_the_oracles_arrays(cuda_ok):
     assert rc == 0
     f, _ = device_build(raw, lab, n, c)
     S = o["n_sv"]
+    # the inputs first: the built arrays are the oracle's bits
+    np.testing.assert_array_equal(f.query.cpu().numpy(), o["query"])
+    np.testing.assert_array_equal(f.img.cpu().numpy().view(np.uint32), o["img"].view(np.uint32))
+    np.testing.assert_array_equal(f.centroids.cpu().numpy().view(np.uint32), o["cent"].view(np.uint32))
+    np.testing.assert_array_equal(f.label_ptr.cpu().numpy(), o["lptr"])
     g = np.repeat(F.frame("hard").gauss[:1], S)
     cent = o["cent"].reshape(3, S).T.astype(np.float64)
     g["m_k"] = cent
