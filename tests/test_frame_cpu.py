@@ -260,3 +260,34 @@ def test_oracle_frame_build_is_the_reference_host_build(case):
     assert (o["n_vox"], o["n_sv"]) == (r["n_vox"], r["n_sv"])
     for k in ("query", "img", "cent", "lptr"):
         np.testing.assert_array_equal(o[k].view(np.uint8), r[k].view(np.uint8), err_msg=k)
+
+
+def test_abi_frame_build_refuses_bad_sizes_and_parameters_without_a_gpu():
+    """Every argument check of tgmm_frame_build happens on the host before any device work."""
+    lib = L.gmem()
+    p = L.TgmmFrameBuildParams()
+    lib.tgmm_frame_build_default_params(C.byref(p))
+    nv, ns = C.c_int64(0), C.c_int32(0)
+    fake = C.c_void_p(4096)  # never dereferenced: each call below is refused first
+    ws = 1 << 40
+
+    def call(dims, n=10, label=fake, params=p, max_vox=1, max_sv=1):
+        d = (C.c_int32 * 3)(*dims)
+        return lib.tgmm_frame_build(fake, label, d, n, C.byref(params), fake, ws, fake, fake, fake, fake, None,
+                                    max_vox, max_sv, C.byref(nv), C.byref(ns), None)
+
+    assert call((0, 4, 4)) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), n=0) == L.TGMM_ERR_INVALID_ARG
+    assert call((4096, 4096, 256)) == L.TGMM_ERR_BAD_SIZE            # 2^32 voxels
+    assert call((4, 4, 4), n=(1 << 24) + 1) == L.TGMM_ERR_BAD_SIZE
+    assert call((4, 4, 4), label=C.c_void_p(4100)) == L.TGMM_ERR_INVALID_ARG  # label not 16-byte aligned
+    assert b"aligned" in lib.tgmm_last_error()
+    bad = L.TgmmFrameBuildParams(p.max_nuclei_size, 1.5, p.conn3d, p.min_nuclei_size)
+    assert call((4, 4, 4), params=bad) == L.TGMM_ERR_INVALID_ARG
+    bad = L.TgmmFrameBuildParams(-1, p.max_percentile, p.conn3d, p.min_nuclei_size)
+    assert call((4, 4, 4), params=bad) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), max_vox=-1) == L.TGMM_ERR_INVALID_ARG
+    ms = (C.c_float * L.TGMM_FRAME_BUILD_STAGES)()
+    d = (C.c_int32 * 3)(4, 4, 4)
+    assert lib.tgmm_frame_build_timed(fake, fake, d, 10, C.byref(p), fake, ws, fake, fake, fake, fake, None, 1, 1,
+                                      C.byref(nv), C.byref(ns), None, None) == L.TGMM_ERR_INVALID_ARG
