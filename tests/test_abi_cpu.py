@@ -200,3 +200,38 @@ def test_gmm_xml_document_parses_and_carries_each_gaussian(tmp_path):
         np.testing.assert_allclose(W, W.T)
         np.testing.assert_allclose(W[0], g["W_k"][i][[0, 1, 2]], rtol=1e-5, atol=1e-12)
     assert L.gmem().tgmm_write_gmm_xml(None, g.ctypes.data, 1) == L.TGMM_ERR_INVALID_ARG
+
+
+def test_frame_build_usage_compiles_and_links(tmp_path):
+    """The C usage of the frame preparation documented for integrators compiles against the
+    header and links against the library."""
+    src = tmp_path / "use_frame_build.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "tgmm_gmem.h"
+int prepare(const uint16_t* raw_dev, const uint32_t* label_dev, int32_t X, int32_t Y, int32_t Z,
+            int32_t n_labels, void* ws_dev, int64_t ws, float* query_dev, float* img_dev, float* cent_dev,
+            int64_t* lptr_dev, uint16_t* thr_dev, int64_t max_vox, int32_t max_sv, int32_t K, void* stream,
+            TgmmFrame* out) {
+  TgmmFrameBuildParams fp;
+  tgmm_frame_build_default_params(&fp);
+  int32_t dims[3] = {X, Y, Z};
+  if (ws < tgmm_frame_build_bytes(dims, n_labels)) return TGMM_ERR_BAD_SIZE;
+  int64_t n_vox;
+  int32_t n_sv;
+  int rc = tgmm_frame_build(raw_dev, label_dev, dims, n_labels, &fp, ws_dev, ws, query_dev, img_dev, cent_dev,
+                            lptr_dev, thr_dev, max_vox, max_sv, &n_vox, &n_sv, stream);
+  if (rc != TGMM_OK) {
+    fprintf(stderr, "%s\n", tgmm_last_error());
+    return rc;
+  }
+  TgmmFrame f = {query_dev, img_dev, cent_dev, lptr_dev, n_vox, n_sv, K};
+  *out = f;
+  return TGMM_OK;
+}
+int main(void) { return 0; }
+''')
+    exe = tmp_path / "use_frame_build"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", str(src), "-I" + INC, L.GMEM_SO,
+                        "-Wl,-rpath," + os.path.dirname(L.GMEM_SO), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
