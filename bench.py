@@ -186,33 +186,63 @@ def cpu_model() -> str:
 
 
 def cpu_baseline(frame, threads=None, single=False):
-    """The reference's FP32 kernel arithmetic (oracle REF32 port) on the host cores, one EM
-    iteration of the workload frame as the bounded sample (repeated until half a second has
-    passed, for small frames), scaled to 20 iterations; with `single`, the same sample on one
-    thread too, for context."""
+    """The reference's FP32 kernel arithmetic (the oracle's REF32 port, OpenMP over the host
+    cores) on the workload frame: one whole EM call, the same 20 iterations the GPU runs, as
+    the bounded sample; with `single`, one iteration of it on one thread, for context."""
     from oracle import oracle as O
     n = threads or os.cpu_count() or 1
-    p = O.params(max_iter=1, tol=-1.0, mode=O.MODE_REF32)
-
-    def sample(t):
-        O.lib().or_set_num_threads(t)
-        reps, t0 = 0, time.perf_counter()
-        while True:
-            O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, p)
-            reps += 1
-            el = time.perf_counter() - t0
-            if el >= 0.5:
-                return el / reps
-    dt = sample(n)
-    info = {"value": 1.0 / (EM_ITERS * dt), "unit": UNIT, "cores": n, "kind": "port", "cpu_model": cpu_model(),
-            "sample": f"1 of {EM_ITERS} EM iterations of the workload frame with the FP32 OpenMP port of the "
-                      f"reference kernels ({dt:.2f} s), scaled to {EM_ITERS} iterations"}
+    O.lib().or_set_num_threads(n)
+    t0 = time.perf_counter()
+    out = O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss,
+                   O.params(max_iter=EM_ITERS, tol=-1.0, mode=O.MODE_REF32))
+    dt = time.perf_counter() - t0
+    assert out["iterations"] == EM_ITERS
+    info = {"value": 1.0 / dt, "unit": UNIT, "cores": n, "kind": "port", "cpu_model": cpu_model(),
+            "sample": f"one whole EM call ({EM_ITERS} iterations) of the workload frame with the FP32 OpenMP port "
+                      f"of the reference kernels ({dt:.2f} s)"}
     if single:
-        d1 = sample(1)
+        O.lib().or_set_num_threads(1)
+        t0 = time.perf_counter()
+        O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss,
+                 O.params(max_iter=1, tol=-1.0, mode=O.MODE_REF32))
+        d1 = time.perf_counter() - t0
         O.lib().or_set_num_threads(n)
         info["single_thread"] = {"value": 1.0 / (EM_ITERS * d1), "unit": UNIT, "cores": 1,
-                                 "sample": f"the same iteration on one thread ({d1:.2f} s)"}
+                                 "sample": f"one of the {EM_ITERS} iterations on one thread ({d1:.2f} s), "
+                                           f"scaled to {EM_ITERS}"}
     return info, dt
+
+
+PARITY_TOL = {"rnk_max_abs": 1e-5, "m_max_abs_voxel": 1e-3, "w_max_rel": 1e-4, "ll_rel": 1e-6}
+
+
+def parity_vs_oracle(frame, got):
+    """The GPU call's outputs (got: gauss records, rnk, ind, ll) against the FP64 oracle's
+    EM on the same frame and parameters: kNN candidates and supervoxel assignments exact,
+    the largest errors of rnk, means, precision matrices (relative to the largest entry of
+    each) and log-likelihood beside their tolerances.  Outside every timed region."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    o = O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss,
+                 O.params(max_iter=EM_ITERS, tol=-1.0))
+    dt = time.perf_counter() - t0
+    gg, og = got["gauss"], o["gauss"]
+    a = og["m_o"][:, 0] > -1e31
+    wscale = np.max(np.abs(og["W_k"][a]), axis=1, keepdims=True)
+    assign = bool(np.array_equal(gg["supervoxelNum"], og["supervoxelNum"]) and all(
+        np.array_equal(gg["supervoxelIdx"][k][:og["supervoxelNum"][k]], og["supervoxelIdx"][k][:og["supervoxelNum"][k]])
+        for k in range(og.shape[0])))
+    err = {"ind_equal": bool(np.array_equal(got["ind"], o["ind"])), "assignments_equal": assign,
+           "alive_equal": bool(np.array_equal(gg["m_o"][:, 0] > -1e31, a)),
+           "rnk_max_abs": float(np.max(np.abs(got["rnk"] - o["rnk"]))),
+           "m_max_abs_voxel": float(np.max(np.abs(gg["m_k"][a] - og["m_k"][a]))),
+           "w_max_rel": float(np.max(np.abs(gg["W_k"][a] - og["W_k"][a]) / wscale)),
+           "ll_rel": abs(got["ll"] - o["ll"]) / abs(o["ll"])}
+    err["within_tolerance"] = bool(err["ind_equal"] and err["assignments_equal"] and err["alive_equal"] and
+                                   all(err[k] <= v for k, v in PARITY_TOL.items()))
+    err["tolerance"] = PARITY_TOL
+    err["oracle"] = f"FP64 CPU oracle, {EM_ITERS} iterations, {os.cpu_count()} threads ({dt:.1f} s)"
+    return err
 
 
 def reference_gpu(frame, reps=3):
@@ -303,27 +333,43 @@ def run_reference(args):
     if args.workload == "frames":
         run_reference_frames(args)
         return
+    from oracle import oracle as O
     from tgmm_b200 import synth
     spec = spec_for(args.workload)
     frame = synth.generate(spec, seed=args.seed)
+    n = os.cpu_count() or 1
+    O.lib().or_set_num_threads(n)
+    p = O.params(max_iter=EM_ITERS, tol=-1.0, mode=O.MODE_REF32)
     times = []
-    info = None
     for i in range(args.warmup + args.steps):
-        info, dt = cpu_baseline(frame)
+        t0 = time.perf_counter()
+        out = O.em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, p)
+        dt = time.perf_counter() - t0
+        assert out["iterations"] == EM_ITERS
         if i >= args.warmup:
             times.append(dt)
-    per_frame = EM_ITERS * float(np.sum(times)) / len(times)
+    per_frame = float(np.mean(times))
     value = 1.0 / per_frame
-    info["value"] = value
+    info = {"value": value, "unit": UNIT, "cores": n, "kind": "port", "cpu_model": cpu_model(),
+            "sample": f"each step one whole EM call ({EM_ITERS} iterations) of the workload frame with the FP32 "
+                      f"OpenMP port of the reference kernels on {n} threads (mean {per_frame:.2f} s)"}
     gpu_ref = reference_gpu(frame)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_frame * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload], "n_vox": frame.n_vox, "n_sv": frame.n_sv,
-                       "n_gauss": frame.n_gauss},
+            "config": config_of(args.workload, frame),
             "cpu_baseline": info, "reference_gpu": gpu_ref,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config_of(workload, frame, **extra):
+    """The config object both arms print for a single-frame workload."""
+    c = {"workload": WORKLOADS[workload], "n_vox": frame.n_vox, "n_sv": frame.n_sv, "n_gauss": frame.n_gauss,
+         "em_iterations": EM_ITERS, "l2": "inputs larger than L2 (16 B x n_vox)" if workload == "c2" else
+         "inputs fit in L2", "ll_precision": "mixed", "ll_mode": "as_reference"}
+    c.update(extra)
+    return c
 
 
 def run_ours(args):
@@ -365,6 +411,8 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     check = plan.run_device(df, gm.copy_(gm0), rnk, ind, params, stats=True)
     assert check["iterations"] == EM_ITERS, check
+    got = {"gauss": gm.cpu().numpy().view(L.GAUSS_DTYPE).copy(), "rnk": rnk.cpu().numpy(), "ind": ind.cpu().numpy(),
+           "ll": check["ll"]}
 
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     if world > 1:
@@ -418,24 +466,24 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = run_e2e(frame, df, plan, params, dev, args)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_baseline(frame, single=True)
+        parity = parity_vs_oracle(frame, got)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-                "config": {"workload": WORKLOADS[args.workload], "n_vox": N, "n_sv": S, "n_gauss": K,
-                           "em_iterations": EM_ITERS,
-                           "knn_lanes_per_supervoxel": knn_lanes, "knn_in_voxel_pass": knn_fused,
-                           "knn_grid_searches_after_iteration_1": check["knn_searches"],
-                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (16 B x n_vox)",
-                           "ll_precision": "mixed", "ll_mode": "as_reference"},
+                "config": config_of(args.workload, frame, knn_lanes_per_supervoxel=knn_lanes,
+                                    knn_in_voxel_pass=knn_fused,
+                                    knn_grid_searches_after_iteration_1=check["knn_searches"],
+                                    parallelism=f"replicas x{world}"),
                 "voxel_iters_per_s": voxel_iters,
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "gpu_launches": kernels_per_call(knn_fused) * args.steps,
-                "roofline": roofline, "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
+                "roofline": roofline, "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu,
+                "parity": parity}
         print(json.dumps(line), flush=True)
     plan.close()
     if world > 1:

@@ -120,6 +120,21 @@ typedef struct TgmmFrame {
   int32_t n_gauss;
 } TgmmFrame;
 
+/* Bits of TgmmEmStats.device_flags: what the kernels met during the call.  The overflow
+ * bits name the exact slower branch a frame took (results are the same either way); the
+ * others make the call return an error status. */
+#define TGMM_FLAG_BAD_CSR 1         /* labelListPtr not a CSR over the voxels (TGMM_ERR_BAD_CSR) */
+#define TGMM_FLAG_NAN_INPUT 2       /* NaN coordinate or intensity (TGMM_ERR_NAN_INPUT) */
+#define TGMM_FLAG_FEW_GAUSS 4       /* fewer than 5 Gaussians in a frame (TGMM_ERR_BAD_SIZE) */
+#define TGMM_FLAG_BUCKET_OVERFLOW 8 /* a Gaussian was a candidate of more than 32 (slot, supervoxel)
+                                       pairs: its M-step sums came from an ordered scan of the frame */
+#define TGMM_FLAG_ASSIGN_OVERFLOW 16 /* more than 32 supervoxels with rnk > 0.5 on one Gaussian: its
+                                        supervoxelIdx came from an ordered scan of the frame */
+#define TGMM_FLAG_CELL_OVERFLOW 32  /* more than 32 Gaussian centres in one kNN grid cell: the
+                                       frame's kNN scanned every Gaussian */
+#define TGMM_FLAG_STAGE_TIMEOUT 64  /* a voxel tile copy missed the plan's wait limit
+                                       (TGMM_ERR_DEVICE_FLAG; the outputs are not valid) */
+
 typedef struct TgmmEmStats {
   int32_t iterations;       /* EM iterations executed (numIterEM-1 in the reference) */
   int32_t converged;        /* 1 if stopped by the tolerance test */
@@ -201,7 +216,9 @@ int tgmm_knn_k(const float* query_dev, int64_t n_query, const float* ref_dev, in
  * TGMM_KNN_NOALLOC_MAX_REF reference points (TGMM_ERR_BAD_SIZE beyond).  The first call on a
  * device looks the array's device address up with that device current; make that first call
  * before any stream capture.  All calls share the one array: calls that overlap on the GPU
- * (different streams, or different host threads) race and must be serialised by the caller. */
+ * (different streams, or different host threads) race and must be serialised by the caller.
+ * The looked-up address is kept for the life of the process: after cudaDeviceReset on a
+ * device, do not call this entry point on that device again. */
 #define TGMM_KNN_NOALLOC_MAX_REF 65535
 int tgmm_knn_noalloc(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
                      int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
@@ -304,6 +321,13 @@ int tgmm_plan_set_knn_group(TgmmPlan* plan, int32_t lanes);
  * bits; running them together pays off when the voxel pass leaves the SMs idle (small
  * frames), apart when the batch is large.  No reference counterpart. */
 int tgmm_plan_set_knn_fusion(TgmmPlan* plan, int32_t on);
+/* Wait limit, in nanoseconds, of each voxel tile copy of the voxel passes (default 1 s;
+ * 1 ns .. 60 s).  No reference counterpart.  A copy that misses it flags its frame with
+ * TGMM_FLAG_STAGE_TIMEOUT and the call returns TGMM_ERR_DEVICE_FLAG; the warp that met it
+ * still waits for its own copies in flight (bounded by 1 s) before it leaves, and the next
+ * call on the plan starts from a clean state.  A short limit exercises that path. */
+int tgmm_plan_set_stage_wait(TgmmPlan* plan, int64_t wait_ns);
+
 /* The plan's current kNN/E-step width and arrangement (either pointer may be NULL). */
 int tgmm_plan_tuning(TgmmPlan* plan, int32_t* lanes, int32_t* fused);
 

@@ -4,7 +4,9 @@
 # oracle/_ref/libtgmm_ref.so.  Nothing is copied from the reference tree.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${TGMM_REFERENCE_SRC:-/root/reference/nmeth.3036-S2/src}
+# the reference project's src/ tree: TGMM_REFERENCE_SRC, else a checkout named "reference"
+# beside this repository
+REF=${TGMM_REFERENCE_SRC:-$HERE/../../reference/nmeth.3036-S2/src}
 OUT="$HERE/_ref"
 if [ ! -d "$REF/UtilsCUDA" ]; then
   echo "reference sources not found at $REF; skipping" >&2

@@ -54,6 +54,47 @@ def _displace(frame, seed, sigma=3.0):
     return frame
 
 
+def _split(frame, piece=12):
+    """Every supervoxel cut into consecutive pieces of `piece` voxels (the last piece takes
+    the rest), each piece a supervoxel with its FP32 intensity-weighted centroid: each
+    Gaussian becomes a candidate of many small supervoxels (more than the 32 pairs of its
+    M-step bucket) and takes more than 32 of them (rnk > 0.5), so both ordered-scan
+    branches run."""
+    lp = frame.label_ptr
+    cuts = [0]
+    for s in range(frame.n_sv):
+        a, b = int(lp[s]), int(lp[s + 1])
+        p = a + piece
+        while p < b:
+            if b - p < piece // 2:
+                break
+            cuts.append(p)
+            p += piece
+        cuts.append(b)
+    cuts = np.array(sorted(set(cuts)), np.int64)
+    N = frame.n_vox
+    q = frame.query.reshape(3, N).astype(np.float64)
+    w = frame.img.astype(np.float64)
+    sw = np.add.reduceat(w, cuts[:-1])
+    cent = np.stack([np.add.reduceat(q[d] * w, cuts[:-1]) / sw for d in range(3)]).astype(np.float32)
+    frame.label_ptr = cuts
+    frame.centroids = np.ascontiguousarray(cent.reshape(-1))
+    frame.sv_nucleus = np.zeros(cuts.size - 1, np.int32)
+    return frame
+
+
+def _crowd(frame, seed, n_copies=40, sigma=0.05):
+    """n_copies near-copies of Gaussian 0 within sigma voxels of it: more centres in one
+    kNN grid cell than the cell holds (32), so the frame's kNN scans every Gaussian."""
+    rng = np.random.default_rng(seed)
+    g = frame.gauss.copy()
+    extra = np.repeat(g[:1], n_copies)
+    extra["m_k"] += rng.normal(0, sigma, size=(n_copies, 3))
+    extra["m_o"] = extra["m_k"]
+    frame.gauss = np.concatenate([g, extra]).astype(L.GAUSS_DTYPE)
+    return frame
+
+
 @functools.lru_cache(maxsize=None)
 def frame(name: str):
     if name == "tiny":
@@ -68,6 +109,10 @@ def frame(name: str):
         return synth.generate(SPEC_BIG, seed=5)
     if name == "moved":
         return _displace(synth.generate(SPEC_SMALL, seed=21), 21)
+    if name == "split":
+        return _split(synth.generate(SPEC_SMALL, seed=31))
+    if name == "crowded":
+        return _crowd(synth.generate(SPEC_SMALL, seed=41), 41)
     raise KeyError(name)
 
 

@@ -74,6 +74,18 @@ def test_default_params_are_the_reference_defaults():
     assert p.max_iter_em == 400 and p.tol_likelihood == 1e-6 and p.w4dof == 1
     assert (p.lambda_min, p.lambda_max, p.max_excentricity) == (0.02, 0.2222, 9.0)
     assert p.ll_mode == L.TGMM_LL_AS_REFERENCE
+    # the Python defaults (set without loading the engine) are the library's, byte for byte
+    c = L.TgmmEmParams()
+    L.gmem().tgmm_default_params(C.byref(c))
+    assert bytes(p) == bytes(c)
+
+
+def test_device_flag_bits_are_the_headers():
+    src = open(os.path.join(INC, "tgmm_gmem.h")).read()
+    bits = dict((k, int(v)) for k, v in re.findall(r"#define (TGMM_FLAG_[A-Z_]+) (\d+)", src))
+    assert len(bits) == 7
+    for k, v in bits.items():
+        assert getattr(L, k) == v, k
 
 
 def test_plan_bytes_is_monotone():
@@ -179,6 +191,7 @@ def test_width_setter_refuses_bad_arguments_without_a_gpu():
     assert lib.tgmm_plan_autotune(None, 1, None, None, None, None, None, 1, None, None) == L.TGMM_ERR_INVALID_ARG
     assert lib.tgmm_plan_set_knn_fusion(None, 1) == L.TGMM_ERR_INVALID_ARG
     assert lib.tgmm_plan_tuning(None, None, None) == L.TGMM_ERR_INVALID_ARG
+    assert lib.tgmm_plan_set_stage_wait(None, 1000) == L.TGMM_ERR_INVALID_ARG
 
 
 def test_gmm_xml_document_parses_and_carries_each_gaussian(tmp_path):

@@ -138,7 +138,25 @@ def test_otsu_threshold_cases():
     assert 10.0 <= t < 200.0
 
 
+def _without_a_device(body):
+    """Runs body (a function of this module) in a child process that sees no CUDA device,
+    so that a host check dropped or reordered shows up as a CUDA error on the host instead
+    of a kernel launched on the made-up addresses these tests pass."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    code = f"import sys; sys.path[:0] = [{here!r}, {os.path.dirname(here)!r}]; import test_frame_cpu as t; t.{body}()"
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+
+
 def test_abi_frame_build_checks_arguments_without_a_gpu():
+    _without_a_device("_check_frame_build_arguments")
+
+
+def _check_frame_build_arguments():
     lib = L.gmem()
     dims = (C.c_int32 * 3)(64, 48, 16)
     assert lib.tgmm_frame_build_bytes(dims, 0) == -1
@@ -264,6 +282,10 @@ def test_oracle_frame_build_is_the_reference_host_build(case):
 
 def test_abi_frame_build_refuses_bad_sizes_and_parameters_without_a_gpu():
     """Every argument check of tgmm_frame_build happens on the host before any device work."""
+    _without_a_device("_check_frame_build_refusals")
+
+
+def _check_frame_build_refusals():
     lib = L.gmem()
     p = L.TgmmFrameBuildParams()
     lib.tgmm_frame_build_default_params(C.byref(p))

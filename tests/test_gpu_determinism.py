@@ -1,0 +1,74 @@
+"""Run-to-run determinism of the EM: equal inputs give equal bytes.
+
+No kernel uses float atomics; per-frame sums are fixed-order sums of chunk partials or
+integer fixed-point sums; the M-step visits each Gaussian's pairs in ascending (slot,
+supervoxel) order; the kNN keeps (distance, index) order whatever order a grid cell was
+filled in.  These tests hold the Gaussian records (every byte), rnk and ind of one call
+equal across 20 repeats on one plan, across fresh plans, and after the plan ran other
+frames (so no state of an earlier call leaks into a later one).
+"""
+import numpy as np
+import pytest
+
+import _fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+
+def _call(plan, name, iters=20):
+    import torch
+    from tgmm_b200 import engine as E
+    f = F.frame(name)
+    gm = E.gauss_to_device(f.gauss)
+    rnk = torch.empty(5 * f.n_sv, device="cuda")
+    ind = torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda")
+    st = plan.run_device(_call.frames.setdefault(name, E.to_device(f)), gm, rnk, ind, F.params(iters))
+    return gm.cpu().numpy(), rnk.cpu().numpy(), ind.cpu().numpy(), st
+
+
+_call.frames = {}
+
+
+def _same(a, b, what):
+    for x, y, part in zip(a[:3], b[:3], ("gauss", "rnk", "ind")):
+        xb, yb = np.ascontiguousarray(x).view(np.uint8), np.ascontiguousarray(y).view(np.uint8)
+        assert np.array_equal(xb, yb), (what, part, int(np.count_nonzero(xb != yb)))
+
+
+def _plan_for(*names, frames=1):
+    from tgmm_b200 import engine as E
+    fs = [F.frame(n) for n in names]
+    return E.Plan(max(f.n_vox for f in fs), max(f.n_sv for f in fs), max(f.n_gauss for f in fs), max_frames=frames)
+
+
+@pytest.mark.parametrize("name", ["hard", "c1"])
+def test_twenty_calls_on_one_plan_are_bit_identical(cuda_ok, name):
+    plan = _plan_for(name)
+    first = _call(plan, name)
+    for i in range(19):
+        _same(first, _call(plan, name), f"{name} repeat {i + 1}")
+    plan.close()
+
+
+@pytest.mark.parametrize("name", ["hard", "c1"])
+def test_fresh_plans_are_bit_identical(cuda_ok, name):
+    outs = []
+    for _ in range(3):
+        plan = _plan_for(name)
+        outs.append(_call(plan, name))
+        plan.close()
+    for i in (1, 2):
+        _same(outs[0], outs[i], f"{name} fresh plan {i}")
+
+
+def test_no_state_leaks_between_calls(cuda_ok):
+    """One plan runs hard, c1, big, moved, split and hard again; each result equals the one
+    from a plan that ran only that frame."""
+    names = ["hard", "c1", "big", "moved", "split", "hard"]
+    shared = _plan_for(*names)
+    got = [_call(shared, n) for n in names]
+    shared.close()
+    for n, g in zip(names, got):
+        alone = _plan_for(n)
+        _same(_call(alone, n), g, f"{n} after other frames")
+        alone.close()

@@ -9,14 +9,12 @@ import numpy as np
 import pytest
 
 import _fixtures as F
+from _parity import compare
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["tiny", "small", "c1", "hard", "big", "moved"]
-RNK_TOL = 1e-5
-M_TOL = 1e-3
-W_RTOL = 1e-4
+CASES = ["tiny", "small", "c1", "hard", "big", "moved", "split", "crowded"]
 
 
 def gpu_run(name, iters=20, tol=-1.0, **kw):
@@ -35,30 +33,6 @@ def oracle_run(name, iters=20, tol=-1.0, ll_mode=O.LL_AS_REFERENCE, mode=O.MODE_
     f = F.frame(name)
     return O.em_run(f.query, f.img, f.centroids, f.label_ptr, f.gauss,
                     O.params(max_iter=iters, tol=tol, ll_mode=ll_mode, mode=mode))
-
-
-def compare(g, o, ll_rtol=1e-6):
-    assert g["iterations"] == o["iterations"]
-    np.testing.assert_array_equal(g["ind"], o["ind"])
-    assert np.max(np.abs(g["rnk"] - o["rnk"])) <= RNK_TOL
-    gg, og = g["gauss"], o["gauss"]
-    alive_g = gg["m_o"][:, 0] > -1e31
-    alive_o = og["m_o"][:, 0] > -1e31
-    np.testing.assert_array_equal(alive_g, alive_o)
-    np.testing.assert_array_equal(gg["supervoxelNum"], og["supervoxelNum"])
-    for k in range(gg.shape[0]):
-        n = og["supervoxelNum"][k]
-        np.testing.assert_array_equal(gg["supervoxelIdx"][k][:n], og["supervoxelIdx"][k][:n])
-    a = alive_o
-    assert np.max(np.abs(gg["m_k"][a] - og["m_k"][a])) <= M_TOL
-    wscale = np.max(np.abs(og["W_k"][a]), axis=1, keepdims=True)
-    assert np.max(np.abs(gg["W_k"][a] - og["W_k"][a]) / wscale) <= W_RTOL
-    for key in ("nu_k", "beta_k", "alpha_k"):
-        np.testing.assert_allclose(gg[key][a], og[key][a], rtol=1e-9, atol=1e-9)
-    assert abs(g["ll"] - o["ll"]) <= ll_rtol * abs(o["ll"])
-    assert abs(g["ll_true"] - o["ll_true"]) <= ll_rtol * abs(o["ll_true"])
-    assert abs(g["ll_as_reference"] - o["ll_as_reference"]) <= ll_rtol * abs(o["ll_as_reference"])
-    assert g["n_dead"] == o["n_dead"]
 
 
 @pytest.mark.parametrize("name", CASES)

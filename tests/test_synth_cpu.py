@@ -79,3 +79,24 @@ def test_time_series_motion_and_division():
     nxt = synth.evolve_nuclei(nuc, synth.TINY, rng, divide_frac=0.5)
     assert nxt.n > nuc.n
     assert np.all(nxt.centre >= 0) and np.all(nxt.centre <= np.array(synth.TINY.dims) - 1)
+
+
+def test_bench_reference_arm_never_maps_the_engine():
+    """bench.py --impl reference (the reference's CPU arithmetic, each step one whole 20-iteration
+    EM call) runs on the CPU and never loads the CUDA engine library: the data generator and
+    the CPU arithmetic need nothing from it."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'c1', '--steps', '1', "
+            "'--warmup', '0']; runpy.run_path('bench.py', run_name='__main__'); "
+            "print('MAPPED', 'libtgmm_gmem.so' in open('/proc/self/maps').read())")
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert lines[-1] == "MAPPED False"
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["config"]["em_iterations"] == 20
+    assert abs(line["ms_per_step"] - 1e3 / line["value"]) < 1e-6 * line["ms_per_step"]

@@ -37,6 +37,15 @@ TGMM_LL_TRUE = 1
 TGMM_LLPREC_MIXED = 0
 TGMM_LLPREC_FP64 = 1
 
+# TgmmEmStats.device_flags bits (tgmm_gmem.h)
+TGMM_FLAG_BAD_CSR = 1
+TGMM_FLAG_NAN_INPUT = 2
+TGMM_FLAG_FEW_GAUSS = 4
+TGMM_FLAG_BUCKET_OVERFLOW = 8
+TGMM_FLAG_ASSIGN_OVERFLOW = 16
+TGMM_FLAG_CELL_OVERFLOW = 32
+TGMM_FLAG_STAGE_TIMEOUT = 64
+
 TGMM_KERNEL_MOMENTS = 0
 TGMM_KERNEL_LL_PASS = 2
 TGMM_KERNEL_LL_PASS_KNN = 3
@@ -179,6 +188,7 @@ GMEM_FUNCS = {
     "tgmm_plan_time_kernel": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP]),
     "tgmm_plan_set_knn_group": (C.c_int, [_VP, C.c_int32]),
     "tgmm_plan_set_knn_fusion": (C.c_int, [_VP, C.c_int32]),
+    "tgmm_plan_set_stage_wait": (C.c_int, [_VP, C.c_int64]),
     "tgmm_plan_tuning": (C.c_int, [_VP, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "tgmm_plan_autotune": (C.c_int, [_VP, C.c_int32, C.POINTER(TgmmFrame), C.POINTER(_VP), C.POINTER(_VP),
                                      C.POINTER(_VP), C.POINTER(TgmmEmParams), C.c_int32, C.POINTER(C.c_int32), _VP]),
@@ -254,8 +264,15 @@ def check(code, where):
 
 
 def default_params(**overrides) -> TgmmEmParams:
+    """The values tgmm_default_params fills in (the reference defaults,
+    parseConfigFile.h:152-195), set here without loading the engine library, so that
+    code which only generates data or runs the CPU arithmetic never maps it."""
     p = TgmmEmParams()
-    gmem().tgmm_default_params(C.byref(p))
+    p.max_iter_em, p.w4dof, p.tol_likelihood = 400, 1, 1e-6
+    p.lambda_min, p.lambda_max, p.max_excentricity = 0.02, 0.2222, 9.0
+    p.scale[:] = [1.0, 1.0, 1.0]
+    p.reg_scale[:] = [0.0, 0.0, 0.0]
+    p.ll_mode, p.ll_precision, p.frame = TGMM_LL_AS_REFERENCE, TGMM_LLPREC_MIXED, 0
     for k, v in overrides.items():
         if k in ("scale", "reg_scale"):
             getattr(p, k)[:] = [float(x) for x in v]

@@ -195,6 +195,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.kpos = (float4*)(b + P->L.kpos);
   D.work = (int32_t*)(b + P->L.work);
   D.knn_group = 8;
+  D.stage_wait_ns = 1000000000ull;
   e = configure_kernels(D, d->device);
   if (e != cudaSuccess) {
     tgmm_plan_destroy(P);
@@ -536,6 +537,20 @@ int tgmm_plan_set_knn_fusion(TgmmPlan* P, int32_t on) {
   for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // captured with the other arrangement
   P->graphs.clear();
   P->fuse_knn = on == 1;
+  return TGMM_OK;
+}
+
+int tgmm_plan_set_stage_wait(TgmmPlan* P, int64_t wait_ns) {
+  if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_stage_wait: null plan");
+  if (wait_ns < 1 || wait_ns > 60000000000LL)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_stage_wait: the limit must be 1 ns .. 60 s");
+  std::lock_guard<std::mutex> lock(P->mu);
+  if (P->dev.stage_wait_ns == (unsigned long long)wait_ns) return TGMM_OK;
+  TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
+  if (P->used) TG_CUDA(cudaEventSynchronize(P->done_ev), "wait for the previous call on this plan");
+  for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);  // captured with the old limit
+  P->graphs.clear();
+  P->dev.stage_wait_ns = (unsigned long long)wait_ns;
   return TGMM_OK;
 }
 

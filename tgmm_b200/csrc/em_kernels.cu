@@ -1376,7 +1376,7 @@ constexpr int kLLStages = TGMM_LL_STAGES;     // tile slots per warp
 constexpr int kLLBlocks = TGMM_LL_BLOCKS;     // resident blocks per SM the pass is compiled for
 constexpr int kLLSpan = kLLTile + 4;          // floats per component in a slot (16-byte slack)
 constexpr int kLLSlotFloats = 4 * kLLSpan;    // x, y, z, I
-constexpr unsigned long long kLLWaitNs = 1000000000ull;  // a slot not filled within 1 s counts as lost
+constexpr unsigned long long kLLWaitNs = 1000000000ull;  // default wait limit of a slot, and the drain's bound
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -1401,12 +1401,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Waits for the phase with the given parity; false after kLLWaitNs without it.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+// Waits for the phase with the given parity; false after limit_ns without it.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kLLWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
 }
 // Global -> shared bulk copy (non-multicast) completing on the mbarrier at `bar`.
@@ -1830,7 +1830,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
         gi++;
       }
       const unsigned q = gc % kLLStages;
-      if (!__all_sync(0xffffffffu, mbar_wait(bar0 + 8 * q, (gc / kLLStages) & 1))) return nullptr;
+      if (!__all_sync(0xffffffffu, mbar_wait(bar0 + 8 * q, (gc / kLLStages) & 1, P.stage_wait_ns))) return nullptr;
       return wbuf + q * kLLSlotFloats;
     };
     if constexpr (kMom) {
@@ -1943,8 +1943,11 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     sn = s2;
     ic = in;
   }
-  if (failed) {  // a tile never arrived: wait for the copies still in flight, report, leave
-    for (unsigned g = gc + 1; g < gi; g++) mbar_wait(bar0 + 8 * (g % kLLStages), (g / kLLStages) & 1);
+  if (failed) {
+    // a tile was not delivered within the plan's wait limit: before the warp leaves, every
+    // copy it issued -- the late one included -- must have landed in its shared memory, so
+    // it waits for them with the fixed bound kLLWaitNs, then reports and leaves
+    for (unsigned g = gc; g < gi; g++) mbar_wait(bar0 + 8 * (g % kLLStages), (g / kLLStages) & 1, kLLWaitNs);
     if (lane == 0) atomicOr(&S->flags, F_STAGE_TIMEOUT);
   }
   cp_wait_all();
@@ -2407,6 +2410,7 @@ cudaError_t knn_grid_in_scratch(const float* q, int64_t nq, const float* ref, in
   const size_t off_state = 0, off_cnt = 256, off_start = off_cnt + 4 * (size_t)budget,
                off_cur = off_start + 4 * ((size_t)budget + 1), off_rc = off_cur + 4 * (size_t)budget,
                off_refs = (off_rc + 4 * (size_t)nref + 255) / 256 * 256;
+  static_assert(sizeof(FrameState) <= 256, "the grid geometry record fits the scratch's 256-byte header");
   FrameState* S = (FrameState*)(buf + off_state);
   int* cnt = (int*)(buf + off_cnt);
   int* start = (int*)(buf + off_start);

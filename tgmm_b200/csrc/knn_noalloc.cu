@@ -5,7 +5,9 @@
 // path where an allocation's latency or failure is unacceptable, and code inside a region
 // where the driver is not to be asked for memory.  Their scratch here is one file-scope
 // device array, created when the library is loaded on a device and kept until the process
-// exits.
+// exits.  Its device address is looked up once per device and kept; cudaDeviceReset on a
+// device ends the context that held the array, so a process that resets a device must not
+// call this entry point on that device again.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -63,6 +63,11 @@ enum : int {
   F_CELL_OVERFLOW = 32,
   F_STAGE_TIMEOUT = 64  // a voxel tile copy did not complete within its wait limit
 };
+static_assert(F_BAD_CSR == TGMM_FLAG_BAD_CSR && F_NAN_INPUT == TGMM_FLAG_NAN_INPUT &&
+                  F_FEW_GAUSS == TGMM_FLAG_FEW_GAUSS && F_BUCKET_OVERFLOW == TGMM_FLAG_BUCKET_OVERFLOW &&
+                  F_ASSIGN_OVERFLOW == TGMM_FLAG_ASSIGN_OVERFLOW && F_CELL_OVERFLOW == TGMM_FLAG_CELL_OVERFLOW &&
+                  F_STAGE_TIMEOUT == TGMM_FLAG_STAGE_TIMEOUT,
+              "the device flags are the public TgmmEmStats.device_flags bits");
 
 struct FrameDesc {
   const float* query;
@@ -181,6 +186,7 @@ struct DevPlan {
   int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
   int32_t knn_group;  // lanes per supervoxel of the kNN/E-step (8, 16 or 32)
   int32_t iter;       // the EM iteration a launch belongs to (1-based; set per launch)
+  unsigned long long stage_wait_ns;  // wait limit of a voxel tile copy (default 1 s)
   float4* kpos;  // per Gaussian: the float centre the kNN sees (x, y, z; w = 1 live, 0 dead)
   double* ec;   // per Gaussian E-step record, kEcStride doubles: nu W [6], m [3], 3/beta, psi(alpha)+eLD/2
   double* llc;  // per Gaussian, 10 doubles: -nu*W/2 (off-diagonals doubled) [6], log weight [1], m [3]

@@ -135,6 +135,22 @@ class Plan:
         return [stats_dict(x) for x in st] if st is not None else None
 
 
+    def set_stage_wait(self, ns: int):
+        """Wait limit of the voxel passes' tile copies (default 1 s)."""
+        L.check(self.lib.tgmm_plan_set_stage_wait(self.h, int(ns)), "tgmm_plan_set_stage_wait")
+
+    def run_host_status(self, df: DeviceFrame, gauss: np.ndarray, params: L.TgmmEmParams):
+        """tgmm_em_run returning (status, stats) instead of raising on a non-zero status."""
+        g = np.ascontiguousarray(np.asarray(gauss).astype(L.GAUSS_DTYPE))
+        S = df.n_sv
+        rnk = torch.empty(5 * S, dtype=torch.float32, device=df.img.device)
+        ind = torch.empty(5 * S, dtype=torch.int32, device=df.img.device)
+        st = L.TgmmEmStats()
+        cf = df.cframe()
+        rc = self.lib.tgmm_em_run(self.h, C.byref(cf), g.ctypes.data, rnk.data_ptr(), ind.data_ptr(), None,
+                                  C.byref(params), C.byref(st), torch.cuda.current_stream().cuda_stream)
+        return rc, stats_dict(st)
+
     def set_knn_group(self, lanes: int):
         L.check(self.lib.tgmm_plan_set_knn_group(self.h, lanes), "tgmm_plan_set_knn_group")
 
