@@ -14,6 +14,7 @@
  *                               UtilsCUDA/GMEMupdateCUDA.h:92-98 (body GMEMupdateCUDA.cu:3985-4421)
  *   tgmm_knn                 <- knnCUDAinPlace, UtilsCUDA/knnCuda.h:225-226 (knnCuda.cu:781-817)
  *   tgmm_knn_k               <- knnCUDA_, temporalLogicalRules/knnCUDA/knnCuda.h:48-58
+ *   tgmm_local_likelihood    <- calculateLocalLikelihood, UtilsCUDA/GMEMupdateCUDA.h:120-127
  *   tgmm_update_priors       <- GaussianMixtureModel::updatePriors, GaussianMixtureModel.cpp:892-910,
  *                               plus the nu_k*=2, W_k/=2 step of mainTrackingGaussianMixtureModel.cpp:961-969
  *   tgmm_frame_upload        <- GMEMinitializeMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:132-137
@@ -222,6 +223,22 @@ int tgmm_knn_k(const float* query_dev, int64_t n_query, const float* ref_dev, in
 #define TGMM_KNN_NOALLOC_MAX_REF 65535
 int tgmm_knn_noalloc(const float* query_dev, int64_t n_query, const float* ref_xyz_dev,
                      int32_t n_ref, const float scale[3], int32_t* ind_dev, void* stream);
+
+/* Local log-likelihood of supervoxel lists, the likelihood the split round compares before
+ * and after a proposed division (calculateLocalLikelihood, UtilsCUDA/GMEMupdateCUDA.h:120-127;
+ * body GMEMupdateCUDA.cu:2952-3055, kernel :1989-2103).  For list i (supervoxel indices
+ * list_idx[list_ptr[i] .. list_ptr[i+1]), host arrays; a supervoxel listed twice counts twice)
+ * ll_out[i] (host) = the sum over its supervoxels s of the reference's as-reference
+ * log-likelihood of s's voxels under s's five candidates ind_dev[j*n_sv+s] and the Gaussians
+ * gm_dev (n_gauss records, device): each voxel's density is
+ * sum_j sqrt(det W_j nu_j^3)/(2 pi)^{3/2} exp(-nu_j d'W_j d/2) alpha_j/A, A the sum of alpha
+ * over all n_gauss records, and of the voxels t, t + 1024, ... of s only the last with a
+ * positive density adds I ln(density).  Every step in FP64 (the reference sums in float).  An
+ * empty list gives 0.  The frame needs query, img, label_ptr, n_vox and n_sv (centroids are not
+ * read).  Synchronises `stream`. */
+int tgmm_local_likelihood(const TgmmFrame* frame, const int32_t* ind_dev, const TgmmGaussian* gm_dev,
+                          int32_t n_gauss, const int32_t* list_ptr, const int32_t* list_idx, int32_t n_lists,
+                          double* ll_out, void* stream);
 
 /* Posterior -> prior for the next time point, on the device (served form):
  * N_k = nu_k - nu_o; m_o = m_k; beta_o = max(beta_pct*N_k, 1e-5);

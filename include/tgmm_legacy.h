@@ -11,6 +11,7 @@
  *   GMEMreleaseMemoryWithSupervoxels               <- UtilsCUDA/GMEMupdateCUDA.h:140-144
  *   GMEMvariationalInferenceCUDAWithSupervoxels    <- UtilsCUDA/GMEMupdateCUDA.h:92-98
  *   copyScaleToDvice                               <- UtilsCUDA/GMEMupdateCUDA.h:82
+ *   calculateLocalLikelihood                       <- UtilsCUDA/GMEMupdateCUDA.h:120-127
  *   knnCUDAinPlace, setDeviceCUDA, uploadScaleCUDA, knnCUDA_ (temporalLogicalRules/knnCUDA),
  *   selectCUDAdeviceMaxMemory                      <- UtilsCUDA/knnCuda.h:225-231
  *   regularizePrecisionMatrixConstants             <- constants.h:19-45 (the library carries
@@ -22,6 +23,7 @@
 #ifdef __cplusplus
 #include <ostream>
 #include <string>
+#include <vector>
 
 #include "tgmm_gmem.h"
 
@@ -81,6 +83,14 @@ void GMEMvariationalInferenceCUDAWithSupervoxels(float* queryCUDA, float* imgDat
                                                  double tolLikelihood, int devCUDA, int frame, bool W4DOF,
                                                  std::string debugPath = "");
 void copyScaleToDvice(float* scale);
+/* The local log-likelihood of supervoxel lists (UtilsCUDA/GMEMupdateCUDA.h:120-127): the
+ * frame and the candidates (indCUDA) on the device, the Gaussians (vecGMtemp, ref_nb records)
+ * on the host, one value per list into localLikelihood (resized to the list count; an empty
+ * list leaves its entry as it was); rnkCUDA is not read.  Over tgmm_local_likelihood. */
+void calculateLocalLikelihood(std::vector<double>& localLikelihood,
+                              const std::vector<std::vector<int> >& listSupervoxels, float* queryCUDA,
+                              float* imgDataCUDA, float* rnkCUDA, int* indCUDA, GaussianMixtureModelCUDA* vecGMtemp,
+                              long long int* labelListPtrCUDA, long long int query_nb, int ref_nb, int numLabels);
 void knnCUDAinPlace(int* indCUDA, float* queryCUDA, float* refTemp, long long int query_nb, int ref_nb);
 /* The tracking graph's supervoxel kNN (temporalLogicalRules/knnCUDA/knnCuda.h:48-58): host
  * query (SoA) and ref (SoA) in, ind (and dist, if not NULL) out, KNN <= 11; over tgmm_knn_k. */

@@ -37,5 +37,11 @@ g++ $CXXF -c "$HSD/hierarchicalSegmentation.cpp" -o "$OUT/f1_hs.o"
 g++ $CXXF -c "$HERE/ref_f1_harness.cpp" -o "$OUT/ref_f1_harness.o"
 g++ -shared -Wl,--no-undefined -o "$OUT/libtgmm_ref_f1.so" "$OUT/f1_supervoxel.o" "$OUT/f1_lgd.o" "$OUT/f1_hs.o" \
   "$OUT/constants.o" "$OUT/ref_f1_harness.o"
+# the split proposal of the Gaussian class (host C++ with the vendored Eigen; runs without a GPU)
+g++ -std=gnu++11 $CXXF -c "$REF/GaussianMixtureModel.cpp" -o "$OUT/gmm_class.o"
+g++ -std=gnu++11 $CXXF -c "$REF/external/xmlParser2/xmlParser.cpp" -o "$OUT/gmm_xml.o"
+g++ -std=gnu++11 $CXXF -c "$HERE/ref_split_harness.cpp" -o "$OUT/ref_split_harness.o"
+g++ -shared -Wl,--no-undefined -o "$OUT/libtgmm_ref_gmm.so" "$OUT/gmm_class.o" "$OUT/gmm_xml.o" "$OUT/constants.o" \
+  "$OUT/ref_split_harness.o"
 rm -f "$OUT"/*.o
-echo "built $OUT/libtgmm_ref.so $OUT/libtgmm_ref_f3.so $OUT/libtgmm_ref_f1.so"
+echo "built $OUT/libtgmm_ref.so $OUT/libtgmm_ref_f3.so $OUT/libtgmm_ref_f1.so $OUT/libtgmm_ref_gmm.so"

@@ -56,6 +56,10 @@ def lib():
         _lib.or_regularize.argtypes = [vp, C.c_int32, C.POINTER(C.c_float), C.c_int32, C.c_double, C.c_double,
                                        C.c_double]
         _lib.or_update_priors.argtypes = [vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
+        _lib.or_local_likelihood.argtypes = [vp, C.c_int32, vp, vp, C.c_int64, vp, C.c_int32, vp, vp, vp, C.c_int32,
+                                             C.c_int32, vp]
+        _lib.or_local_likelihood.restype = C.c_int
+        _lib.or_split_proposal.argtypes = [vp, C.POINTER(C.c_float), vp, vp]
         _lib.or_set_num_threads.argtypes = [C.c_int]
         _lib.or_num_threads.restype = C.c_int
     return _lib
@@ -96,6 +100,65 @@ def em_run(query, img, cent, lptr, gauss, p: OrParams, threads: int = 0):
     return dict(gauss=g, rnk=rnk, ind=ind, ll_hist=hist[:st.iterations], iterations=st.iterations,
                 converged=st.converged, ll=st.ll, ll_true=st.ll_true, ll_as_reference=st.ll_as_reference,
                 total_alpha=st.total_alpha, n_dead=st.n_dead)
+
+
+def split_proposal(rec, scale=(1.0, 1.0, 2.0)):
+    """The principal-axis split of one 288-byte record (GaussianMixtureModel::splitGaussian
+    and updatePriorsAfterSplitProposal on both halves): (the split Gaussian, the new one)."""
+    g = np.ascontiguousarray(np.asarray(rec).reshape(1)).copy()
+    a, b = g.copy(), g.copy()
+    sc = (C.c_float * 3)(*scale)
+    lib().or_split_proposal(_p(g), sc, _p(a), _p(b))
+    return a[0], b[0]
+
+
+REF_GMM_SO = os.path.join(HERE, "_ref", "libtgmm_ref_gmm.so")
+_ref_gmm = None
+
+
+def ref_gmm_available() -> bool:
+    return os.path.exists(REF_GMM_SO)
+
+
+def ref_split_gaussian(rec, scale=(1.0, 1.0, 2.0)):
+    """The reference's own GaussianMixtureModel::splitGaussian(GM, id) and
+    updatePriorsAfterSplitProposal (host code, compiled from its sources)."""
+    global _ref_gmm
+    if _ref_gmm is None:
+        _ref_gmm = C.CDLL(REF_GMM_SO)
+        _ref_gmm.ref_split_gaussian.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_void_p, C.c_void_p]
+        _ref_gmm.ref_split_gaussian.restype = C.c_int
+    g = np.ascontiguousarray(np.asarray(rec).reshape(1)).copy()
+    a, b = g.copy(), g.copy()
+    sc = (C.c_float * 3)(*scale)
+    if _ref_gmm.ref_split_gaussian(_p(g), sc, _p(a), _p(b)) != 0:
+        raise RuntimeError("reference split failed")
+    return a[0], b[0]
+
+
+def lists_csr(lists):
+    """A list of supervoxel-index lists as CSR arrays (list_ptr int32, list_idx int32)."""
+    ptr = np.zeros(len(lists) + 1, np.int32)
+    ptr[1:] = np.cumsum([len(x) for x in lists])
+    idx = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in lists]) if ptr[-1] else
+                               np.zeros(1, np.int32))
+    return ptr, idx
+
+
+def local_likelihood(query, img, lptr, ind, gauss, lists, mode=MODE_FP64):
+    """The local log-likelihood of each supervoxel list (calculateLocalLikelihood) under the
+    Gaussians `gauss` with each supervoxel's candidates `ind` (slot-major, 5*S)."""
+    g = np.ascontiguousarray(gauss)
+    lp = np.ascontiguousarray(lptr, np.int64)
+    ind = np.ascontiguousarray(ind, np.int32)
+    ptr, idx = lists_csr(lists)
+    out = np.zeros(len(lists), np.float64)
+    rc = lib().or_local_likelihood(_p(g), g.shape[0], _p(np.ascontiguousarray(query, np.float32)),
+                                   _p(np.ascontiguousarray(img, np.float32)), img.shape[0], _p(lp), lp.shape[0] - 1,
+                                   _p(ind), _p(ptr), _p(idx), len(lists), mode, _p(out))
+    if rc != 0:
+        raise ValueError("local_likelihood: supervoxel or candidate index out of range")
+    return out
 
 
 def knn(query, ref_xyz, scale=(1.0, 1.0, 2.0), reference_rule=False):
@@ -144,6 +207,8 @@ def ref_lib():
         _ref.ref_knn.restype = C.c_int
         _ref.ref_write_gmm_xml.argtypes = [C.c_char_p, vp, C.c_int]
         _ref.ref_write_gmm_xml.restype = C.c_int
+        _ref.ref_local_likelihood.argtypes = [vp, vp, vp, C.c_longlong, C.c_int, vp, vp, C.c_int, vp, vp, C.c_int, vp]
+        _ref.ref_local_likelihood.restype = C.c_int
     return _ref
 
 
@@ -178,6 +243,22 @@ def ref_knn(query, ref_xyz, scale=(1.0, 1.0, 2.0)):
     if rc != 0:
         raise RuntimeError(f"reference kNN failed ({rc})")
     return ind
+
+
+def ref_local_likelihood(query, img, lptr, ind, gauss, lists):
+    """The reference's own calculateLocalLikelihood (its GPU kernels) on host arrays."""
+    g = np.ascontiguousarray(gauss).copy()
+    q = np.ascontiguousarray(query, np.float32).copy()
+    im = np.ascontiguousarray(img, np.float32).copy()
+    lp = np.ascontiguousarray(lptr, np.int64).copy()
+    ind = np.ascontiguousarray(ind, np.int32).copy()
+    ptr, idx = lists_csr(lists)
+    out = np.zeros(len(lists), np.float64)
+    rc = ref_lib().ref_local_likelihood(_p(q), _p(im), _p(lp), im.shape[0], lp.shape[0] - 1, _p(ind), _p(g),
+                                        g.shape[0], _p(ptr), _p(idx), len(lists), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"reference local likelihood failed ({rc})")
+    return out
 
 
 def ref_write_gmm_xml(path, gauss):

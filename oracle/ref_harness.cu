@@ -7,6 +7,7 @@
 
 #include <fstream>
 #include <string>
+#include <vector>
 
 #include "GMEMupdateCUDA.h"
 #include "knnCuda.h"
@@ -60,4 +61,33 @@ extern "C" int ref_write_gmm_xml(const char* path, void* gauss, int n) {
   for (int i = 0; i < n; i++) g[i].writeXML(os, i);
   GaussianMixtureModelCUDA::writeXMLfooter(os);
   return os.good() ? 0 : 2;
+}
+
+// The reference's calculateLocalLikelihood: frame arrays, candidates (ind, slot-major 5*S)
+// and Gaussians on the host; the supervoxel lists as CSR (list_ptr[n+1], list_idx); one
+// double per list out.
+extern "C" int ref_local_likelihood(float* query, float* img, long long* lptr, long long N, int S, int* ind,
+                                    void* gauss, int K, int* list_ptr, int* list_idx, int n_lists, double* out) {
+  float *qd = 0, *id = 0;
+  long long* ld = 0;
+  int* indd = 0;
+  cudaMalloc(&qd, sizeof(float) * 3 * N);
+  cudaMalloc(&id, sizeof(float) * N);
+  cudaMalloc(&ld, sizeof(long long) * (S + 1));
+  cudaMalloc(&indd, sizeof(int) * 5 * (size_t)S);
+  cudaMemcpy(qd, query, sizeof(float) * 3 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(id, img, sizeof(float) * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(ld, lptr, sizeof(long long) * (S + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(indd, ind, sizeof(int) * 5 * (size_t)S, cudaMemcpyHostToDevice);
+  std::vector<std::vector<int> > lists(n_lists);
+  for (int i = 0; i < n_lists; i++) lists[i].assign(list_idx + list_ptr[i], list_idx + list_ptr[i + 1]);
+  std::vector<double> ll;
+  calculateLocalLikelihood(ll, lists, qd, id, NULL, indd, (GaussianMixtureModelCUDA*)gauss, ld, N, K, S);
+  for (int i = 0; i < n_lists; i++) out[i] = ll[i];
+  cudaError_t e = cudaDeviceSynchronize();
+  cudaFree(qd);
+  cudaFree(id);
+  cudaFree(ld);
+  cudaFree(indd);
+  return e == cudaSuccess ? 0 : 2;
 }

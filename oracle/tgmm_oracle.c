@@ -725,6 +725,137 @@ static inline double voxel_density(const OrGaussian* const* c, double x0, double
   return acc;
 }
 
+/* Split proposal of one Gaussian record (GaussianMixtureModel::splitGaussian(GM, id),
+ * GaussianMixtureModel.cpp:514-557, then updatePriorsAfterSplitProposal :912-922 on both halves),
+ * with N_k = nu_k - nu_o as copyFromGMEM_CUDA derives it (variationalInference.cpp:1008):
+ * S = nu W / (s_i s_j) (float products of the scale); lmin, v = its smallest eigenvalue and
+ * eigenvector, lmax its largest; sigma = 1/sqrt(max(lmin, 1e-3)); both halves get
+ * W = (lmax / nu) I with W_ii *= s_i s_i and N_k / 2; a = m + sigma v, b = a - 2 sigma v; then
+ * m_o = m_k, beta_o = max(N_k/2, 1e-5), nu_o = max(N_k/2, 3), W_o = W_k nu_k / nu_o.  The sign of
+ * v is fixed by making its largest-magnitude component positive (the reference takes Eigen's
+ * solver's sign, so a and b may trade places against it). */
+void or_split_proposal(const OrGaussian* g, const float scale[3], OrGaussian* a, OrGaussian* b) {
+  static const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  double w[6], d[3], v[9];
+  for (int e = 0; e < 6; e++)
+    w[e] = (g->W_k[e] * g->nu_k) / (double)(scale[ij[e][0]] * scale[ij[e][1]]);
+  or_eig3(w, d, v);
+  int imin = 0, imax = 0;
+  for (int i = 1; i < 3; i++) {
+    if (d[i] < d[imin]) imin = i;
+    if (d[i] > d[imax]) imax = i;
+  }
+  double u[3] = {v[3 * imin], v[3 * imin + 1], v[3 * imin + 2]};
+  int big = 0;
+  for (int i = 1; i < 3; i++)
+    if (fabs(u[i]) > fabs(u[big])) big = i;
+  if (u[big] < 0)
+    for (int i = 0; i < 3; i++) u[i] = -u[i];
+  double smax = d[imin];
+  if (smax < 1e-3) smax = 1e-3;
+  const double sm2 = 1.0 / sqrt(smax);
+  const double smin = d[imax];
+  const double nk = 0.5 * (g->nu_k - g->nu_o);
+  *a = *g;
+  for (int e = 0; e < 6; e++) a->W_k[e] = 0.0;
+  a->W_k[0] = smin / g->nu_k * (double)(scale[0] * scale[0]);
+  a->W_k[3] = smin / g->nu_k * (double)(scale[1] * scale[1]);
+  a->W_k[5] = smin / g->nu_k * (double)(scale[2] * scale[2]);
+  for (int i = 0; i < 3; i++) a->m_k[i] = g->m_k[i] + sm2 * u[i];
+  *b = *a;
+  for (int i = 0; i < 3; i++) b->m_k[i] = a->m_k[i] - 2.0 * sm2 * u[i];
+  OrGaussian* h[2] = {a, b};
+  for (int q = 0; q < 2; q++) {
+    OrGaussian* x = h[q];
+    for (int i = 0; i < 3; i++) x->m_o[i] = x->m_k[i];
+    x->beta_o = 0.5 * nk > 1e-5 ? 0.5 * nk : 1e-5;
+    x->nu_o = 0.5 * nk > 3.0 ? 0.5 * nk : 3.0;
+    for (int e = 0; e < 6; e++) x->W_o[e] = x->W_k[e] * x->nu_k / x->nu_o;
+  }
+}
+
+/* Local log-likelihood of supervoxel lists (calculateLocalLikelihood, GMEMupdateCUDA.cu:2952-3055,
+ * over addLocalLikelihoodWithSupervoxels :2876-2949 and GMEMcomputeLocalLikelihoodKernelWithSupervoxels
+ * :1989-2103).  total alpha = sum of alpha_k over all K records (calculateTotalAlpha).  For list i and
+ * each supervoxel s in it (duplicates count again), its five candidates ind[j*S+s]: thread t of 1024
+ * keeps I*ln(density) of the last voxel of its stride with a positive density (the cache overwrite,
+ * :2083-2084); the supervoxel's value is the sum of the 1024 slots.  FP64 mode sums in FP64 in list
+ * order; REF32 mode reproduces the float cache, the per-block tree, the power-of-two sumVector pass
+ * over the list's values and the host double sum (:2899-2944).  An empty list gives 0 (the reference
+ * skips it and leaves the zero of its resize, :3037).  Returns -1 on an index out of range. */
+int or_local_likelihood(const OrGaussian* g, int32_t K, const float* query, const float* img, int64_t N,
+                        const int64_t* lptr, int32_t S, const int32_t* ind, const int32_t* list_ptr,
+                        const int32_t* list_idx, int32_t n_lists, int32_t mode, double* out) {
+  const double total_alpha = or_total_alpha(g, K, mode);
+  int bad = 0;
+  for (int32_t i = 0; i < n_lists; i++)
+    for (int32_t p = list_ptr[i]; p < list_ptr[i + 1]; p++) {
+      if (list_idx[p] < 0 || list_idx[p] >= S) bad = 1;
+      else
+        for (int j = 0; j < OR_J; j++) {
+          const int32_t k = ind[(int64_t)j * S + list_idx[p]];
+          if (k < 0 || k >= K) bad = 1;
+        }
+    }
+  if (bad) return -1;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int32_t i = 0; i < n_lists; i++) {
+    const int32_t n = list_ptr[i + 1] - list_ptr[i];
+    if (n == 0) {
+      out[i] = 0.0;
+      continue;
+    }
+    double sum64 = 0.0;
+    int size = 1;
+    while (size < n) size <<= 1;
+    float* vec32 = (float*)calloc(size, sizeof(float));
+    for (int32_t q = 0; q < n; q++) {
+      const int32_t s = list_idx[list_ptr[i] + q];
+      const OrGaussian* c[OR_J];
+      for (int j = 0; j < OR_J; j++) c[j] = &g[ind[(int64_t)j * S + s]];
+      double cache64[OR_BLK];
+      float cache[OR_BLK];
+      for (int t = 0; t < OR_BLK; t++) {
+        cache64[t] = 0.0;
+        cache[t] = 0.0f;
+      }
+      for (int64_t v = lptr[s]; v < lptr[s + 1]; v++) {
+        const double dens = voxel_density(c, query[v], query[N + v], query[2 * N + v], total_alpha);
+        if (dens > 0.0) {
+          const double term = (double)img[v] * log(dens);
+          const int t = (int)((v - lptr[s]) % OR_BLK);
+          cache64[t] = term;
+          cache[t] = (float)term;
+        }
+      }
+      double r64 = 0.0;
+      for (int t = 0; t < OR_BLK; t++) r64 += cache64[t];
+      sum64 += r64;
+      for (int h = OR_BLK / 2; h > 0; h /= 2)
+        for (int t = 0; t < h; t++) cache[t] += cache[t + h];
+      vec32[q] = cache[0];
+    }
+    if (mode == OR_MODE_FP64) {
+      out[i] = sum64;
+    } else {
+      const int threads = size < OR_BLK ? size : OR_BLK;
+      const int grids = (size + threads - 1) / threads;
+      double ll = 0.0;
+      float* cache = (float*)malloc(sizeof(float) * threads);
+      for (int b = 0; b < grids; b++) {
+        for (int t = 0; t < threads; t++) cache[t] = vec32[(int64_t)b * threads + t];
+        for (int h = threads / 2; h > 0; h /= 2)
+          for (int t = 0; t < h; t++) cache[t] += cache[t + h];
+        ll = (b == 0) ? (double)cache[0] : ll + (double)cache[0];
+      }
+      free(cache);
+      out[i] = ll;
+    }
+    free(vec32);
+  }
+  return 0;
+}
+
 /* Log-likelihood (GMEMcomputeLikelihoodKernelWithSupervoxels, GMEMupdateCUDA.cu:1913-1978,
  * addTotalLikelihoodWithSupervoxels :2834-2873).
  * ll_true  = sum over every voxel of I*ln(density), densities <= 0 skipped;

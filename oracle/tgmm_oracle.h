@@ -98,6 +98,10 @@ void or_kill(OrGaussian* g, int32_t K, double* Nk, double total_alpha);
 void or_loglik(const OrGaussian* g, const float* query, const float* img, int64_t N,
                const int64_t* lptr, int32_t S, const int32_t* ind, double total_alpha,
                int32_t mode, double* ll_true, double* ll_as_ref);
+void or_split_proposal(const OrGaussian* g, const float scale[3], OrGaussian* a, OrGaussian* b);
+int or_local_likelihood(const OrGaussian* g, int32_t K, const float* query, const float* img, int64_t N,
+                        const int64_t* lptr, int32_t S, const int32_t* ind, const int32_t* list_ptr,
+                        const int32_t* list_idx, int32_t n_lists, int32_t mode, double* out);
 void or_update_priors(OrGaussian* g, int32_t K, double beta_pct, double nu_pct,
                       double alpha_pct, double alpha_total);
 void or_assign_supervoxels(const float* rnk, const int32_t* ind, int32_t S, OrGaussian* g,

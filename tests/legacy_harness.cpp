@@ -1,7 +1,7 @@
 // legacy_harness.cpp -- a minimal program written against the reference's C++ interface
 // (the calls of mainTrackingGaussianMixtureModel.cpp:1065-1107), linked against
 // libtgmm_gmem.so.  Usage: legacy_harness <dir> <maxIterEM> <tol>
-// Reads <dir>/{query,img,cent,lptr,gauss}.bin, writes <dir>/{gauss_out,rnk,ind}.bin.
+// Reads <dir>/{query,img,cent,lptr,gauss}.bin, writes <dir>/{gauss_out,rnk,ind,local}.bin.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -59,9 +59,16 @@ int main(int argc, char** argv) {
   std::vector<int> ind(5 * (size_t)S);
   cudaMemcpy(rnk.data(), rnkCUDA, rnk.size() * 4, cudaMemcpyDeviceToHost);
   cudaMemcpy(ind.data(), indCUDA, ind.size() * 4, cudaMemcpyDeviceToHost);
+  // the split round's local likelihood around every Gaussian (main:1303-1331): its
+  // supervoxels after the EM, under the EM's mixture and candidates
+  std::vector<std::vector<int> > lists(K);
+  for (int k = 0; k < K; k++) lists[k].assign(g[k].supervoxelIdx, g[k].supervoxelIdx + g[k].supervoxelNum);
+  std::vector<double> local;
+  calculateLocalLikelihood(local, lists, queryCUDA, imgCUDA, rnkCUDA, indCUDA, g, lptrCUDA, N, K, S);
   GMEMreleaseMemoryWithSupervoxels(&queryCUDA, &imgCUDA, &rnkCUDA, &indCUDA, &indTrCUDA, &centCUDA, &lptrCUDA);
   spill(dir + "/gauss_out.bin", gm.data(), gm.size());
   spill(dir + "/rnk.bin", rnk.data(), rnk.size() * 4);
   spill(dir + "/ind.bin", ind.data(), ind.size() * 4);
+  spill(dir + "/local.bin", local.data(), local.size() * 8);
   return 0;
 }

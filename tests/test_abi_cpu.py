@@ -27,6 +27,7 @@ LEGACY_SYMBOLS = [
     "_Z43GMEMvariationalInferenceCUDAWithSupervoxelsPfS_S_S_PiS0_S_PxP24GaussianMixtureModelCUDAxitidiibNSt7__cxx11"
     "12basic_stringIcSt11char_traitsIcESaIcEEE",
     "_ZN24GaussianMixtureModelCUDA8writeXMLERSoi",
+    "_Z24calculateLocalLikelihoodRSt6vectorIdSaIdEERKS_IS_IiSaIiEESaIS4_EEPfS9_S9_PiP24GaussianMixtureModelCUDAPxxii",
     "_ZN34regularizePrecisionMatrixConstants9lambdaMinE",
     "_ZN34regularizePrecisionMatrixConstants9lambdaMaxE",
     "_ZN34regularizePrecisionMatrixConstants15maxExcentricityE",

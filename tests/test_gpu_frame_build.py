@@ -153,7 +153,7 @@ def test_em_on_the_built_frame_is_the_em_on_the_oracles_arrays(cuda_ok):
     # equal inputs give equal bytes: every field of every Gaussian record, the rows that
     # differ named in the message
     for name in a["gauss"].dtype.names:
-        x, y = a["gauss"][name], b["gauss"][name]
+        x, y = np.ascontiguousarray(a["gauss"][name]), np.ascontiguousarray(b["gauss"][name])
         rows = np.flatnonzero((x.view(np.uint8).reshape(x.shape[0], -1) !=
                                y.view(np.uint8).reshape(y.shape[0], -1)).any(axis=1))
         assert rows.size == 0, (name, rows[:10].tolist(), x[rows[:3]], y[rows[:3]])

@@ -46,3 +46,11 @@ def test_legacy_entry_points_match_the_c_abi(cuda_ok, tmp_path, name):
     np.testing.assert_array_equal(rnk, want["rnk"])
     for k in L.GAUSS_DTYPE.names:
         np.testing.assert_array_equal(g[k], want["gauss"][k], err_msg=k)
+    # calculateLocalLikelihood around every Gaussian equals tgmm_local_likelihood bit for bit
+    local = np.fromfile(d / "local.bin", dtype=np.float64)
+    lists = [list(x["supervoxelIdx"][:x["supervoxelNum"]]) for x in g]
+    import torch
+    got = E.local_likelihood(df, torch.from_numpy(ind).cuda(), E.gauss_to_device(g), lists)
+    empty = np.array([len(x) == 0 for x in lists])
+    np.testing.assert_array_equal(local[~empty], got[~empty])
+    assert np.all(local[empty] == 0.0)

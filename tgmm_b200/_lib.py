@@ -169,6 +169,7 @@ GMEM_FUNCS = {
                                     C.POINTER(_VP), C.POINTER(TgmmEmParams), C.POINTER(TgmmEmStats), _VP]),
     "tgmm_knn": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.POINTER(C.c_float), _VP, _VP]),
     "tgmm_knn_noalloc": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.POINTER(C.c_float), _VP, _VP]),
+    "tgmm_local_likelihood": (C.c_int, [C.POINTER(TgmmFrame), _VP, _VP, C.c_int32, _VP, _VP, C.c_int32, _VP, _VP]),
     "tgmm_update_priors": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
                                      _VP]),
     "tgmm_frame_upload": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int64, C.c_int32, C.POINTER(TgmmFrame)]),

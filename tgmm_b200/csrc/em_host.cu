@@ -39,7 +39,7 @@ int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
   // byte offsets of every device array inside one allocation
-  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_order, ord_hist, ord_cur, sv_rec, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
+  int64_t info, frames, state, gchunks, g_frame, gd, fixed, cell_refs, cell_cnt, bcnt, bucket, acnt, abucket, ape, apf, dead, ec, llc, kpos, work, sv_frame, sv_order, ord_hist, ord_cur, sv_rec, sv_ll, vox4, mom, cand, rnk, nbr, nbr_b, llp, gm_scratch, total;
 };
 
 Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells) {
@@ -76,6 +76,8 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.ord_hist = take(4 * 64 * (int64_t)d.max_frames);
   L.ord_cur = take(4 * 64 * (int64_t)d.max_frames);
   L.sv_rec = take((int64_t)sizeof(SvRec) * S);
+  L.sv_ll = take((int64_t)sizeof(SvLL) * S);
+  L.vox4 = take(16 * d.max_vox);
   L.mom = take(8 * S * kNumMoments);
   L.cand = take(2 * 4 * S * kJ);
   L.rnk = take(2 * 4 * S * kJ);
@@ -206,6 +208,8 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.ord_hist = (int32_t*)(b + P->L.ord_hist);
   D.ord_cur = (int32_t*)(b + P->L.ord_cur);
   D.sv_rec = (SvRec*)(b + P->L.sv_rec);
+  D.sv_ll = (SvLL*)(b + P->L.sv_ll);
+  D.vox4 = (float4*)(b + P->L.vox4);
   D.mom = (double*)(b + P->L.mom);
   D.cand = (int32_t*)(b + P->L.cand);
   D.rnk = (float*)(b + P->L.rnk);
@@ -270,10 +274,13 @@ int stage_batch(TgmmPlan* P, int32_t n, const TgmmFrame* fr, TgmmGaussian* const
   if (tv > P->desc.max_vox || ts > P->desc.max_sv || tg > P->desc.max_gauss)
     return fail(TGMM_ERR_BAD_SIZE, "batch exceeds plan capacity");
   ts = tg = 0;
+  int64_t vb = 0;
   for (int32_t f = 0; f < n; f++) {
     const TgmmFrame& F = fr[f];
     FrameDesc& D = P->s_frames[f];
     memset(&D, 0, sizeof(D));
+    D.vox_base = vb;
+    vb += F.n_vox;
     D.query = F.query;
     D.img = F.img;
     D.cent = F.centroids;

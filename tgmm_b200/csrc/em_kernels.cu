@@ -279,6 +279,18 @@ __device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s,
   r.c2 = D.cent[2 * (int64_t)D.n_sv + sl];
   r.r0 = r0;
   P.sv_rec[s] = r;
+  SvLL l;
+  l.v0 = D.vox_base + (nt ? a : 0);
+  l.nv = nv;
+  l.ntiles = nt;
+  l.r0 = r0;
+  l.frame = f;
+  l.frame_nsv = D.n_sv;
+  l.c0 = r.c0;
+  l.c1 = r.c1;
+  l.c2 = r.c2;
+  l.pad[0] = l.pad[1] = 0;
+  P.sv_ll[s] = l;
 }
 
 // ===========================================================================
@@ -1401,8 +1413,27 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Waits for the phase with the given parity; false after limit_ns without it.
+__device__ __forceinline__ bool mbar_test_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for the phase with the given parity; false after limit_ns without it.  try_wait
+// suspends the thread for a while until the phase completes, so at the default limit the
+// clock is read only between its returns; a limit below 1 ms polls with the non-blocking
+// test_wait, so that the limit is kept to the clock's resolution.
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+  if (limit_ns < 1000000ull) {
+    if (mbar_test_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_test_wait(bar, parity))
+      if (global_ns() - t0 > limit_ns) return false;
+    return true;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity))
@@ -1449,7 +1480,8 @@ __device__ __forceinline__ void ll_issue(const SvRec& R, int t, float* slot, uns
 // candidate ids (stage A, two supervoxels ahead) and its candidates' constants (10
 // doubles each) with its frame's ln(sum alpha) and done flag (stage B, one ahead).
 struct LLRec {
-  SvRec rec;
+  SvRec rec;  // the moment pass and the FP64 pass: the SoA spans of the input arrays
+  SvLL ll;    // the moment pass and the FP32 pass: the place in the centred voxel stream
   int32_t cand[8];
 };
 struct LLConst {
@@ -1471,27 +1503,44 @@ static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOf
               "slots and records stay 16-byte aligned");
 static_assert(kLLBlocks * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "the voxel pass's blocks fit an SM");
 
-// Stage A: the record and candidate ids of supervoxel s.
-template <bool kCand>
+// Stage A: the records (SoA spans: kRec; centred-stream place: kLL) and candidate ids
+// (kCand) of supervoxel s, one lane per 16-byte chunk or id.
+template <bool kRec, bool kLL, bool kCand>
 __device__ __forceinline__ void ll_fetch_a(const DevPlan& P, LLRec& X, int s) {
   const int lane = threadIdx.x & 31;
-  constexpr int kRecChunks = (int)sizeof(SvRec) / 16;
-  if (lane < kRecChunks)
+  constexpr int kRecChunks = kRec ? (int)sizeof(SvRec) / 16 : 0;
+  constexpr int kLLChunks = kLL ? (int)sizeof(SvLL) / 16 : 0;
+  static_assert(kRecChunks + kLLChunks + kJ <= 32, "one lane per chunk");
+  if (lane < kRecChunks) {
     cp_async16(reinterpret_cast<char*>(&X.rec) + 16 * lane, reinterpret_cast<const char*>(P.sv_rec + s) + 16 * lane);
-  else if (kCand && lane < kRecChunks + kJ)
-    cp_async4(&X.cand[lane - kRecChunks], cand_buf(P, P.iter) + (int64_t)s * kJ + (lane - kRecChunks));
+  } else if (lane < kRecChunks + kLLChunks) {
+    const int c = lane - kRecChunks;
+    cp_async16(reinterpret_cast<char*>(&X.ll) + 16 * c, reinterpret_cast<const char*>(P.sv_ll + s) + 16 * c);
+  } else if (kCand && lane < kRecChunks + kLLChunks + kJ) {
+    const int j = lane - kRecChunks - kLLChunks;
+    cp_async4(&X.cand[j], cand_buf(P, P.iter) + (int64_t)s * kJ + j);
+  }
 }
 // Stage B (after A landed): the candidates' constants and the frame scalars.
-__device__ __forceinline__ void ll_fetch_b(const DevPlan& P, const LLRec& A, LLConst& X) {
+__device__ __forceinline__ void ll_fetch_b(const DevPlan& P, const LLRec& A, int frame, LLConst& X) {
   const int lane = threadIdx.x & 31;
   if (lane < 5 * kJ) {
     const int j = lane / 5, c = lane % 5;
     cp_async16(&X.llc[j][2 * c], P.llc + (int64_t)A.cand[j] * 10 + 2 * c);
   } else if (lane == 5 * kJ) {
-    cp_async8(&X.ln_alpha, &P.state[A.rec.frame].ln_alpha);
+    cp_async8(&X.ln_alpha, &P.state[frame].ln_alpha);
   } else if (lane == 5 * kJ + 1) {
-    cp_async4(&X.done, &P.state[A.rec.frame].done);
+    cp_async4(&X.done, &P.state[frame].done);
   }
+}
+
+// Tile t of a supervoxel from the centred voxel stream: one bulk copy of its float4 voxels
+// (16 bytes each, so every tile starts and ends on a 16-byte boundary).
+__device__ __forceinline__ void ll_issue4(const float4* vox4, const SvLL& R, int t, float* slot, unsigned bar) {
+  const int off = t == 0 ? 0 : R.r0 + kLLTile * (t - 1);
+  const unsigned bytes = 16u * (unsigned)(t == 0 ? R.r0 : kLLTile);
+  mbar_expect_tx(bar, bytes);
+  bulk_g2s(smem_addr(slot), (unsigned long long)(vox4 + R.v0 + off), bytes, bar);
 }
 
 // Evaluation of one voxel in the three modes: 0 FP32 4-DOF, 1 FP32 general, 2 FP64.
@@ -1502,6 +1551,8 @@ struct VoxelEval {
   __device__ __forceinline__ float operator()(float x, float y, float z, float c0, float c1, float c2) const {
     return voxel_ll_f32<kMode == 0>(C, x - c0, y - c1, z - c2);
   }
+  // from e = x - c as the moment pass stored it (the same FP32 value as x - c0 above)
+  __device__ __forceinline__ float e(float e0, float e1, float e2) const { return voxel_ll_f32<kMode == 0>(C, e0, e1, e2); }
   __device__ __forceinline__ static bool ok(float l) { return l > -745.13f; }  // exp(l) is a positive double
 };
 template <>
@@ -1536,6 +1587,24 @@ __device__ __forceinline__ void ll_tile(const Eval& eval, const float* __restric
     const bool in = kFull || u * 32 + lane < rem;
     allok = allok && (ok || !in);
     tsum += (in && ok) ? (T)bi[32 * u] * l : (T)0;
+  }
+}
+
+// The same tile from the centred voxel stream: lane voxels o = u*32 + lane, each one float4
+// (e0, e1, e2, I) read with one shared-memory load.
+template <class Eval, bool kFull>
+__device__ __forceinline__ void ll_tile4(const Eval& eval, const float4* __restrict__ slot, int rem, float& tsum,
+                                         bool& allok) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int u = 0; u < kLLTile / 32; u++) {
+    if (!kFull && u * 32 >= rem) break;
+    const float4 v = slot[32 * u + lane];
+    const float l = eval.e(v.x, v.y, v.z);
+    const bool ok = Eval::ok(l);
+    const bool in = kFull || u * 32 + lane < rem;
+    allok = allok && (ok || !in);
+    tsum += (in && ok) ? v.w * l : 0.0f;
   }
 }
 
@@ -1579,12 +1648,42 @@ __device__ __forceinline__ double ll_fixup(const Eval& eval, const SvRec& R, uns
   return add;
 }
 
+// The centred-stream forms of ll_walk_back and ll_fixup: v = the supervoxel's voxels in vox4.
+template <class Eval>
+__device__ __forceinline__ double ll_walk_back4(const Eval& eval, const float4* v, int i) {
+  for (int i2 = i - 1024; i2 >= 0; i2 -= 1024) {
+    const float4 x = v[i2];
+    const float l2 = eval.e(x.x, x.y, x.z);
+    if (Eval::ok(l2)) return (double)x.w * (double)l2;
+  }
+  return 0.0;
+}
+
+template <class Eval>
+__device__ __forceinline__ double ll_fixup4(const Eval& eval, const float4* v, int nt, int r0, unsigned mask) {
+  const int lane = threadIdx.x & 31;
+  double add = 0.0;
+  for (int k = 0; k < kKeptTiles; k++) {
+    if (!(mask & (1u << k))) continue;
+    const int t = nt - kKeptTiles + k;
+    const int start = t == 0 ? 0 : r0 + (t - 1) * kLLTile;
+    const int rem = t == 0 ? r0 : kLLTile;
+    for (int o = lane; o < rem; o += 32) {
+      const int i = start + o;
+      const float4 x = v[i];
+      if (!Eval::ok(eval.e(x.x, x.y, x.z))) add += ll_walk_back4(eval, v, i);
+    }
+  }
+  return add;
+}
+
 // The moment pass's tile t (landed in `slot`): the 19 sums e, ee', I, Ie, Iee' (e = x - c in
-// FP32, FP64 accumulation) of the lane's voxels o = u*32 + lane; nan_seen turns true on a
-// NaN coordinate or intensity.
+// FP32, FP64 accumulation) of the lane's voxels o = u*32 + lane, each voxel also written to
+// the centred voxel stream (out: the tile's first voxel there) as (e0, e1, e2, I); nan_seen
+// turns true on a NaN coordinate or intensity.
 template <bool kFull>
 __device__ __forceinline__ void mom_tile(const float* __restrict__ slot, const int* sht, int rem, float c0, float c1,
-                                         float c2, double* m, bool& nan_seen) {
+                                         float c2, double* m, bool& nan_seen, float4* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const float* bx = slot + sht[0] + lane;
   const float* by = slot + kLLSpan + sht[1] + lane;
@@ -1596,7 +1695,9 @@ __device__ __forceinline__ void mom_tile(const float* __restrict__ slot, const i
     if (!kFull && u * 32 + lane >= rem) continue;
     const float x = bx[32 * u], y = by[32 * u], z = bz[32 * u], I = bi[32 * u];
     nan_seen |= isnan(x) || isnan(y) || isnan(z) || isnan(I);
-    const double e0 = (double)(x - c0), e1 = (double)(y - c1), e2 = (double)(z - c2);
+    const float e0f = x - c0, e1f = y - c1, e2f = z - c2;
+    out[32 * u + lane] = make_float4(e0f, e1f, e2f, I);
+    const double e0 = (double)e0f, e1 = (double)e1f, e2 = (double)e2f;
     const double wI = (double)I;
     m[M_E0] += e0;
     m[M_E1] += e1;
@@ -1622,14 +1723,15 @@ __device__ __forceinline__ void mom_tile(const float* __restrict__ slot, const i
 }
 
 __device__ __forceinline__ void mom_consume(const float* slot, const int* pk, int t, int r0, float c0, float c1,
-                                            float c2, double* m, bool& nan_seen) {
+                                            float c2, double* m, bool& nan_seen, float4* sv_out) {
   const int sft = t == 0 ? 0 : 4;
   const int sht[4] = {(pk[0] >> sft) & 3, (pk[1] >> sft) & 3, (pk[2] >> sft) & 3, (pk[3] >> sft) & 3};
   const int rem = t == 0 ? r0 : kLLTile;
+  float4* out = sv_out + (t == 0 ? 0 : r0 + kLLTile * (t - 1));
   if (rem == kLLTile)
-    mom_tile<true>(slot, sht, rem, c0, c1, c2, m, nan_seen);
+    mom_tile<true>(slot, sht, rem, c0, c1, c2, m, nan_seen, out);
   else
-    mom_tile<false>(slot, sht, rem, c0, c1, c2, m, nan_seen);
+    mom_tile<false>(slot, sht, rem, c0, c1, c2, m, nan_seen, out);
 }
 
 // Tile t (landed in `slot`) of the current supervoxel: its sum goes to lt, and to lr when
@@ -1649,6 +1751,25 @@ __device__ __forceinline__ void ll_consume(const Eval& eval, const float* slot, 
     ll_tile<Eval, true>(eval, slot, sht, rem, c0, c1, c2, tsum, allok);
   else
     ll_tile<Eval, false>(eval, slot, sht, rem, c0, c1, c2, tsum, allok);
+  lt += (double)tsum;
+  if (t >= nt - kKeptTiles) {
+    lr += (double)tsum;
+    if (nv > 1024 && __any_sync(0xffffffffu, !allok)) fix |= 1u << (t - (nt - kKeptTiles));
+  }
+}
+
+// The centred-stream form of ll_consume (FP32 terms).
+template <class Eval>
+__device__ __forceinline__ void ll_consume4(const Eval& eval, const float* slot, int t, int nt, int nv, int r0,
+                                            double& lt, double& lr, unsigned& fix) {
+  const float4* s4 = reinterpret_cast<const float4*>(slot);
+  const int rem = t == 0 ? r0 : kLLTile;
+  float tsum = 0.0f;
+  bool allok = true;
+  if (rem == kLLTile)
+    ll_tile4<Eval, true>(eval, s4, rem, tsum, allok);
+  else
+    ll_tile4<Eval, false>(eval, s4, rem, tsum, allok);
   lt += (double)tsum;
   if (t >= nt - kKeptTiles) {
     lr += (double)tsum;
@@ -1711,6 +1832,11 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // reads them.
 template <bool kFp64, int G, bool kMom>
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
+  // the FP32 log-likelihood streams the centred voxel stream (one float4 per voxel, one bulk
+  // copy per tile); the moment pass reads the input arrays (and writes that stream), the FP64
+  // log-likelihood reads the input arrays too (its terms start from the exact x - c)
+  constexpr bool kAos = !kFp64 && !kMom;
+  constexpr bool kRec = !kAos, kLLr = kAos || kMom, kCand = !kMom;
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ LLShared64 sh64[kFp64 ? kWarpsPerBlockV : 1];
@@ -1765,13 +1891,14 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
   if (lane == 0 && sc < total) tk = take();
   int sn = sc < total ? __shfl_sync(0xffffffffu, tk, 0) : total;
   if (lane == 0 && sn < total) tk = take();
+  auto frame_of = [](const LLRec& A) { return kAos ? A.ll.frame : A.rec.frame; };
   if (sc < total) {
-    ll_fetch_a<!kMom>(P, RA[0], sc);
-    if (sn < total) ll_fetch_a<!kMom>(P, RA[1], sn);
+    ll_fetch_a<kRec, kLLr, kCand>(P, RA[0], sc);
+    if (sn < total) ll_fetch_a<kRec, kLLr, kCand>(P, RA[1], sn);
     cp_commit();
     cp_wait_all();
     __syncwarp();
-    if (!kMom) ll_fetch_b(P, RA[0], RB[0]);
+    if (!kMom) ll_fetch_b(P, RA[0], frame_of(RA[0]), RB[0]);
     cp_commit();
   }
   // the next iteration's kNN/E-step items
@@ -1802,19 +1929,22 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
     const LLRec& NA = RA[(i + 1) % 3];
     const int s2 = __shfl_sync(0xffffffffu, tk, 0);
     if (lane == 0 && s2 < total) tk = take();
-    if (!kMom && sn < total) ll_fetch_b(P, NA, RB[(i + 1) & 1]);
-    if (s2 < total) ll_fetch_a<!kMom>(P, RA[(i + 2) % 3], s2);
+    if (!kMom && sn < total) ll_fetch_b(P, NA, frame_of(NA), RB[(i + 1) & 1]);
+    if (s2 < total) ll_fetch_a<kRec, kLLr, kCand>(P, RA[(i + 2) % 3], s2);
     cp_commit();
     if (knn_more) knn_step();  // while this supervoxel's tiles and records land
     int in = 0;
-    const int n_nt = sn < total ? NA.rec.ntiles : 0;  // the next one's tiles may start early
-    const int nv = CA.rec.nv, nt = CA.rec.ntiles, f = CA.rec.frame, nsv = CA.rec.frame_nsv;
-    const float c0 = CA.rec.c0, c1 = CA.rec.c1, c2 = CA.rec.c2;
+    const int n_nt = sn < total ? (kAos ? NA.ll.ntiles : NA.rec.ntiles) : 0;  // the next one's tiles may start early
+    const int nv = kAos ? CA.ll.nv : CA.rec.nv, nt = kAos ? CA.ll.ntiles : CA.rec.ntiles;
+    const int f = frame_of(CA), nsv = kAos ? CA.ll.frame_nsv : CA.rec.frame_nsv;
+    const float c0 = kAos ? CA.ll.c0 : CA.rec.c0, c1 = kAos ? CA.ll.c1 : CA.rec.c1, c2 = kAos ? CA.ll.c2 : CA.rec.c2;
     S = &P.state[f];
-    int pk[4];  // slot offsets of the components: tile 0 in bits 0-1, later tiles in bits 4-5
+    int pk[4] = {0, 0, 0, 0};  // SoA slot offsets of the components: tile 0 in bits 0-1, later tiles in bits 4-5
+    if constexpr (kRec) {
 #pragma unroll
-    for (int c = 0; c < 4; c++) pk[c] = (int)(CA.rec.nf[c] >> 16);
-    const int r0 = CA.rec.r0;
+      for (int c = 0; c < 4; c++) pk[c] = (int)(CA.rec.nf[c] >> 16);
+    }
+    const int r0 = kAos ? CA.ll.r0 : CA.rec.r0;
     // the next staged tile of the supervoxel (of ntr): the ring is refilled first, with the
     // current supervoxel's tiles and then the next one's; nullptr if the tile never arrived
     auto ring_next = [&](int ntr) -> const float* {
@@ -1825,7 +1955,10 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
         const int tt = mine ? ic++ : in++;
         if (lane == 0) {
           const unsigned q = gi % kLLStages;
-          ll_issue(mine ? CA.rec : NA.rec, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
+          if constexpr (kAos)
+            ll_issue4(P.vox4, mine ? CA.ll : NA.ll, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
+          else
+            ll_issue(mine ? CA.rec : NA.rec, tt, wbuf + q * kLLSlotFloats, bar0 + 8 * q);
         }
         gi++;
       }
@@ -1845,7 +1978,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
           failed = true;
           break;
         }
-        mom_consume(slot, pk, t, r0, c0, c1, c2, m, nan_seen);
+        mom_consume(slot, pk, t, r0, c0, c1, c2, m, nan_seen, P.vox4 + CA.ll.v0);
         gc++;
       }
       if (failed) break;
@@ -1905,23 +2038,26 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
         break;
       }
       if (compute) {
-        if (kFp64)
+        if constexpr (kFp64)
           ll_consume(VoxelEval<2>{sh64[warp]}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
         else if (w4m == 0xffffffffu)
-          ll_consume(VoxelEval<0>{cf}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+          ll_consume4(VoxelEval<0>{cf}, slot, t, nt, nv, r0, lt, lr, fix);
         else
-          ll_consume(VoxelEval<1>{cf}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+          ll_consume4(VoxelEval<1>{cf}, slot, t, nt, nv, r0, lt, lr, fix);
       }
       gc++;
     }
     if (failed) break;
     if (fix) {
-      if (kFp64)
+      if constexpr (kFp64) {
         lr += ll_fixup(VoxelEval<2>{sh64[warp]}, CA.rec, fix, c0, c1, c2);
-      else if (w4m == 0xffffffffu)
-        lr += ll_fixup(VoxelEval<0>{cf}, CA.rec, fix, c0, c1, c2);
-      else
-        lr += ll_fixup(VoxelEval<1>{cf}, CA.rec, fix, c0, c1, c2);
+      } else {
+        const float4* v = P.vox4 + CA.ll.v0;
+        if (w4m == 0xffffffffu)
+          lr += ll_fixup4(VoxelEval<0>{cf}, v, nt, r0, fix);
+        else
+          lr += ll_fixup4(VoxelEval<1>{cf}, v, nt, r0, fix);
+      }
     }
     if (run) {
       lt = warp_sum(lt);

@@ -202,6 +202,43 @@ void GMEMvariationalInferenceCUDAWithSupervoxels(float* queryCUDA, float* imgDat
   cudaEventDestroy(t1);
 }
 
+void calculateLocalLikelihood(std::vector<double>& localLikelihood, const std::vector<std::vector<int> >& lists,
+                              float* queryCUDA, float* imgDataCUDA, float* rnkCUDA, int* indCUDA,
+                              GaussianMixtureModelCUDA* vecGMtemp, long long int* labelListPtrCUDA,
+                              long long int query_nb, int ref_nb, int numLabels) {
+  (void)rnkCUDA;  // the reference's signature carries it; the local likelihood does not read it
+  localLikelihood.resize(lists.size());
+  std::vector<int32_t> ptr(lists.size() + 1, 0), idx, which;
+  for (size_t i = 0; i < lists.size(); i++) {
+    if (!lists[i].empty()) which.push_back((int32_t)i);  // the reference skips empty lists
+  }
+  if (which.empty()) return;
+  ptr.assign(which.size() + 1, 0);
+  for (size_t w = 0; w < which.size(); w++) {
+    const std::vector<int>& l = lists[which[w]];
+    idx.insert(idx.end(), l.begin(), l.end());
+    ptr[w + 1] = (int32_t)idx.size();
+  }
+  TgmmGaussian* gd = nullptr;
+  check_cuda(cudaMalloc((void**)&gd, sizeof(TgmmGaussian) * (size_t)ref_nb), "calculateLocalLikelihood: cudaMalloc");
+  check_cuda(cudaMemcpy(gd, vecGMtemp, sizeof(TgmmGaussian) * (size_t)ref_nb, cudaMemcpyHostToDevice),
+             "calculateLocalLikelihood: upload");
+  TgmmFrame f{};
+  f.query = queryCUDA;
+  f.img = imgDataCUDA;
+  f.label_ptr = reinterpret_cast<const int64_t*>(labelListPtrCUDA);
+  f.centroids = nullptr;
+  f.n_vox = query_nb;
+  f.n_sv = numLabels;
+  f.n_gauss = ref_nb;
+  std::vector<double> out(which.size());
+  const int rc = tgmm_local_likelihood(&f, indCUDA, gd, ref_nb, ptr.data(), idx.data(), (int32_t)which.size(),
+                                       out.data(), nullptr);
+  cudaFree(gd);
+  if (rc != TGMM_OK) die("calculateLocalLikelihood");
+  for (size_t w = 0; w < which.size(); w++) localLikelihood[which[w]] = out[w];
+}
+
 void copyScaleToDvice(float* scale) {
   LegacyState& S = state();
   for (int d = 0; d < 3; d++) S.reg_scale[d] = scale[d];

@@ -4,6 +4,8 @@
 // Layout in HBM (capacities fixed at plan creation):
 //   per Gaussian, SoA doubles  [component][max_gauss]: beta, nu, alpha, m[3], W[6],
 //                              beta_o, nu_o, alpha_o, m_o[3], W_o[6], eLD[2], psiA[2]
+//   per voxel                  the centred voxel stream [max_vox] float4 (e = x - c, I),
+//                              written once per call, read by every log-likelihood pass
 //   per supervoxel             moments [19][max_sv] doubles (centred at the supervoxel
 //                              centroid: sum e, sum e e', sum I, sum I e, sum I e e'),
 //                              cand/rnk [max_sv][5], ll partials [2][max_sv]
@@ -78,6 +80,7 @@ struct FrameDesc {
   float* rnk_out;    // device, 5*n_sv, slot-major
   int32_t* ind_out;  // device, 5*n_sv, slot-major, frame-local Gaussian ids
   int64_t n_vox;
+  int64_t vox_base;  // the frame's first voxel in the plan's centred voxel stream (vox4)
   int32_t n_sv, n_gauss;
   int32_t sv_base, g_base;
   int32_t cell_base, cell_budget;
@@ -148,6 +151,18 @@ struct SvRec {
 };
 static_assert(sizeof(SvRec) == 128, "SvRec is eight 16-byte chunks");
 
+// Per-supervoxel record of the log-likelihood pass: where the supervoxel's voxels sit in
+// the plan's centred voxel stream vox4 (one float4 per voxel: x - c0, y - c1, z - c2 in FP32
+// and I, written once per call by the moment pass), its tiles (end-aligned like SvRec's: tile
+// 0 holds r0 voxels, later tiles kVoxTile), its frame and its centroid.
+struct SvLL {
+  long long v0;
+  int32_t nv, ntiles, r0, frame, frame_nsv;
+  float c0, c1, c2;
+  int32_t pad[2];
+};
+static_assert(sizeof(SvLL) == 48, "SvLL is three 16-byte chunks");
+
 struct BatchInfo {
   int32_t n_frames;
   int32_t total_sv;
@@ -196,6 +211,8 @@ struct DevPlan {
   int32_t* ord_hist;  // [max_frames][64]: per frame, supervoxels per tile-count bucket, then bases
   int32_t* ord_cur;   // [max_frames][64]: cursors of the scatter
   SvRec* sv_rec;
+  SvLL* sv_ll;
+  float4* vox4;  // [max_vox]: the centred voxel stream of the batch (see SvLL)
   double* mom;
   int32_t* cand;  // [2][max_sv][kJ]: candidates of the odd / even iterations' E-steps
   float* rnk;     // [2][max_sv][kJ]: their responsibilities

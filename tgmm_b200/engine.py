@@ -190,6 +190,23 @@ def knn(query: torch.Tensor, ref_xyz: torch.Tensor, scale=(1.0, 1.0, 2.0), strea
     return ind
 
 
+def local_likelihood(df: DeviceFrame, ind: torch.Tensor, gm_dev: torch.Tensor, lists, stream=None) -> np.ndarray:
+    """tgmm_local_likelihood: one FP64 value per supervoxel list (host lists of supervoxel
+    indices) under the Gaussians gm_dev (device records) with each supervoxel's candidates
+    ind (device, slot-major 5*n_sv)."""
+    ptr = np.zeros(len(lists) + 1, np.int32)
+    ptr[1:] = np.cumsum([len(x) for x in lists])
+    idx = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in lists]) if ptr[-1] else
+                               np.zeros(1, np.int32))
+    out = np.zeros(len(lists), np.float64)
+    cf = df.cframe()
+    n_gauss = gm_dev.numel() // 288
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L.check(L.gmem().tgmm_local_likelihood(C.byref(cf), ind.data_ptr(), gm_dev.data_ptr(), n_gauss, ptr.ctypes.data,
+                                           idx.ctypes.data, len(lists), out.ctypes.data, s), "tgmm_local_likelihood")
+    return out
+
+
 def update_priors(gm_dev: torch.Tensor, n: int, beta_pct=0.01, nu_pct=1.0, alpha_pct=0.8, alpha_total=-1.0,
                   compute_alpha_total=True, stream=None):
     s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
