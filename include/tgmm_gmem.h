@@ -15,6 +15,9 @@
  *   tgmm_knn                 <- knnCUDAinPlace, UtilsCUDA/knnCuda.h:225-226 (knnCuda.cu:781-817)
  *   tgmm_knn_k               <- knnCUDA_, temporalLogicalRules/knnCUDA/knnCuda.h:48-58
  *   tgmm_local_likelihood    <- calculateLocalLikelihood, UtilsCUDA/GMEMupdateCUDA.h:120-127
+ *   tgmm_split_proposal      <- GaussianMixtureModel::splitGaussian(GM, id) + updatePriorsAfterSplitProposal,
+ *                               GaussianMixtureModel.cpp:514-557, 912-922
+ *   tgmm_split_round         <- the split round, mainTrackingGaussianMixtureModel.cpp:1233-1507
  *   tgmm_update_priors       <- GaussianMixtureModel::updatePriors, GaussianMixtureModel.cpp:892-910,
  *                               plus the nu_k*=2, W_k/=2 step of mainTrackingGaussianMixtureModel.cpp:961-969
  *   tgmm_frame_upload        <- GMEMinitializeMemoryWithSupervoxels, UtilsCUDA/GMEMupdateCUDA.h:132-137
@@ -239,6 +242,37 @@ int tgmm_knn_noalloc(const float* query_dev, int64_t n_query, const float* ref_x
 int tgmm_local_likelihood(const TgmmFrame* frame, const int32_t* ind_dev, const TgmmGaussian* gm_dev,
                           int32_t n_gauss, const int32_t* list_ptr, const int32_t* list_idx, int32_t n_lists,
                           double* ll_out, void* stream);
+
+/* The split proposal of one Gaussian (GaussianMixtureModel::splitGaussian(GM, id),
+ * GaussianMixtureModel.cpp:514-557, then updatePriorsAfterSplitProposal, :912-922, on both
+ * halves), on host records: S = nu W / (s_i s_j); lmin, v its smallest eigenvalue and
+ * eigenvector, lmax its largest; sigma = 1/sqrt(max(lmin, 1e-3)); both halves take
+ * W = (lmax/nu) I with W_ii *= s_i s_i and N_k/2 (N_k = nu_k - nu_o); *a (the split Gaussian)
+ * at m + sigma v, *b (the new one) at m - sigma v; then m_o = m_k, beta_o = max(N_k/2, 1e-5),
+ * nu_o = max(N_k/2, 3), W_o = W_k nu_k / nu_o.  v's sign makes its largest-magnitude
+ * component positive (the reference takes its Eigen solver's sign, so a and b can trade
+ * places against it).  Host only; no device work. */
+int tgmm_split_proposal(const TgmmGaussian* g, const float scale[3], TgmmGaussian* a, TgmmGaussian* b);
+
+/* The split round of one time point (mainTrackingGaussianMixtureModel.cpp:1233-1507) with the
+ * candidates chosen by the caller (the reference's 3D Haar classifier picks them) and the
+ * accept/reject decision left to the caller (the reference's likelihoodRatioTestSplitMerge,
+ * called at main:1373, is not defined in its sources).  gm_host holds the n_gauss records of
+ * the first EM (with its supervoxelIdx/Num) and room for n_split more; ind_dev that EM's
+ * candidates (5*n_sv).  For each candidate cand[i] (distinct, alive):
+ *   ll_before[i] = tgmm_local_likelihood of its supervoxels under the first EM's mixture;
+ *   it is split by tgmm_split_proposal (scale: params->reg_scale, or scale when that is all
+ *   zero), the new Gaussian stored at gm_host[n_gauss + i]; every other Gaussian gets
+ *   fixed = 1, as the reference fixes them for this EM (clear them before the next frame; a
+ *   candidate keeps its own flag);
+ * then the EM on the n_gauss + n_split records (tgmm_em_run: gm_host updated, rnk_dev and
+ * ind_out_dev written, stats if not NULL), and ll_after[i] = the local log-likelihood of the
+ * same supervoxels under the new mixture and candidates.  The plan must hold
+ * n_gauss + n_split Gaussians.  Synchronises `stream`. */
+int tgmm_split_round(TgmmPlan* plan, const TgmmFrame* frame, TgmmGaussian* gm_host, int32_t n_gauss,
+                     const int32_t* ind_dev, const int32_t* cand, int32_t n_split, float* rnk_dev,
+                     int32_t* ind_out_dev, const TgmmEmParams* params, double* ll_before, double* ll_after,
+                     TgmmEmStats* stats, void* stream);
 
 /* Posterior -> prior for the next time point, on the device (served form):
  * N_k = nu_k - nu_o; m_o = m_k; beta_o = max(beta_pct*N_k, 1e-5);

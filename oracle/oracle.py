@@ -112,6 +112,30 @@ def split_proposal(rec, scale=(1.0, 1.0, 2.0)):
     return a[0], b[0]
 
 
+def split_round(query, img, cent, lptr, gauss, ind, cand, p: OrParams):
+    """The split round restated (mainTrackingGaussianMixtureModel.cpp:1233-1507, candidates
+    given): the local log-likelihood of each candidate's supervoxels before, the principal-axis
+    split of each candidate (the new Gaussian appended), every other Gaussian fixed, the EM on
+    the split mixture, the local log-likelihood of the same supervoxels after."""
+    g = np.ascontiguousarray(gauss).copy()
+    K = g.shape[0]
+    lists = [[int(s) for s in g["supervoxelIdx"][k][:g["supervoxelNum"][k]]] for k in cand]
+    before = local_likelihood(query, img, lptr, ind, g, lists)
+    g2 = np.zeros(K + len(cand), g.dtype)  # (np.concatenate would drop the record's padding)
+    g2[:K] = g
+    for k in range(K):
+        if k not in set(cand):
+            g2["fixed"][k] = 1
+    scale = tuple(p.scale)
+    for i, k in enumerate(cand):
+        a, b = split_proposal(g2[k], scale)
+        g2[k] = a
+        g2[K + i] = b
+    out = em_run(query, img, cent, lptr, g2, p)
+    after = local_likelihood(query, img, lptr, out["ind"], out["gauss"], lists)
+    return dict(before=before, after=after, split=g2, **out)
+
+
 REF_GMM_SO = os.path.join(HERE, "_ref", "libtgmm_ref_gmm.so")
 _ref_gmm = None
 
