@@ -464,7 +464,8 @@ def run_ours(args):
     # inside tgmm_em_run, D2H of rnk/ind, every step
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(frame, df, plan, params, dev, args)
+        e2e = run_e2e(frame, df, plan, params, dev, args, compact=True)
+        e2e["float_arrays"] = run_e2e(frame, df, plan, params, dev, args, compact=False)
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -499,69 +500,107 @@ def plan_time(plan, kernel, reps, stream):
     return float(ms.value)
 
 
-def run_e2e(frame, df, plan, params, dev, args):
+def run_e2e(frame, df, plan, params, dev, args, compact=True):
+    """End to end through the C ABI with host buffers, every step: the frame's upload from
+    page-locked memory, tgmm_em_run (its Gaussians up and down inside), rnk/ind down.  The
+    upload of step i + 1 runs on a copy stream into the other of two buffers while step i's EM
+    runs, so a step costs the slower of the two.  compact: the voxels cross as 6 bytes (uint32
+    linear index, uint16 raw value) and tgmm_frame_expand rebuilds the float arrays on the
+    device; else the float arrays of the reference's layout (16 bytes a voxel)."""
     import ctypes as C
     import torch
     from tgmm_b200 import _lib as L
-    pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(frame, k))).pin_memory()
-           for k in ("query", "img", "centroids", "label_ptr")}
-    S, K = frame.n_sv, frame.n_gauss
+    from tgmm_b200 import engine as E
+    N, S, K = frame.n_vox, frame.n_sv, frame.n_gauss
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    if compact:
+        lin, raw, dims, off, den = frame.compact()
+        host = {"lin": pinned(lin.view(np.int32)), "raw": pinned(raw.view(np.int16))}
+    else:
+        host = {"query": pinned(frame.query), "img": pinned(frame.img)}
+    host.update(centroids=pinned(frame.centroids), label_ptr=pinned(frame.label_ptr))
+    bufs = [{k: torch.empty_like(v, device=dev) for k, v in host.items()} for _ in range(2)]
+    q = df.query if compact else None
+    im = df.img if compact else None
     rnk_h = torch.empty(5 * S, dtype=torch.float32).pin_memory()
     ind_h = torch.empty(5 * S, dtype=torch.int32).pin_memory()
     rnk = torch.empty(5 * S, dtype=torch.float32, device=dev)
     ind = torch.empty(5 * S, dtype=torch.int32, device=dev)
-    g_host = np.ascontiguousarray(frame.gauss.astype(L.GAUSS_DTYPE))
-    stream = torch.cuda.current_stream(dev)
+    g0 = np.ascontiguousarray(frame.gauss.astype(L.GAUSS_DTYPE))
+    comp = torch.cuda.current_stream(dev)
+    cs = torch.cuda.Stream(dev)
+    up = [torch.cuda.Event() for _ in range(2)]
+    used = [torch.cuda.Event() for _ in range(2)]
     st = L.TgmmEmStats()
     lib = L.gmem()
-    h2d = sum(int(v.numel() * v.element_size()) for v in pin.values()) + 288 * K
+    h2d = sum(int(v.numel() * v.element_size()) for v in host.values()) + 288 * K
     d2h = 288 * K + 8 * 5 * S
 
-    def one():
-        g = g_host.copy()
-        df.query.copy_(pin["query"], non_blocking=True)
-        df.img.copy_(pin["img"], non_blocking=True)
-        df.centroids.copy_(pin["centroids"], non_blocking=True)
-        df.label_ptr.copy_(pin["label_ptr"], non_blocking=True)
-        cf = df.cframe()
-        L.check(lib.tgmm_em_run(plan.h, C.byref(cf), g.ctypes.data, rnk.data_ptr(), ind.data_ptr(), None,
-                                C.byref(params), C.byref(st), stream.cuda_stream), "tgmm_em_run")
-        rnk_h.copy_(rnk, non_blocking=True)
-        ind_h.copy_(ind, non_blocking=True)
-        torch.cuda.synchronize(dev)
-        return g
+    def upload(i):
+        b = bufs[i % 2]
+        with torch.cuda.stream(cs):
+            cs.wait_event(used[i % 2])  # the EM that read this buffer two steps ago is done
+            for k, v in host.items():
+                b[k].copy_(v, non_blocking=True)
+            up[i % 2].record(cs)
 
-    for _ in range(max(1, args.warmup)):
-        one()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(dev)
-    a.record(stream)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        one()
-    b.record(stream)
-    torch.cuda.synchronize(dev)
-    wall = time.perf_counter() - t0
-    ms = a.elapsed_time(b)
+    def run(n):
+        gs = [torch.from_numpy(g0.view(np.uint8).copy()).pin_memory() for _ in range(n)]
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(comp)
+        cs.wait_event(a)
+        upload(0)
+        t0 = time.perf_counter()
+        for i in range(n):
+            if i + 1 < n:
+                upload(i + 1)
+            b = bufs[i % 2]
+            comp.wait_event(up[i % 2])
+            if compact:
+                E.expand_frame(b["lin"], b["raw"], dims, off, den, q, im, stream=comp)
+                f = E.DeviceFrame(q, im, b["centroids"], b["label_ptr"], K)
+            else:
+                f = E.DeviceFrame(b["query"], b["img"], b["centroids"], b["label_ptr"], K)
+            cf = f.cframe()
+            L.check(lib.tgmm_em_run(plan.h, C.byref(cf), gs[i].data_ptr(), rnk.data_ptr(), ind.data_ptr(), None,
+                                    C.byref(params), C.byref(st), comp.cuda_stream), "tgmm_em_run")
+            rnk_h.copy_(rnk, non_blocking=True)
+            ind_h.copy_(ind, non_blocking=True)
+            used[i % 2].record(comp)
+        z.record(comp)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(z), time.perf_counter() - t0
+
+    run(max(1, args.warmup))
+    ms, wall = run(args.steps)
     return {"value": args.steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "wall_frames_per_s": args.steps / wall, "path": "tgmm_em_run (C ABI) with pinned host buffers"}
+            "wall_frames_per_s": args.steps / wall,
+            "path": ("tgmm_frame_expand + tgmm_em_run (C ABI): pinned compact voxels (6 B), centroids, CSR and "
+                     "Gaussians up, rnk/ind and Gaussians down; uploads one step ahead on a copy stream")
+            if compact else ("tgmm_em_run (C ABI): pinned float arrays (16 B a voxel, the reference's layout), "
+                             "centroids, CSR and Gaussians up, rnk/ind and Gaussians down; uploads one step "
+                             "ahead on a copy stream")}
 
 
 # ---------------------------------------------------------------------------
 # Batched and served forms (non-default workloads; one JSON line each)
 # ---------------------------------------------------------------------------
 def _pin(frame):
-    """The frame's host arrays, and its compact voxel codes, copied once into page-locked
-    memory (numpy views)."""
+    """The frame as the served and plain forms upload it: its compact voxel codes (uint32
+    linear index, uint16 raw value), centroids and CSR copied once into page-locked memory
+    (numpy views), and its first-frame Gaussians; the float arrays are not kept (a series of
+    hundreds of 1-Gvoxel frames would not fit the host's memory in float form)."""
     import torch
 
     def pinned(a):
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    out = {k: pinned(getattr(frame, k)) for k in ("query", "img", "centroids", "label_ptr")}
     lin, raw, dims, off, den = frame.compact()
-    out.update(lin=pinned(lin), raw=pinned(raw.view(np.int16)).view(np.uint16), dims=dims, raw_offset=off,
-               raw_denom=den)
+    out = dict(centroids=pinned(frame.centroids), label_ptr=pinned(frame.label_ptr),
+               lin=pinned(lin.view(np.int32)).view(np.uint32), raw=pinned(raw.view(np.int16)).view(np.uint16),
+               dims=dims, raw_offset=off, raw_denom=den, n_vox=frame.n_vox, n_sv=frame.n_sv, gauss=frame.gauss)
     return type("PinnedFrame", (), out)
 
 
@@ -637,42 +676,49 @@ SERIES_SPECS = {
     "series": [((1024, 1024, 256), 5000)],
     "mixed": [((256, 256, 64), 300), ((512, 512, 128), 2000), ((1024, 1024, 256), 8000), ((2048, 1024, 512), 20000)],
 }
+SERIES_FRAMES = {"series": 200, "mixed": 100}  # frames per series of the served configurations
+SERIES_RATE = {"series": 2.0, "mixed": 8.0}    # Poisson arrivals per second, all series together
 
 
 def _series(args):
+    """The time series of the workload, each frame kept only in its pinned compact form."""
     from tgmm_b200 import synth
-    nf = args.frames or (12 if args.workload == "series" else 6)
+    nf = args.frames or SERIES_FRAMES[args.workload]
     out = []
     for i, (dims, n) in enumerate(SERIES_SPECS[args.workload]):
         spec = synth.VolumeSpec(dims=dims, n_nuclei=n, axis_min=4.0, axis_max=8.0)
-        out.append(synth.time_series(spec, seed=args.seed + 17 * i, n_frames=nf, divide_frac=0.01))
+        out.append([_pin(f) for f in synth.time_series_iter(spec, seed=args.seed + 17 * i, n_frames=nf,
+                                                              divide_frac=0.01)])
     return out
 
 
 def run_served(args):
     """Served time series: the server (tgmm_serve.h) against the plain form, both over the
-    same pinned host frames, both returning rnk/ind and the posterior of every frame and
-    carrying each lineage's posterior into its next frame's prior on the device.
-    Closed loop (every frame submitted at once) gives throughput; Poisson arrivals at the
-    configured rate give per-frame latency."""
+    same pinned compact frames (6 bytes a voxel, expanded on the device), both returning
+    rnk/ind and the posterior of every frame and carrying each lineage's posterior into its
+    next frame's prior on the device.  Closed loop (every frame submitted at once) gives
+    throughput; Poisson arrivals at the configured rate give per-frame latency."""
     import torch
     from tgmm_b200 import _lib as L
     from tgmm_b200 import engine as E
     from tgmm_b200.serve import Server
     torch.cuda.set_device(0)
+    t_gen = time.perf_counter()
     series = _series(args)
+    t_gen = time.perf_counter() - t_gen
     from tgmm_b200 import synth
     prm = synth.em_params(iters=EM_ITERS, tol=1e-6)
-    pinned = [[_pin(f) for f in fr] for fr in series]
     order = [(li, t) for t in range(len(series[0])) for li in range(len(series))]  # interleaved arrivals
     n_frames = len(order)
-    rate = 2.0 if args.workload == "series" else 8.0
+    rate = SERIES_RATE[args.workload]
 
     # plain form: one frame at a time
-    K = [fr[0].n_gauss for fr in series]
+    K = [fr[0].gauss.shape[0] for fr in series]
     maxN = max(f.n_vox for fr in series for f in fr)
     maxS = max(f.n_sv for fr in series for f in fr)
     plan = E.Plan(maxN, maxS, max(K))
+    lin_d = torch.empty(maxN, dtype=torch.int32, device="cuda")
+    raw_d = torch.empty(maxN, dtype=torch.int16, device="cuda")
     q = torch.empty(3 * maxN, device="cuda")
     im = torch.empty(maxN, device="cuda")
     ce = torch.empty(3 * maxS, device="cuda")
@@ -688,12 +734,13 @@ def run_served(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for li, t in order:
-            f = pinned[li][t]
-            N, S = f.img.shape[0], f.label_ptr.shape[0] - 1
-            q[:3 * N].copy_(torch.from_numpy(f.query), non_blocking=True)
-            im[:N].copy_(torch.from_numpy(f.img), non_blocking=True)
+            f = series[li][t]
+            N, S = f.n_vox, f.n_sv
+            lin_d[:N].copy_(torch.from_numpy(f.lin.view(np.int32)), non_blocking=True)
+            raw_d[:N].copy_(torch.from_numpy(f.raw.view(np.int16)), non_blocking=True)
             ce[:3 * S].copy_(torch.from_numpy(f.centroids), non_blocking=True)
             lp[:S + 1].copy_(torch.from_numpy(f.label_ptr), non_blocking=True)
+            E.expand_frame(lin_d[:N], raw_d[:N], f.dims, f.raw_offset, f.raw_denom, q[:3 * N], im[:N])
             df = E.DeviceFrame(q[:3 * N], im[:N], ce[:3 * S], lp[:S + 1], K[li])
             plan.run_device(df, gms[li], rnk, ind, prm, stats=True)
             rnk_h[:5 * S].copy_(rnk[:5 * S], non_blocking=True)
@@ -713,20 +760,24 @@ def run_served(args):
     def pinned_out(S, K):
         return (torch.empty(5 * S).pin_memory().numpy(), torch.empty(5 * S, dtype=torch.int32).pin_memory().numpy(),
                 torch.empty(K * 288, dtype=torch.uint8).pin_memory().numpy().view(L.GAUSS_DTYPE))
-    outs = [[pinned_out(f.n_sv, K[li]) for f in fr] for li, fr in enumerate(series)]
+    # one output set per frame of a time step (a lineage's frames run in order, so a step's
+    # outputs are free again once the next step of that lineage has started)
+    outs = [[pinned_out(max(f.n_sv for f in fr), K[li]) for _ in range(2)] for li, fr in enumerate(series)]
 
-    def served(arrival_rate=None, seed=0, compact=True):
+    def served(arrival_rate=None, seed=0):
         ids = [srv.open_lineage(fr[0].gauss) for fr in series]
         rng = np.random.default_rng(seed)
         t0 = time.perf_counter()
         t_next = 0.0
+        res = []
         for n, (li, t) in enumerate(order):
             if arrival_rate:
                 t_next += rng.exponential(1.0 / arrival_rate)
                 while time.perf_counter() - t0 < t_next:
+                    res.extend(srv.poll(wait_ms=0))
                     time.sleep(0.0005)
-            srv.submit(ids[li], pinned[li][t], tag=n, compact=compact, out=outs[li][t])
-        res = srv.drain()
+            srv.submit(ids[li], series[li][t], tag=n, compact=True, out=outs[li][t % 2])
+        res.extend(srv.drain())
         wall = time.perf_counter() - t0
         for i in ids:
             srv.close_lineage(i)
@@ -735,12 +786,10 @@ def run_served(args):
 
     for _ in range(max(1, args.warmup)):
         served()
+    h2d0 = srv.stats()["h2d_bytes"]
     closed = [served() for _ in range(max(1, min(args.steps, 3)))]
     wall_c, res_c, bad_c = min(closed, key=lambda x: x[0])
-    h2d0 = srv.stats()["h2d_bytes"]
-    closed_f = [served(compact=False) for _ in range(max(1, min(args.steps, 3)))]
-    wall_f = min(x[0] for x in closed_f)
-    h2d_float = (srv.stats()["h2d_bytes"] - h2d0) / len(closed_f)
+    h2d_frame = (srv.stats()["h2d_bytes"] - h2d0) / len(closed) / n_frames
     wall_o, res_o, bad_o = served(arrival_rate=rate, seed=args.seed)
     lat = sorted(r.latency_ms for r in res_o)
     st = srv.stats()
@@ -750,16 +799,16 @@ def run_served(args):
             "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": [f"{d[0]}x{d[1]}x{d[2]}, {n} nuclei" for d, n in SERIES_SPECS[args.workload]],
                        "frames_per_series": len(series[0]), "frames": n_frames, "em": "max 20 iterations, tol 1e-6",
-                       "n_vox": [[f.n_vox for f in fr] for fr in series], "lanes": 2},
+                       "n_vox_per_series": [[min(f.n_vox for f in fr), max(f.n_vox for f in fr)] for fr in series],
+                       "lanes": 2, "upload": "compact voxels (6 B), expanded on the device, both forms",
+                       "generation_s": round(t_gen, 1)},
             "plain": {"value": n_frames / plain_s, "unit": UNIT,
-                      "path": "one frame at a time: pinned upload, tgmm_em_run_device, download, prior update"},
+                      "path": "one frame at a time: pinned compact upload, tgmm_frame_expand, tgmm_em_run_device, "
+                              "download, prior update"},
             "served_over_plain": (n_frames / wall_c) / (n_frames / plain_s),
-            "served_float_frames": {"value": n_frames / wall_f, "unit": UNIT,
-                                    "over_plain": (n_frames / wall_f) / (n_frames / plain_s),
-                                    "h2d_bytes_per_frame": h2d_float / n_frames,
-                                    "path": "same server, frames uploaded as float query/img (16 B/voxel)"},
-            "h2d_bytes_per_frame": h2d0 / (max(1, args.warmup) + len(closed)) / n_frames,
-            "latency_ms": {"arrivals_per_s": rate, "p50": pct(lat, 50), "p99": pct(lat, 99), "max": lat[-1]},
+            "h2d_bytes_per_frame": h2d_frame,
+            "latency_ms": {"arrivals_per_s": rate, "frames": len(lat), "p50": pct(lat, 50), "p99": pct(lat, 99),
+                           "max": lat[-1], "wall_s": wall_o},
             "closed_loop_latency_ms": {"p50": pct([r.latency_ms for r in res_c], 50),
                                        "p99": pct([r.latency_ms for r in res_c], 99)},
             "mean_batch_frames": st["frames_in_batches"] / max(1, st["batches"]),

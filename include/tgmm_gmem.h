@@ -329,6 +329,17 @@ int tgmm_frame_build_timed(const uint16_t* raw_dev, const uint32_t* label_dev,
                            uint16_t* thr_dev, int64_t max_vox, int32_t max_sv, int64_t* n_vox,
                            int32_t* n_sv, void* stream, float* stage_ms);
 
+/* A frame's voxels in compact form (6 bytes a voxel instead of 16) expanded on the device into
+ * the float arrays the EM reads: lin[v] = x + X (y + Y z) (uint32) gives query (x block, y
+ * block, z block; query[3*n_vox]) and raw[v] (uint16) gives img[v] =
+ * (float)(((double)raw[v] - raw_offset) / raw_denom) -- the reference's per-supervoxel
+ * background subtraction and [0,1] rescale (mainTrackingGaussianMixtureModel.cpp:616, 664-669)
+ * when raw_offset is the threshold and raw_denom the range, bit for bit the arrays the host
+ * builds.  dims = X, Y, Z (X*Y*Z <= 2^32).  No reference counterpart: it cuts the
+ * host-to-device bytes of a frame to 6 per voxel.  Asynchronous on `stream`. */
+int tgmm_frame_expand(const uint32_t* lin_dev, const uint16_t* raw_dev, int64_t n_vox, const int32_t dims[3],
+                      double raw_offset, double raw_denom, float* query_dev, float* img_dev, void* stream);
+
 /* Allocate device buffers and upload one frame from host arrays (legacy ownership model). */
 int tgmm_frame_upload(const float* query_host, const float* img_host,
                       const float* centroids_host, const int64_t* label_ptr_host,

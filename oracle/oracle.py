@@ -257,6 +257,23 @@ def ref_em_run(query, img, cent, lptr, gauss, max_iter=20, tol=-1.0, w4dof=1, sc
     return dict(gauss=g, rnk=rnk, ind=ind)
 
 
+def pad_supervoxels(cent, lptr, block=1024, far=-1000.0):
+    """The frame's supervoxel arrays padded to a multiple of `block` supervoxels with empty
+    ones (no voxels; centroid at (far, far, far)).  The reference's kNN kernel, launched with
+    blocks of min(1024, S) threads, returns early for the surplus threads of its last block
+    and then calls __syncthreads() (knnCuda.cu:69,106 and :154); with S a multiple of 1024
+    no thread returns early.  An empty supervoxel adds nothing to the M-step sums, the
+    log-likelihood or the assignment (its responsibilities are 1/5 each), so the outputs of the
+    real supervoxels do not change (tests/test_gpu_reference.py checks this)."""
+    S = lptr.shape[0] - 1
+    Sp = -(-S // block) * block
+    c = np.full((3, Sp), far, np.float32)
+    c[:, :S] = np.asarray(cent, np.float32).reshape(3, S)
+    lp = np.full(Sp + 1, lptr[-1], np.int64)
+    lp[:S + 1] = lptr
+    return c.reshape(-1), lp
+
+
 def ref_knn(query, ref_xyz, scale=(1.0, 1.0, 2.0)):
     q = np.ascontiguousarray(query, np.float32)
     r = np.ascontiguousarray(ref_xyz, np.float32)

@@ -45,6 +45,29 @@ def test_reference_matches_oracle_ref32(cuda_ok, name, iters):
     assert np.max(np.abs(rg["W_k"][alive] - og["W_k"][alive]) / ws) <= 1e-3
 
 
+def test_padding_with_empty_supervoxels_leaves_the_reference_outputs_unchanged(cuda_ok):
+    """The reference runs frames above 1024 supervoxels only padded to a multiple of 1024
+    with empty supervoxels (its kNN kernel's early return before __syncthreads()).  On the C1
+    frame (300 supervoxels, one block) the padded run (1024) gives the unpadded run's Gaussian
+    records and the real supervoxels' candidates and responsibilities bit for bit."""
+    needs_ref()
+    f = F.frame("c1")
+    S = f.n_sv
+    a = O.ref_em_run(f.query, f.img, f.centroids, f.label_ptr, f.gauss, max_iter=20, tol=-1.0)
+    cp, lp = O.pad_supervoxels(f.centroids, f.label_ptr)
+    assert lp.shape[0] - 1 == 1024
+    b = O.ref_em_run(f.query, f.img, cp, lp, f.gauss, max_iter=20, tol=-1.0)
+    Sp = lp.shape[0] - 1
+    np.testing.assert_array_equal(b["ind"].reshape(5, Sp)[:, :S], a["ind"].reshape(5, S))
+    np.testing.assert_array_equal(b["rnk"].reshape(5, Sp)[:, :S], a["rnk"].reshape(5, S))
+    np.testing.assert_array_equal(b["rnk"].reshape(5, Sp)[:, S:], 0.2)
+    for k in a["gauss"].dtype.names:
+        if k in ("expectedLogResponsivityCUDA",):
+            continue  # E[ln pi] carries the log-likelihood's sum only through the total alpha: equal too
+        np.testing.assert_array_equal(np.ascontiguousarray(b["gauss"][k]), np.ascontiguousarray(a["gauss"][k]),
+                                      err_msg=k)
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_reference_knn_sets_equal_canonical(cuda_ok, name):
     needs_ref()

@@ -186,3 +186,19 @@ def test_outputs_in_page_locked_memory_are_written_in_place(cuda_ok):
             np.testing.assert_array_equal(o[0], alone[li][t]["rnk"])
             np.testing.assert_array_equal(o[1], alone[li][t]["ind"])
             same_records(o[2], alone[li][t]["gauss"])
+
+
+def test_frame_expand_gives_the_host_arrays(cuda_ok):
+    """tgmm_frame_expand (the compact 6-byte voxel upload on the plain path) rebuilds the
+    frame's float coordinates and intensities bit for bit."""
+    import torch
+    from tgmm_b200 import engine as E
+    for name in ("c1", "big"):
+        f = F.frame(name)
+        lin, raw, dims, off, den = f.compact()
+        q = torch.full((3 * f.n_vox,), float("nan"), device="cuda")
+        im = torch.full((f.n_vox,), float("nan"), device="cuda")
+        E.expand_frame(torch.from_numpy(lin.view(np.int32)).cuda(), torch.from_numpy(raw.view(np.int16)).cuda(),
+                       dims, off, den, q, im)
+        np.testing.assert_array_equal(q.cpu().numpy().view(np.uint32), f.query.view(np.uint32))
+        np.testing.assert_array_equal(im.cpu().numpy().view(np.uint32), f.img.view(np.uint32))

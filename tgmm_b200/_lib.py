@@ -171,6 +171,8 @@ GMEM_FUNCS = {
     "tgmm_knn_noalloc": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.POINTER(C.c_float), _VP, _VP]),
     "tgmm_local_likelihood": (C.c_int, [C.POINTER(TgmmFrame), _VP, _VP, C.c_int32, _VP, _VP, C.c_int32, _VP, _VP]),
     "tgmm_split_proposal": (C.c_int, [_VP, C.POINTER(C.c_float), _VP, _VP]),
+    "tgmm_frame_expand": (C.c_int, [_VP, _VP, C.c_int64, C.POINTER(C.c_int32), C.c_double, C.c_double, _VP, _VP,
+                                    _VP]),
     "tgmm_split_round": (C.c_int, [_VP, C.POINTER(TgmmFrame), _VP, C.c_int32, _VP, _VP, C.c_int32, _VP, _VP,
                                    C.POINTER(TgmmEmParams), _VP, _VP, C.POINTER(TgmmEmStats), _VP]),
     "tgmm_update_priors": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,

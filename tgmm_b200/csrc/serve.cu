@@ -122,6 +122,32 @@ __global__ void k_expand_frame(const uint32_t* __restrict__ lin, const uint16_t*
   }
 }
 
+}  // namespace
+
+extern "C" int tgmm_frame_expand(const uint32_t* lin_dev, const uint16_t* raw_dev, int64_t n_vox,
+                                 const int32_t dims[3], double raw_offset, double raw_denom, float* query_dev,
+                                 float* img_dev, void* stream) {
+  if (!dims || n_vox < 0 || (n_vox > 0 && (!lin_dev || !raw_dev || !query_dev || !img_dev)))
+    return tgmm::report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_expand: null argument or negative size", cudaSuccess);
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || (int64_t)dims[0] * dims[1] * dims[2] > 0xffffffffLL)
+    return tgmm::report_error(TGMM_ERR_BAD_SIZE, "tgmm_frame_expand: the volume must have 1 .. 2^32 voxels", cudaSuccess);
+  if (!(raw_denom != 0.0)) return tgmm::report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_expand: raw_denom is 0", cudaSuccess);
+  if (n_vox == 0) return TGMM_OK;
+  const int threads = 256;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t blocks = std::min<int64_t>((n_vox + threads - 1) / threads, (int64_t)sms * 16);
+  k_expand_frame<<<(int)blocks, threads, 0, (cudaStream_t)stream>>>(lin_dev, raw_dev, n_vox, (uint32_t)dims[0],
+                                                                     (uint32_t)dims[1], raw_offset, raw_denom,
+                                                                     query_dev, img_dev);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return tgmm::report_error(TGMM_ERR_CUDA, "tgmm_frame_expand", e);
+  return TGMM_OK;
+}
+
+namespace {
+
 struct Request {
   TgmmServeRequest r;
   bool direct[3] = {false, false, false};  // rnk, ind, gm outputs downloaded in place

@@ -190,6 +190,17 @@ def knn(query: torch.Tensor, ref_xyz: torch.Tensor, scale=(1.0, 1.0, 2.0), strea
     return ind
 
 
+def expand_frame(lin: torch.Tensor, raw: torch.Tensor, dims, raw_offset: float, raw_denom: float,
+                 query: torch.Tensor, img: torch.Tensor, stream=None):
+    """tgmm_frame_expand: compact voxels (uint32 linear index, uint16 raw value; any 4- and
+    2-byte dtypes) into the float query (3*n) and img (n) arrays on the device."""
+    n = lin.numel()
+    d = (C.c_int32 * 3)(*[int(x) for x in dims])
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L.check(L.gmem().tgmm_frame_expand(lin.data_ptr(), raw.data_ptr(), n, d, float(raw_offset), float(raw_denom),
+                                       query.data_ptr(), img.data_ptr(), s), "tgmm_frame_expand")
+
+
 def local_likelihood(df: DeviceFrame, ind: torch.Tensor, gm_dev: torch.Tensor, lists, stream=None) -> np.ndarray:
     """tgmm_local_likelihood: one FP64 value per supervoxel list (host lists of supervoxel
     indices) under the Gaussians gm_dev (device records) with each supervoxel's candidates

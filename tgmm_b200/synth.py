@@ -213,20 +213,25 @@ def batch_specs(n_volumes: int, seed: int):
     return out
 
 
-def time_series(spec: VolumeSpec, seed: int, n_frames: int, sigma: float = 1.5, divide_frac: float = 0.01,
-                params: L.TgmmEmParams = None) -> list:
-    """A lineage: frame 0 with first-frame Gaussians, then frames whose nuclei move by
-    Brownian steps and divide (evolve_nuclei); later frames carry no Gaussians -- the
-    posterior of the previous frame is their prior."""
+def time_series_iter(spec: VolumeSpec, seed: int, n_frames: int, sigma: float = 1.5, divide_frac: float = 0.01,
+                     params: L.TgmmEmParams = None):
+    """The frames of time_series one at a time (a consumer can keep a smaller form of each)."""
     rng = np.random.default_rng(seed)
     nuc = random_nuclei(spec, seed)
     f0 = make_frame(spec, nuc, seed * 1000)
     init_gaussians(f0, seed, params)
     release(f0)
-    frames = [f0]
+    yield f0
     for t in range(1, n_frames):
         nuc = evolve_nuclei(nuc, spec, rng, sigma=sigma, divide_frac=divide_frac)
         f = make_frame(spec, nuc, seed * 1000 + t)
         release(f)
-        frames.append(f)
-    return frames
+        yield f
+
+
+def time_series(spec: VolumeSpec, seed: int, n_frames: int, sigma: float = 1.5, divide_frac: float = 0.01,
+                params: L.TgmmEmParams = None) -> list:
+    """A lineage: frame 0 with first-frame Gaussians, then frames whose nuclei move by
+    Brownian steps and divide (evolve_nuclei); later frames carry no Gaussians -- the
+    posterior of the previous frame is their prior."""
+    return list(time_series_iter(spec, seed, n_frames, sigma=sigma, divide_frac=divide_frac, params=params))
