@@ -249,25 +249,28 @@ def reference_gpu(frame, reps=3):
     """The reference's own GPU path (GMEMvariationalInferenceCUDAWithSupervoxels compiled from
     its sources for sm_100a) on the workload frame, per synchronous call with host arrays in
     and out as its callers use it (its context creation, allocations and copies included).
-    Only for frames of at most 1024 supervoxels: its kNN kernel returns early for surplus
-    threads before a __syncthreads(), well-defined only when no thread of a block leaves."""
+    Its kNN kernel returns early for the surplus threads of its last block before a
+    __syncthreads(), well-defined only when no thread of a block leaves: a frame above 1024
+    supervoxels runs padded to a multiple of 1024 with empty supervoxels, which leaves the real
+    supervoxels' outputs unchanged (checked on the C1 frame by tests/test_gpu_reference.py)."""
     from oracle import oracle as O
     if not O.ref_available():
         return {"unavailable": "oracle/_ref/libtgmm_ref.so not built (the reference sources were absent)"}
+    cent, lptr, padded = frame.centroids, frame.label_ptr, 0
     if frame.n_sv > 1024:
-        return {"unavailable": f"{frame.n_sv} supervoxels: the reference's kNN kernel is only well-defined "
-                               f"up to 1024 (early return before __syncthreads, knnCuda.cu:69,106)"}
+        cent, lptr = O.pad_supervoxels(frame.centroids, frame.label_ptr)
+        padded = lptr.shape[0] - 1 - frame.n_sv
     try:
-        O.ref_em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, max_iter=EM_ITERS)  # warm
+        O.ref_em_run(frame.query, frame.img, cent, lptr, frame.gauss, max_iter=EM_ITERS)  # warm
     except (OSError, RuntimeError) as e:
         return {"unavailable": f"the reference's GPU path did not run: {str(e).splitlines()[0]}"}
     ts = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        O.ref_em_run(frame.query, frame.img, frame.centroids, frame.label_ptr, frame.gauss, max_iter=EM_ITERS)
+        O.ref_em_run(frame.query, frame.img, cent, lptr, frame.gauss, max_iter=EM_ITERS)
         ts.append(time.perf_counter() - t0)
     ms = 1e3 * float(np.median(ts))
-    return {"value": 1e3 / ms, "unit": UNIT, "ms_per_call": ms, "calls": reps,
+    return {"value": 1e3 / ms, "unit": UNIT, "ms_per_call": ms, "calls": reps, "padded_supervoxels": padded,
             "path": "the reference's GPU path compiled from its sources, host arrays in and out, per call"}
 
 
