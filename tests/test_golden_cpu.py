@@ -8,6 +8,8 @@ reference's GPU EM compiled from its sources; see tests/golden/make_golden.py).
   supervoxel assignments as the reference; the remaining difference is the reference's
   FP32 accumulation (responsibilities <= 1e-4, means <= 1e-3 voxel, precision matrices
   <= 5e-3 relative)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -49,3 +51,25 @@ def test_fp64_oracle_agrees_with_reference(name, it):
     o = O.em_run(f.query, f.img, f.centroids, f.label_ptr, f.gauss,
                  O.params(max_iter=it, tol=-1.0, mode=O.MODE_FP64))
     G.compare_with_reference(z, it, o, f.n_sv, rnk_tol=1e-4, m_tol=1e-3, w_rtol=5e-3, same_slot_order=False)
+
+
+def _local_golden():
+    with np.load(os.path.join(G.GOLDEN, "local_ll.npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+LOCAL_CASES = ["c1", "hard", "big"]
+
+
+@pytest.mark.parametrize("name", LOCAL_CASES)
+def test_local_likelihood_oracle_reproduces_reference(name):
+    """The oracle's local log-likelihood against the reference's own calculateLocalLikelihood
+    (tests/golden/local_ll.npz, written by make_local_golden.py after the reference's own EM):
+    the float-sum mode to 1e-6 relative, the FP64 mode to the reference's float error."""
+    z, f = _local_golden(), F.frame(name)
+    assert str(z[f"{name}_input_sha256"]) == G.input_digest(f)
+    ptr, idx = z[f"{name}_list_ptr"], z[f"{name}_list_idx"]
+    lists = [list(idx[ptr[i]:ptr[i + 1]]) for i in range(ptr.shape[0] - 1)]
+    args = (f.query, f.img, f.label_ptr, z[f"{name}_ind"], z[f"{name}_gauss"], lists)
+    np.testing.assert_allclose(O.local_likelihood(*args, mode=O.MODE_REF32), z[f"{name}_ll"], rtol=1e-6)
+    np.testing.assert_allclose(O.local_likelihood(*args), z[f"{name}_ll"], rtol=2e-5)

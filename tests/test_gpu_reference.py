@@ -60,7 +60,7 @@ def test_padding_with_empty_supervoxels_leaves_the_reference_outputs_unchanged(c
     Sp = lp.shape[0] - 1
     np.testing.assert_array_equal(b["ind"].reshape(5, Sp)[:, :S], a["ind"].reshape(5, S))
     np.testing.assert_array_equal(b["rnk"].reshape(5, Sp)[:, :S], a["rnk"].reshape(5, S))
-    np.testing.assert_array_equal(b["rnk"].reshape(5, Sp)[:, S:], 0.2)
+    np.testing.assert_array_equal(b["rnk"].reshape(5, Sp)[:, S:], np.float32(0.2))  # 1/5 each
     for k in a["gauss"].dtype.names:
         np.testing.assert_array_equal(np.ascontiguousarray(b["gauss"][k]), np.ascontiguousarray(a["gauss"][k]),
                                       err_msg=k)

@@ -287,6 +287,27 @@ def default_params(**overrides) -> TgmmEmParams:
     return p
 
 
+def records(g) -> np.ndarray:
+    """A contiguous copy of Gaussian records in the 288-byte layout with every padding byte
+    zero (numpy leaves the three bytes after `fixed` uninitialised in a converted copy, which
+    would make equal records compare unequal as bytes)."""
+    g = np.asarray(g)
+    out = np.zeros(g.shape, GAUSS_DTYPE)
+    for name in GAUSS_DTYPE.names:
+        out[name] = g[name]
+    return out
+
+
+def records_equal(a, b) -> bool:
+    """Every named field of two record arrays equal bit for bit (padding bytes ignored)."""
+    a, b = np.asarray(a), np.asarray(b)
+    for name in GAUSS_DTYPE.names:
+        x, y = np.ascontiguousarray(a[name]), np.ascontiguousarray(b[name])
+        if x.shape != y.shape or x.tobytes() != y.tobytes():
+            return False
+    return True
+
+
 def ptr(a) -> int:
     """Address of a numpy array or a torch tensor."""
     if hasattr(a, "data_ptr"):

@@ -50,8 +50,7 @@ def to_device(frame, device="cuda", pin=False, n_gauss: int | None = None) -> De
 
 
 def gauss_to_device(g: np.ndarray, device="cuda") -> torch.Tensor:
-    g = np.ascontiguousarray(np.asarray(g).astype(L.GAUSS_DTYPE))
-    return torch.from_numpy(g.view(np.uint8).copy()).to(device)
+    return torch.from_numpy(L.records(g).view(np.uint8)).to(device)
 
 
 def gauss_from_device(t: torch.Tensor) -> np.ndarray:
@@ -95,7 +94,7 @@ class Plan:
 
     # -- single frame, Gaussians on the host (the reference's ownership model) --
     def run_host(self, df: DeviceFrame, gauss: np.ndarray, params: L.TgmmEmParams, stream=None, want_ind_tr=False):
-        g = np.ascontiguousarray(np.asarray(gauss).astype(L.GAUSS_DTYPE))
+        g = L.records(gauss)
         S = df.n_sv
         rnk = torch.empty(5 * S, dtype=torch.float32, device=df.img.device)
         ind = torch.empty(5 * S, dtype=torch.int32, device=df.img.device)
@@ -141,7 +140,7 @@ class Plan:
 
     def run_host_status(self, df: DeviceFrame, gauss: np.ndarray, params: L.TgmmEmParams):
         """tgmm_em_run returning (status, stats) instead of raising on a non-zero status."""
-        g = np.ascontiguousarray(np.asarray(gauss).astype(L.GAUSS_DTYPE))
+        g = L.records(gauss)
         S = df.n_sv
         rnk = torch.empty(5 * S, dtype=torch.float32, device=df.img.device)
         ind = torch.empty(5 * S, dtype=torch.int32, device=df.img.device)
