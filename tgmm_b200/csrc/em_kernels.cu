@@ -1501,6 +1501,8 @@ constexpr int kLLWarpBytes = (kLLCandOff + (int)sizeof(CandF) + 15) / 16 * 16;
 constexpr size_t kLLSmemBytes = (size_t)kLLWarpBytes * kWarpsPerBlockV;
 static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOff % 16 == 0 && kLLCandOff % 16 == 0,
               "slots and records stay 16-byte aligned");
+// the FP32 forms keep kLLBlocks blocks on an SM (228 KB of shared memory, 1 KB reserved per
+// block, the FP32 forms' one static LLShared64); the FP64 form sizes its own grid
 static_assert(kLLBlocks * (kLLSmemBytes + 1024 + sizeof(LLShared64)) <= 233472, "the voxel pass's blocks fit an SM");
 
 // Stage A: the records (SoA spans: kRec; centred-stream place: kLL) and candidate ids
@@ -2241,7 +2243,7 @@ void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) 
   const int grid = P.ll_blocks;
   const int bs = kWarpsPerBlockV * 32;
   if (fp64)
-    k_ll_pass<true, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
+    k_ll_pass<true, 0, false><<<P.ll_blocks64, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 8)
     k_ll_pass<false, 8, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 16)
@@ -2282,20 +2284,25 @@ cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStr
 }
 
 cudaError_t configure_kernels(DevPlan& P, int device) {
-  // every form of the voxel pass: its dynamic shared memory, and the blocks per SM the
-  // persistent grid is sized for (the fewest of the forms)
-  const void* forms[6] = {(const void*)k_ll_pass<true, 0, false>,  (const void*)k_ll_pass<false, 0, false>,
-                          (const void*)k_ll_pass<false, 8, false>, (const void*)k_ll_pass<false, 16, false>,
-                          (const void*)k_ll_pass<false, 32, false>, (const void*)k_ll_pass<false, 0, true>};
-  int sms = 0, per = 1 << 30;
+  // every form of the voxel pass: its dynamic shared memory, and the blocks per SM its
+  // persistent grid is sized for -- the fewest of the FP32 forms and the moment pass, and
+  // separately the FP64 form, whose per-warp FP64 constants take more shared memory
+  const void* forms[6] = {(const void*)k_ll_pass<false, 0, false>, (const void*)k_ll_pass<false, 8, false>,
+                          (const void*)k_ll_pass<false, 16, false>, (const void*)k_ll_pass<false, 32, false>,
+                          (const void*)k_ll_pass<false, 0, true>, (const void*)k_ll_pass<true, 0, false>};
+  int sms = 0, per = 1 << 30, per64 = 1 << 30;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  for (const void* fn : forms) {
+  for (int i = 0; i < 6; i++) {
     int p = 0;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, fn, kWarpsPerBlockV * 32, kLLSmemBytes);
-    per = p < per ? p : per;
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(forms[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, forms[i], kWarpsPerBlockV * 32, kLLSmemBytes);
+    int& m = i < 5 ? per : per64;
+    m = p < m ? p : m;
   }
   P.ll_blocks = sms * (per > 0 && per < (1 << 30) ? per : 1);
+  P.ll_blocks64 = sms * (per64 > 0 && per64 < (1 << 30) ? per64 : 1);
   return e;
 }
 void launch_assign(const DevPlan& P, cudaStream_t st) {

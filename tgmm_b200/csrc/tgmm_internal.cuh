@@ -198,7 +198,8 @@ struct DevPlan {
   double* alpha_part_f;
   int32_t* dead_part;
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
-  int32_t ll_blocks;  // resident blocks of the voxel pass (SMs x blocks per SM)
+  int32_t ll_blocks;    // resident blocks of the voxel pass's FP32 forms (SMs x blocks per SM)
+  int32_t ll_blocks64;  // the same for its FP64 form
   int32_t knn_group;  // lanes per supervoxel of the kNN/E-step (8, 16 or 32)
   int32_t iter;       // the EM iteration a launch belongs to (1-based; set per launch)
   unsigned long long stage_wait_ns;  // wait limit of a voxel tile copy (default 1 s)
