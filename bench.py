@@ -360,19 +360,19 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_frame * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_of(args.workload, frame),
+            "config": config_of(args.workload, frame, world),
             "cpu_baseline": info, "reference_gpu": gpu_ref,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def config_of(workload, frame, **extra):
-    """The config object both arms print for a single-frame workload."""
-    c = {"workload": WORKLOADS[workload], "n_vox": frame.n_vox, "n_sv": frame.n_sv, "n_gauss": frame.n_gauss,
-         "em_iterations": EM_ITERS, "l2": "inputs larger than L2 (16 B x n_vox)" if workload == "c2" else
-         "inputs fit in L2", "ll_precision": "mixed", "ll_mode": "as_reference"}
-    c.update(extra)
-    return c
+def config_of(workload, frame, world=1):
+    """The config object both arms print for a single-frame workload (the same keys and
+    values in both, so that the two lines describe one workload)."""
+    return {"workload": WORKLOADS[workload], "n_vox": frame.n_vox, "n_sv": frame.n_sv, "n_gauss": frame.n_gauss,
+            "em_iterations": EM_ITERS, "l2": "inputs larger than L2 (16 B x n_vox)" if workload == "c2" else
+            "inputs fit in L2", "ll_precision": "mixed", "ll_mode": "as_reference",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_ours(args):
@@ -479,10 +479,9 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-                "config": config_of(args.workload, frame, knn_lanes_per_supervoxel=knn_lanes,
-                                    knn_in_voxel_pass=knn_fused,
-                                    knn_grid_searches_after_iteration_1=check["knn_searches"],
-                                    parallelism=f"replicas x{world}"),
+                "config": config_of(args.workload, frame, world),
+                "tuning": {"knn_lanes_per_supervoxel": knn_lanes, "knn_in_voxel_pass": knn_fused,
+                           "knn_grid_searches_after_iteration_1": check["knn_searches"]},
                 "voxel_iters_per_s": voxel_iters,
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "gpu_launches": kernels_per_call(knn_fused) * args.steps,
@@ -753,9 +752,52 @@ def run_served(args):
             torch.cuda.synchronize()
         return time.perf_counter() - t0
 
+    qf_h = torch.empty(3 * maxN).pin_memory()
+    imf_h = torch.empty(maxN).pin_memory()
+
+    def float_frame(f):
+        """The frame's float arrays in the reference's layout, rebuilt on the host from its
+        compact codes (the values the generator produced, bit for bit)."""
+        X, Y, _ = f.dims
+        lin = f.lin.astype(np.int64)
+        N = f.n_vox
+        q = qf_h[:3 * N].numpy().reshape(3, N)
+        q[0] = lin % X
+        q[1] = (lin // X) % Y
+        q[2] = lin // (X * Y)
+        imf_h[:N].numpy()[:] = ((f.raw.astype(np.float64) - f.raw_offset) / f.raw_denom).astype(np.float32)
+
+    def plain_float_sweep():
+        """The plain form with the reference's float arrays (16 B a voxel) uploaded: per frame
+        the same work as plain_sweep; the host-side rebuild of each frame's float arrays into
+        the page-locked staging buffers happens between frames and is not timed."""
+        gms = [E.gauss_to_device(fr[0].gauss) for fr in series]
+        gm_h = [torch.empty(k * 288, dtype=torch.uint8).pin_memory() for k in K]
+        torch.cuda.synchronize()
+        total = 0.0
+        for li, t in order:
+            f = series[li][t]
+            N, S = f.n_vox, f.n_sv
+            float_frame(f)
+            t0 = time.perf_counter()
+            q[:3 * N].copy_(qf_h[:3 * N], non_blocking=True)
+            im[:N].copy_(imf_h[:N], non_blocking=True)
+            ce[:3 * S].copy_(torch.from_numpy(f.centroids), non_blocking=True)
+            lp[:S + 1].copy_(torch.from_numpy(f.label_ptr), non_blocking=True)
+            df = E.DeviceFrame(q[:3 * N], im[:N], ce[:3 * S], lp[:S + 1], K[li])
+            plan.run_device(df, gms[li], rnk, ind, prm, stats=True)
+            rnk_h[:5 * S].copy_(rnk[:5 * S], non_blocking=True)
+            ind_h[:5 * S].copy_(ind[:5 * S], non_blocking=True)
+            gm_h[li].copy_(gms[li].view(torch.uint8), non_blocking=True)
+            E.update_priors(gms[li], K[li])
+            torch.cuda.synchronize()
+            total += time.perf_counter() - t0
+        return total
+
     for _ in range(max(1, args.warmup)):
         plain_sweep()
     plain_s = min(plain_sweep() for _ in range(max(1, min(args.steps, 3))))
+    plain_float_s = plain_float_sweep()
 
     # served form; outputs into page-locked buffers, as the plain form's
     srv = Server(params=prm, lanes=2, max_batch_frames=16, max_batch_vox=max(1 << 25, 2 * maxN))
@@ -808,7 +850,12 @@ def run_served(args):
             "plain": {"value": n_frames / plain_s, "unit": UNIT,
                       "path": "one frame at a time: pinned compact upload, tgmm_frame_expand, tgmm_em_run_device, "
                               "download, prior update"},
+            "plain_float_arrays": {"value": n_frames / plain_float_s, "unit": UNIT,
+                                   "path": "one frame at a time as above, the frame uploaded as the reference's "
+                                           "float arrays (16 B a voxel) instead of compact codes; the host-side "
+                                           "rebuild of those arrays between frames is not timed"},
             "served_over_plain": (n_frames / wall_c) / (n_frames / plain_s),
+            "served_over_plain_float_arrays": (n_frames / wall_c) / (n_frames / plain_float_s),
             "h2d_bytes_per_frame": h2d_frame,
             "latency_ms": {"arrivals_per_s": rate, "frames": len(lat), "p50": pct(lat, 50), "p99": pct(lat, 99),
                            "max": lat[-1], "wall_s": wall_o},
