@@ -297,18 +297,7 @@ __device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s,
 // build_maps: per frame -- supervoxel/Gaussian -> frame maps, CSR validation,
 // centroid bounding box and grid geometry, EM state reset.
 // ===========================================================================
-// Programmatic dependent launch: the EM's kernels after the first are launched so that their
-// blocks may be scheduled while the kernel before them finishes; each one's first statement
-// waits (griddepcontrol.wait) until the kernels before it have completed and their memory is
-// visible, and then lets the kernel after it be scheduled (griddepcontrol.launch_dependents).
-// Only launch latency overlaps; no kernel reads anything before its wait.
-__device__ __forceinline__ void dep_wait_and_release() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
-  dep_wait_and_release();
   const int f = blockIdx.x;
   if (f >= P.info->n_frames) return;
   const FrameDesc D = load_desc(P, f);
@@ -525,7 +514,6 @@ __device__ __forceinline__ void chunk_done(const DevPlan& P, int f, int n_chunks
 // import: AoS (288-byte records) -> SoA, validation, preparation of iteration 1.
 // ===========================================================================
 __global__ void __launch_bounds__(kGChunk) k_import(DevPlan P) {
-  dep_wait_and_release();
   const int c = blockIdx.x;
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
@@ -583,7 +571,6 @@ __device__ __forceinline__ int order_bucket(const FrameDesc& D, int sl) {
 // k_sv_records: thread per supervoxel -- its stream record, and its bucket counted in its
 // frame's histogram (lanes of a warp with the same frame and bucket add once).
 __global__ void __launch_bounds__(256) k_sv_records(DevPlan P) {
-  dep_wait_and_release();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool in = s < P.info->total_sv;
   int key = -1;
@@ -600,7 +587,6 @@ __global__ void __launch_bounds__(256) k_sv_records(DevPlan P) {
 
 // k_order_base: one warp per frame -- the buckets' first places, largest tile counts first.
 __global__ void __launch_bounds__(32) k_order_base(DevPlan P) {
-  dep_wait_and_release();
   const int f = blockIdx.x;
   if (f >= P.info->n_frames || threadIdx.x != 0) return;
   int run = 0;
@@ -615,7 +601,6 @@ __global__ void __launch_bounds__(32) k_order_base(DevPlan P) {
 // (one atomic per warp and bucket).  Places within a bucket depend on the run; the voxel
 // pass's sums do not.
 __global__ void __launch_bounds__(256) k_order_scatter(DevPlan P) {
-  dep_wait_and_release();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool in = s < P.info->total_sv;
   int key = -1, base = 0;
@@ -963,7 +948,6 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
 
 template <int G>
 __global__ void __launch_bounds__(kKnnWarps * 32, kKnnBlocks) k_knn_estep(DevPlan P) {
-  dep_wait_and_release();
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1), gbase = lane - gl;
   const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << gbase;
@@ -1069,7 +1053,6 @@ __device__ void ordered_scan(const DevPlan& P, const FrameDesc& D, int it, int k
 // (:1693-1809).  Writes the chunk's alpha sum for the kill step.
 // ===========================================================================
 __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
-  dep_wait_and_release();
   // two blocks per Gaussian chunk (twice the SMs busy): block b covers half b%2 of chunk b/2
   const int c = blockIdx.x >> 1, half = blockIdx.x & 1;
   if (c >= P.info->n_gchunks) return;
@@ -1224,7 +1207,6 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
 // with the post-update alpha total, then the preparation of the next iteration.
 // ===========================================================================
 __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
-  dep_wait_and_release();
   const int c = blockIdx.x;
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
@@ -1886,7 +1868,6 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // reads them.
 template <bool kFp64, int G, bool kMom>
 __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
-  dep_wait_and_release();
   // the FP32 log-likelihood streams the centred voxel stream (one float4 per voxel, one bulk
   // copy per tile); the moment pass reads the input arrays (and writes that stream), the FP64
   // log-likelihood reads the input arrays too (its terms start from the exact x - c)
@@ -2156,7 +2137,6 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
 // GMEMupdateCUDA.cu:4310-4350) and SoA -> AoS.
 // ===========================================================================
 __global__ void __launch_bounds__(kSvPerBlockT) k_assign(DevPlan P) {
-  dep_wait_and_release();
   const int s = blockIdx.x * kSvPerBlockT + threadIdx.x;
   if (s >= P.info->total_sv) return;
   const int f = P.sv_frame[s];
@@ -2185,7 +2165,6 @@ __global__ void __launch_bounds__(kSvPerBlockT) k_assign(DevPlan P) {
 }
 
 __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
-  dep_wait_and_release();
   const int c = blockIdx.x;
   if (c >= P.info->n_gchunks) return;
   const GChunk ch = P.gchunks[c];
@@ -2266,62 +2245,47 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
 // ---------------------------------------------------------------------------
 static inline int div_up(int a, int b) { return (a + b - 1) / b; }
 
-// A launch whose blocks may start while the previous kernel in the stream finishes (see
-// dep_wait_and_release, the first statement of each such kernel).
-template <typename... Args>
-static void launch_dep(void (*k)(Args...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k, args...);
-}
-
 void launch_build_maps(const DevPlan& P, cudaStream_t st) {
-  launch_dep(k_build_maps, P.max_frames, kFrameThreads, 0, st, P);
+  k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
 }
-void launch_import(const DevPlan& P, cudaStream_t st) { launch_dep(k_import, P.max_gchunks, kGChunk, 0, st, P); }
+void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
 void launch_order(const DevPlan& P, cudaStream_t st) {
-  launch_dep(k_sv_records, div_up(P.max_sv, 256), 256, 0, st, P);
-  launch_dep(k_order_base, P.max_frames, 32, 0, st, P);
-  launch_dep(k_order_scatter, div_up(P.max_sv, 256), 256, 0, st, P);
+  k_sv_records<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
+  k_order_base<<<P.max_frames, 32, 0, st>>>(P);
+  k_order_scatter<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
 }
 void launch_moments(const DevPlan& P, cudaStream_t st) {
-  launch_dep(k_ll_pass<false, 0, true>, P.ll_blocks, kWarpsPerBlockV * 32, kLLSmemBytes, st, P);
+  k_ll_pass<false, 0, true><<<P.ll_blocks, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
   const int G = P.knn_group;
   const int grid = div_up(P.max_sv, kKnnWarps * 32 / G);
   if (G == 32)
-    launch_dep(k_knn_estep<32>, grid, kKnnWarps * 32, 0, st, P);
+    k_knn_estep<32><<<grid, kKnnWarps * 32, 0, st>>>(P);
   else if (G == 16)
-    launch_dep(k_knn_estep<16>, grid, kKnnWarps * 32, 0, st, P);
+    k_knn_estep<16><<<grid, kKnnWarps * 32, 0, st>>>(P);
   else
-    launch_dep(k_knn_estep<8>, grid, kKnnWarps * 32, 0, st, P);
+    k_knn_estep<8><<<grid, kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
-  launch_dep(k_mstep_update, 2 * P.max_gchunks, kMChunk, 0, st, P);
+  k_mstep_update<<<2 * P.max_gchunks, kMChunk, 0, st>>>(P);
 }
-void launch_kill_prep(const DevPlan& P, cudaStream_t st) { launch_dep(k_kill_prep, P.max_gchunks, kGChunk, 0, st, P); }
+void launch_kill_prep(const DevPlan& P, cudaStream_t st) {
+  k_kill_prep<<<P.max_gchunks, kGChunk, 0, st>>>(P);
+}
 void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) {
   const int grid = P.ll_blocks;
   const int bs = kWarpsPerBlockV * 32;
   if (fp64)
-    launch_dep(k_ll_pass<true, 0, false>, P.ll_blocks64, bs, kLLSmemBytes, st, P);
+    k_ll_pass<true, 0, false><<<P.ll_blocks64, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 8)
-    launch_dep(k_ll_pass<false, 8, false>, grid, bs, kLLSmemBytes, st, P);
+    k_ll_pass<false, 8, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 16)
-    launch_dep(k_ll_pass<false, 16, false>, grid, bs, kLLSmemBytes, st, P);
+    k_ll_pass<false, 16, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 32)
-    launch_dep(k_ll_pass<false, 32, false>, grid, bs, kLLSmemBytes, st, P);
+    k_ll_pass<false, 32, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else
-    launch_dep(k_ll_pass<false, 0, false>, grid, bs, kLLSmemBytes, st, P);
+    k_ll_pass<false, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
 }
 
 // Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging
@@ -2376,9 +2340,9 @@ cudaError_t configure_kernels(DevPlan& P, int device) {
   return e;
 }
 void launch_assign(const DevPlan& P, cudaStream_t st) {
-  launch_dep(k_assign, div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st, P);
+  k_assign<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);
 }
-void launch_export(const DevPlan& P, cudaStream_t st) { launch_dep(k_export, P.max_gchunks, kGChunk, 0, st, P); }
+void launch_export(const DevPlan& P, cudaStream_t st) { k_export<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
 
 
 // ---------------------------------------------------------------------------
