@@ -1308,6 +1308,27 @@ struct CandF {
   float u4[3], A4[6], b4;
 };
 
+// The candidates' constants from shared memory into a register copy; the 4-DOF form leaves the
+// W02 and W12 entries (zero there) out, so that they are not kept live.
+template <bool kW4>
+__device__ __forceinline__ CandF load_cand(const CandF& S) {
+  CandF C;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) C.u[q][d] = S.u[q][d];
+#pragma unroll
+    for (int e = 0; e < 6; e++) C.A[q][e] = (kW4 && (e == 2 || e == 4)) ? make_float2(0.0f, 0.0f) : S.A[q][e];
+    C.b[q] = S.b[q];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) C.u4[d] = S.u4[d];
+#pragma unroll
+  for (int e = 0; e < 6; e++) C.A4[e] = (kW4 && (e == 2 || e == 4)) ? 0.0f : S.A4[e];
+  C.b4 = S.b4;
+  return C;
+}
+
 template <bool kW4>
 __device__ __forceinline__ float2 eval_pair(const CandF& C, int q, float2 E0, float2 E1, float2 E2) {
   const float2 d0 = __fadd2_rn(E0, C.u[q][0]);  // u stored negated
@@ -2062,39 +2083,45 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
         cs->b4 = __double2float_rn(b);
     }
     __syncwarp();
-    const CandF cf = *cs;
     double lt = 0.0, lr = 0.0;
     unsigned fix = 0;  // kept tiles with voxels of zero density
     // a finished frame issues no more tiles; those issued early are consumed unread
     const int ntr = run ? nt : ic;
-    for (int t = 0; t < ntr; t++) {
-      const float* slot = ring_next(ntr);
-      if (!slot) {
-        failed = true;
-        break;
+    // the supervoxel's tiles and, rarely, the kept window's zero-density voxels, with the
+    // candidates' constants of one evaluation form held in registers through the loop (the
+    // 4-DOF form keeps 40 floats live, the general one 50)
+    auto run_tiles = [&](const auto& eval) {
+      for (int t = 0; t < ntr; t++) {
+        const float* slot = ring_next(ntr);
+        if (!slot) {
+          failed = true;
+          break;
+        }
+        if (compute) {
+          if constexpr (kFp64)
+            ll_consume(eval, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
+          else
+            ll_consume4(eval, slot, t, nt, nv, r0, lt, lr, fix);
+        }
+        gc++;
       }
-      if (compute) {
+      if (!failed && fix) {
         if constexpr (kFp64)
-          ll_consume(VoxelEval<2>{sh64[warp]}, slot, pk, t, nt, nv, r0, c0, c1, c2, lt, lr, fix);
-        else if (w4m == 0xffffffffu)
-          ll_consume4(VoxelEval<0>{cf}, slot, t, nt, nv, r0, lt, lr, fix);
+          lr += ll_fixup(eval, CA.rec, fix, c0, c1, c2);
         else
-          ll_consume4(VoxelEval<1>{cf}, slot, t, nt, nv, r0, lt, lr, fix);
+          lr += ll_fixup4(eval, P.vox4 + CA.ll.v0, nt, r0, fix);
       }
-      gc++;
+    };
+    if constexpr (kFp64) {
+      run_tiles(VoxelEval<2>{sh64[warp]});
+    } else if (w4m == 0xffffffffu) {
+      const CandF cf = load_cand<true>(*cs);
+      run_tiles(VoxelEval<0>{cf});
+    } else {
+      const CandF cf = load_cand<false>(*cs);
+      run_tiles(VoxelEval<1>{cf});
     }
     if (failed) break;
-    if (fix) {
-      if constexpr (kFp64) {
-        lr += ll_fixup(VoxelEval<2>{sh64[warp]}, CA.rec, fix, c0, c1, c2);
-      } else {
-        const float4* v = P.vox4 + CA.ll.v0;
-        if (w4m == 0xffffffffu)
-          lr += ll_fixup4(VoxelEval<0>{cf}, v, nt, r0, fix);
-        else
-          lr += ll_fixup4(VoxelEval<1>{cf}, v, nt, r0, fix);
-      }
-    }
     if (run) {
       lt = warp_sum(lt);
       lr = warp_sum(lr);
