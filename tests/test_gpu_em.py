@@ -191,3 +191,30 @@ def test_capacity_and_params_rejected(cuda_ok):
         plan.run_host(E.to_device(f), f.gauss, p)
     assert ei.value.code == L.TGMM_ERR_NOT_SET
     plan.close()
+
+
+def test_page_locked_gaussians_give_the_same_result(cuda_ok):
+    """tgmm_em_run reads page-locked Gaussian records with a kernel (so that they do not queue
+    behind the caller's uploads on the copy engines) and copies pageable ones: both give the
+    same bytes."""
+    import ctypes as C
+    import torch
+    from tgmm_b200 import _lib as L
+    from tgmm_b200 import engine as E
+    f = F.frame("hard")
+    df = E.to_device(f)
+    plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
+    want = plan.run_host(df, f.gauss, F.params(20))
+    pinned = torch.from_numpy(L.records(f.gauss).view(np.uint8)).pin_memory()
+    rnk = torch.empty(5 * f.n_sv, device="cuda")
+    ind = torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda")
+    st = L.TgmmEmStats()
+    cf = df.cframe()
+    prm = F.params(20)
+    rc = L.gmem().tgmm_em_run(plan.h, C.byref(cf), pinned.data_ptr(), rnk.data_ptr(), ind.data_ptr(), None,
+                              C.byref(prm), C.byref(st), torch.cuda.current_stream().cuda_stream)
+    assert rc == L.TGMM_OK
+    plan.close()
+    assert L.records_equal(pinned.numpy().view(L.GAUSS_DTYPE), want["gauss"])
+    np.testing.assert_array_equal(rnk.cpu().numpy(), want["rnk"])
+    np.testing.assert_array_equal(ind.cpu().numpy(), want["ind"])

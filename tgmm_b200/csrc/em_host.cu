@@ -725,7 +725,18 @@ int tgmm_em_run(TgmmPlan* P, const TgmmFrame* frame, TgmmGaussian* gm_host, floa
   if (orc) return orc;
   TgmmGaussian* scratch = (TgmmGaussian*)(P->base + P->L.gm_scratch);
   const size_t bytes = sizeof(TgmmGaussian) * (size_t)frame->n_gauss;
-  TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");
+  // page-locked records are read by the SMs, so that they do not wait behind large uploads
+  // the caller has in flight on the copy engines (e.g. its next frame); others are copied
+  cudaPointerAttributes pa;
+  const void* mapped = nullptr;
+  if (cudaPointerGetAttributes(&pa, gm_host) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer &&
+      ((uintptr_t)pa.devicePointer & 15) == 0)
+    mapped = pa.devicePointer;
+  cudaGetLastError();  // a pageable pointer may leave an error behind on older drivers
+  if (mapped)
+    TG_CUDA(launch_copy_from_host(scratch, mapped, bytes, st), "upload Gaussians");
+  else
+    TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");
   TgmmEmStats local;
   int rc = tgmm_em_run_batch(P, 1, frame, &scratch, &rnk_dev, &ind_dev, params, stats ? stats : &local, stream);
   if (rc != TGMM_OK && rc != TGMM_ERR_NAN_INPUT) return rc;

@@ -2315,6 +2315,23 @@ void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) 
     k_ll_pass<false, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
 }
 
+// Page-locked host memory read by the SMs (16 bytes a thread, coalesced) into device memory.
+// A copy engine processes its copies in order, so a small upload issued behind a large one on
+// another stream waits for it; reads issued by a kernel do not queue behind those copies.
+__global__ void __launch_bounds__(256) k_copy_from_host(uint4* __restrict__ dst, const uint4* __restrict__ src,
+                                                        size_t n16) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st) {
+  const size_t n16 = bytes / 16;
+  if (n16 == 0) return cudaSuccess;
+  const int blocks = (int)std::min<size_t>((n16 + 255) / 256, 148 * 4);
+  k_copy_from_host<<<blocks, 256, 0, st>>>((uint4*)dst, (const uint4*)src_mapped, n16);
+  return cudaGetLastError();
+}
+
 // Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging
 // a batch takes no copy engine: a batch is not queued behind large uploads of other frames.
 constexpr int kStageChunk16 = 1536;

@@ -263,6 +263,9 @@ cudaError_t configure_kernels(DevPlan& P, int device);
 // parameters (the tail up to the next 16 bytes is written with zeros)
 cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 void launch_export(const DevPlan& P, cudaStream_t st);
+// bytes (a multiple of 16) from page-locked host memory (its device-mapped address, 16-byte
+// aligned) to device memory, read by a kernel rather than a copy engine
+cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st);
 
 // standalone kNN (tgmm_knn): brute force over refs in shared memory tiles
 cudaError_t knn_bruteforce(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
