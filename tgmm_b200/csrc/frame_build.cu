@@ -150,6 +150,71 @@ __device__ __forceinline__ void scan_label(uint32_t l, uint32_t v, uint32_t X, u
   }
 }
 
+// The four consecutive voxels v..v+3 of one lane (labels q), one distinct nonzero label at a
+// time: the lane's voxels of that label give a count and a coordinate extent, the lanes of the
+// warp holding the same label combine theirs (match, reductions) and one of them adds the sums
+// into the supervoxel's count and box.  Neighbouring voxels almost always share a label, so a
+// warp usually takes one round for its 128 voxels.
+__device__ __forceinline__ void scan_group(uint4 q, uint32_t v, uint32_t X, uint32_t XY, int32_t n, int lane,
+                                           FbWork& w) {
+  uint32_t l[4] = {q.x, q.y, q.z, q.w};
+  bool bad = false;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (l[i] > (uint32_t)n) {
+      bad = true;
+      l[i] = 0;
+    }
+  if (bad) atomicOr(&w.stat->flags, 1u);
+  const uint32_t z = v / XY, r = v - z * XY, y = r / X, x = r - y * X;
+  while (true) {
+    const uint32_t cur = l[0] ? l[0] : l[1] ? l[1] : l[2] ? l[2] : l[3];
+    if (!__any_sync(0xffffffffu, cur != 0)) break;
+    int cnt = 0;
+    int32_t x0 = 0x7fffffff, x1 = -1, y0 = 0x7fffffff, y1 = -1, z0 = 0x7fffffff, z1 = -1;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (cur != 0 && l[i] == cur) {
+        uint32_t xi = x + i, yi = y, zi = z;
+        if (xi >= X) {  // the group runs into the next row
+          const uint32_t vi = v + i;
+          zi = vi / XY;
+          const uint32_t ri = vi - zi * XY;
+          yi = ri / X;
+          xi = ri - yi * X;
+        }
+        x0 = min(x0, (int32_t)xi);
+        x1 = max(x1, (int32_t)xi);
+        y0 = min(y0, (int32_t)yi);
+        y1 = max(y1, (int32_t)yi);
+        z0 = min(z0, (int32_t)zi);
+        z1 = max(z1, (int32_t)zi);
+        cnt++;
+        l[i] = 0;
+      }
+    }
+    const unsigned m = __match_any_sync(0xffffffffu, cur);
+    cnt = (int)__reduce_add_sync(m, (unsigned)cnt);
+    x0 = __reduce_min_sync(m, x0);
+    x1 = __reduce_max_sync(m, x1);
+    y0 = __reduce_min_sync(m, y0);
+    y1 = __reduce_max_sync(m, y1);
+    z0 = __reduce_min_sync(m, z0);
+    z1 = __reduce_max_sync(m, z1);
+    if (cur != 0 && (m & ((1u << lane) - 1u)) == 0) {
+      const int s = (int)cur - 1;
+      FbBox* b = &w.box[s];
+      atomicAdd(&w.cnt[s], cnt);
+      atomicMin(&b->lo[0], x0);
+      atomicMax(&b->hi[0], x1);
+      atomicMin(&b->lo[1], y0);
+      atomicMax(&b->hi[1], y1);
+      atomicMin(&b->lo[2], z0);
+      atomicMax(&b->hi[2], z1);
+    }
+  }
+}
+
 // One pass over the label volume, four labels per lane (16-byte loads); warps whose 128
 // labels are all 0 (most of a volume) do nothing more.  Coordinates in 32-bit arithmetic
 // (X*Y*Z < 2^32).
@@ -173,10 +238,7 @@ __global__ void __launch_bounds__(256) k_fb_scan(const uint32_t* __restrict__ la
     for (int u = 0; u < kFbScanDepth; u++) {
       if (__ballot_sync(0xffffffffu, (q[u].x | q[u].y | q[u].z | q[u].w) != 0) == 0) continue;
       const uint32_t v = (uint32_t)(4 * (base + u * G + lane));
-      scan_label(q[u].x, v, X, XY, n, lane, w);
-      scan_label(q[u].y, v + 1, X, XY, n, lane, w);
-      scan_label(q[u].z, v + 2, X, XY, n, lane, w);
-      scan_label(q[u].w, v + 3, X, XY, n, lane, w);
+      scan_group(q[u], v, X, XY, n, lane, w);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x < 32) {  // the last nvol % 4 labels
