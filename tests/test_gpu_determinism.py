@@ -82,3 +82,36 @@ def test_no_state_leaks_between_calls(cuda_ok):
         alone = _plan_for(n)
         _same(_call(alone, n), g, f"{n} after other frames")
         alone.close()
+
+
+@pytest.mark.parametrize("name", ["hard", "c1", "moved"])
+@pytest.mark.parametrize("tol", [0.0, 1e-6])
+def test_converged_batch_skips_iterations_without_changing_a_bit(cuda_ok, monkeypatch, name, tol):
+    """With a tolerance the captured EM wraps each iteration in a conditional graph node that
+    runs only while a frame is still running.  The result equals, byte for byte, the same call
+    launched kernel by kernel (TGMM_NO_GRAPH=1), where every iteration after convergence still
+    launches and finds its frames done; the frame converges before the iteration limit."""
+    from tgmm_b200 import _lib as L
+    from tgmm_b200 import engine as E
+    f = F.frame(name)
+    plan = _plan_for(name)
+    df = E.to_device(f)
+
+    def call():
+        import torch
+        gm = E.gauss_to_device(f.gauss)
+        rnk = torch.empty(5 * f.n_sv, device="cuda")
+        ind = torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda")
+        st = plan.run_device(df, gm, rnk, ind, F.params(20, tol=tol))
+        return gm.cpu().numpy().view(L.GAUSS_DTYPE), rnk.cpu().numpy(), ind.cpu().numpy(), st
+
+    graph = call()
+    monkeypatch.setenv("TGMM_NO_GRAPH", "1")
+    eager = call()
+    monkeypatch.delenv("TGMM_NO_GRAPH")
+    again = call()
+    plan.close()
+    assert graph[3]["converged"] and graph[3]["iterations"] < 20, graph[3]
+    assert (graph[3]["iterations"], graph[3]["ll"]) == (eager[3]["iterations"], eager[3]["ll"])
+    _same(graph, eager, f"{name} tol {tol}: conditional graph vs every iteration launched")
+    _same(graph, again, f"{name} tol {tol}: graph replayed")

@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "tgmm_internal.cuh"
@@ -109,7 +110,9 @@ struct TgmmPlan {
   cudaStream_t last_stream = nullptr;  // its stream
   bool used = false;
   bool fuse_knn = false;  // the voxel pass runs the next iteration's kNN/E-step (autotuned)
-  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (max_iter, ll_prec) -> exec
+  // (max_iter, ll_prec, conditional iterations) -> exec
+  std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+  cudaStream_t body_stream = nullptr;  // captures the bodies of the conditional iterations
   // host copy of the tables of the last staged batch
   BatchInfo s_info{};
   std::vector<FrameDesc> s_frames;
@@ -161,6 +164,7 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   e = cudaMemset(P->base, 0, P->L.total);
   if (e == cudaSuccess) e = cudaMallocHost(&P->h_state, sizeof(FrameState) * d->max_frames);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->body_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->done_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     tgmm_plan_destroy(P);
@@ -225,6 +229,7 @@ int tgmm_plan_destroy(TgmmPlan* P) {
   if (P->used) cudaEventSynchronize(P->done_ev);
   for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+  if (P->body_stream) cudaStreamDestroy(P->body_stream);
   if (P->done_ev) cudaEventDestroy(P->done_ev);
   if (P->h_state) cudaFreeHost(P->h_state);
   if (P->base) cudaFree(P->base);
@@ -350,11 +355,51 @@ int stage_tables(TgmmPlan* P, cudaStream_t st) {
   return TGMM_OK;
 }
 
+// Appends to the graph being captured on `st` one conditional (IF) node whose body is what
+// `body` enqueues (captured on the plan's body stream), preceded by k_iter_cond, which sets
+// the node's condition on the device: whether any frame of the batch still runs.
+template <class F>
+int capture_if_running(TgmmPlan* P, const DevPlan& D, cudaStream_t st, F body) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  unsigned long long id = 0;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  TG_CUDA(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd), "capture info");
+  if (cs != cudaStreamCaptureStatusActive) return fail(TGMM_ERR_CUDA, "conditional iteration outside a capture");
+  cudaGraphConditionalHandle h;
+  TG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault), "conditional handle");
+  launch_iter_cond(D, h, st);
+  TG_CUDA(cudaGetLastError(), "iteration condition");
+  TG_CUDA(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd), "capture info");
+  std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+  cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+  prm.conditional.handle = h;
+  prm.conditional.type = cudaGraphCondTypeIf;
+  prm.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  TG_CUDA(cudaGraphAddNode(&node, g, dv.data(), dv.size(), &prm), "conditional node");
+  TG_CUDA(cudaStreamBeginCaptureToGraph(P->body_stream, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal),
+          "begin body capture");
+  body(P->body_stream);
+  cudaGraph_t bg = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(P->body_stream, &bg);
+  TG_CUDA(cudaGetLastError(), "iteration body");
+  TG_CUDA(e, "end body capture");
+  TG_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+          "capture dependencies");
+  return TGMM_OK;
+}
+
 // The whole EM (after the tables are staged) as a stream of async operations on `st`.
 // Each launch carries its iteration number.  With fuse_knn the voxel pass of iteration t
 // also runs the kNN/E-step of iteration t + 1 (mixed-precision voxel terms only); else that
-// kernel follows the pass.
-int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
+// kernel follows the pass.  With `cond` (a graph capture with a convergence tolerance) each
+// iteration is a conditional graph node that runs only while a frame of the batch is still
+// running, so a batch that converged early launches none of the remaining iterations' kernels
+// (which would all find their frames done and return).
+int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, bool cond, cudaStream_t st) {
   DevPlan D = P->dev;
   D.iter = 1;
   launch_build_maps(D, st);
@@ -366,14 +411,22 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
   if (max_iter >= 1) launch_knn_estep(D, st);
   for (int it = 1; it <= max_iter; it++) {
     D.iter = it;
-    launch_mstep_update(D, st);
-    launch_kill_prep(D, st);
-    const bool more = it < max_iter;
-    launch_ll_pass(D, fp64, more && fuse ? D.knn_group : 0, st);
-    if (more && !fuse) {
-      DevPlan N = D;
-      N.iter = it + 1;
-      launch_knn_estep(N, st);
+    auto body = [&, D, it](cudaStream_t s) {
+      launch_mstep_update(D, s);
+      launch_kill_prep(D, s);
+      const bool more = it < max_iter;
+      launch_ll_pass(D, fp64, more && fuse ? D.knn_group : 0, s);
+      if (more && !fuse) {
+        DevPlan N = D;
+        N.iter = it + 1;
+        launch_knn_estep(N, s);
+      }
+    };
+    if (cond) {
+      const int rc = capture_if_running(P, D, st, body);
+      if (rc) return rc;
+    } else {
+      body(st);
     }
   }
   launch_assign(D, st);
@@ -387,14 +440,16 @@ bool use_graphs() {
   return !(e && e[0] == '1');
 }
 
-int run_batch(TgmmPlan* P, int max_iter, int ll_prec, cudaStream_t st) {
-  if (!use_graphs()) return enqueue_em(P, max_iter, ll_prec, st);
-  auto key = std::make_pair(max_iter, ll_prec);
+int run_batch(TgmmPlan* P, int max_iter, int ll_prec, double tol, cudaStream_t st) {
+  if (!use_graphs()) return enqueue_em(P, max_iter, ll_prec, false, st);
+  // a negative tolerance runs every iteration: no conditional nodes
+  const bool cond = tol >= 0.0;
+  auto key = std::make_tuple(max_iter, ll_prec, cond ? 1 : 0);
   auto it = P->graphs.find(key);
   if (it == P->graphs.end()) {
     cudaGraph_t g = nullptr;
     TG_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    int rc = enqueue_em(P, max_iter, ll_prec, P->cap_stream);
+    int rc = enqueue_em(P, max_iter, ll_prec, cond, P->cap_stream);
     cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
     if (rc != TGMM_OK) {
       if (g) cudaGraphDestroy(g);
@@ -506,7 +561,7 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
   if (rc) return rc;
   rc = stage_tables(P, st);
   if (rc) return rc;
-  rc = run_batch(P, params->max_iter_em, params->ll_precision, st);
+  rc = run_batch(P, params->max_iter_em, params->ll_precision, params->tol_likelihood, st);
   if (rc) return rc;
   TG_CUDA(cudaEventRecord(P->done_ev, st), "record");
   P->used = true;
@@ -622,7 +677,7 @@ int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, T
             rc = fail(TGMM_ERR_CUDA, "tgmm_plan_autotune: copy Gaussians", cudaGetLastError());
         if (rc == TGMM_OK) rc = stage_tables(P, st);
         if (rc == TGMM_OK && cudaEventRecord(ev[0], st) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "record");
-        if (rc == TGMM_OK) rc = run_batch(P, tp.max_iter_em, tp.ll_precision, st);
+        if (rc == TGMM_OK) rc = run_batch(P, tp.max_iter_em, tp.ll_precision, tp.tol_likelihood, st);
         if (rc == TGMM_OK && cudaEventRecord(ev[1], st) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "record");
         if (rc == TGMM_OK && cudaEventSynchronize(ev[1]) != cudaSuccess) rc = fail(TGMM_ERR_CUDA, "synchronize");
         float ms = 0.0f;

@@ -2383,6 +2383,21 @@ cudaError_t configure_kernels(DevPlan& P, int device) {
   P.ll_blocks64 = sms * (per64 > 0 && per64 < (1 << 30) ? per64 : 1);
   return e;
 }
+// The condition of the next iteration's conditional graph node: whether any frame of the
+// batch is still running (its done flag is set by the voxel pass's convergence test, or at
+// the start for a frame that cannot run).  A batch whose frames have all stopped skips the
+// remaining iterations' launches, which would find nothing to do.
+__global__ void __launch_bounds__(1024) k_iter_cond(DevPlan P, cudaGraphConditionalHandle h) {
+  const int nf = P.info->n_frames;
+  int running = 0;
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) running |= P.state[f].done == 0;
+  running = __syncthreads_or(running);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, running ? 1u : 0u);
+}
+void launch_iter_cond(const DevPlan& P, cudaGraphConditionalHandle h, cudaStream_t st) {
+  k_iter_cond<<<1, 1024, 0, st>>>(P, h);
+}
+
 void launch_assign(const DevPlan& P, cudaStream_t st) {
   k_assign<<<div_up(P.max_sv, kSvPerBlockT), kSvPerBlockT, 0, st>>>(P);
 }

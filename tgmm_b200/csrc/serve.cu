@@ -170,7 +170,7 @@ struct Lane {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
   bool busy = false;
-  bool tuned = false;  // the plan's kNN/E-step width tuned on the lane's first batch
+  bool tuned = false;  // the plan's kNN/E-step width and arrangement set (see launch)
   int launch_rc = TGMM_OK;
   int32_t batch_id = 0;
   std::vector<Request*> reqs;
@@ -317,9 +317,17 @@ void TgmmServer::launch(Lane& L) {
     go += L.n_gauss[i];
   }
   if (rc == TGMM_OK && !L.tuned) {
-    int32_t lanes = 0;
-    rc = tgmm_plan_autotune(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, 2, &lanes, L.st);
-    L.tuned = true;
+    // the server's first batch tunes its lane's plan; every other lane takes the same
+    // setting, so no later batch (and no lane first used late in a stream) pays for tuning
+    int32_t width = 0, fused = 0;
+    rc = tgmm_plan_autotune(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, 2, &width, L.st);
+    if (rc == TGMM_OK) rc = tgmm_plan_tuning(L.plan, &width, &fused);
+    for (Lane& O : lanes)
+      if (rc == TGMM_OK && &O != &L) {
+        rc = tgmm_plan_set_knn_group(O.plan, width);
+        if (rc == TGMM_OK) rc = tgmm_plan_set_knn_fusion(O.plan, fused);
+      }
+    for (Lane& O : lanes) O.tuned = true;
   }
   if (rc == TGMM_OK)
     rc = tgmm_em_run_batch(L.plan, n, fr.data(), gm.data(), rnk.data(), ind.data(), &desc.params, nullptr, L.st);

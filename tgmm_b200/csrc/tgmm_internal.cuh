@@ -257,6 +257,7 @@ void launch_knn_estep(const DevPlan& P, cudaStream_t st);
 void launch_mstep_update(const DevPlan& P, cudaStream_t st);
 void launch_kill_prep(const DevPlan& P, cudaStream_t st);
 void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st);
+void launch_iter_cond(const DevPlan& P, cudaGraphConditionalHandle h, cudaStream_t st);
 void launch_assign(const DevPlan& P, cudaStream_t st);
 cudaError_t configure_kernels(DevPlan& P, int device);
 // bytes from host memory to 16-byte aligned device memory through kernel launch
