@@ -467,8 +467,9 @@ def run_ours(args):
     # inside tgmm_em_run, D2H of rnk/ind, every step
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(frame, df, plan, params, dev, args, compact=True)
-        e2e["float_arrays"] = run_e2e(frame, df, plan, params, dev, args, compact=False)
+        e2e = run_e2e(frame, df, plan, params, dev, args, form="runs")
+        e2e["compact_6_bytes"] = run_e2e(frame, df, plan, params, dev, args, form="compact")
+        e2e["float_arrays"] = run_e2e(frame, df, plan, params, dev, args, form="float")
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -502,13 +503,16 @@ def plan_time(plan, kernel, reps, stream):
     return float(ms.value)
 
 
-def run_e2e(frame, df, plan, params, dev, args, compact=True):
+def run_e2e(frame, df, plan, params, dev, args, form="runs"):
     """End to end through the C ABI with host buffers, every step: the frame's upload from
     page-locked memory, tgmm_em_run (its Gaussians up and down inside), rnk/ind down.  The
     upload of step i + 1 runs on a copy stream into the other of two buffers while step i's EM
-    runs, so a step costs the slower of the two.  compact: the voxels cross as 6 bytes (uint32
-    linear index, uint16 raw value) and tgmm_frame_expand rebuilds the float arrays on the
-    device; else the float arrays of the reference's layout (16 bytes a voxel)."""
+    runs, so a step costs the slower of the two.  form "runs": the voxels cross as runs of
+    consecutive linear indices (uint32 start, uint16 length, per supervoxel int32 run pointers)
+    and uint16 raw values, about 3 bytes a voxel, and tgmm_frame_expand_runs rebuilds the float
+    arrays on the device; "compact": 6 bytes a voxel (uint32 linear index, uint16 raw value)
+    through tgmm_frame_expand; "float": the float arrays of the reference's layout (16 bytes a
+    voxel)."""
     import ctypes as C
     import torch
     from tgmm_b200 import _lib as L
@@ -517,7 +521,12 @@ def run_e2e(frame, df, plan, params, dev, args, compact=True):
 
     def pinned(a):
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    if compact:
+    compact = form != "float"
+    if form == "runs":
+        rp, rs, rl, raw, dims, off, den = frame.runs()
+        host = {"run_ptr": pinned(rp), "run_start": pinned(rs.view(np.int32)), "run_len": pinned(rl.view(np.int16)),
+                "raw": pinned(raw.view(np.int16))}
+    elif form == "compact":
         lin, raw, dims, off, den = frame.compact()
         host = {"lin": pinned(lin.view(np.int32)), "raw": pinned(raw.view(np.int16))}
     else:
@@ -561,7 +570,11 @@ def run_e2e(frame, df, plan, params, dev, args, compact=True):
                 upload(i + 1)
             b = bufs[i % 2]
             comp.wait_event(up[i % 2])
-            if compact:
+            if form == "runs":
+                E.expand_runs(b["run_ptr"], b["run_start"], b["run_len"], b["raw"], b["label_ptr"], dims, off, den, q,
+                              im, stream=comp)
+                f = E.DeviceFrame(q, im, b["centroids"], b["label_ptr"], K)
+            elif compact:
                 E.expand_frame(b["lin"], b["raw"], dims, off, den, q, im, stream=comp)
                 f = E.DeviceFrame(q, im, b["centroids"], b["label_ptr"], K)
             else:
@@ -580,30 +593,42 @@ def run_e2e(frame, df, plan, params, dev, args, compact=True):
     ms, wall = run(args.steps)
     return {"value": args.steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "wall_frames_per_s": args.steps / wall,
-            "path": ("tgmm_frame_expand + tgmm_em_run (C ABI): pinned compact voxels (6 B), centroids, CSR and "
-                     "Gaussians up, rnk/ind and Gaussians down; uploads one step ahead on a copy stream")
-            if compact else ("tgmm_em_run (C ABI): pinned float arrays (16 B a voxel, the reference's layout), "
-                             "centroids, CSR and Gaussians up, rnk/ind and Gaussians down; uploads one step "
-                             "ahead on a copy stream")}
+            "path": {"runs": "tgmm_frame_expand_runs + tgmm_em_run (C ABI): pinned voxel runs (uint32 start, uint16 "
+                             "length, int32 pointer per supervoxel) and uint16 raw values (~3 B a voxel), centroids, "
+                             "CSR and Gaussians up, rnk/ind and Gaussians down; uploads one step ahead on a copy stream",
+                     "compact": "tgmm_frame_expand + tgmm_em_run (C ABI): pinned compact voxels (6 B), centroids, CSR "
+                                "and Gaussians up, rnk/ind and Gaussians down; uploads one step ahead on a copy stream",
+                     "float": "tgmm_em_run (C ABI): pinned float arrays (16 B a voxel, the reference's layout), "
+                              "centroids, CSR and Gaussians up, rnk/ind and Gaussians down; uploads one step ahead on "
+                              "a copy stream"}[form]}
 
 
 # ---------------------------------------------------------------------------
 # Batched and served forms (non-default workloads; one JSON line each)
 # ---------------------------------------------------------------------------
 def _pin(frame):
-    """The frame as the served and plain forms upload it: its compact voxel codes (uint32
-    linear index, uint16 raw value), centroids and CSR copied once into page-locked memory
-    (numpy views), and its first-frame Gaussians; the float arrays are not kept (a series of
-    hundreds of 1-Gvoxel frames would not fit the host's memory in float form)."""
+    """The frame as the served and plain forms upload it: its voxel runs (int32 pointer per
+    supervoxel, uint32 start, uint16 length) and uint16 raw values, centroids and CSR copied
+    once into page-locked memory (numpy views), and its first-frame Gaussians; the float
+    arrays are not kept (a series of hundreds of 1-Gvoxel frames would not fit the host's
+    memory in float form)."""
     import torch
 
     def pinned(a):
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    lin, raw, dims, off, den = frame.compact()
-    out = dict(centroids=pinned(frame.centroids), label_ptr=pinned(frame.label_ptr),
-               lin=pinned(lin.view(np.int32)).view(np.uint32), raw=pinned(raw.view(np.int16)).view(np.uint16),
+    rp, rs, rl, raw, dims, off, den = frame.runs()
+    out = dict(centroids=pinned(frame.centroids), label_ptr=pinned(frame.label_ptr), run_ptr=pinned(rp),
+               run_start=pinned(rs.view(np.int32)).view(np.uint32), run_len=pinned(rl.view(np.int16)).view(np.uint16),
+               raw=pinned(raw.view(np.int16)).view(np.uint16),
                dims=dims, raw_offset=off, raw_denom=den, n_vox=frame.n_vox, n_sv=frame.n_sv, gauss=frame.gauss)
     return type("PinnedFrame", (), out)
+
+
+def _lin_of(f):
+    """A pinned frame's linear voxel indices, rebuilt on the host from its runs."""
+    rl = f.run_len.astype(np.int64)
+    pos = np.arange(int(rl.sum())) - np.repeat(np.cumsum(rl) - rl, rl)
+    return np.repeat(f.run_start.astype(np.int64), rl) + pos
 
 
 def run_batch64(args):
@@ -683,7 +708,7 @@ SERIES_RATE = {"series": 2.0, "mixed": 8.0}    # Poisson arrivals per second, al
 
 
 def _series(args):
-    """The time series of the workload, each frame kept only in its pinned compact form."""
+    """The time series of the workload, each frame kept only in its pinned run form."""
     from tgmm_b200 import synth
     nf = args.frames or SERIES_FRAMES[args.workload]
     out = []
@@ -696,7 +721,7 @@ def _series(args):
 
 def run_served(args):
     """Served time series: the server (tgmm_serve.h) against the plain form, both over the
-    same pinned compact frames (6 bytes a voxel, expanded on the device), both returning
+    same pinned frames as voxel runs (about 3 bytes a voxel, expanded on the device), both returning
     rnk/ind and the posterior of every frame and carrying each lineage's posterior into its
     next frame's prior on the device.  Closed loop (every frame submitted at once) gives
     throughput; Poisson arrivals at the configured rate give per-frame latency."""
@@ -719,7 +744,10 @@ def run_served(args):
     maxN = max(f.n_vox for fr in series for f in fr)
     maxS = max(f.n_sv for fr in series for f in fr)
     plan = E.Plan(maxN, maxS, max(K))
-    lin_d = torch.empty(maxN, dtype=torch.int32, device="cuda")
+    maxR = max(f.run_start.shape[0] for fr in series for f in fr)
+    rp_d = torch.empty(maxS + 1, dtype=torch.int32, device="cuda")
+    rs_d = torch.empty(maxR, dtype=torch.int32, device="cuda")
+    rl_d = torch.empty(maxR, dtype=torch.int16, device="cuda")
     raw_d = torch.empty(maxN, dtype=torch.int16, device="cuda")
     q = torch.empty(3 * maxN, device="cuda")
     im = torch.empty(maxN, device="cuda")
@@ -738,11 +766,15 @@ def run_served(args):
         for li, t in order:
             f = series[li][t]
             N, S = f.n_vox, f.n_sv
-            lin_d[:N].copy_(torch.from_numpy(f.lin.view(np.int32)), non_blocking=True)
+            R = f.run_start.shape[0]
+            rp_d[:S + 1].copy_(torch.from_numpy(f.run_ptr), non_blocking=True)
+            rs_d[:R].copy_(torch.from_numpy(f.run_start.view(np.int32)), non_blocking=True)
+            rl_d[:R].copy_(torch.from_numpy(f.run_len.view(np.int16)), non_blocking=True)
             raw_d[:N].copy_(torch.from_numpy(f.raw.view(np.int16)), non_blocking=True)
             ce[:3 * S].copy_(torch.from_numpy(f.centroids), non_blocking=True)
             lp[:S + 1].copy_(torch.from_numpy(f.label_ptr), non_blocking=True)
-            E.expand_frame(lin_d[:N], raw_d[:N], f.dims, f.raw_offset, f.raw_denom, q[:3 * N], im[:N])
+            E.expand_runs(rp_d[:S + 1], rs_d[:R], rl_d[:R], raw_d[:N], lp[:S + 1], f.dims, f.raw_offset, f.raw_denom,
+                          q[:3 * N], im[:N])
             df = E.DeviceFrame(q[:3 * N], im[:N], ce[:3 * S], lp[:S + 1], K[li])
             plan.run_device(df, gms[li], rnk, ind, prm, stats=True)
             rnk_h[:5 * S].copy_(rnk[:5 * S], non_blocking=True)
@@ -757,9 +789,9 @@ def run_served(args):
 
     def float_frame(f):
         """The frame's float arrays in the reference's layout, rebuilt on the host from its
-        compact codes (the values the generator produced, bit for bit)."""
+        voxel runs (the values the generator produced, bit for bit)."""
         X, Y, _ = f.dims
-        lin = f.lin.astype(np.int64)
+        lin = _lin_of(f)
         N = f.n_vox
         q = qf_h[:3 * N].numpy().reshape(3, N)
         q[0] = lin % X
@@ -821,7 +853,7 @@ def run_served(args):
                 while time.perf_counter() - t0 < t_next:
                     res.extend(srv.poll(wait_ms=0))
                     time.sleep(0.0005)
-            srv.submit(ids[li], series[li][t], tag=n, compact=True, out=outs[li][t % 2])
+            srv.submit(ids[li], series[li][t], tag=n, runs=True, out=outs[li][t % 2])
         res.extend(srv.drain())
         wall = time.perf_counter() - t0
         for i in ids:
@@ -845,14 +877,15 @@ def run_served(args):
             "config": {"workload": [f"{d[0]}x{d[1]}x{d[2]}, {n} nuclei" for d, n in SERIES_SPECS[args.workload]],
                        "frames_per_series": len(series[0]), "frames": n_frames, "em": "max 20 iterations, tol 1e-6",
                        "n_vox_per_series": [[min(f.n_vox for f in fr), max(f.n_vox for f in fr)] for fr in series],
-                       "lanes": 2, "upload": "compact voxels (6 B), expanded on the device, both forms",
+                       "lanes": 2, "upload": "voxel runs and raw values (~3 B a voxel), expanded on the device, "
+                                             "both forms",
                        "generation_s": round(t_gen, 1)},
             "plain": {"value": n_frames / plain_s, "unit": UNIT,
-                      "path": "one frame at a time: pinned compact upload, tgmm_frame_expand, tgmm_em_run_device, "
+                      "path": "one frame at a time: pinned run upload, tgmm_frame_expand_runs, tgmm_em_run_device, "
                               "download, prior update"},
             "plain_float_arrays": {"value": n_frames / plain_float_s, "unit": UNIT,
                                    "path": "one frame at a time as above, the frame uploaded as the reference's "
-                                           "float arrays (16 B a voxel) instead of compact codes; the host-side "
+                                           "float arrays (16 B a voxel) instead of voxel runs; the host-side "
                                            "rebuild of those arrays between frames is not timed"},
             "served_over_plain": (n_frames / wall_c) / (n_frames / plain_s),
             "served_over_plain_float_arrays": (n_frames / wall_c) / (n_frames / plain_float_s),

@@ -340,6 +340,22 @@ int tgmm_frame_build_timed(const uint16_t* raw_dev, const uint32_t* label_dev,
 int tgmm_frame_expand(const uint32_t* lin_dev, const uint16_t* raw_dev, int64_t n_vox, const int32_t dims[3],
                       double raw_offset, double raw_denom, float* query_dev, float* img_dev, void* stream);
 
+/* The same float arrays from runs, about 3 bytes a voxel for nuclei volumes (a supervoxel's
+ * voxels, ascending in linear index, fall into runs of consecutive indices, ~6 voxels each in
+ * the synthetic frames): the voxels of supervoxel s (label_ptr[s] .. label_ptr[s+1]) are the
+ * runs run_ptr[s] .. run_ptr[s+1] in order, run r being the run_len[r] linear indices
+ * run_start[r], run_start[r] + 1, ...; raw[v] (uint16, voxel order) as tgmm_frame_expand.  The
+ * runs of a supervoxel must cover exactly its voxel range: nothing is written outside that
+ * range whatever the tables say, and voxels they leave out keep what the arrays held.  A
+ * supervoxel with an invalid range is skipped (the EM flags the CSR), and no run outside
+ * 0 .. n_runs is read.  No reference
+ * counterpart: it halves the host-to-device bytes of tgmm_frame_expand's codes.
+ * Asynchronous on `stream`; every array on the device. */
+int tgmm_frame_expand_runs(const int32_t* run_ptr_dev, const uint32_t* run_start_dev, const uint16_t* run_len_dev,
+                           const uint16_t* raw_dev, const int64_t* label_ptr_dev, int32_t n_sv, int64_t n_runs,
+                           int64_t n_vox, const int32_t dims[3], double raw_offset, double raw_denom, float* query_dev,
+                           float* img_dev, void* stream);
+
 /* Allocate device buffers and upload one frame from host arrays (legacy ownership model). */
 int tgmm_frame_upload(const float* query_host, const float* img_host,
                       const float* centroids_host, const int64_t* label_ptr_host,

@@ -96,6 +96,13 @@ typedef struct TgmmServeRequest {
   int32_t dims[3];              /* X, Y, Z of the volume (compact form) */
   double raw_offset;            /* compact form: intensity offset (the foreground threshold) */
   double raw_denom;             /* compact form: intensity denominator (max - threshold) */
+  /* Run form (query, img and lin NULL; raw, dims, raw_offset, raw_denom as the compact form):
+   * the voxels of supervoxel s are the runs run_ptr[s] .. run_ptr[s+1], run r the run_len[r]
+   * consecutive linear indices from run_start[r] (see tgmm_frame_expand_runs). */
+  const int32_t* run_ptr;       /* host, n_sv + 1 */
+  const uint32_t* run_start;    /* host, n_runs */
+  const uint16_t* run_len;      /* host, n_runs */
+  int64_t n_runs;
 } TgmmServeRequest;
 
 int tgmm_server_submit(TgmmServer* s, const TgmmServeRequest* r);

@@ -53,8 +53,8 @@ def same_records(a, b):
         np.testing.assert_array_equal(a[name], b[name], err_msg=name)
 
 
-@pytest.mark.parametrize("compact", [False, True])
-def test_served_mix_is_bit_identical_to_alone(cuda_ok, compact):
+@pytest.mark.parametrize("form", ["float", "compact", "runs"])
+def test_served_mix_is_bit_identical_to_alone(cuda_ok, form):
     from tgmm_b200.serve import Server
     prm = params()
     series = lineages()
@@ -63,7 +63,7 @@ def test_served_mix_is_bit_identical_to_alone(cuda_ok, compact):
         ids = [srv.open_lineage(fr[0].gauss) for fr in series]
         for t in range(N_FRAMES):  # interleaved arrivals of all lineages
             for li, fr in enumerate(series):
-                srv.submit(ids[li], fr[t], tag=li * 100 + t, compact=compact)
+                srv.submit(ids[li], fr[t], tag=li * 100 + t, compact=form == "compact", runs=form == "runs")
         res = {r.tag: r for r in srv.drain()}
         st = srv.stats()
     assert len(res) == len(series) * N_FRAMES
@@ -202,3 +202,58 @@ def test_frame_expand_gives_the_host_arrays(cuda_ok):
                        dims, off, den, q, im)
         np.testing.assert_array_equal(q.cpu().numpy().view(np.uint32), f.query.view(np.uint32))
         np.testing.assert_array_equal(im.cpu().numpy().view(np.uint32), f.img.view(np.uint32))
+
+
+def _expand_runs(f, rp, rs, rl, raw, dims, off, den):
+    import torch
+    from tgmm_b200 import engine as E
+    q = torch.full((3 * f.n_vox,), float("nan"), device="cuda")
+    im = torch.full((f.n_vox,), float("nan"), device="cuda")
+    E.expand_runs(torch.from_numpy(rp).cuda(), torch.from_numpy(rs.view(np.int32)).cuda(),
+                  torch.from_numpy(rl.view(np.int16)).cuda(), torch.from_numpy(raw.view(np.int16)).cuda(),
+                  torch.from_numpy(np.ascontiguousarray(f.label_ptr)).cuda(), dims, off, den, q, im)
+    return q.cpu().numpy(), im.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["tiny", "c1", "big", "split"])
+def test_frame_expand_runs_gives_the_host_arrays(cuda_ok, name):
+    """tgmm_frame_expand_runs (runs of consecutive linear indices, about 3 bytes a voxel) rebuilds
+    the frame's float coordinates and intensities bit for bit; supervoxels with more than 32
+    runs ("big") and many small supervoxels ("split") included."""
+    f = F.frame(name)
+    rp, rs, rl, raw, dims, off, den = f.runs()
+    assert rs.shape[0] < f.n_vox
+    q, im = _expand_runs(f, rp, rs, rl, raw, dims, off, den)
+    np.testing.assert_array_equal(q.view(np.uint32), f.query.view(np.uint32))
+    np.testing.assert_array_equal(im.view(np.uint32), f.img.view(np.uint32))
+
+
+def test_frame_expand_runs_with_runs_cut_short(cuda_ok):
+    """The same frame with every run cut to at most 3 voxels (many runs per supervoxel, several
+    groups of 32 per warp) gives the same arrays."""
+    f = F.frame("c1")
+    lin, raw, dims, off, den = f.compact()
+    rp, rs, rl = synth.runs_of(lin, f.label_ptr, max_len=3)
+    q, im = _expand_runs(f, rp, rs, rl, raw, dims, off, den)
+    np.testing.assert_array_equal(q.view(np.uint32), f.query.view(np.uint32))
+    np.testing.assert_array_equal(im.view(np.uint32), f.img.view(np.uint32))
+
+
+def test_frame_expand_runs_never_writes_outside_a_supervoxel(cuda_ok):
+    """A run table that claims more voxels than a supervoxel holds writes nothing past the
+    supervoxel's range: the next supervoxel's voxels and the array ends keep their values."""
+    import torch
+    from tgmm_b200 import engine as E
+    lp = np.array([0, 4, 10], np.int64)
+    rp = np.array([0, 1, 2], np.int32)
+    rs = np.array([100, 500], np.uint32)
+    rl = np.array([9, 6], np.uint16)  # supervoxel 0 holds 4 voxels, the table says 9
+    raw = np.arange(200, 210, dtype=np.uint16)
+    q = torch.full((30,), -1.0, device="cuda")
+    im = torch.full((10,), -1.0, device="cuda")
+    E.expand_runs(torch.from_numpy(rp).cuda(), torch.from_numpy(rs.view(np.int32)).cuda(),
+                  torch.from_numpy(rl.view(np.int16)).cuda(), torch.from_numpy(raw.view(np.int16)).cuda(),
+                  torch.from_numpy(lp).cuda(), (64, 64, 8), 150.0, 100.0, q, im)
+    x = q.cpu().numpy()[:10]
+    np.testing.assert_array_equal(x[:4], [36, 37, 38, 39])   # 100..103 in rows of 64
+    np.testing.assert_array_equal(x[4:], [52, 53, 54, 55, 56, 57])  # supervoxel 1 from 500

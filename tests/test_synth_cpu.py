@@ -100,3 +100,24 @@ def test_bench_reference_arm_never_maps_the_engine():
     line = json.loads(lines[-2])
     assert line["impl"] == "reference" and line["value"] > 0 and line["config"]["em_iterations"] == 20
     assert abs(line["ms_per_step"] - 1e3 / line["value"]) < 1e-6 * line["ms_per_step"]
+
+
+def test_runs_cover_each_supervoxel_in_order():
+    """synth.runs_of: each supervoxel's runs expand to its voxels' linear indices in order; runs
+    never cross a supervoxel boundary and are split at max_len."""
+    f = synth.generate(synth.TINY, seed=3)
+    lin = f.compact()[0].astype(np.int64)
+    for max_len in (65535, 5, 1):
+        rp, rs, rl = synth.runs_of(lin, f.label_ptr, max_len=max_len)
+        assert rp.dtype == np.int32 and rs.dtype == np.uint32 and rl.dtype == np.uint16
+        assert rp[0] == 0 and rp[-1] == rs.shape[0] and rl.max() <= max_len and rl.min() >= 1
+        for s in range(f.n_sv):
+            a, b = f.label_ptr[s], f.label_ptr[s + 1]
+            got = np.concatenate([np.arange(int(x), int(x) + int(n)) for x, n in
+                                  zip(rs[rp[s]:rp[s + 1]], rl[rp[s]:rp[s + 1]])] or [np.zeros(0, np.int64)])
+            np.testing.assert_array_equal(got, lin[a:b])
+    # one long run, an empty supervoxel, a run cut at max_len
+    rp, rs, rl = synth.runs_of(np.arange(200000), np.array([0, 150000, 150000, 200000]))
+    np.testing.assert_array_equal(rp, [0, 3, 3, 4])
+    np.testing.assert_array_equal(rl, [65535, 65535, 18930, 50000])
+    np.testing.assert_array_equal(rs, [0, 65535, 131070, 150000])

@@ -135,6 +135,7 @@ class TgmmServeRequest(C.Structure):
         ("centroids", C.c_void_p), ("label_ptr", C.c_void_p), ("n_vox", C.c_int64), ("n_sv", C.c_int32),
         ("rnk_out", C.c_void_p), ("ind_out", C.c_void_p), ("gm_out", C.c_void_p), ("lin", C.c_void_p),
         ("raw", C.c_void_p), ("dims", C.c_int32 * 3), ("raw_offset", C.c_double), ("raw_denom", C.c_double),
+        ("run_ptr", C.c_void_p), ("run_start", C.c_void_p), ("run_len", C.c_void_p), ("n_runs", C.c_int64),
     ]
 
 
@@ -173,6 +174,8 @@ GMEM_FUNCS = {
     "tgmm_split_proposal": (C.c_int, [_VP, C.POINTER(C.c_float), _VP, _VP]),
     "tgmm_frame_expand": (C.c_int, [_VP, _VP, C.c_int64, C.POINTER(C.c_int32), C.c_double, C.c_double, _VP, _VP,
                                     _VP]),
+    "tgmm_frame_expand_runs": (C.c_int, [_VP, _VP, _VP, _VP, _VP, C.c_int32, C.c_int64, C.c_int64,
+                                         C.POINTER(C.c_int32), C.c_double, C.c_double, _VP, _VP, _VP]),
     "tgmm_split_round": (C.c_int, [_VP, C.POINTER(TgmmFrame), _VP, C.c_int32, _VP, _VP, C.c_int32, _VP, _VP,
                                    C.POINTER(TgmmEmParams), _VP, _VP, C.POINTER(TgmmEmStats), _VP]),
     "tgmm_update_priors": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,

@@ -71,11 +71,21 @@ class Arena {
   std::map<int64_t, int64_t> free_;
 };
 
-// Device bytes of one frame: inputs, outputs and (compact form) the uploaded voxel codes,
-// each 256-byte aligned.
+// How a request's voxels cross to the device: the float arrays, the 6-byte codes, or runs.
+enum class Form { kFloat, kCompact, kRuns };
+
+Form form_of(const TgmmServeRequest& r) {
+  if (!r.query && !r.img && !r.lin && r.raw && r.run_ptr && r.run_start && r.run_len) return Form::kRuns;
+  if (!r.query && !r.img && r.lin && r.raw) return Form::kCompact;
+  return Form::kFloat;
+}
+
+// Device bytes of one frame: inputs, outputs and (compact and run forms) the uploaded voxel
+// codes, each 256-byte aligned.
 struct FrameLayout {
-  int64_t query, img, cent, lptr, rnk, ind, lin, raw, total;
-  FrameLayout(int64_t n_vox, int32_t n_sv, bool compact = false) {
+  int64_t query, img, cent, lptr, rnk, ind, lin = -1, raw = -1, rptr = -1, rstart = -1, rlen = -1, total;
+  FrameLayout(const TgmmServeRequest& r) : FrameLayout(r.n_vox, r.n_sv, form_of(r), r.n_runs) {}
+  FrameLayout(int64_t n_vox, int32_t n_sv, Form form, int64_t n_runs) {
     int64_t o = 0;
     auto take = [&](int64_t b) {
       const int64_t at = o;
@@ -88,13 +98,16 @@ struct FrameLayout {
     lptr = take(8 * ((int64_t)n_sv + 1));
     rnk = take(4 * (int64_t)TGMM_J * n_sv);
     ind = take(4 * (int64_t)TGMM_J * n_sv);
-    lin = compact ? take(4 * n_vox) : -1;
-    raw = compact ? take(2 * n_vox) : -1;
+    if (form == Form::kCompact) lin = take(4 * n_vox);
+    if (form != Form::kFloat) raw = take(2 * n_vox);
+    if (form == Form::kRuns) {
+      rptr = take(4 * ((int64_t)n_sv + 1));
+      rstart = take(4 * n_runs);
+      rlen = take(2 * n_runs);
+    }
     total = o;
   }
 };
-
-bool is_compact(const TgmmServeRequest& r) { return !r.query && !r.img && r.lin && r.raw; }
 
 // Host memory the device can copy into directly (page-locked or registered).
 bool page_locked(const void* p) {
@@ -122,7 +135,97 @@ __global__ void k_expand_frame(const uint32_t* __restrict__ lin, const uint16_t*
   }
 }
 
+// Runs -> the float frame.  A warp per supervoxel s walks its runs rp[s] .. rp[s+1] in groups
+// of 32 (a run per lane): a warp scan of the lengths places each run inside the supervoxel's
+// voxel range lptr[s] .. lptr[s+1], then the lanes write the group's voxels together (voxel j
+// of the group belongs to the run whose scanned end is the first above j), so that the stores
+// are coalesced.  Nothing is written outside the supervoxel's range, whatever the run table
+// says.  Coordinates and intensities as k_expand_frame.
+__global__ void __launch_bounds__(256) k_expand_runs(const int32_t* __restrict__ rp, const uint32_t* __restrict__ rs,
+                                                     const uint16_t* __restrict__ rl, const uint16_t* __restrict__ raw,
+                                                     const int64_t* __restrict__ lptr, int32_t n_sv, int64_t n_runs,
+                                                     int64_t n, uint32_t X, uint32_t Y, double off, double den,
+                                                     float* __restrict__ query, float* __restrict__ img) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < n_sv; s += warps) {
+    const int64_t v0 = lptr[s], v1 = lptr[s + 1];
+    if (v0 < 0 || v1 < v0 || v1 > n) continue;  // an invalid CSR, which the EM reports
+    // runs outside 0 .. n_runs are never read
+    const int64_t r0 = max((int64_t)rp[s], (int64_t)0), r1 = min((int64_t)rp[s + 1], n_runs);
+    int64_t base = v0;
+    for (int64_t r = r0; r < r1 && base < v1; r += 32) {
+      const bool has = r + lane < r1;
+      const int len = has ? (int)rl[r + lane] : 0;
+      const uint32_t st = has ? rs[r + lane] : 0u;
+      int inc = len;  // inclusive scan of the lengths
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      const int total = __shfl_sync(0xffffffffu, inc, 31);
+      for (int j0 = 0; j0 < total; j0 += 32) {
+        const int j = j0 + lane;
+        int m = 0;  // lanes whose run ends at or before voxel j
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int t = __shfl_sync(0xffffffffu, inc, m + step - 1);
+          if (t <= j) m += step;
+        }
+        const int end = __shfl_sync(0xffffffffu, inc, m);
+        const int lm = __shfl_sync(0xffffffffu, len, m);
+        const uint32_t sm = __shfl_sync(0xffffffffu, st, m);
+        const int64_t i = base + j;
+        if (j < total && i < v1) {
+          const uint32_t v = sm + (uint32_t)(j - (end - lm));
+          const uint32_t q = v / X;
+          query[i] = (float)(v - q * X);
+          query[n + i] = (float)(q % Y);
+          query[2 * n + i] = (float)(q / Y);
+          img[i] = (float)(((double)raw[i] - off) / den);
+        }
+      }
+      base += total;
+    }
+  }
+}
+
+int expand_runs(const int32_t* rp, const uint32_t* rs, const uint16_t* rl, const uint16_t* raw, const int64_t* lptr,
+                int32_t n_sv, int64_t n_runs, int64_t n_vox, const int32_t* dims, double off, double den, float* query,
+                float* img, cudaStream_t st) {
+  if (n_sv == 0 || n_vox == 0) return TGMM_OK;
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t blocks = std::min<int64_t>(((int64_t)n_sv + 7) / 8, (int64_t)sms * 8);
+  k_expand_runs<<<(int)blocks, 256, 0, st>>>(rp, rs, rl, raw, lptr, n_sv, n_runs, n_vox, (uint32_t)dims[0],
+                                             (uint32_t)dims[1], off, den, query, img);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return tgmm::report_error(TGMM_ERR_CUDA, "tgmm_frame_expand_runs", e);
+  return TGMM_OK;
+}
+
 }  // namespace
+
+extern "C" int tgmm_frame_expand_runs(const int32_t* run_ptr_dev, const uint32_t* run_start_dev,
+                                      const uint16_t* run_len_dev, const uint16_t* raw_dev,
+                                      const int64_t* label_ptr_dev, int32_t n_sv, int64_t n_runs, int64_t n_vox,
+                                      const int32_t dims[3], double raw_offset, double raw_denom, float* query_dev,
+                                      float* img_dev, void* stream) {
+  if (!dims || n_vox < 0 || n_sv < 0 || n_runs < 0 ||
+      (n_vox > 0 && n_sv > 0 &&
+       (!run_ptr_dev || !run_start_dev || !run_len_dev || !raw_dev || !label_ptr_dev || !query_dev || !img_dev)))
+    return tgmm::report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_expand_runs: null argument or negative size",
+                              cudaSuccess);
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || (int64_t)dims[0] * dims[1] * dims[2] > 0xffffffffLL)
+    return tgmm::report_error(TGMM_ERR_BAD_SIZE, "tgmm_frame_expand_runs: the volume must have 1 .. 2^32 voxels",
+                              cudaSuccess);
+  if (!(raw_denom != 0.0))
+    return tgmm::report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_expand_runs: raw_denom is 0", cudaSuccess);
+  return expand_runs(run_ptr_dev, run_start_dev, run_len_dev, raw_dev, label_ptr_dev, n_sv, n_runs, n_vox, dims,
+                     raw_offset,
+                     raw_denom, query_dev, img_dev, (cudaStream_t)stream);
+}
 
 extern "C" int tgmm_frame_expand(const uint32_t* lin_dev, const uint16_t* raw_dev, int64_t n_vox,
                                  const int32_t dims[3], double raw_offset, double raw_denom, float* query_dev,
@@ -296,7 +399,7 @@ void TgmmServer::launch(Lane& L) {
   int64_t so = 0, go = 0;
   for (int i = 0; i < n && rc == TGMM_OK; i++) {
     Request* q = L.reqs[i];
-    const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
+    const FrameLayout lay(q->r);
     char* base = dev + q->off;
     const int64_t N = q->r.n_vox, S = q->r.n_sv;
     const cudaError_t e = cudaStreamWaitEvent(L.st, q->ready, 0);  // its upload
@@ -395,12 +498,27 @@ void TgmmServer::complete(Lane& L) {
 // Upload of an admitted frame on the copy stream (lock held; the copies are asynchronous
 // from page-locked memory).
 int TgmmServer::upload(Request* q) {
-  const bool cpt = is_compact(q->r);
-  const FrameLayout lay(q->r.n_vox, q->r.n_sv, cpt);
+  const Form form = form_of(q->r);
+  const FrameLayout lay(q->r);
   char* base = dev + q->off;
   const int64_t N = q->r.n_vox, S = q->r.n_sv;
   cudaError_t e = cudaSuccess;
-  if (cpt) {
+  if (form == Form::kRuns) {
+    // the label_ptr the expansion reads goes up first
+    const int64_t R = q->r.n_runs;
+    e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.rptr, q->r.run_ptr, 4 * (S + 1), cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.rstart, q->r.run_start, 4 * R, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.rlen, q->r.run_len, 2 * R, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.raw, q->r.raw, 2 * N, cudaMemcpyHostToDevice, copy);
+    if (e == cudaSuccess &&
+        expand_runs((const int32_t*)(base + lay.rptr), (const uint32_t*)(base + lay.rstart),
+                    (const uint16_t*)(base + lay.rlen), (const uint16_t*)(base + lay.raw),
+                    (const int64_t*)(base + lay.lptr), (int32_t)S, R, N, q->r.dims, q->r.raw_offset, q->r.raw_denom,
+                    (float*)(base + lay.query), (float*)(base + lay.img), copy) != TGMM_OK)
+      e = cudaErrorLaunchFailure;
+    h2d_bytes += 2 * N + 6 * R + 4 * (S + 1);
+  } else if (form == Form::kCompact) {
     e = cudaMemcpyAsync(base + lay.lin, q->r.lin, 4 * N, cudaMemcpyHostToDevice, copy);
     if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.raw, q->r.raw, 2 * N, cudaMemcpyHostToDevice, copy);
     if (e == cudaSuccess && N > 0) {
@@ -419,7 +537,8 @@ int TgmmServer::upload(Request* q) {
     h2d_bytes += 16 * N;
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.cent, q->r.centroids, 12 * S, cudaMemcpyHostToDevice, copy);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, copy);
+  if (e == cudaSuccess && form != Form::kRuns)
+    e = cudaMemcpyAsync(base + lay.lptr, q->r.label_ptr, 8 * (S + 1), cudaMemcpyHostToDevice, copy);
   h2d_bytes += 12 * S + 8 * (S + 1);
   if (e == cudaSuccess) {
     if (free_events.empty()) {
@@ -445,7 +564,7 @@ void TgmmServer::admit() {
       if (q->off < 0) waiting.push_back(q);
   std::sort(waiting.begin(), waiting.end(), [](const Request* a, const Request* b) { return a->seq < b->seq; });
   for (Request* q : waiting) {
-    const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
+    const FrameLayout lay(q->r);
     const int64_t off = arena->alloc(lay.total);
     if (off < 0) break;  // later frames wait behind this one: admission keeps arrival order
     q->off = off;
@@ -471,7 +590,7 @@ void TgmmServer::run() {
         finish(q, TGMM_ERR_INVALID_ARG, nullptr, -1, 0);
         continue;
       }
-      const FrameLayout lay(q->r.n_vox, q->r.n_sv, is_compact(q->r));
+      const FrameLayout lay(q->r);
       if (q->r.n_vox > desc.max_batch_vox || q->r.n_sv > desc.max_batch_sv ||
           it->second.n_gauss > desc.max_batch_gauss) {
         finish(q, TGMM_ERR_BAD_SIZE, nullptr, -1, 0);
@@ -692,11 +811,16 @@ int tgmm_server_read_lineage(TgmmServer* S, int32_t id, TgmmGaussian* gm) {
 
 int tgmm_server_submit(TgmmServer* S, const TgmmServeRequest* r) {
   if (!S || !r) return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: null argument");
-  const bool cpt = is_compact(*r);
-  if ((!cpt && (!r->query || !r->img)) || !r->centroids || !r->label_ptr || r->n_vox < 0 || r->n_sv < 1)
+  const Form form = form_of(*r);
+  if ((form == Form::kFloat && (!r->query || !r->img)) || !r->centroids || !r->label_ptr || r->n_vox < 0 ||
+      r->n_sv < 1)
     return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad frame");
-  if (cpt && (r->dims[0] < 1 || r->dims[1] < 1 || r->dims[2] < 1 || !(r->raw_denom != 0.0)))
-    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad compact frame");
+  if (form != Form::kFloat &&
+      (r->dims[0] < 1 || r->dims[1] < 1 || r->dims[2] < 1 || (int64_t)r->dims[0] * r->dims[1] * r->dims[2] > 0xffffffffLL ||
+       !(r->raw_denom != 0.0)))
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad compact or run frame");
+  if (form == Form::kRuns && (r->n_runs < 0 || r->n_runs > r->n_vox))
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_server_submit: bad run count");
   Request* q = new Request();
   q->r = *r;
   {
@@ -767,10 +891,14 @@ int tgmm_server_selftest(void) {
   check(a.used() == 0 && a.fragments() == 1);  // fully coalesced
   check(a.alloc(10 * kGranule) == 0);
   check(a.peak() == 10 * kGranule);
-  const FrameLayout lay(1000, 10);
-  check(lay.total % kGranule == 0 && lay.img >= 12 * 1000 && lay.ind + 4 * 5 * 10 <= lay.total && lay.lin < 0);
-  const FrameLayout cl(1000, 10, true);
-  check(cl.lin > cl.ind && cl.raw >= cl.lin + 4000 && cl.raw + 2000 <= cl.total);
+  const FrameLayout lay(1000, 10, Form::kFloat, 0);
+  check(lay.total % kGranule == 0 && lay.img >= 12 * 1000 && lay.ind + 4 * 5 * 10 <= lay.total && lay.lin < 0 &&
+        lay.raw < 0 && lay.rptr < 0);
+  const FrameLayout cl(1000, 10, Form::kCompact, 0);
+  check(cl.lin > cl.ind && cl.raw >= cl.lin + 4000 && cl.raw + 2000 <= cl.total && cl.rptr < 0);
+  const FrameLayout rl(1000, 10, Form::kRuns, 300);
+  check(rl.lin < 0 && rl.raw > rl.ind && rl.rptr >= rl.raw + 2000 && rl.rstart >= rl.rptr + 44 &&
+        rl.rlen >= rl.rstart + 1200 && rl.rlen + 600 <= rl.total);
   return bad;
 }
 

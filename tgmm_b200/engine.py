@@ -200,6 +200,19 @@ def expand_frame(lin: torch.Tensor, raw: torch.Tensor, dims, raw_offset: float, 
                                        query.data_ptr(), img.data_ptr(), s), "tgmm_frame_expand")
 
 
+def expand_runs(run_ptr: torch.Tensor, run_start: torch.Tensor, run_len: torch.Tensor, raw: torch.Tensor,
+                label_ptr: torch.Tensor, dims, raw_offset: float, raw_denom: float, query: torch.Tensor,
+                img: torch.Tensor, stream=None):
+    """tgmm_frame_expand_runs: runs (int32 run_ptr, 4-byte run_start, 2-byte run_len) and raw
+    values (2-byte) over the CSR label_ptr into the float query (3*n) and img (n) arrays."""
+    d = (C.c_int32 * 3)(*[int(x) for x in dims])
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    L.check(L.gmem().tgmm_frame_expand_runs(run_ptr.data_ptr(), run_start.data_ptr(), run_len.data_ptr(),
+                                            raw.data_ptr(), label_ptr.data_ptr(), label_ptr.numel() - 1,
+                                            run_start.numel(), raw.numel(), d, float(raw_offset), float(raw_denom),
+                                            query.data_ptr(), img.data_ptr(), s), "tgmm_frame_expand_runs")
+
+
 def local_likelihood(df: DeviceFrame, ind: torch.Tensor, gm_dev: torch.Tensor, lists, stream=None) -> np.ndarray:
     """tgmm_local_likelihood: one FP64 value per supervoxel list (host lists of supervoxel
     indices) under the Gaussians gm_dev (device records) with each supervoxel's candidates

@@ -123,11 +123,14 @@ class Server:
         return g
 
     def submit(self, lineage: int, frame, tag: int, want_rnk: bool = True, want_gauss: bool = True,
-               compact: bool = False, out=None) -> None:
+               compact: bool = False, out=None, runs: bool = False) -> None:
         """frame: an object with query, img, centroids, label_ptr (host arrays of the
         reference layout), e.g. synth.Frame.  With compact=True the voxels go as
         (lin, raw, dims, raw_offset, raw_denom): taken from the frame's attributes of those
-        names when present, else from frame.compact().  The arrays are used in place.
+        names when present, else from frame.compact().  With runs=True they go as runs
+        (run_ptr, run_start, run_len, raw, dims, raw_offset, raw_denom): from the frame's
+        attributes of those names when present, else from frame.runs().  The arrays are used
+        in place.
         out: optional (rnk, ind, gauss) arrays to receive the outputs (page-locked ones are
         written by the device directly)."""
         if tag in self._pending:
@@ -138,7 +141,23 @@ class Server:
         r = L.TgmmServeRequest()
         r.lineage, r.tag = lineage, tag
         r.centroids, r.label_ptr = ce.ctypes.data, lp.ctypes.data
-        if compact:
+        if runs:
+            if hasattr(frame, "run_start"):
+                rp, rs, rl, raw, dims, off, den = (frame.run_ptr, frame.run_start, frame.run_len, frame.raw,
+                                                   frame.dims, frame.raw_offset, frame.raw_denom)
+            else:
+                rp, rs, rl, raw, dims, off, den = frame.runs()
+            rp = np.ascontiguousarray(rp, np.int32)
+            rs = np.ascontiguousarray(rs, np.uint32)
+            rl = np.ascontiguousarray(rl, np.uint16)
+            raw = np.ascontiguousarray(raw, np.uint16)
+            arrs = [rp, rs, rl, raw, ce, lp]
+            r.run_ptr, r.run_start, r.run_len, r.raw = rp.ctypes.data, rs.ctypes.data, rl.ctypes.data, raw.ctypes.data
+            r.n_runs = rs.shape[0]
+            r.dims[:] = list(dims)
+            r.raw_offset, r.raw_denom = off, den
+            r.n_vox = raw.shape[0]
+        elif compact:
             if hasattr(frame, "lin"):
                 lin, raw, dims, off, den = frame.lin, frame.raw, frame.dims, frame.raw_offset, frame.raw_denom
             else:

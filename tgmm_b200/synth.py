@@ -109,6 +109,13 @@ class Frame:
         thr = float(np.float32(self.spec.threshold))
         return lin.astype(np.uint32), self.raw, (X, Y, Z), thr, float(self.max_fg) - thr
 
+    def runs(self):
+        """The frame's voxels as runs (see runs_of): (run_ptr int32 [S+1], run_start uint32,
+        run_len uint16, raw uint16, dims, offset, denominator), about 3 bytes per voxel."""
+        lin, raw, dims, off, den = self.compact()
+        rp, rs, rl = runs_of(lin, self.label_ptr)
+        return rp, rs, rl, raw, dims, off, den
+
     @property
     def n_vox(self):
         return int(self.img.shape[0])
@@ -120,6 +127,28 @@ class Frame:
     @property
     def n_gauss(self):
         return int(self.gauss.shape[0]) if self.gauss is not None else 0
+
+
+def runs_of(lin: np.ndarray, label_ptr: np.ndarray, max_len: int = 65535):
+    """Runs of consecutive linear indices, supervoxel by supervoxel (label_ptr, ascending
+    voxels within each): a run starts at a supervoxel's first voxel, after a gap in the
+    indices, and every max_len voxels.  Returns run_ptr (int32, S+1: the runs of supervoxel s
+    are run_ptr[s] .. run_ptr[s+1]), run_start (uint32) and run_len (uint16)."""
+    lin = np.asarray(lin).astype(np.int64)
+    lp = np.asarray(label_ptr, np.int64)
+    n = lin.shape[0]
+    S = lp.shape[0] - 1
+    start = np.ones(n, bool)
+    start[1:] = lin[1:] != lin[:-1] + 1
+    start[lp[:-1][lp[:-1] < n]] = True
+    # split runs longer than max_len: the position within its run of every voxel
+    idx = np.flatnonzero(start)
+    pos = np.arange(n) - np.repeat(idx, np.diff(np.append(idx, n)))
+    start |= (pos % max_len == 0)
+    idx = np.flatnonzero(start)
+    run_len = np.diff(np.append(idx, n))
+    run_ptr = np.searchsorted(idx, lp, side="left").astype(np.int32)
+    return run_ptr, lin[idx].astype(np.uint32), run_len.astype(np.uint16)
 
 
 def make_frame(spec: VolumeSpec, nuclei: Nuclei, seed: int) -> Frame:
