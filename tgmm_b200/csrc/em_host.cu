@@ -113,6 +113,8 @@ struct TgmmPlan {
   // (max_iter, ll_prec, conditional iterations) -> exec
   std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
   cudaStream_t body_stream = nullptr;  // captures the bodies of the conditional iterations
+  cudaStream_t fork_stream = nullptr;  // the records' branch of a call (fetch, import)
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   // host copy of the tables of the last staged batch
   BatchInfo s_info{};
   std::vector<FrameDesc> s_frames;
@@ -165,6 +167,9 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   if (e == cudaSuccess) e = cudaMallocHost(&P->h_state, sizeof(FrameState) * d->max_frames);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->fork_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->join_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->done_ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     tgmm_plan_destroy(P);
@@ -230,6 +235,9 @@ int tgmm_plan_destroy(TgmmPlan* P) {
   for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   if (P->body_stream) cudaStreamDestroy(P->body_stream);
+  if (P->fork_stream) cudaStreamDestroy(P->fork_stream);
+  if (P->fork_ev) cudaEventDestroy(P->fork_ev);
+  if (P->join_ev) cudaEventDestroy(P->join_ev);
   if (P->done_ev) cudaEventDestroy(P->done_ev);
   if (P->h_state) cudaFreeHost(P->h_state);
   if (P->base) cudaFree(P->base);
@@ -403,9 +411,17 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, bool cond, cudaStream_t s
   DevPlan D = P->dev;
   D.iter = 1;
   launch_build_maps(D, st);
-  launch_import(D, st);
+  // two branches after the frame maps: the Gaussian records (fetched from the caller's
+  // page-locked memory where the descriptor names it, then imported) beside the supervoxel
+  // order and the moment pass, which need no Gaussian; joined before the first kNN/E-step
+  TG_CUDA(cudaEventRecord(P->fork_ev, st), "fork");
+  TG_CUDA(cudaStreamWaitEvent(P->fork_stream, P->fork_ev, 0), "fork");
+  launch_fetch_records(D, P->fork_stream);
+  launch_import(D, P->fork_stream);
+  TG_CUDA(cudaEventRecord(P->join_ev, P->fork_stream), "join");
   launch_order(D, st);
   launch_moments(D, st);
+  TG_CUDA(cudaStreamWaitEvent(st, P->join_ev, 0), "join");
   const bool fp64 = ll_prec == TGMM_LLPREC_FP64;
   const bool fuse = P->fuse_knn && !fp64;
   if (max_iter >= 1) launch_knn_estep(D, st);
@@ -546,9 +562,12 @@ int flags_to_status(int flags) {
 
 extern "C" {
 
-int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
-                      float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params,
-                      TgmmEmStats* stats, void* stream) {
+namespace {
+// tgmm_em_run_batch; gm_src (optional, one per frame) names page-locked host records (their
+// device-mapped addresses) that the call's graph copies into gm_dev first.
+int em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
+                 float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params, TgmmEmStats* stats,
+                 void* stream, const TgmmGaussian* const* gm_src) {
   if (!P || !frames || !gm_dev || !rnk_dev || !ind_dev) return fail(TGMM_ERR_INVALID_ARG, "null argument");
   int rc = validate_params(params);
   if (rc) return rc;
@@ -557,6 +576,8 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
   rc = stage_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params);
   if (rc) return rc;
+  if (gm_src)
+    for (int32_t f = 0; f < n_frames; f++) P->s_frames[f].gm_src = gm_src[f];
   rc = order_after_previous(P, st);
   if (rc) return rc;
   rc = stage_tables(P, st);
@@ -573,6 +594,13 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
     return flags_to_status(fo);
   }
   return TGMM_OK;
+}
+}  // namespace
+
+int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, TgmmGaussian* const* gm_dev,
+                      float* const* rnk_dev, int32_t* const* ind_dev, const TgmmEmParams* params,
+                      TgmmEmStats* stats, void* stream) {
+  return em_run_batch(P, n_frames, frames, gm_dev, rnk_dev, ind_dev, params, stats, stream, nullptr);
 }
 
 int tgmm_plan_set_knn_group(TgmmPlan* P, int32_t lanes) {
@@ -780,20 +808,20 @@ int tgmm_em_run(TgmmPlan* P, const TgmmFrame* frame, TgmmGaussian* gm_host, floa
   if (orc) return orc;
   TgmmGaussian* scratch = (TgmmGaussian*)(P->base + P->L.gm_scratch);
   const size_t bytes = sizeof(TgmmGaussian) * (size_t)frame->n_gauss;
-  // page-locked records are read by the SMs, so that they do not wait behind large uploads
-  // the caller has in flight on the copy engines (e.g. its next frame); others are copied
   cudaPointerAttributes pa;
   const void* mapped = nullptr;
   if (cudaPointerGetAttributes(&pa, gm_host) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer &&
       ((uintptr_t)pa.devicePointer & 15) == 0)
     mapped = pa.devicePointer;
   cudaGetLastError();  // a pageable pointer may leave an error behind on older drivers
-  if (mapped)
-    TG_CUDA(launch_copy_from_host(scratch, mapped, bytes, st), "upload Gaussians");
-  else
-    TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");
+  // page-locked records are read by the call's graph, beside the supervoxel order and the
+  // moment pass (and by the SMs, so not behind uploads the caller has in flight on the copy
+  // engines); others are copied first
+  if (!mapped) TG_CUDA(cudaMemcpyAsync(scratch, gm_host, bytes, cudaMemcpyHostToDevice, st), "upload Gaussians");
+  const TgmmGaussian* src = (const TgmmGaussian*)mapped;
   TgmmEmStats local;
-  int rc = tgmm_em_run_batch(P, 1, frame, &scratch, &rnk_dev, &ind_dev, params, stats ? stats : &local, stream);
+  int rc = em_run_batch(P, 1, frame, &scratch, &rnk_dev, &ind_dev, params, stats ? stats : &local, stream,
+                        mapped ? &src : nullptr);
   if (rc != TGMM_OK && rc != TGMM_ERR_NAN_INPUT) return rc;
   TG_CUDA(cudaMemcpyAsync(gm_host, scratch, bytes, cudaMemcpyDeviceToHost, st), "download Gaussians");
   if (ind_tr_dev) {

@@ -2275,6 +2275,24 @@ static inline int div_up(int a, int b) { return (a + b - 1) / b; }
 void launch_build_maps(const DevPlan& P, cudaStream_t st) {
   k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
 }
+// The caller's page-locked records into the plan's device records, 16 bytes a thread, read
+// by the SMs over the bus (not a copy engine, so they do not queue behind the caller's own
+// uploads), for every frame whose descriptor names a source.
+__global__ void __launch_bounds__(256) k_fetch_records(DevPlan P) {
+  const int nf = P.info->n_frames;
+  for (int f = 0; f < nf; f++) {
+    const FrameDesc& D = P.frames[f];
+    const uint4* src = reinterpret_cast<const uint4*>(D.gm_src);
+    if (!src) continue;
+    uint4* dst = reinterpret_cast<uint4*>(D.gm);
+    const int64_t n16 = (int64_t)D.n_gauss * (int64_t)sizeof(TgmmGaussian) / 16;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16; i += (int64_t)gridDim.x * blockDim.x)
+      dst[i] = src[i];
+  }
+}
+void launch_fetch_records(const DevPlan& P, cudaStream_t st) {
+  k_fetch_records<<<min(P.max_gchunks * (kGChunk * (int)sizeof(TgmmGaussian) / 16 / 256), 148 * 4), 256, 0, st>>>(P);
+}
 void launch_import(const DevPlan& P, cudaStream_t st) { k_import<<<P.max_gchunks, kGChunk, 0, st>>>(P); }
 void launch_order(const DevPlan& P, cudaStream_t st) {
   k_sv_records<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
@@ -2313,23 +2331,6 @@ void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) 
     k_ll_pass<false, 32, false><<<grid, bs, kLLSmemBytes, st>>>(P);
   else
     k_ll_pass<false, 0, false><<<grid, bs, kLLSmemBytes, st>>>(P);
-}
-
-// Page-locked host memory read by the SMs (16 bytes a thread, coalesced) into device memory.
-// A copy engine processes its copies in order, so a small upload issued behind a large one on
-// another stream waits for it; reads issued by a kernel do not queue behind those copies.
-__global__ void __launch_bounds__(256) k_copy_from_host(uint4* __restrict__ dst, const uint4* __restrict__ src,
-                                                        size_t n16) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
-    dst[i] = src[i];
-}
-
-cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st) {
-  const size_t n16 = bytes / 16;
-  if (n16 == 0) return cudaSuccess;
-  const int blocks = (int)std::min<size_t>((n16 + 255) / 256, 148 * 4);
-  k_copy_from_host<<<blocks, 256, 0, st>>>((uint4*)dst, (const uint4*)src_mapped, n16);
-  return cudaGetLastError();
 }
 
 // Host tables reach the device as launch parameters of k_stage (24 KB a launch), so staging

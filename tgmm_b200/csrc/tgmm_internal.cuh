@@ -77,6 +77,9 @@ struct FrameDesc {
   const float* cent;
   const int64_t* lptr;
   TgmmGaussian* gm;  // device AoS records of this frame
+  // the caller's page-locked host records (their device-mapped address), copied into gm by
+  // the call's graph beside the voxel work; nullptr when gm already holds the records
+  const TgmmGaussian* gm_src;
   float* rnk_out;    // device, 5*n_sv, slot-major
   int32_t* ind_out;  // device, 5*n_sv, slot-major, frame-local Gaussian ids
   int64_t n_vox;
@@ -250,6 +253,7 @@ __device__ __forceinline__ float* rnk_buf(const DevPlan& P, int it) {
 
 // ---- kernel launchers (em_kernels.cu) ----
 void launch_build_maps(const DevPlan& P, cudaStream_t st);
+void launch_fetch_records(const DevPlan& P, cudaStream_t st);
 void launch_import(const DevPlan& P, cudaStream_t st);
 void launch_order(const DevPlan& P, cudaStream_t st);
 void launch_moments(const DevPlan& P, cudaStream_t st);
@@ -264,9 +268,6 @@ cudaError_t configure_kernels(DevPlan& P, int device);
 // parameters (the tail up to the next 16 bytes is written with zeros)
 cudaError_t launch_stage_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 void launch_export(const DevPlan& P, cudaStream_t st);
-// bytes (a multiple of 16) from page-locked host memory (its device-mapped address, 16-byte
-// aligned) to device memory, read by a kernel rather than a copy engine
-cudaError_t launch_copy_from_host(void* dst, const void* src_mapped, size_t bytes, cudaStream_t st);
 
 // standalone kNN (tgmm_knn): brute force over refs in shared memory tiles
 cudaError_t knn_bruteforce(const float* query, int64_t nq, const float* ref_xyz, int32_t nref,
