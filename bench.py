@@ -507,7 +507,8 @@ def run_e2e(frame, df, plan, params, dev, args, form="runs"):
     """End to end through the C ABI with host buffers, every step: the frame's upload from
     page-locked memory, tgmm_em_run (its Gaussians up and down inside), rnk/ind down.  The
     upload of step i + 1 runs on a copy stream into the other of two buffers while step i's EM
-    runs, so a step costs the slower of the two.  form "runs": the voxels cross as runs of
+    runs (the expansion of a compact form runs there too), so a step costs the slower of the
+    two.  form "runs": the voxels cross as runs of
     consecutive linear indices (uint32 start, uint16 length, per supervoxel int32 run pointers)
     and uint16 raw values, about 3 bytes a voxel, and tgmm_frame_expand_runs rebuilds the float
     arrays on the device; "compact": 6 bytes a voxel (uint32 linear index, uint16 raw value)
@@ -533,8 +534,10 @@ def run_e2e(frame, df, plan, params, dev, args, form="runs"):
         host = {"query": pinned(frame.query), "img": pinned(frame.img)}
     host.update(centroids=pinned(frame.centroids), label_ptr=pinned(frame.label_ptr))
     bufs = [{k: torch.empty_like(v, device=dev) for k, v in host.items()} for _ in range(2)]
-    q = df.query if compact else None
-    im = df.img if compact else None
+    if compact:  # the expanded float arrays, one pair per buffer
+        for b in bufs:
+            b["query"] = torch.empty_like(df.query)
+            b["img"] = torch.empty_like(df.img)
     rnk_h = torch.empty(5 * S, dtype=torch.float32).pin_memory()
     ind_h = torch.empty(5 * S, dtype=torch.int32).pin_memory()
     rnk = torch.empty(5 * S, dtype=torch.float32, device=dev)
@@ -550,11 +553,17 @@ def run_e2e(frame, df, plan, params, dev, args, form="runs"):
     d2h = 288 * K + 8 * 5 * S
 
     def upload(i):
+        """Step i's frame into buffer i % 2 on the copy stream, expanded there on the device."""
         b = bufs[i % 2]
         with torch.cuda.stream(cs):
             cs.wait_event(used[i % 2])  # the EM that read this buffer two steps ago is done
             for k, v in host.items():
                 b[k].copy_(v, non_blocking=True)
+            if form == "runs":
+                E.expand_runs(b["run_ptr"], b["run_start"], b["run_len"], b["raw"], b["label_ptr"], dims, off, den,
+                              b["query"], b["img"], stream=cs)
+            elif form == "compact":
+                E.expand_frame(b["lin"], b["raw"], dims, off, den, b["query"], b["img"], stream=cs)
             up[i % 2].record(cs)
 
     def run(n):
@@ -570,15 +579,7 @@ def run_e2e(frame, df, plan, params, dev, args, form="runs"):
                 upload(i + 1)
             b = bufs[i % 2]
             comp.wait_event(up[i % 2])
-            if form == "runs":
-                E.expand_runs(b["run_ptr"], b["run_start"], b["run_len"], b["raw"], b["label_ptr"], dims, off, den, q,
-                              im, stream=comp)
-                f = E.DeviceFrame(q, im, b["centroids"], b["label_ptr"], K)
-            elif compact:
-                E.expand_frame(b["lin"], b["raw"], dims, off, den, q, im, stream=comp)
-                f = E.DeviceFrame(q, im, b["centroids"], b["label_ptr"], K)
-            else:
-                f = E.DeviceFrame(b["query"], b["img"], b["centroids"], b["label_ptr"], K)
+            f = E.DeviceFrame(b["query"], b["img"], b["centroids"], b["label_ptr"], K)
             cf = f.cframe()
             L.check(lib.tgmm_em_run(plan.h, C.byref(cf), gs[i].data_ptr(), rnk.data_ptr(), ind.data_ptr(), None,
                                     C.byref(params), C.byref(st), comp.cuda_stream), "tgmm_em_run")
