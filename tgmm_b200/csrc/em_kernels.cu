@@ -797,9 +797,11 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   static_assert(G >= kJ && G <= 32 && (G & (G - 1)) == 0, "a group holds the five candidates");
   // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
-  // what needs only s goes out first, ahead of the frame's state and descriptor: the list
-  // member of this lane and the list's bound, and (into L1) the moments the E-step reads
-  const int f = P.sv_frame[s];
+  // what needs only s goes out first, ahead of the frame's state and descriptor: the
+  // supervoxel's stream record (frame, centroid, voxel count), the list member of this lane
+  // (a global Gaussian index, so that its centre loads beside the frame's state) and the
+  // list's bound, and (into L1) the moments the E-step reads
+  const SvLL R = P.sv_ll[s];
   int lk = 0x7fffffff;
   double nbr_bound = 0.0;
   if (it > 1) {
@@ -808,13 +810,15 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   }
   if (gl < 9) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)(M_E0 + gl) * P.max_sv + s));
   if (G == 8 && gl == 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)M_EE22 * P.max_sv + s));
+  const int f = R.frame;
+  float4 lpos = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (it > 1 && gl < kNbr && lk != 0x7fffffff) lpos = P.kpos[lk];
   const FrameState& S = P.state[f];
   if (*(volatile const int32_t*)&S.done) return;
   const FrameDesc D = load_desc(P, f);
   const int sl = s - D.sv_base;
   const int Sf = D.n_sv;
-  const float q0 = D.cent[sl], q1 = D.cent[(int64_t)Sf + sl], q2 = D.cent[2 * (int64_t)Sf + sl];
-  const int64_t p0 = D.lptr[sl], p1 = D.lptr[sl + 1];
+  const float q0 = R.c0, q1 = R.c1, q2 = R.c2;  // the frame's centroid of s, as the E-step reads it
   GridGeom g;
   for (int d = 0; d < 3; d++) {
     g.lo[d] = S.lo[d];
@@ -836,10 +840,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   float ld = kInfF;
   bool have = false;
   if (it > 1) {
-    if (gl < kNbr && lk != 0x7fffffff) {
-      const float4 r = P.kpos[D.g_base + lk];
-      ld = knn_dist(q0, q1, q2, r.x, r.y, r.z, D.scale);
-    }
+    if (gl < kNbr && lk != 0x7fffffff) ld = knn_dist(q0, q1, q2, lpos.x, lpos.y, lpos.z, D.scale);
     Top5 mine;
     top5_init(mine);
     mine.d[0] = ld;
@@ -856,7 +857,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
       int ij = gl < kNbr ? lk : -1;
       group_max_pair<G>(dj, ij, gmask);
       td0 = dj;
-      ti0 = ij;
+      ti0 = ij >= 0 && ij != 0x7fffffff ? ij - D.g_base : ij;  // the search's frame-local order
       if (gl == 0) atomicAdd(&P.state[f].knn_searches, 1);
     }
     TopN<kNbr> nb;
@@ -877,27 +878,28 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
       }
       group_merge_topn<G, kNbr>(m, nb, gmask);
     }
+    // (frame-local indices from the search; global ones from here on)
 #pragma unroll
     for (int j = 0; j < kJ; j++) {
       t.d[j] = nb.d[j];
-      t.i[j] = nb.i[j];
+      t.i[j] = nb.i[j] == 0x7fffffff ? nb.i[j] : D.g_base + nb.i[j];
     }
     int mi = 0x7fffffff;
 #pragma unroll
     for (int q = 0; q < kNbr; q++)
       if (gl == q) mi = nb.i[q];
-    if (gl < kNbr) P.nbr[(int64_t)s * kNbr + gl] = mi;
+    if (gl < kNbr) P.nbr[(int64_t)s * kNbr + gl] = mi == 0x7fffffff ? mi : D.g_base + mi;
     if (gl == 0)
       P.nbr_b[s] = nb.d[kNbr - 1] < kInfF ? sqrt((double)nb.d[kNbr - 1]) * (1.0 - 1e-6) - 4e-3 + disp : (double)kInfF;
   }
-  // E-step: candidate j on lane j of the group
+  // E-step: candidate j on lane j of the group (its voxel count: 0 for an invalid range, which
+  // flags the frame)
   const int par = it & 1;
-  const double n = (p0 >= 0 && p1 >= p0 && p1 <= D.n_vox) ? (double)(p1 - p0) : 0.0;
-  int kl = 0;
+  const double n = (double)R.nv;
+  int k = 0;
 #pragma unroll
   for (int j = 0; j < kJ; j++)
-    if (gl == j) kl = t.i[j];
-  const int k = D.g_base + kl;
+    if (gl == j) k = t.i[j];
   double Lj = 0.0;
   if (gl < kJ && n != 0.0) {
     const double* E = P.ec + (int64_t)k * kEcStride;
@@ -1411,6 +1413,10 @@ __device__ __forceinline__ double voxel_ll_fp64(const LLShared64& C, float x0, f
 #ifndef TGMM_LL_BLOCKS
 #define TGMM_LL_BLOCKS 2
 #endif
+#ifndef TGMM_LL_WARPS
+#define TGMM_LL_WARPS 8
+#endif
+constexpr int kLLWarps = TGMM_LL_WARPS;       // warps per block of the voxel pass
 constexpr int kLLTile = kVoxTile;             // voxels per tile (kVoxTile / 32 per lane)
 constexpr int kLLStages = TGMM_LL_STAGES;     // tile slots per warp
 constexpr int kLLBlocks = TGMM_LL_BLOCKS;     // resident blocks per SM the pass is compiled for
@@ -1526,7 +1532,7 @@ constexpr int kLLRecOff = (kLLBarOff + kLLStages * 8 + 15) / 16 * 16;
 constexpr int kLLConstOff = kLLRecOff + 3 * (int)sizeof(LLRec);
 constexpr int kLLCandOff = kLLConstOff + 2 * (int)sizeof(LLConst);
 constexpr int kLLWarpBytes = (kLLCandOff + (int)sizeof(CandF) + 15) / 16 * 16;
-constexpr size_t kLLSmemBytes = (size_t)kLLWarpBytes * kWarpsPerBlockV;
+constexpr size_t kLLSmemBytes = (size_t)kLLWarpBytes * kLLWarps;
 static_assert((kLLSlotFloats * 4) % 16 == 0 && kLLRecOff % 16 == 0 && kLLConstOff % 16 == 0 && kLLCandOff % 16 == 0,
               "slots and records stay 16-byte aligned");
 // the FP32 forms keep kLLBlocks blocks on an SM (228 KB of shared memory, 1 KB reserved per
@@ -1888,7 +1894,7 @@ __device__ void frame_converge(const DevPlan& P, int f) {
 // buffers, so it runs ahead of the convergence test; a frame that converges here never
 // reads them.
 template <bool kFp64, int G, bool kMom>
-__global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(DevPlan P) {
+__global__ void __launch_bounds__(kLLWarps * 32, kLLBlocks) k_ll_pass(DevPlan P) {
   // the FP32 log-likelihood streams the centred voxel stream (one float4 per voxel, one bulk
   // copy per tile); the moment pass reads the input arrays (and writes that stream), the FP64
   // log-likelihood reads the input arrays too (its terms start from the exact x - c)
@@ -1896,7 +1902,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
   constexpr bool kRec = !kAos, kLLr = kAos || kMom, kCand = !kMom;
   const int total = P.info->total_sv;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __shared__ LLShared64 sh64[kFp64 ? kWarpsPerBlockV : 1];
+  __shared__ LLShared64 sh64[kFp64 ? kLLWarps : 1];
   extern __shared__ __align__(128) unsigned char ll_smem[];
   unsigned char* wbase = ll_smem + (size_t)warp * kLLWarpBytes;
   float* wbuf = reinterpret_cast<float*>(wbase);
@@ -2152,7 +2158,7 @@ __global__ void __launch_bounds__(kWarpsPerBlockV * 32, kLLBlocks) k_ll_pass(Dev
   cp_wait_all();
   publish();
   while (knn_more) knn_step();
-  if (lane == 0 && atomicAdd(&P.work[1], 1) == (int)(gridDim.x * kWarpsPerBlockV) - 1) {
+  if (lane == 0 && atomicAdd(&P.work[1], 1) == (int)(gridDim.x * kLLWarps) - 1) {
     P.work[0] = 0;
     P.work[1] = 0;
     P.work[2] = 0;
@@ -2300,7 +2306,7 @@ void launch_order(const DevPlan& P, cudaStream_t st) {
   k_order_scatter<<<div_up(P.max_sv, 256), 256, 0, st>>>(P);
 }
 void launch_moments(const DevPlan& P, cudaStream_t st) {
-  k_ll_pass<false, 0, true><<<P.ll_blocks, kWarpsPerBlockV * 32, kLLSmemBytes, st>>>(P);
+  k_ll_pass<false, 0, true><<<P.ll_blocks, kLLWarps * 32, kLLSmemBytes, st>>>(P);
 }
 void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
   const int G = P.knn_group;
@@ -2320,7 +2326,7 @@ void launch_kill_prep(const DevPlan& P, cudaStream_t st) {
 }
 void launch_ll_pass(const DevPlan& P, int fp64, int knn_group, cudaStream_t st) {
   const int grid = P.ll_blocks;
-  const int bs = kWarpsPerBlockV * 32;
+  const int bs = kLLWarps * 32;
   if (fp64)
     k_ll_pass<true, 0, false><<<P.ll_blocks64, bs, kLLSmemBytes, st>>>(P);
   else if (knn_group == 8)
@@ -2376,7 +2382,7 @@ cudaError_t configure_kernels(DevPlan& P, int device) {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(forms[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLLSmemBytes);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, forms[i], kWarpsPerBlockV * 32, kLLSmemBytes);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, forms[i], kLLWarps * 32, kLLSmemBytes);
     int& m = i < 5 ? per : per64;
     m = p < m ? p : m;
   }
