@@ -42,7 +42,15 @@ __device__ __forceinline__ int warp_sum_i(int v) {
 __device__ __forceinline__ double warp_sum_range(const double* a, int base, int n) {
   const int lane = threadIdx.x & 31;
   double s = 0.0;
-  for (int i = lane; i < n; i += 32) s += a[base + i];
+  int i = lane;
+  for (; i + 96 < n; i += 128) {  // four loads in flight, added in the same order
+    const double a0 = a[base + i], a1 = a[base + i + 32], a2 = a[base + i + 64], a3 = a[base + i + 96];
+    s += a0;
+    s += a1;
+    s += a2;
+    s += a3;
+  }
+  for (; i < n; i += 32) s += a[base + i];
   return warp_sum(s);
 }
 
