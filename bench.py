@@ -289,7 +289,7 @@ def run_reference_frames(args):
     import torch
     from oracle import oracle as O
     spec = fb_spec(args)
-    raw, lab, S, Nfg, _ = fb_volume(spec, args.seed, torch.device("cpu"))
+    raw, lab, S, Nfg, _, _ = fb_volume(spec, args.seed, torch.device("cpu"))
     X, Y, Z = spec.dims
     raw_n = raw.numpy().view(np.uint16).reshape(Z, Y, X)
     lab_n = lab.numpy().view(np.uint32).reshape(Z, Y, X)
@@ -910,7 +910,9 @@ def fb_volume(spec, seed, device):
     """A synthetic frame's supervoxels scattered into full volumes on the device: the raw
     image (background 100-129, the frame's foreground values) and the label volume (its
     supervoxels, 1-based).  Returns (raw int16, label int32, n_labels, labelled voxels,
-    summed bounding-box voxels)."""
+    summed bounding-box voxels, lists): lists holds the same segmentation as per-supervoxel
+    pixel lists on the device (lin int32 bits of uint32 indices, val int16 bits of the raw
+    values, ptr int64), the form tgmm_frame_build_lists reads."""
     import torch
     from tgmm_b200 import synth
     fr = synth.make_frame(spec, synth.random_nuclei(spec, seed), seed)
@@ -933,7 +935,9 @@ def fb_volume(spec, seed, device):
     lab = torch.zeros(nvol, dtype=torch.int32, device=device)
     lab[lin] = torch.repeat_interleave(torch.arange(1, S + 1, device=device, dtype=torch.int32),
                                        torch.from_numpy(np.diff(lp)).to(device))
-    return raw, lab, S, N, box
+    lists = {"lin": lin.to(torch.int32), "val": raw[lin].clone(),
+             "ptr": torch.from_numpy(np.ascontiguousarray(lp, np.int64)).to(device)}
+    return raw, lab, S, N, box, lists
 
 
 def run_frames(args):
@@ -948,7 +952,7 @@ def run_frames(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     spec = fb_spec(args)
-    raw, lab, S, Nfg, box = fb_volume(spec, args.seed + rank, dev)
+    raw, lab, S, Nfg, box, lists = fb_volume(spec, args.seed + rank, dev)
     X, Y, Z = spec.dims
     nvol = X * Y * Z
     b = E.FrameBuilder((X, Y, Z), S, device=dev, max_vox=Nfg)
@@ -999,6 +1003,55 @@ def run_frames(args):
         e2e = {"value": world * args.steps / (float(te.item()) / 1e3), "unit": "volumes/s",
                "h2d_bytes_per_step": 6 * nvol, "d2h_bytes_per_step": 64,
                "path": "pinned raw + label upload, then tgmm_frame_build (reads its sizes back)"}
+    # the same segmentation as per-supervoxel pixel lists (the tracking program's form): no
+    # volume on the device, so no scan; outputs compared with the volume form's
+    ql, il = f.query.clone(), f.img.clone()
+    lin_d, val_d, ptr_d = lists["lin"], lists["val"], lists["ptr"]
+    for _ in range(args.warmup):
+        b.build_lists(lin_d, val_d, ptr_d, read_thr=False)
+    lstages = []
+    for _ in range(3):
+        ms = []
+        fl, _ = b.build_lists(lin_d, val_d, ptr_d, stage_ms=ms, read_thr=False)
+        lstages.append(ms)
+    same_lists = bool(fl.n_vox == f.n_vox and torch.equal(fl.query, ql) and torch.equal(fl.img, il))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.build_lists(lin_d, val_d, ptr_d, read_thr=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tl = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tl, op=dist.ReduceOp.MAX)
+    lists_line = {"value": world * args.steps / (float(tl.item()) / 1e3), "unit": "volumes/s",
+                  "stage_ms": dict(zip(["clear+init", "k_fbl_boxes", "(no CSR step)", "(no grouping step)", "k_fb_trim",
+                                        "k_fb_order", "k_fb_csr", "k_fb_emit"],
+                                       [round(float(x), 4) for x in np.mean(np.array(lstages), axis=0)])),
+                  "same_outputs_as_volume_form": same_lists,
+                  "path": "tgmm_frame_build_lists: per-supervoxel pixel lists (uint32 linear indices, uint16 raw "
+                          "values, int64 CSR) resident"}
+    if not args.no_e2e:
+        host = {k: v.cpu().pin_memory() for k, v in lists.items()}
+        for _ in range(2):
+            for k in host:
+                lists[k].copy_(host[k], non_blocking=True)
+            b.build_lists(lin_d, val_d, ptr_d, read_thr=False)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            for k in host:
+                lists[k].copy_(host[k], non_blocking=True)
+            b.build_lists(lin_d, val_d, ptr_d, read_thr=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        lists_line["e2e"] = {"value": world * args.steps / (float(te.item()) / 1e3), "unit": "volumes/s",
+                             "h2d_bytes_per_step": sum(int(v.numel() * v.element_size()) for v in host.values()),
+                             "d2h_bytes_per_step": 64,
+                             "path": "pinned pixel-list upload, then tgmm_frame_build_lists (reads its sizes back)"}
     # roofline of the dominant step, from the events between the steps
     algo = {"k_fb_scan": 4 * nvol, "k_fb_group": 4 * box + 8 * Nfg,
             "k_fb_emit": 6 * Nfg + 16 * f.n_vox}
@@ -1055,7 +1108,7 @@ def run_frames(args):
                            "n_vox_out": f.n_vox, "n_sv_out": f.n_sv, "l2": "inputs larger than L2"},
                 "stage_ms": dict(zip(FB_STAGES, [round(float(x), 4) for x in stage])),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
-                "gpu_launches": 8 * args.steps}
+                "gpu_launches": 8 * args.steps, "pixel_lists": lists_line}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

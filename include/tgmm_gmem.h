@@ -329,6 +329,28 @@ int tgmm_frame_build_timed(const uint16_t* raw_dev, const uint32_t* label_dev,
                            uint16_t* thr_dev, int64_t max_vox, int32_t max_sv, int64_t* n_vox,
                            int32_t* n_sv, void* stream, float* stage_ms);
 
+/* The same build from the segmentation as per-supervoxel pixel lists, the form the tracking
+ * program holds it in (supervoxel::PixelIdxList, temporalLogicalRules/supervoxel.h:72; the
+ * lists main:553-651 trims), so that no volume crosses to the device: supervoxel s
+ * (label s+1 of tgmm_frame_build) is lin[lists_ptr[s] .. lists_ptr[s+1]) (uint32 linear
+ * indices, x fastest, strictly ascending, inside the volume; the lists disjoint) with the raw
+ * values val[...] of those voxels (uint16).  lists_ptr: n_labels + 1 int64 on the device, 0 ..
+ * n_list.  Outputs, their sizes and the status codes as tgmm_frame_build, bit for bit the same
+ * arrays for the same segmentation; a list that is not ascending, leaves the volume or a CSR
+ * outside 0 .. n_list gives TGMM_ERR_DEVICE_FLAG.  A flood that leaves shared memory (box above
+ * 65536 voxels) finds a neighbour in the supervoxel's own list by binary search, as the
+ * reference's lower_bound does.  workspace: tgmm_frame_build_lists_bytes(dims, n_labels,
+ * n_list) bytes.  stage_ms (optional, host): TGMM_FRAME_BUILD_STAGES step times as
+ * tgmm_frame_build_timed's (the scan's place holds the lists' check and boxes; no CSR or
+ * grouping step).  Synchronous on `stream` (the sizes are read back). */
+int64_t tgmm_frame_build_lists_bytes(const int32_t dims[3], int32_t n_labels, int64_t n_list);
+int tgmm_frame_build_lists(const uint32_t* lin_dev, const uint16_t* val_dev, const int64_t* lists_ptr_dev,
+                           int64_t n_list, const int32_t dims[3], int32_t n_labels,
+                           const TgmmFrameBuildParams* p, void* workspace_dev, int64_t workspace_bytes,
+                           float* query_dev, float* img_dev, float* centroids_dev, int64_t* label_ptr_dev,
+                           uint16_t* thr_dev, int64_t max_vox, int32_t max_sv, int64_t* n_vox, int32_t* n_sv,
+                           void* stream, float* stage_ms);
+
 /* A frame's voxels in compact form (6 bytes a voxel instead of 16) expanded on the device into
  * the float arrays the EM reads: lin[v] = x + X (y + Y z) (uint32) gives query (x block, y
  * block, z block; query[3*n_vox]) and raw[v] (uint16) gives img[v] =

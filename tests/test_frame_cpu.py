@@ -313,3 +313,42 @@ def _check_frame_build_refusals():
     d = (C.c_int32 * 3)(4, 4, 4)
     assert lib.tgmm_frame_build_timed(fake, fake, d, 10, C.byref(p), fake, ws, fake, fake, fake, fake, None, 1, 1,
                                       C.byref(nv), C.byref(ns), None, None) == L.TGMM_ERR_INVALID_ARG
+
+
+def test_abi_list_build_refuses_bad_arguments_without_a_gpu():
+    """Every argument check of tgmm_frame_build_lists happens on the host before any device work."""
+    _without_a_device("_check_list_build_refusals")
+
+
+def _check_list_build_refusals():
+    lib = L.gmem()
+    p = L.TgmmFrameBuildParams()
+    lib.tgmm_frame_build_default_params(C.byref(p))
+    nv, ns = C.c_int64(0), C.c_int32(0)
+    fake = C.c_void_p(4096)  # never dereferenced: each call below is refused first
+    ws = 1 << 40
+    ms = (C.c_float * L.TGMM_FRAME_BUILD_STAGES)()
+
+    def call(dims, n=10, n_list=50, lin=fake, ptr=fake, params=p, max_vox=1, max_sv=1, wsb=ws):
+        d = (C.c_int32 * 3)(*dims)
+        return lib.tgmm_frame_build_lists(lin, fake, ptr, n_list, d, n, C.byref(params), fake, wsb, fake, fake, fake,
+                                          fake, None, max_vox, max_sv, C.byref(nv), C.byref(ns), None, ms)
+
+    assert call((0, 4, 4)) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), n=0) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), n_list=-1) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), lin=None) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), ptr=None) == L.TGMM_ERR_INVALID_ARG
+    assert call((4096, 4096, 256)) == L.TGMM_ERR_BAD_SIZE            # 2^32 voxels
+    assert call((4, 4, 4), n_list=65) == L.TGMM_ERR_BAD_SIZE          # more entries than voxels
+    assert call((4, 4, 4), n=(1 << 24) + 1) == L.TGMM_ERR_BAD_SIZE
+    bad = L.TgmmFrameBuildParams(p.max_nuclei_size, 1.5, p.conn3d, p.min_nuclei_size)
+    assert call((4, 4, 4), params=bad) == L.TGMM_ERR_INVALID_ARG
+    bad = L.TgmmFrameBuildParams(p.max_nuclei_size, p.max_percentile, 5, p.min_nuclei_size)
+    assert call((4, 4, 4), params=bad) == L.TGMM_ERR_INVALID_ARG
+    assert call((4, 4, 4), max_sv=-1) == L.TGMM_ERR_INVALID_ARG
+    need = lib.tgmm_frame_build_lists_bytes((C.c_int32 * 3)(4, 4, 4), 10, 50)
+    assert need > 0
+    assert call((4, 4, 4), n_list=50, wsb=need - 1) == L.TGMM_ERR_BAD_SIZE
+    assert b"workspace" in lib.tgmm_last_error()
+    assert lib.tgmm_frame_build_lists_bytes((C.c_int32 * 3)(4, 4, 4), 10, -1) == -1

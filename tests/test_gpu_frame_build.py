@@ -157,3 +157,68 @@ def test_em_on_the_built_frame_is_the_em_on_the_oracles_arrays(cuda_ok):
         rows = np.flatnonzero((x.view(np.uint8).reshape(x.shape[0], -1) !=
                                y.view(np.uint8).reshape(y.shape[0], -1)).any(axis=1))
         assert rows.size == 0, (name, rows[:10].tolist(), x[rows[:3]], y[rows[:3]])
+
+
+def _lists(raw, lab, n):
+    """The segmentation as the tracking program holds it: per supervoxel its voxels' linear
+    indices, ascending (PixelIdxList), with their raw values."""
+    ptr, lin = O.supervoxel_lists(lab, n)
+    return ptr.astype(np.int64), lin.astype(np.uint32), raw.reshape(-1)[lin.astype(np.int64)].astype(np.uint16)
+
+
+def list_build(raw, lab, n, c):
+    import torch
+    from tgmm_b200 import engine as E
+    Z, Y, X = raw.shape
+    b = E.FrameBuilder((X, Y, Z), n, max_nuclei_size=c["max_size"], max_percentile=c["max_pct"], conn3d=c["conn"],
+                       min_nuclei_size=c["min_size"])
+    ptr, lin, val = _lists(raw, lab, n)
+    f, thr = b.build_lists(torch.from_numpy(lin.view(np.int32)).cuda(), torch.from_numpy(val.view(np.int16)).cuda(),
+                           torch.from_numpy(ptr).cuda())
+    torch.cuda.synchronize()
+    return f, thr
+
+
+@pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
+def test_list_build_is_the_oracles(cuda_ok, case):
+    """tgmm_frame_build_lists (the segmentation as per-supervoxel pixel lists, no volume on the
+    device) gives the oracle's arrays bit for bit, as the volume form does; the last volume
+    holds a supervoxel whose box exceeds the shared-memory flood (binary search in its list)."""
+    c = _params(case)
+    raw, lab, n = _volume(case)
+    rc, o = O.frame_build(raw, lab, n, O.frame_params(c["max_size"], c["max_pct"], c["conn"], c["min_size"]))
+    assert rc == 0
+    f, thr = list_build(raw, lab, n, c)
+    assert (f.n_vox, f.n_sv) == (o["n_vox"], o["n_sv"])
+    np.testing.assert_array_equal(f.query.cpu().numpy().view(np.uint32), o["query"].view(np.uint32))
+    np.testing.assert_array_equal(f.img.cpu().numpy().view(np.uint32), o["img"].view(np.uint32))
+    np.testing.assert_array_equal(f.centroids.cpu().numpy().view(np.uint32), o["cent"].view(np.uint32))
+    np.testing.assert_array_equal(f.label_ptr.cpu().numpy(), o["lptr"])
+    np.testing.assert_array_equal(thr, o["thr"])
+
+
+def test_list_build_refuses_lists_out_of_order(cuda_ok):
+    """A list that is not ascending, or leaves the volume, is refused (TGMM_ERR_DEVICE_FLAG),
+    and the builder works afterwards."""
+    import torch
+    from tgmm_b200 import _lib as L
+    from tgmm_b200 import engine as E
+    raw, lab, n = _volume(dict(seed=1))
+    Z, Y, X = raw.shape
+    ptr, lin, val = _lists(raw, lab, n)
+    b = E.FrameBuilder((X, Y, Z), n)
+    for bad in ("swap", "outside"):
+        l2 = lin.copy()
+        a = int(ptr[3])
+        if bad == "swap":
+            l2[a], l2[a + 1] = l2[a + 1], l2[a]
+        else:
+            l2[a] = X * Y * Z + 5
+        with pytest.raises(L.TgmmError) as ei:
+            b.build_lists(torch.from_numpy(l2.view(np.int32)).cuda(), torch.from_numpy(val.view(np.int16)).cuda(),
+                          torch.from_numpy(ptr).cuda())
+        assert ei.value.code == L.TGMM_ERR_DEVICE_FLAG
+    f, _ = b.build_lists(torch.from_numpy(lin.view(np.int32)).cuda(), torch.from_numpy(val.view(np.int16)).cuda(),
+                         torch.from_numpy(ptr).cuda())
+    rc, o = O.frame_build(raw, lab, n)
+    np.testing.assert_array_equal(f.img.cpu().numpy().view(np.uint32), o["img"].view(np.uint32))

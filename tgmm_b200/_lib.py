@@ -188,6 +188,10 @@ GMEM_FUNCS = {
     "tgmm_knn_k": (C.c_int, [_VP, C.c_int64, _VP, C.c_int32, C.c_int32, C.POINTER(C.c_float), _VP, _VP, _VP]),
     "tgmm_frame_build_default_params": (None, [C.POINTER(TgmmFrameBuildParams)]),
     "tgmm_frame_build_bytes": (C.c_int64, [_VP, C.c_int32]),
+    "tgmm_frame_build_lists_bytes": (C.c_int64, [_VP, C.c_int32, C.c_int64]),
+    "tgmm_frame_build_lists": (C.c_int, [_VP, _VP, _VP, C.c_int64, _VP, C.c_int32, C.POINTER(TgmmFrameBuildParams),
+                                         _VP, C.c_int64, _VP, _VP, _VP, _VP, _VP, C.c_int64, C.c_int32,
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_int32), _VP, _VP]),
     "tgmm_frame_build": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.POINTER(TgmmFrameBuildParams), _VP, C.c_int64, _VP,
                                    _VP, _VP, _VP, _VP, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int32), _VP]),

@@ -80,22 +80,26 @@ struct FbWork {
 
 size_t align_up(size_t x) { return (x + 255) / 256 * 256; }
 
-// Carves the workspace; returns its size (base may be null to measure).
-size_t carve(char* base, int64_t nvol, int32_t n, FbWork* w) {
+// Carves the workspace; returns its size (base may be null to measure).  n_list < 0: the
+// volume form (lists built here, one entry per volume voxel at most); else the list form (the
+// caller's n_list entries, read in place).
+size_t carve(char* base, int64_t nvol, int32_t n, FbWork* w, int64_t n_list = -1) {
   size_t at = 0;
   auto take = [&](size_t bytes) {
     char* p = base ? base + at : nullptr;
     at += align_up(bytes);
     return p;
   };
+  const bool lists = n_list >= 0;
+  const int64_t ne = lists ? n_list : nvol;
   w->cnt = (int32_t*)take(4 * (size_t)n);
   w->box = (FbBox*)take(sizeof(FbBox) * (size_t)n);
-  w->uptr = (int64_t*)take(8 * ((size_t)n + 1));
-  w->ulin = (uint32_t*)take(4 * (size_t)nvol);
-  w->uval = (uint16_t*)take(2 * (size_t)nvol);
-  w->queue = (uint32_t*)take(4 * (size_t)nvol);
+  w->uptr = lists ? nullptr : (int64_t*)take(8 * ((size_t)n + 1));
+  w->ulin = lists ? nullptr : (uint32_t*)take(4 * (size_t)nvol);
+  w->uval = lists ? nullptr : (uint16_t*)take(2 * (size_t)nvol);
+  w->queue = (uint32_t*)take(4 * (size_t)ne);
   w->bits = (uint32_t*)take(4 * (size_t)((nvol + 31) / 32));
-  w->ukeep = (uint8_t*)take((size_t)nvol);
+  w->ukeep = (uint8_t*)take((size_t)ne);
   w->tcnt = (int32_t*)take(4 * (size_t)n);
   w->thr = (uint32_t*)take(4 * (size_t)n);
   w->tcent = (float*)take(12 * (size_t)n);
@@ -332,6 +336,51 @@ __global__ void __launch_bounds__(256) k_fb_group(const uint32_t* __restrict__ l
   if (lane == 0 && at != w.uptr[s + 1]) atomicOr(&w.stat->flags, 4u);  // box and count disagree
 }
 
+// List form: a warp per supervoxel checks its list (ascending linear indices inside the
+// volume; else the lists are flagged inconsistent) and takes its count and box.
+__global__ void __launch_bounds__(256) k_fbl_boxes(int32_t X, int32_t Y, int64_t nvol, int64_t n_list, int32_t n,
+                                                   FbWork w) {
+  const int lane = threadIdx.x & 31;
+  const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  if (s >= n) return;
+  const int64_t a = w.uptr[s], b = w.uptr[s + 1];
+  if (a < 0 || b < a || b > n_list || b - a > 0x7fffffff) {  // nothing of such a list is read
+    if (lane == 0) {
+      atomicOr(&w.stat->flags, 4u);
+      w.cnt[s] = 0;
+    }
+    return;
+  }
+  const uint32_t XY = (uint32_t)X * (uint32_t)Y;
+  int32_t lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-1, -1, -1};
+  bool bad = false;
+  for (int64_t i = a + lane; i < b; i += 32) {
+    const uint32_t v = w.ulin[i];
+    bad |= (int64_t)v >= nvol || (i > a && w.ulin[i - 1] >= v);
+    const uint32_t zz = v / XY, r = v - zz * XY, yy = r / (uint32_t)X;
+    const int32_t c[3] = {(int32_t)(r - yy * (uint32_t)X), (int32_t)yy, (int32_t)zz};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo[d] = min(lo[d], c[d]);
+      hi[d] = max(hi[d], c[d]);
+    }
+  }
+  const bool any_bad = __any_sync(0xffffffffu, bad);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+  }
+  if (lane == 0) {
+    if (any_bad) atomicOr(&w.stat->flags, 4u);
+    w.cnt[s] = (int32_t)(b - a);
+    for (int d = 0; d < 3; d++) {
+      w.box[s].lo[d] = lo[d];
+      w.box[s].hi[d] = hi[d];
+    }
+  }
+}
+
 // The k-th smallest value (0-based) from a 256-bin histogram, by one warp: each lane holds 8
 // bins, a scan over the lanes finds the lane holding it.  0 <= k < the histogram's total.
 __device__ void warp_hist_select(const int32_t* h, int32_t k, int32_t* bucket, int32_t* rest) {
@@ -368,6 +417,7 @@ __device__ __forceinline__ void decode(uint32_t v, uint32_t X, uint32_t XY, int3
   *x = (int32_t)(r - yy * X), *y = (int32_t)yy, *z = (int32_t)zz;
 }
 
+template <bool kLists>
 __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __restrict__ label,
                                                             const uint16_t* __restrict__ raw, int64_t nvol,
                                                             int32_t X, int32_t Y, int32_t Z, int32_t n,
@@ -569,7 +619,21 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
         for (int j = 0; j < off.n; j++) {
           const int64_t nb = (int64_t)v + off.off[j];
           if (nb < 0 || nb >= nvol) continue;
-          if (label[nb] != want || raw[nb] <= th) continue;
+          if (kLists) {
+            // a voxel of this supervoxel (its ascending list, as lower_bound finds it there)
+            // brighter than the threshold
+            int32_t lo = 0, hi = N;
+            while (lo < hi) {
+              const int32_t mid = (lo + hi) >> 1;
+              if ((int64_t)lin[mid] < nb)
+                lo = mid + 1;
+              else
+                hi = mid;
+            }
+            if (lo >= N || (int64_t)lin[lo] != nb || val[lo] <= th) continue;
+          } else if (label[nb] != want || raw[nb] <= th) {
+            continue;
+          }
           const uint32_t bit = 1u << (nb & 31);
           if (atomicOr(&w.bits[nb >> 5], bit) & bit) continue;
           q[atomicAdd(&s_tail, 1u)] = (uint32_t)nb;
@@ -867,8 +931,8 @@ int frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3
   mark();
   k_fb_group<<<warp_blocks, 256, 0, st>>>(label, raw, X, Y, n, w);
   mark();
-  k_fb_trim<<<n, kFbTrimThreads, 0, st>>>(label, raw, nvol, X, Y, dims[2], n, p->max_nuclei_size, p->max_percentile,
-                                          p->min_nuclei_size, off, w);
+  k_fb_trim<false><<<n, kFbTrimThreads, 0, st>>>(label, raw, nvol, X, Y, dims[2], n, p->max_nuclei_size,
+                                                 p->max_percentile, p->min_nuclei_size, off, w);
   mark();
   k_fb_order<<<1, 1024, 0, st>>>(n, nvol, p->min_nuclei_size, w);
   mark();
@@ -894,6 +958,117 @@ int frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3
   return TGMM_OK;
 }
 }  // namespace
+
+namespace {
+// The list form: the supervoxels' lists as the segmentation holds them (each supervoxel's
+// voxels in ascending linear index with their raw values, CSR over the supervoxels), read in
+// place; the steps after the grouping are the volume form's.
+int frame_build_lists(const uint32_t* lin, const uint16_t* val, const int64_t* lists_ptr, int64_t n_list,
+                      const int32_t dims[3], int32_t n_labels, const TgmmFrameBuildParams* p, void* workspace,
+                      int64_t workspace_bytes, float* query, float* img, float* cent, int64_t* lptr, uint16_t* thr,
+                      int64_t max_vox, int32_t max_sv, int64_t* n_vox_out, int32_t* n_sv_out, cudaStream_t st,
+                      float* stage_ms) {
+  static const char* kWhat = "tgmm_frame_build_lists";
+  if (!lists_ptr || !dims || !p || !workspace || !query || !img || !cent || !lptr || !n_vox_out || !n_sv_out ||
+      n_labels < 1 || n_list < 0 || (n_list > 0 && (!lin || !val)) || max_vox < 0 || max_sv < 0)
+    return report_error(TGMM_ERR_INVALID_ARG, kWhat, cudaSuccess);
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1)
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build_lists: dimensions", cudaSuccess);
+  const int64_t nvol = (int64_t)dims[0] * dims[1] * dims[2];
+  if (nvol >= ((int64_t)1 << 32) || n_labels > (1 << 24) || n_list > nvol)
+    return report_error(TGMM_ERR_BAD_SIZE,
+                        "tgmm_frame_build_lists: more than 2^32 voxels, 2^24 labels or list entries than voxels",
+                        cudaSuccess);
+  if (p->max_nuclei_size < 0 || !(p->max_percentile >= 0.0f && p->max_percentile <= 1.0f))
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build_lists: trimming parameters", cudaSuccess);
+  FbOffsets off;
+  if (!fb_offsets(p->conn3d, dims, &off))
+    return report_error(TGMM_ERR_INVALID_ARG, "tgmm_frame_build_lists: conn3d must be 4, 6, 8, 26 or 74",
+                        cudaSuccess);
+  FbWork w;
+  if ((int64_t)carve(nullptr, nvol, n_labels, &w, n_list) > workspace_bytes)
+    return report_error(TGMM_ERR_BAD_SIZE,
+                        "tgmm_frame_build_lists: workspace smaller than tgmm_frame_build_lists_bytes", cudaSuccess);
+  carve((char*)workspace, nvol, n_labels, &w, n_list);
+  w.uptr = const_cast<int64_t*>(lists_ptr);
+  w.ulin = const_cast<uint32_t*>(lin);
+  w.uval = const_cast<uint16_t*>(val);
+  const int32_t X = dims[0], Y = dims[1], n = n_labels;
+  // with stage_ms: an event before the first step and after each
+  struct Events {
+    cudaEvent_t e[TGMM_FRAME_BUILD_STAGES + 1] = {};
+    int n = 0;
+    ~Events() {
+      for (int i = 0; i < n; i++) cudaEventDestroy(e[i]);
+    }
+  } evs;
+  if (stage_ms)
+    for (; evs.n <= TGMM_FRAME_BUILD_STAGES; evs.n++)
+      if (cudaEventCreate(&evs.e[evs.n]) != cudaSuccess)
+        return report_error(TGMM_ERR_CUDA, "tgmm_frame_build_lists: events", cudaGetLastError());
+  int stage = 0;
+  auto mark = [&]() {
+    if (stage_ms) cudaEventRecord(evs.e[stage++], st);
+  };
+  mark();
+  cudaError_t e = cudaMemsetAsync(w.bits, 0, 4 * (size_t)((nvol + 31) / 32), st);
+  if (e != cudaSuccess) return report_error(TGMM_ERR_CUDA, kWhat, e);
+  const unsigned warp_blocks = (unsigned)(((int64_t)n * 32 + 255) / 256);
+  k_fb_init<<<(n + 255) / 256, 256, 0, st>>>(n, w);
+  mark();
+  k_fbl_boxes<<<warp_blocks, 256, 0, st>>>(X, Y, nvol, n_list, n, w);
+  mark();
+  mark();  // no CSR to build: the lists come with theirs
+  mark();  // no grouping: the lists are grouped
+  k_fb_trim<true><<<n, kFbTrimThreads, 0, st>>>(nullptr, nullptr, nvol, X, Y, dims[2], n, p->max_nuclei_size,
+                                                p->max_percentile, p->min_nuclei_size, off, w);
+  mark();
+  k_fb_order<<<1, 1024, 0, st>>>(n, nvol, p->min_nuclei_size, w);
+  mark();
+  k_fb_csr<<<1, 1024, 0, st>>>(max_vox, max_sv, w, lptr);
+  mark();
+  k_fb_emit<<<warp_blocks, 256, 0, st>>>(X, Y, max_vox, max_sv, w, lptr, query, img, cent, thr);
+  mark();
+  FbStat h;
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, w.stat, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return report_error(TGMM_ERR_CUDA, kWhat, e);
+  if (stage_ms)
+    for (int i = 0; i < TGMM_FRAME_BUILD_STAGES; i++) cudaEventElapsedTime(&stage_ms[i], evs.e[i], evs.e[i + 1]);
+  if (h.flags & 4u)
+    return report_error(TGMM_ERR_DEVICE_FLAG,
+                        "tgmm_frame_build_lists: a list is not ascending inside the volume, or the CSR is invalid",
+                        cudaSuccess);
+  *n_vox_out = h.n_vox;
+  *n_sv_out = h.n_sv;
+  if (h.flags & 2u)
+    return report_error(TGMM_ERR_NO_SUPERVOXEL, "tgmm_frame_build_lists: every supervoxel was erased", cudaSuccess);
+  if (h.n_vox > max_vox || h.n_sv > max_sv)
+    return report_error(TGMM_ERR_BAD_SIZE,
+                        "tgmm_frame_build_lists: more voxels or supervoxels than the outputs hold", cudaSuccess);
+  return TGMM_OK;
+}
+}  // namespace
+
+extern "C" int64_t tgmm_frame_build_lists_bytes(const int32_t dims[3], int32_t n_labels, int64_t n_list) {
+  if (!dims || dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || n_labels < 1 || n_list < 0) return -1;
+  const int64_t nvol = (int64_t)dims[0] * dims[1] * dims[2];
+  FbWork w;
+  return (int64_t)carve(nullptr, nvol, n_labels, &w, n_list);
+}
+
+extern "C" int tgmm_frame_build_lists(const uint32_t* lin, const uint16_t* val, const int64_t* lists_ptr,
+                                      int64_t n_list, const int32_t dims[3], int32_t n_labels,
+                                      const TgmmFrameBuildParams* p, void* workspace, int64_t workspace_bytes,
+                                      float* query, float* img, float* cent, int64_t* lptr, uint16_t* thr,
+                                      int64_t max_vox, int32_t max_sv, int64_t* n_vox_out, int32_t* n_sv_out,
+                                      void* stream, float* stage_ms) {
+  if (stage_ms)
+    for (int i = 0; i < TGMM_FRAME_BUILD_STAGES; i++) stage_ms[i] = 0.0f;
+  return frame_build_lists(lin, val, lists_ptr, n_list, dims, n_labels, p, workspace, workspace_bytes, query, img,
+                           cent, lptr, thr, max_vox, max_sv, n_vox_out, n_sv_out, (cudaStream_t)stream, stage_ms);
+}
 
 extern "C" int tgmm_frame_build(const uint16_t* raw, const uint32_t* label, const int32_t dims[3], int32_t n_labels,
                                 const TgmmFrameBuildParams* p, void* workspace, int64_t workspace_bytes, float* query,

@@ -285,3 +285,33 @@ class FrameBuilder:
         N, S = n_vox.value, n_sv.value
         f = DeviceFrame(self.query[:3 * N], self.img[:N], self.cent[:3 * S], self.lptr[:S + 1], n_gauss)
         return f, (self.thr[:S].cpu().numpy().view(np.uint16).copy() if read_thr else None)
+
+    def build_lists(self, lin: torch.Tensor, val: torch.Tensor, lists_ptr: torch.Tensor, n_gauss: int = 0,
+                    stream=None, stage_ms=None, read_thr=True):
+        """tgmm_frame_build_lists: the segmentation as per-supervoxel pixel lists on the device
+        -- lin (4-byte linear indices, ascending within each list), val (their 2-byte raw
+        values), lists_ptr (int64, n_labels + 1) -- instead of volumes.  The same outputs as
+        build().  The list workspace is allocated on first use for the largest list seen."""
+        n_list = int(lin.numel())
+        if val.numel() != n_list or val.element_size() != 2 or lin.element_size() != 4 or \
+                lists_ptr.numel() != self.n_labels + 1 or lists_ptr.dtype != torch.int64:
+            raise ValueError("lin and val need one entry per listed voxel, lists_ptr n_labels + 1 int64")
+        nbytes = self.lib.tgmm_frame_build_lists_bytes(self.dims, self.n_labels, n_list)
+        if nbytes < 0:
+            raise ValueError("tgmm_frame_build_lists_bytes: bad sizes")
+        if getattr(self, "list_ws", None) is None or self.list_ws.numel() < nbytes:
+            self.list_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.query.device)
+        n_vox, n_sv = C.c_int64(0), C.c_int32(0)
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        ms = (C.c_float * L.TGMM_FRAME_BUILD_STAGES)() if stage_ms is not None else None
+        L.check(self.lib.tgmm_frame_build_lists(lin.data_ptr(), val.data_ptr(), lists_ptr.data_ptr(), n_list,
+                                                self.dims, self.n_labels, C.byref(self.params),
+                                                self.list_ws.data_ptr(), self.list_ws.numel(), self.query.data_ptr(),
+                                                self.img.data_ptr(), self.cent.data_ptr(), self.lptr.data_ptr(),
+                                                self.thr.data_ptr(), self.max_vox, self.n_labels, C.byref(n_vox),
+                                                C.byref(n_sv), s, ms), "tgmm_frame_build_lists")
+        if stage_ms is not None:
+            stage_ms[:] = list(ms)
+        N, S = n_vox.value, n_sv.value
+        f = DeviceFrame(self.query[:3 * N], self.img[:N], self.cent[:3 * S], self.lptr[:S + 1], n_gauss)
+        return f, (self.thr[:S].cpu().numpy().view(np.uint16).copy() if read_thr else None)
