@@ -34,7 +34,7 @@ namespace tgmm {
 namespace {
 
 constexpr int kFbMaxOff = 74;
-constexpr int kFbTrimThreads = 256;
+constexpr int kFbTrimThreads = 256;  // also the Otsu histogram's bins: a thread per bin
 constexpr int kFbScanDepth = 4;  // 16-byte label groups each lane of the scan has in flight
 
 struct FbBox {
@@ -45,7 +45,25 @@ struct FbOffsets {
   int64_t off[kFbMaxOff];    // linear-index offsets, as the reference builds them
   int8_t d[kFbMaxOff][3];    // their (dx, dy, dz)
   int32_t n;
+  // unsigned division of a 32-bit linear index by X and by X*Y as a multiply-high and shifts
+  // (Granlund and Montgomery's method; exact for every 32-bit numerator)
+  uint32_t mx, mxy;
+  int32_t lx, lxy;
 };
+
+// The magic number m and the shift l of the division by d (1 <= d < 2^32): l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1.
+void div_magic(uint32_t d, uint32_t* m, int32_t* l) {
+  int32_t k = 0;
+  while (((uint64_t)1 << k) < d) k++;
+  *m = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << k) - d)) / d + 1);
+  *l = k;
+}
+
+__device__ __forceinline__ uint32_t div_by_magic(uint32_t n, uint32_t m, int32_t l) {
+  const uint32_t t = __umulhi(n, m);
+  return l == 0 ? n : (t + ((n - t) >> 1)) >> (l - 1);
+}
 
 // per-call scalars shared by the kernels
 struct FbStat {
@@ -412,8 +430,10 @@ __device__ void warp_hist_select(const int32_t* h, int32_t k, int32_t* bucket, i
 
 constexpr int kFbMaskWords = 2048;  // bounding boxes up to 65536 voxels flood in shared memory
 
-__device__ __forceinline__ void decode(uint32_t v, uint32_t X, uint32_t XY, int32_t* x, int32_t* y, int32_t* z) {
-  const uint32_t zz = v / XY, r = v - zz * XY, yy = r / X;
+// A linear index's coordinates, with the precomputed divisions of `o`.
+__device__ __forceinline__ void decode(uint32_t v, uint32_t X, uint32_t XY, const FbOffsets& o, int32_t* x,
+                                       int32_t* y, int32_t* z) {
+  const uint32_t zz = div_by_magic(v, o.mxy, o.lxy), r = v - zz * XY, yy = div_by_magic(r, o.mx, o.lx);
   *x = (int32_t)(r - yy * X), *y = (int32_t)yy, *z = (int32_t)zz;
 }
 
@@ -429,7 +449,6 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
   __shared__ uint32_t s_min, s_max, s_seed, s_tail;
   __shared__ int32_t s_b1, s_r1, s_b2, s_r2, s_l1, s_l2, s_rr, s_best;
   __shared__ float s_mm;
-  __shared__ float st_v[32], st_x[32], st_y[32], st_z[32];
   __shared__ uint32_t s_cand[kFbMaskWords], s_reach[kFbMaskWords];
   const int s = blockIdx.x, t = threadIdx.x, lane = t & 31;
   if (w.stat->flags) return;
@@ -494,21 +513,51 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     if (v == s_max) atomicMin(&s_seed, (uint32_t)i);
   }
   __syncthreads();
-  if (t < 32) {
-    warp_hist_select(h_lo1, s_r1, &s_l1, &s_rr);
-    warp_hist_select(h_lo2, s_r2, &s_l2, &s_rr);
-    if (t == 0) {
-      // Otsu: the between-class sums in the reference's order
+  // Otsu's running sums over the bins (thread t = bin t): the class weights by a block scan of
+  // the counts, the class sums of bin * count in the reference's FP32 order.  When their total
+  // is below 2^24 every FP32 partial sum is an exact integer, so the scan's integers are those
+  // bits; larger supervoxels sum in order on one thread.
+  {
+    const int64_t hb = h_ot[t], tb = (int64_t)t * hb;
+    int64_t w_inc = hb, s_inc = tb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t yw = __shfl_up_sync(0xffffffffu, w_inc, o), ys = __shfl_up_sync(0xffffffffu, s_inc, o);
+      if (lane >= o) {
+        w_inc += yw;
+        s_inc += ys;
+      }
+    }
+    __shared__ int64_t s_ws[kFbTrimThreads / 32], s_ss[kFbTrimThreads / 32];
+    if (lane == 31) {
+      s_ws[t >> 5] = w_inc;
+      s_ss[t >> 5] = s_inc;
+    }
+    __syncthreads();
+    int64_t w_before = 0, s_before = 0, s_total = 0;
+#pragma unroll
+    for (int q = 0; q < kFbTrimThreads / 32; q++) {
+      if (q < (t >> 5)) {
+        w_before += s_ws[q];
+        s_before += s_ss[q];
+      }
+      s_total += s_ss[q];
+    }
+    s_wb[t] = (int32_t)(w_before + w_inc);
+    if (s_total < (1 << 24)) {
+      s_sumb[t] = (float)(s_before + s_inc);
+    } else if (t == 0) {
       float sum_b = 0.0f;
-      int32_t wb = 0;
       for (int bin = 0; bin < 256; bin++) {
-        wb += h_ot[bin];
         sum_b = __fadd_rn(sum_b, (float)(bin * h_ot[bin]));
-        s_wb[bin] = wb;
         s_sumb[bin] = sum_b;
       }
     }
-    __syncwarp();
+  }
+  __syncthreads();
+  if (t < 32) {
+    warp_hist_select(h_lo1, s_r1, &s_l1, &s_rr);
+    warp_hist_select(h_lo2, s_r2, &s_l2, &s_rr);
     // the bin of the largest between-class variance (the first of equals; 0 if none is > 0)
     float best_v = 0.0f;
     int32_t best_b = 0x7fffffff;
@@ -567,14 +616,14 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     for (int32_t i = t; i < N; i += kFbTrimThreads)
       if (val[i] > th) {
         int32_t x, y, z;
-        decode(lin[i], uX, XY, &x, &y, &z);
+        decode(lin[i], uX, XY, off, &x, &y, &z);
         const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
         atomicOr(&s_cand[li >> 5], 1u << (li & 31));
       }
     __syncthreads();
     if (t == 0 && val[s_seed] > th) {
       int32_t x, y, z;
-      decode(lin[s_seed], uX, XY, &x, &y, &z);
+      decode(lin[s_seed], uX, XY, off, &x, &y, &z);
       const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
       s_reach[li >> 5] |= 1u << (li & 31);
       q[0] = lin[s_seed];
@@ -597,13 +646,13 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
       const uint32_t v = q[i];
       if (shared_path) {
         int32_t x, y, z;
-        decode(v, uX, XY, &x, &y, &z);
+        decode(v, uX, XY, off, &x, &y, &z);
         for (int j = 0; j < off.n; j++) {
           int32_t tx = x + off.d[j][0], ty = y + off.d[j][1], tz = z + off.d[j][2];
           if (tx < 0 || tx >= X || ty < 0 || ty >= Y) {  // wraps: where the linear offset lands
             const int64_t nb = (int64_t)v + off.off[j];
             if (nb < 0 || nb >= nvol) continue;
-            decode((uint32_t)nb, uX, XY, &tx, &ty, &tz);
+            decode((uint32_t)nb, uX, XY, off, &tx, &ty, &tz);
           } else if (tz < 0 || tz >= Z) {
             continue;
           }
@@ -650,7 +699,7 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
     bool in;
     if (shared_path) {
       int32_t x, y, z;
-      decode(v, uX, XY, &x, &y, &z);
+      decode(v, uX, XY, off, &x, &y, &z);
       const int32_t li = (x - bx.lo[0]) + bw * ((y - bx.lo[1]) + bh * (z - bx.lo[2]));
       in = (s_reach[li >> 5] >> (li & 31)) & 1u;
     } else {  // the flood's bits were set by atomics at L2: read them there
@@ -663,8 +712,11 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
   __syncthreads();
   if (t >= 32) return;
   // warp 0: the centroid in list order (FP32, as the reference sums it) and the range of the
-  // background-subtracted values
-  const unsigned below = (1u << lane) - 1u;
+  // background-subtracted values.  Each lane forms its voxel's products and stages them (zeros
+  // for a voxel not kept: every term is non-negative, so adding +0 leaves a sum's bits as they
+  // are); the four running sums then add the group's 32 entries in lane order (list order), from
+  // broadcast loads issued ahead of the additions, so the chains hold only the additions.
+  __shared__ float4 st4[32];
   float sw = 0.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
   uint32_t smin = 0xffffffffu, smax = 0;
   for (int32_t i0 = 0; i0 < N; i0 += 32) {
@@ -677,27 +729,28 @@ __global__ void __launch_bounds__(kFbTrimThreads) k_fb_trim(const uint32_t* __re
       in = keep[i] != 0;
     }
     const unsigned m = __ballot_sync(0xffffffffu, in);
+    float I = 0.0f, px = 0.0f, py = 0.0f, pz = 0.0f;
     if (in) {
-      const int p = __popc(m & below);
       int32_t x, y, z;
-      decode(v, uX, XY, &x, &y, &z);
-      st_v[p] = (float)r;
-      st_x[p] = (float)x;
-      st_y[p] = (float)y;
-      st_z[p] = (float)z;
+      decode(v, uX, XY, off, &x, &y, &z);
+      I = (float)r;
+      px = __fmul_rn(I, (float)x);
+      py = __fmul_rn(I, (float)y);
+      pz = __fmul_rn(I, (float)z);
       const uint32_t sub = (uint16_t)(r - th);
       smin = min(smin, sub);
       smax = max(smax, sub);
     }
+    st4[lane] = make_float4(I, px, py, pz);
     __syncwarp();
-    if (lane == 0) {
-      const int c = __popc(m);
-      for (int p = 0; p < c; p++) {
-        const float I = st_v[p];
-        sw = __fadd_rn(sw, I);
-        c0 = __fadd_rn(c0, __fmul_rn(I, st_x[p]));
-        c1 = __fadd_rn(c1, __fmul_rn(I, st_y[p]));
-        c2 = __fadd_rn(c2, __fmul_rn(I, st_z[p]));
+    if (m) {
+#pragma unroll
+      for (int p = 0; p < 32; p++) {
+        const float4 e = st4[p];
+        sw = __fadd_rn(sw, e.x);
+        c0 = __fadd_rn(c0, e.y);
+        c1 = __fadd_rn(c1, e.z);
+        c2 = __fadd_rn(c2, e.w);
       }
     }
     __syncwarp();
@@ -856,6 +909,8 @@ int fb_offsets(int32_t conn, const int32_t dims[3], FbOffsets* o) {
         n++;
       }
   o->n = n;
+  div_magic((uint32_t)X, &o->mx, &o->lx);
+  div_magic((uint32_t)XY, &o->mxy, &o->lxy);
   return n;
 }
 
