@@ -65,7 +65,7 @@ Layout make_layout(const TgmmPlanDesc& d, int32_t max_gchunks, int32_t max_cells
   L.bucket = take(4 * G * kBucketCap);
   L.acnt = take(4 * G);
   L.abucket = take(4 * G * kBucketCap);
-  L.ape = take(8 * 2 * (int64_t)max_gchunks);
+  L.ape = take(8 * 2 * (int64_t)max_gchunks * 3);  // the M-step's sums, minima and NaN flags
   L.apf = take(8 * (int64_t)max_gchunks);
   L.dead = take(4 * (int64_t)max_gchunks);
   L.ec = take(8 * kEcStride * G);
@@ -199,6 +199,8 @@ int tgmm_plan_create(const TgmmPlanDesc* d, TgmmPlan** out) {
   D.acnt = (int32_t*)(b + P->L.acnt);
   D.abucket = (int32_t*)(b + P->L.abucket);
   D.alpha_part_e = (double*)(b + P->L.ape);
+  D.alpha_min_e = D.alpha_part_e + 2 * (int64_t)mgc;
+  D.nan_e = (int32_t*)(D.alpha_min_e + 2 * (int64_t)mgc);
   D.alpha_part_f = (double*)(b + P->L.apf);
   D.dead_part = (int32_t*)(b + P->L.dead);
   D.ec = (double*)(b + P->L.ec);

@@ -1143,9 +1143,16 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   if (ovf)
     for (int i = 0; i < 10; i++) A[i] = s_ovf_acc[threadIdx.x][i];
   double alpha = 0.0, move = 0.0;
+  // what the kill step tests: this Gaussian's alpha if it is live and not fixed, and whether
+  // its W or this iteration's E[ln|Lambda|] holds a NaN
+  double amin = kInf;
+  bool nanw = false;
   const int cur = P.iter & 1, nxt = cur ^ 1;
   if (valid) {
     const bool alive = !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k];
+    nanw = isnan(gcomp(P, G_ELD0 + cur, k));
+    if (!alive)
+      for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
     if (alive) {
       const double N = A[0];
       double xb[3] = {0, 0, 0}, Sk[6] = {0, 0, 0, 0, 0, 0};
@@ -1191,6 +1198,8 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
       rc.max_exc = D.max_exc;
       regularize_W(W, nu, rc);
       for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = W[e];
+      for (int e = 0; e < 6; e++) nanw = nanw || isnan(W[e]);
+      amin = alpha_n;
       // the next iteration's records, as if the Gaussian survives the kill step (which
       // rewrites them for the Gaussians it kills)
       move = write_records(P, D, k, nxt, false, W, nu, alpha_n, beta, mn, true);
@@ -1204,6 +1213,28 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   }
   const double a = block_sum_n<kMChunk>(alpha, shd);
   if (threadIdx.x == 0) P.alpha_part_e[blockIdx.x] = a;
+  {
+    __shared__ double s_amin[kMChunk / 32];
+    __shared__ int s_nan[kMChunk / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+    const int wn = __any_sync(0xffffffffu, nanw) ? 1 : 0;
+    if ((threadIdx.x & 31) == 0) {
+      s_amin[threadIdx.x >> 5] = amin;
+      s_nan[threadIdx.x >> 5] = wn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = kInf;
+      int nn = 0;
+      for (int i = 0; i < kMChunk / 32; i++) {
+        m = fmin(m, s_amin[i]);
+        nn |= s_nan[i];
+      }
+      P.alpha_min_e[blockIdx.x] = m;
+      P.nan_e[blockIdx.x] = nn;
+    }
+  }
   // the block's largest move of a kNN centre, rounded up to a float (non-negative floats
   // order as their bits)
   float mv = __double2float_ru(move);
@@ -1241,12 +1272,42 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     was_dead = is_dead_prior(gcomp(P, G_MO0, k));
     fixed = P.fixed[k] != 0;
   }
+  __shared__ int s_fast;
   if (threadIdx.x < 32) {
     const double tot = warp_sum_range(P.alpha_part_e, 2 * D.gchunk_base, 2 * D.n_gchunks);
-    if (threadIdx.x == 0) s_total = tot;
+    // no Gaussian of the frame can die this iteration when none has a NaN and the smallest
+    // live alpha passes the rule against this total
+    double amin = kInf;
+    int nn = 0;
+    for (int i = threadIdx.x; i < 2 * D.n_gchunks; i += 32) {
+      amin = fmin(amin, P.alpha_min_e[2 * D.gchunk_base + i]);
+      nn |= P.nan_e[2 * D.gchunk_base + i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+    nn = __any_sync(0xffffffffu, nn != 0);
+    if (threadIdx.x == 0) {
+      s_total = tot;
+      s_fast = !nn && !(amin / tot < TGMM_MIN_PI_FOR_DEAD);
+    }
   }
   __syncthreads();
   const double total = s_total;
+  if (s_fast) {
+    // nothing dies: the live Gaussians go into the grid, and the frame's first chunk writes
+    // its totals (the post-kill total is the M-step's; the dead count stays)
+    if (valid && !was_dead) grid_insert(P, D, S, k, centre);
+    if (c == D.gchunk_base && threadIdx.x == 0) {
+      FrameState* Sw = &P.state[ch.frame];
+      Sw->total_alpha = total;
+      Sw->ln_alpha = log(total);
+      Sw->psi_total[nxt] = digamma(total);
+      Sw->blk_done = 0;
+      Sw->disp_cum += (double)__uint_as_float(Sw->disp_max);
+      Sw->disp_max = 0u;
+    }
+    return;
+  }
   double alpha = 0.0;
   int dead = 0;
   if (valid) {

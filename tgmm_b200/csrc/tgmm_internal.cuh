@@ -198,6 +198,10 @@ struct DevPlan {
   int32_t* acnt;
   int32_t* abucket;
   double* alpha_part_e;
+  // per M-step block: the smallest alpha of its live, non-fixed Gaussians (+inf if none), and
+  // 1 when one of its Gaussians has a NaN in W or in this iteration's E[ln|Lambda|]
+  double* alpha_min_e;
+  int32_t* nan_e;
   double* alpha_part_f;
   int32_t* dead_part;
   int32_t* work;   // [0] next supervoxel of the voxel pass, [1] warps that left it
