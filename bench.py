@@ -37,11 +37,12 @@ EM_ITERS = 20
 
 
 def kernels_per_call(knn_fused: bool) -> int:
-    """Kernels the engine launches per EM call: 3 table stagings (k_stage), build_maps,
-    import, the 3 order kernels (sv_records, order_base, order_scatter), the moment pass,
-    the first iteration's knn_estep, 3 per iteration (mstep_update, kill_prep, ll_pass), the
-    later iterations' knn_estep unless the voxel pass runs them, assign, export."""
-    return 3 + 7 + 3 * EM_ITERS + (0 if knn_fused else EM_ITERS - 1) + 2
+    """Kernels the engine launches per EM call: 3 table stagings (k_stage), build_maps, the
+    records' fetch and import, the 3 order kernels (sv_records, order_base, order_scatter), the
+    moment pass, the first iteration's knn_estep, 3 per iteration (mstep_update, kill_prep,
+    ll_pass), the later iterations' knn_estep unless the voxel pass runs them, assign, export
+    (a fixed iteration count: no conditional iterations)."""
+    return 3 + 8 + 3 * EM_ITERS + (0 if knn_fused else EM_ITERS - 1) + 2
 
 
 def parse():
