@@ -1273,20 +1273,41 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     fixed = P.fixed[k] != 0;
   }
   __shared__ int s_fast;
-  if (threadIdx.x < 32) {
-    const double tot = warp_sum_range(P.alpha_part_e, 2 * D.gchunk_base, 2 * D.n_gchunks);
-    // no Gaussian of the frame can die this iteration when none has a NaN and the smallest
-    // live alpha passes the rule against this total
-    double amin = kInf;
-    int nn = 0;
-    for (int i = threadIdx.x; i < 2 * D.n_gchunks; i += 32) {
-      amin = fmin(amin, P.alpha_min_e[2 * D.gchunk_base + i]);
-      nn |= P.nan_e[2 * D.gchunk_base + i];
+  {
+    // the frame's M-step block partials, spread over the whole block so that their loads are
+    // in flight together: the alpha total (a fixed order: each thread's partials in order, a
+    // butterfly per warp, the warps in order -- the same bits in every block of the frame),
+    // the smallest live alpha and the NaN flags.  No Gaussian of the frame can die this
+    // iteration when none has a NaN and the smallest live alpha passes the rule.
+    __shared__ double s_wt[kGChunk / 32], s_wm[kGChunk / 32];
+    __shared__ int s_wn[kGChunk / 32];
+    const int nb = 2 * D.n_gchunks, base = 2 * D.gchunk_base;
+    double tp = 0.0, mp = kInf;
+    int np = 0;
+    for (int i = threadIdx.x; i < nb; i += kGChunk) {
+      tp += P.alpha_part_e[base + i];
+      mp = fmin(mp, P.alpha_min_e[base + i]);
+      np |= P.nan_e[base + i];
     }
+    tp = warp_sum(tp);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
-    nn = __any_sync(0xffffffffu, nn != 0);
+    for (int o = 16; o > 0; o >>= 1) mp = fmin(mp, __shfl_xor_sync(0xffffffffu, mp, o));
+    np = __any_sync(0xffffffffu, np != 0);
+    if ((threadIdx.x & 31) == 0) {
+      s_wt[threadIdx.x >> 5] = tp;
+      s_wm[threadIdx.x >> 5] = mp;
+      s_wn[threadIdx.x >> 5] = np;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
+      double tot = 0.0, amin = kInf;
+      int nn = 0;
+#pragma unroll
+      for (int w = 0; w < kGChunk / 32; w++) {
+        tot += s_wt[w];
+        amin = fmin(amin, s_wm[w]);
+        nn |= s_wn[w];
+      }
       s_total = tot;
       s_fast = !nn && !(amin / tot < TGMM_MIN_PI_FOR_DEAD);
     }
