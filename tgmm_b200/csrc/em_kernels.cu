@@ -423,7 +423,7 @@ __device__ __forceinline__ int ref_cell_of(const FrameState& S, const FrameDesc&
 // which bounds the kNN neighbour lists.
 __device__ __forceinline__ double write_records(const DevPlan& P, const FrameDesc& D, int k, int parity, bool dead,
                                                 const double* W, double nu, double alpha, double beta,
-                                                const double* m, bool track) {
+                                                const double* m, bool track, float4 o = float4{}) {
   const double psa = digamma(alpha);
   const double eld = dead ? -1e32 : expected_log_det(W, nu);
   gcomp(P, G_PSIA0 + parity, k) = psa;
@@ -451,8 +451,7 @@ __device__ __forceinline__ double write_records(const DevPlan& P, const FrameDes
   const float y = __double2float_rn(m[1]);
   const float z = __double2float_rn(m[2]);
   double move = 0.0;
-  if (track && !dead) {
-    const float4 o = P.kpos[k];
+  if (track && !dead) {  // o: the centre kpos held before (loaded by the caller)
     if (o.w != 0.0f) {
       const double a = ((double)x - (double)o.x) * (double)D.scale[0];
       const double b = ((double)y - (double)o.y) * (double)D.scale[1];
@@ -1092,8 +1091,23 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   for (int i = 0; i < 10; i++) A[i] = 0.0;
   double mref[3] = {0, 0, 0};
   bool ovf = false;
+  // the Gaussian's own inputs of the update, loaded ahead of the bucket work so that they
+  // arrive beside it: the prior (m_o also re-centres the pairs), its fixed flag, this
+  // iteration's E[ln|Lambda|] (the kill step's NaN test) and the centre the kNN saw
+  const int cur = P.iter & 1, nxt = cur ^ 1;
+  double bo = 0.0, nuo = 0.0, alo = 0.0, Wo[6] = {0, 0, 0, 0, 0, 0}, eld_cur = 0.0, alpha_old = 0.0;
+  bool fixed_k = false;
+  float4 kp_old = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (valid) {
     for (int d = 0; d < 3; d++) mref[d] = gcomp(P, G_MO0 + d, k);
+    bo = gcomp(P, G_BETAO, k);
+    nuo = gcomp(P, G_NUO, k);
+    alo = gcomp(P, G_ALPHAO, k);
+    for (int e = 0; e < 6; e++) Wo[e] = gcomp(P, G_WO0 + e, k);
+    eld_cur = gcomp(P, G_ELD0 + cur, k);
+    alpha_old = gcomp(P, G_ALPHA, k);
+    fixed_k = P.fixed[k] != 0;
+    kp_old = P.kpos[k];
     const int n = P.bcnt[k];
     P.bcnt[k] = 0;
     if (n > kBucketCap) {
@@ -1147,10 +1161,9 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
   // its W or this iteration's E[ln|Lambda|] holds a NaN
   double amin = kInf;
   bool nanw = false;
-  const int cur = P.iter & 1, nxt = cur ^ 1;
   if (valid) {
-    const bool alive = !is_dead_prior(gcomp(P, G_MO0, k)) && !P.fixed[k];
-    nanw = isnan(gcomp(P, G_ELD0 + cur, k));
+    const bool alive = !is_dead_prior(mref[0]) && !fixed_k;
+    nanw = isnan(eld_cur);
     if (!alive)
       for (int e = 0; e < 6; e++) nanw = nanw || isnan(gcomp(P, G_W0 + e, k));
     if (alive) {
@@ -1162,22 +1175,19 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
         const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
         for (int e = 0; e < 6; e++) Sk[e] = A[4 + e] - A[1 + ia[e]] * A[1 + ib[e]] * iN;
       }
-      const double bo = gcomp(P, G_BETAO, k);
       const double beta = bo + N;
       const double ib_ = 1.0 / beta;
-      const double nu = gcomp(P, G_NUO, k) + N;
-      const double alpha_n = fmax(gcomp(P, G_ALPHAO, k) + N, 0.0);
+      const double nu = nuo + N;
+      const double alpha_n = fmax(alo + N, 0.0);
       gcomp(P, G_BETA, k) = beta;
       gcomp(P, G_NU, k) = nu;
       gcomp(P, G_ALPHA, k) = alpha_n;
-      double mo[3], mn[3];
+      const double* mo = mref;
+      double mn[3];
       for (int d = 0; d < 3; d++) {
-        mo[d] = gcomp(P, G_MO0 + d, k);
         mn[d] = (bo * mo[d] + N * xb[d]) * ib_;
         gcomp(P, G_M0 + d, k) = mn[d];
       }
-      double Wo[6];
-      for (int e = 0; e < 6; e++) Wo[e] = gcomp(P, G_WO0 + e, k);
       if (Wo[5] < 1e-8) {
         Wo[5] = 0.5 * (Wo[0] + Wo[3]);
         gcomp(P, G_WO5, k) = Wo[5];
@@ -1200,16 +1210,17 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
       for (int e = 0; e < 6; e++) gcomp(P, G_W0 + e, k) = W[e];
       for (int e = 0; e < 6; e++) nanw = nanw || isnan(W[e]);
       amin = alpha_n;
+      alpha = alpha_n;
       // the next iteration's records, as if the Gaussian survives the kill step (which
       // rewrites them for the Gaussians it kills)
-      move = write_records(P, D, k, nxt, false, W, nu, alpha_n, beta, mn, true);
+      move = write_records(P, D, k, nxt, false, W, nu, alpha_n, beta, mn, true, kp_old);
     } else {
       // fixed or dead: unchanged parameters, unchanged records; psi and E[ln|Lambda|] go
       // on to the next iteration's slot
       gcomp(P, G_PSIA0 + nxt, k) = gcomp(P, G_PSIA0 + cur, k);
-      gcomp(P, G_ELD0 + nxt, k) = gcomp(P, G_ELD0 + cur, k);
+      gcomp(P, G_ELD0 + nxt, k) = eld_cur;
+      alpha = alpha_old;
     }
-    alpha = gcomp(P, G_ALPHA, k);
   }
   const double a = block_sum_n<kMChunk>(alpha, shd);
   if (threadIdx.x == 0) P.alpha_part_e[blockIdx.x] = a;
