@@ -465,9 +465,8 @@ __device__ __forceinline__ double write_records(const DevPlan& P, const FrameDes
 
 // A live Gaussian's float centre (kpos) into its grid cell (capacity kCellCap; a full cell
 // flags the frame, whose kNN then scans every Gaussian).
-__device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k,
-                                            float4 c4) {
-  const int cell = ref_cell_of(S, D, c4.x, c4.y, c4.z);
+// `cell`: ref_cell_of the centre, or -1 (outside every cell: not inserted).
+__device__ __forceinline__ void grid_insert_at(const DevPlan& P, const FrameDesc& D, int cell, int k, float4 c4) {
   if (cell >= 0) {
     const int g = D.cell_base + cell;
     const int pos = atomicAdd(&P.cell_cnt[g], 1);
@@ -476,6 +475,10 @@ __device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D
     else
       atomicOr(&P.state[D.frame_id].flags, F_CELL_OVERFLOW);
   }
+}
+__device__ __forceinline__ void grid_insert(const DevPlan& P, const FrameDesc& D, const FrameState& S, int k,
+                                            float4 c4) {
+  grid_insert_at(P, D, ref_cell_of(S, D, c4.x, c4.y, c4.z), k, c4);
 }
 
 
@@ -823,6 +826,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   const FrameState& S = P.state[f];
   if (*(volatile const int32_t*)&S.done) return;
   const FrameDesc D = load_desc(P, f);
+  const double psi_tot = S.psi_total[it & 1];  // loaded beside the frame's other scalars
   const int sl = s - D.sv_base;
   const int Sf = D.n_sv;
   const float q0 = R.c0, q1 = R.c1, q2 = R.c2;  // the frame's centroid of s, as the E-step reads it
@@ -930,7 +934,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
       const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
       // nu * tr(W D) with nu*W from the record: W00 D00 + W11 D11 + W22 D22 + 2 (W01 D01 + W02 D02 + W12 D12)
       const double tr = e01.x * D00 + e23.y * D11 + e45.y * D22 + 2.0 * (e01.y * D01 + e23.x * D02 + e45.x * D12);
-      Lj = -0.5 * (n * e89.y + tr) + n * (cst - S.psi_total[par]);
+      Lj = -0.5 * (n * e89.y + tr) + n * (cst - psi_tot);
       if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
       if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
     }
@@ -1284,6 +1288,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     fixed = P.fixed[k] != 0;
   }
   __shared__ int s_fast;
+  int cell = -1;
   {
     // the frame's M-step block partials, spread over the whole block so that their loads are
     // in flight together: the alpha total (a fixed order: each thread's partials in order, a
@@ -1304,6 +1309,8 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mp = fmin(mp, __shfl_xor_sync(0xffffffffu, mp, o));
     np = __any_sync(0xffffffffu, np != 0);
+    // the grid cell of a live centre, from the frame's grid geometry, ahead of the barrier
+    if (valid && !was_dead) cell = ref_cell_of(S, D, centre.x, centre.y, centre.z);
     if ((threadIdx.x & 31) == 0) {
       s_wt[threadIdx.x >> 5] = tp;
       s_wm[threadIdx.x >> 5] = mp;
@@ -1328,7 +1335,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
   if (s_fast) {
     // nothing dies: the live Gaussians go into the grid, and the frame's first chunk writes
     // its totals (the post-kill total is the M-step's; the dead count stays)
-    if (valid && !was_dead) grid_insert(P, D, S, k, centre);
+    if (valid && !was_dead) grid_insert_at(P, D, cell, k, centre);
     if (c == D.gchunk_base && threadIdx.x == 0) {
       FrameState* Sw = &P.state[ch.frame];
       Sw->total_alpha = total;
@@ -1357,7 +1364,7 @@ __global__ void __launch_bounds__(kGChunk) k_kill_prep(DevPlan P) {
     } else {
       alpha = a;
       dead = was_dead ? 1 : 0;
-      if (!was_dead) grid_insert(P, D, S, k, centre);
+      if (!was_dead) grid_insert_at(P, D, cell, k, centre);
     }
   }
   chunk_partials(alpha, dead, shd, shi, P.alpha_part_f, P.dead_part, c);
