@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2000)
-    ap.add_argument("--knn-lanes", type=int, choices=[8, 16, 32], default=0,
+    ap.add_argument("--knn-lanes", type=int, choices=[4, 8, 16, 32], default=0,
                     help="fix the kNN/E-step width instead of autotuning (with --knn-fused; for profiling)")
     ap.add_argument("--knn-fused", type=int, choices=[0, 1], default=0,
                     help="with --knn-lanes: 1 = the voxel pass runs the next iteration's kNN/E-step")
@@ -448,7 +448,7 @@ def run_ours(args):
     alone = {"kernel": "k_ll_pass<0, 0, 0> (the voxel pass alone)", "ms_per_launch": ms_ll,
              "algorithmic_bytes_per_launch": vox_bytes, "achieved": vox_bytes / (ms_ll * 1e-3) / 1e9,
              "frac": vox_bytes / (ms_ll * 1e-3) / 1e9 / peak}
-    fused = {"kernel": f"k_ll_pass<0, {knn_lanes}, 0> (the voxel pass running the next iteration's kNN/E-step)",
+    fused = {"kernel": f"k_ll_pass<0, {max(knn_lanes, 8)}, 0> (the voxel pass running the next iteration's kNN/E-step)",
              "ms_per_launch": ms_llk, "algorithmic_bytes_per_launch": vox_bytes + knn_bytes,
              "achieved": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9,
              "frac": (vox_bytes + knn_bytes) / (ms_llk * 1e-3) / 1e9 / peak}

@@ -410,9 +410,10 @@ enum {
 };
 int tgmm_plan_time_kernel(TgmmPlan* plan, int32_t kernel, int32_t reps, float* ms_per_launch, void* stream);
 
-/* Lanes per supervoxel of the kNN/E-step kernel (8, 16 or 32; default 8).  Every width
- * computes the same bits; only the speed differs with the batch (supervoxel count, cells
- * per ring, candidates per cell).  No reference counterpart: the reference runs one fixed
+/* Lanes per supervoxel of the kNN/E-step kernel (4, 8, 16 or 32; default 8; with 4 lanes a
+ * lane holds two list members and lane 0 two candidates, and the kNN/E-step always runs in
+ * its own kernel).  Every width computes the same bits; only the speed differs with the
+ * batch (supervoxel count, cells per ring, candidates per cell).  No reference counterpart: the reference runs one fixed
  * launch shape (knnCuda.cu:781-817, GMEMupdateCUDA.cu:3120-3141). */
 int tgmm_plan_set_knn_group(TgmmPlan* plan, int32_t lanes);
 

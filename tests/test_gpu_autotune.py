@@ -26,12 +26,13 @@ def test_every_width_gives_the_same_bits(cuda_ok, name):
     plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
     try:
         runs = {}
-        for lanes in (8, 16, 32, 8):
+        for lanes in (8, 4, 16, 32, 8):
             plan.set_knn_group(lanes)
             runs.setdefault(lanes, []).append(plan.run_host(df, f.gauss, F.params(20, -1.0)))
     finally:
         plan.close()
     same(runs[8][0], runs[8][1])
+    same(runs[8][0], runs[4][0])
     same(runs[8][0], runs[16][0])
     same(runs[8][0], runs[32][0])
 
@@ -62,7 +63,7 @@ def test_autotune_keeps_the_results(cuda_ok):
         rnks = [torch.empty(5 * f.n_sv, device="cuda") for f in fr]
         inds = [torch.empty(5 * f.n_sv, dtype=torch.int32, device="cuda") for f in fr]
         lanes = tuned.autotune(dfs, gms, rnks, inds, prm, reps=2)
-        assert lanes in (8, 16, 32)
+        assert lanes in (4, 8, 16, 32)
         for g, g0 in zip(gms, gm0):  # the autotuner only reads the Gaussians
             assert torch.equal(g, g0)
         got, _ = run(tuned)
@@ -78,8 +79,13 @@ def test_bad_width_is_refused(cuda_ok):
     f = F.frame("tiny")
     plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
     try:
-        with pytest.raises(L.TgmmError):
-            plan.set_knn_group(4)
+        for bad in (2, 6, 64):
+            with pytest.raises(L.TgmmError):
+                plan.set_knn_group(bad)
+        # groups of 4 lanes always run the kNN/E-step in its own kernel
+        plan.set_knn_group(4)
+        plan.set_knn_fusion(True)
+        assert plan.tuning() == {"knn_lanes": 4, "knn_fused": False}
     finally:
         plan.close()
 
@@ -89,14 +95,15 @@ def test_bad_width_is_refused(cuda_ok):
 def test_knn_in_voxel_pass_gives_the_same_bits(cuda_ok, name, tol):
     """The voxel pass running the next iteration's kNN/E-step gives the bits of the two
     kernels one after the other, also when a frame converges and the kNN/E-step it ran
-    ahead is dropped (tol >= 0), at every width."""
+    ahead is dropped (tol >= 0), at every width; groups of 4 lanes keep their own kernel
+    whatever the fusion setting."""
     from tgmm_b200 import engine as E
     f = F.frame(name)
     df = E.to_device(f)
     plan = E.Plan(f.n_vox, f.n_sv, f.n_gauss)
     try:
         runs = {}
-        for lanes in (8, 32):
+        for lanes in (8, 4, 32):
             plan.set_knn_group(lanes)
             for fused in (False, True, False):
                 plan.set_knn_fusion(fused)

@@ -425,7 +425,8 @@ int enqueue_em(TgmmPlan* P, int max_iter, int ll_prec, bool cond, cudaStream_t s
   launch_moments(D, st);
   TG_CUDA(cudaStreamWaitEvent(st, P->join_ev, 0), "join");
   const bool fp64 = ll_prec == TGMM_LLPREC_FP64;
-  const bool fuse = P->fuse_knn && !fp64;
+  // (the voxel pass carries the kNN/E-step in groups of 8 lanes or more)
+  const bool fuse = P->fuse_knn && !fp64 && D.knn_group >= 8;
   if (max_iter >= 1) launch_knn_estep(D, st);
   for (int it = 1; it <= max_iter; it++) {
     D.iter = it;
@@ -607,8 +608,8 @@ int tgmm_em_run_batch(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, Tg
 
 int tgmm_plan_set_knn_group(TgmmPlan* P, int32_t lanes) {
   if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_group: null plan");
-  if (lanes != 8 && lanes != 16 && lanes != 32)
-    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_group: lanes per supervoxel must be 8, 16 or 32");
+  if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_set_knn_group: lanes per supervoxel must be 4, 8, 16 or 32");
   std::lock_guard<std::mutex> lock(P->mu);
   if (P->dev.knn_group == lanes) return TGMM_OK;
   TG_CUDA(cudaSetDevice(P->desc.device), "cudaSetDevice");
@@ -650,7 +651,7 @@ int tgmm_plan_tuning(TgmmPlan* P, int32_t* lanes, int32_t* fused) {
   if (!P) return fail(TGMM_ERR_INVALID_ARG, "tgmm_plan_tuning: null plan");
   std::lock_guard<std::mutex> lock(P->mu);
   if (lanes) *lanes = P->dev.knn_group;
-  if (fused) *fused = P->fuse_knn ? 1 : 0;
+  if (fused) *fused = P->fuse_knn && P->dev.knn_group >= 8 ? 1 : 0;
   return TGMM_OK;
 }
 
@@ -689,12 +690,12 @@ int tgmm_plan_autotune(TgmmPlan* P, int32_t n_frames, const TgmmFrame* frames, T
   cudaEvent_t ev[2];
   TG_CUDA(cudaEventCreate(&ev[0]), "event");
   TG_CUDA(cudaEventCreate(&ev[1]), "event");
-  const int widths[3] = {8, 16, 32};
+  const int widths[4] = {4, 8, 16, 32};
   float best_ms = 0.0f;
   int best_w = P->dev.knn_group;
   bool best_f = P->fuse_knn, have = false;
   for (int w : widths) {
-    for (int fu = 0; fu < (can_fuse ? 2 : 1); fu++) {
+    for (int fu = 0; fu < (can_fuse && w >= 8 ? 2 : 1); fu++) {
       for (auto& kv : P->graphs) cudaGraphExecDestroy(kv.second);
       P->graphs.clear();
       P->dev.knn_group = w;
@@ -774,7 +775,8 @@ int tgmm_plan_time_kernel(TgmmPlan* P, int32_t kernel, int32_t reps, float* ms, 
   for (int r = 0; r < reps; r++) {
     if (kernel == TGMM_KERNEL_MOMENTS) launch_moments(D, st);
     if (kernel == TGMM_KERNEL_LL_PASS) launch_ll_pass(D, fp64, 0, st);
-    if (kernel == TGMM_KERNEL_LL_PASS_KNN) launch_ll_pass(D, fp64, fp64 ? 0 : D.knn_group, st);
+    // (groups of 4 lanes run the kNN/E-step in their own kernel: the pass is timed with 8)
+    if (kernel == TGMM_KERNEL_LL_PASS_KNN) launch_ll_pass(D, fp64, fp64 ? 0 : std::max(D.knn_group, 8), st);
   }
   TG_CUDA(cudaEventRecord(b, st), "record");
   if (kernel == TGMM_KERNEL_LL_PASS_KNN)

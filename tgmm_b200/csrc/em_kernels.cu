@@ -804,7 +804,10 @@ __device__ void knn_group_search(float q0, float q1, float q2, const float* s, c
 // the frame meanwhile, and the results of an iteration that does not run are never read.
 template <int G>
 __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, int gl, int gbase, unsigned gmask) {
-  static_assert(G >= kJ && G <= 32 && (G & (G - 1)) == 0, "a group holds the five candidates");
+  static_assert(G >= 4 && G <= 32 && (G & (G - 1)) == 0, "groups of 4 to 32 lanes");
+  // per lane: list members gl + G q (q < kM) and candidates gl + G q (q < kC); one of each
+  // for groups of 8 or more lanes
+  constexpr int kM = (kNbr + G - 1) / G, kC = (kJ + G - 1) / G;
   // whole groups leave together; every shuffle below names only the group's lanes
   if (s >= P.info->total_sv) return;
   // what needs only s goes out first, ahead of the frame's state and descriptor: the
@@ -812,17 +815,27 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   // (a global Gaussian index, so that its centre loads beside the frame's state) and the
   // list's bound, and (into L1) the moments the E-step reads
   const SvLL R = P.sv_ll[s];
-  int lk = 0x7fffffff;
+  int lk[kM];
   double nbr_bound = 0.0;
+#pragma unroll
+  for (int q = 0; q < kM; q++) lk[q] = 0x7fffffff;
   if (it > 1) {
-    if (gl < kNbr) lk = P.nbr[(int64_t)s * kNbr + gl];
+#pragma unroll
+    for (int q = 0; q < kM; q++)
+      if (gl + G * q < kNbr) lk[q] = P.nbr[(int64_t)s * kNbr + gl + G * q];
     nbr_bound = P.nbr_b[s];
   }
-  if (gl < 9) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)(M_E0 + gl) * P.max_sv + s));
-  if (G == 8 && gl == 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)M_EE22 * P.max_sv + s));
+#pragma unroll
+  for (int q = 0; q < (9 + G - 1) / G; q++)  // the nine moment rows M_E0 .. M_EE22 over the group
+    if (gl + G * q < 9)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(P.mom + (int64_t)(M_E0 + gl + G * q) * P.max_sv + s));
   const int f = R.frame;
-  float4 lpos = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  if (it > 1 && gl < kNbr && lk != 0x7fffffff) lpos = P.kpos[lk];
+  float4 lpos[kM];
+#pragma unroll
+  for (int q = 0; q < kM; q++) {
+    lpos[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (it > 1 && gl + G * q < kNbr && lk[q] != 0x7fffffff) lpos[q] = P.kpos[lk[q]];
+  }
   const FrameState& S = P.state[f];
   if (*(volatile const int32_t*)&S.done) return;
   const FrameDesc D = load_desc(P, f);
@@ -848,14 +861,24 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   //   sqrt(d5) (1 + 1e-6) + disp < nbr_b = rho (1 - 1e-6) - 4e-3 + disp_b;
   // the margins cover the FP32 rounding of the distances.  Otherwise the supervoxel runs
   // the exact search for the kNbr nearest and keeps them as its new list.
-  float ld = kInfF;
+  float ld[kM];
   bool have = false;
+#pragma unroll
+  for (int q = 0; q < kM; q++) ld[q] = kInfF;
   if (it > 1) {
-    if (gl < kNbr && lk != 0x7fffffff) ld = knn_dist(q0, q1, q2, lpos.x, lpos.y, lpos.z, D.scale);
     Top5 mine;
     top5_init(mine);
-    mine.d[0] = ld;
-    mine.i[0] = lk;
+#pragma unroll
+    for (int q = 0; q < kM; q++) {
+      if (gl + G * q < kNbr && lk[q] != 0x7fffffff)
+        ld[q] = knn_dist(q0, q1, q2, lpos[q].x, lpos[q].y, lpos[q].z, D.scale);
+      if (kM == 1) {
+        mine.d[0] = ld[q];
+        mine.i[0] = lk[q];
+      } else {
+        topn_insert<kJ>(mine, ld[q], lk[q]);
+      }
+    }
     group_merge_topn<G, kJ>(mine, t, gmask);
     have = t.d[kJ - 1] < kInfF && sqrt((double)t.d[kJ - 1]) * (1.0 + 1e-6) + disp < nbr_bound;
   }
@@ -864,8 +887,14 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
     float td0 = kInfF;
     int ti0 = 0x7fffffff;
     if (it > 1) {
-      float dj = gl < kNbr ? ld : -1.0f;  // lanes without a member never win the arg-max
-      int ij = gl < kNbr ? lk : -1;
+      float dj = -1.0f;  // lanes without a member never win the arg-max
+      int ij = -1;
+#pragma unroll
+      for (int q = 0; q < kM; q++)
+        if (gl + G * q < kNbr && before(dj, ij, ld[q], lk[q])) {
+          dj = ld[q];
+          ij = lk[q];
+        }
       group_max_pair<G>(dj, ij, gmask);
       td0 = dj;
       ti0 = ij >= 0 && ij != 0x7fffffff ? ij - D.g_base : ij;  // the search's frame-local order
@@ -895,66 +924,81 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
       t.d[j] = nb.d[j];
       t.i[j] = nb.i[j] == 0x7fffffff ? nb.i[j] : D.g_base + nb.i[j];
     }
-    int mi = 0x7fffffff;
 #pragma unroll
-    for (int q = 0; q < kNbr; q++)
-      if (gl == q) mi = nb.i[q];
-    if (gl < kNbr) P.nbr[(int64_t)s * kNbr + gl] = mi == 0x7fffffff ? mi : D.g_base + mi;
+    for (int m = 0; m < kM; m++) {
+      int mi = 0x7fffffff;
+#pragma unroll
+      for (int q = 0; q < kNbr; q++)
+        if (gl + G * m == q) mi = nb.i[q];
+      if (gl + G * m < kNbr) P.nbr[(int64_t)s * kNbr + gl + G * m] = mi == 0x7fffffff ? mi : D.g_base + mi;
+    }
     if (gl == 0)
       P.nbr_b[s] = nb.d[kNbr - 1] < kInfF ? sqrt((double)nb.d[kNbr - 1]) * (1.0 - 1e-6) - 4e-3 + disp : (double)kInfF;
   }
-  // E-step: candidate j on lane j of the group (its voxel count: 0 for an invalid range, which
+  // E-step: candidate j = gl + G q on its lane (its voxel count: 0 for an invalid range, which
   // flags the frame)
-  const int par = it & 1;
   const double n = (double)R.nv;
-  int k = 0;
+  int kc[kC];
+  double Lc[kC];
 #pragma unroll
-  for (int j = 0; j < kJ; j++)
-    if (gl == j) k = t.i[j];
-  double Lj = 0.0;
-  if (gl < kJ && n != 0.0) {
-    const double* E = P.ec + (int64_t)k * kEcStride;
-    const double2 e01 = *(const double2*)(E), e23 = *(const double2*)(E + 2), e45 = *(const double2*)(E + 4);
-    const double2 e67 = *(const double2*)(E + 6), e89 = *(const double2*)(E + 8), e10 = *(const double2*)(E + 10);
-    const double cst = e10.x;  // psi(alpha) + E[ln|Lambda|]/2, -inf when dead
-    if (cst == -(double)kInfF) {
-      Lj = -(double)kInfF;
-    } else {
-      double G1[3], G2[6];
+  for (int q = 0; q < kC; q++) {
+    const int jj = gl + G * q;
+    int k = 0;
 #pragma unroll
-      for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
+    for (int j = 0; j < kJ; j++)
+      if (jj == j) k = t.i[j];
+    kc[q] = k;
+    double Lj = 0.0;
+    if (jj < kJ && n != 0.0) {
+      const double* E = P.ec + (int64_t)k * kEcStride;
+      const double2 e01 = *(const double2*)(E), e23 = *(const double2*)(E + 2), e45 = *(const double2*)(E + 4);
+      const double2 e67 = *(const double2*)(E + 6), e89 = *(const double2*)(E + 8), e10 = *(const double2*)(E + 10);
+      const double cst = e10.x;  // psi(alpha) + E[ln|Lambda|]/2, -inf when dead
+      if (cst == -(double)kInfF) {
+        Lj = -(double)kInfF;
+      } else {
+        double G1[3], G2[6];
 #pragma unroll
-      for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
-      const double u0 = e67.x - (double)q0, u1 = e67.y - (double)q1, u2 = e89.x - (double)q2;
-      const double D00 = G2[0] - 2.0 * G1[0] * u0 + n * u0 * u0;
-      const double D01 = G2[1] - (G1[0] * u1 + u0 * G1[1]) + n * u0 * u1;
-      const double D02 = G2[2] - (G1[0] * u2 + u0 * G1[2]) + n * u0 * u2;
-      const double D11 = G2[3] - 2.0 * G1[1] * u1 + n * u1 * u1;
-      const double D12 = G2[4] - (G1[1] * u2 + u1 * G1[2]) + n * u1 * u2;
-      const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
-      // nu * tr(W D) with nu*W from the record: W00 D00 + W11 D11 + W22 D22 + 2 (W01 D01 + W02 D02 + W12 D12)
-      const double tr = e01.x * D00 + e23.y * D11 + e45.y * D22 + 2.0 * (e01.y * D01 + e23.x * D02 + e45.x * D12);
-      Lj = -0.5 * (n * e89.y + tr) + n * (cst - psi_tot);
-      if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
-      if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
+        for (int i = 0; i < 3; i++) G1[i] = P.mom[(int64_t)(M_E0 + i) * P.max_sv + s];
+#pragma unroll
+        for (int i = 0; i < 6; i++) G2[i] = P.mom[(int64_t)(M_EE00 + i) * P.max_sv + s];
+        const double u0 = e67.x - (double)q0, u1 = e67.y - (double)q1, u2 = e89.x - (double)q2;
+        const double D00 = G2[0] - 2.0 * G1[0] * u0 + n * u0 * u0;
+        const double D01 = G2[1] - (G1[0] * u1 + u0 * G1[1]) + n * u0 * u1;
+        const double D02 = G2[2] - (G1[0] * u2 + u0 * G1[2]) + n * u0 * u2;
+        const double D11 = G2[3] - 2.0 * G1[1] * u1 + n * u1 * u1;
+        const double D12 = G2[4] - (G1[1] * u2 + u1 * G1[2]) + n * u1 * u2;
+        const double D22 = G2[5] - 2.0 * G1[2] * u2 + n * u2 * u2;
+        // nu * tr(W D) with nu*W from the record: W00 D00 + W11 D11 + W22 D22 + 2 (W01 D01 + W02 D02 + W12 D12)
+        const double tr = e01.x * D00 + e23.y * D11 + e45.y * D22 + 2.0 * (e01.y * D01 + e23.x * D02 + e45.x * D12);
+        Lj = -0.5 * (n * e89.y + tr) + n * (cst - psi_tot);
+        if (Lj < -(double)FLT_MAX) Lj = -(double)kInfF;
+        if (Lj > (double)FLT_MAX) Lj = (double)kInfF;
+      }
     }
+    Lc[q] = Lj;
   }
   // rnk_j = 1 / sum_i exp(L_i - L_j), the sum over i in increasing order
   double Li[kJ];
 #pragma unroll
-  for (int i = 0; i < kJ; i++) Li[i] = __shfl_sync(gmask, Lj, gbase + i);
-  if (gl < kJ) {
-    double acc = 0.0;
+  for (int i = 0; i < kJ; i++) Li[i] = __shfl_sync(gmask, Lc[i / G], gbase + i % G);
 #pragma unroll
-    for (int i = 0; i < kJ; i++) acc += exp(Li[i] - Lj);
-    const float r = __double2float_rn(1.0 / acc);
-    const int j = gl;
-    const int64_t pos = (int64_t)j * Sf + sl;
-    cand_buf(P, it)[(int64_t)s * kJ + j] = k;
-    rnk_buf(P, it)[(int64_t)s * kJ + j] = r;
-    if ((double)r > 1e-3) {
-      const int b = atomicAdd(&P.bcnt[k], 1);
-      if (b < kBucketCap) P.bucket[(int64_t)k * kBucketCap + b] = (int)pos;
+  for (int q = 0; q < kC; q++) {
+    const int j = gl + G * q;
+    if (j < kJ) {
+      const double Lj = Lc[q];
+      const int k = kc[q];
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < kJ; i++) acc += exp(Li[i] - Lj);
+      const float r = __double2float_rn(1.0 / acc);
+      const int64_t pos = (int64_t)j * Sf + sl;
+      cand_buf(P, it)[(int64_t)s * kJ + j] = k;
+      rnk_buf(P, it)[(int64_t)s * kJ + j] = r;
+      if ((double)r > 1e-3) {
+        const int b = atomicAdd(&P.bcnt[k], 1);
+        if (b < kBucketCap) P.bucket[(int64_t)k * kBucketCap + b] = (int)pos;
+      }
     }
   }
 }
@@ -2423,8 +2467,10 @@ void launch_knn_estep(const DevPlan& P, cudaStream_t st) {
     k_knn_estep<32><<<grid, kKnnWarps * 32, 0, st>>>(P);
   else if (G == 16)
     k_knn_estep<16><<<grid, kKnnWarps * 32, 0, st>>>(P);
-  else
+  else if (G == 8)
     k_knn_estep<8><<<grid, kKnnWarps * 32, 0, st>>>(P);
+  else
+    k_knn_estep<4><<<grid, kKnnWarps * 32, 0, st>>>(P);
 }
 void launch_mstep_update(const DevPlan& P, cudaStream_t st) {
   k_mstep_update<<<2 * P.max_gchunks, kMChunk, 0, st>>>(P);
