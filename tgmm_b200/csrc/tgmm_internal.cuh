@@ -43,7 +43,7 @@ constexpr int kCellCap = 32;   // Gaussian centres per kNN grid cell
 #endif
 constexpr int kNbr = TGMM_NBR;  // Gaussians kept per supervoxel in its kNN neighbour list
 constexpr int kRefsPerCell = TGMM_REFS_PER_CELL;  // kNN grid resolution: references per cell
-static_assert(kNbr >= TGMM_J && kNbr <= 8, "a list holds the five candidates, one member per lane of 8");
+static_assert(kNbr >= TGMM_J && kNbr <= 16, "a list holds the five candidates, at most four members per lane of 4");
 constexpr int kEcStride = 12;  // doubles per E-step record
 
 // moment component indices
