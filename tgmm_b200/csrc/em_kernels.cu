@@ -1156,17 +1156,38 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
     alpha_old = gcomp(P, G_ALPHA, k);
     fixed_k = P.fixed[k] != 0;
     kp_old = P.kpos[k];
+    // the bucket's first eight entries load beside its count (entries past the count are
+    // stale and unused; the bucket rows are 128-byte aligned)
+    const int* bk = P.bucket + (int64_t)k * kBucketCap;
+    const int4 b0 = *reinterpret_cast<const int4*>(bk), b1 = *reinterpret_cast<const int4*>(bk + 4);
     const int n = P.bcnt[k];
     P.bcnt[k] = 0;
+    const int t = threadIdx.x;
     if (n > kBucketCap) {
       ovf = true;
       const int o = atomicAdd(&s_novf, 1);
       s_ovf[o] = threadIdx.x;
       atomicOr(&P.state[ch.frame].flags, F_BUCKET_OVERFLOW);
+    } else if (n <= 8) {
+      // up to eight positions (distinct, non-negative): sorted in registers by a 19-comparator
+      // network, the unused slots padded with INT_MAX, then into shared memory
+      int v[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (i >= n) v[i] = INT_MAX;
+      constexpr int kNet[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {1, 2}, {5, 6},
+                                   {0, 4}, {3, 7}, {1, 5}, {2, 6}, {1, 4}, {3, 6}, {2, 4}, {3, 5}, {3, 4}};
+#pragma unroll
+      for (int c2 = 0; c2 < 19; c2++) {
+        const int lo = min(v[kNet[c2][0]], v[kNet[c2][1]]), hi = max(v[kNet[c2][0]], v[kNet[c2][1]]);
+        v[kNet[c2][0]] = lo;
+        v[kNet[c2][1]] = hi;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (i < n) s_bk[i][t] = v[i];
     } else {
       // this Gaussian's bucket into shared memory, sorted there by position
-      const int* bk = P.bucket + (int64_t)k * kBucketCap;
-      const int t = threadIdx.x;
 #pragma unroll 4
       for (int i = 0; i < n; i++) s_bk[i][t] = bk[i];
       for (int i = 1; i < n; i++) {
@@ -1178,6 +1199,8 @@ __global__ void __launch_bounds__(kMChunk) k_mstep_update(DevPlan P) {
         }
         s_bk[q][t] = v;
       }
+    }
+    if (!ovf) {
       // in that order, two pairs' inputs in flight at a time
       int i = 0;
       for (; i + 1 < n; i += 2) {
