@@ -630,14 +630,14 @@ __global__ void __launch_bounds__(256) k_order_scatter(DevPlan P) {
 
 
 // ===========================================================================
-// knn_estep: a group of G lanes per supervoxel (32 / G supervoxels per warp; G = 8, 16
+// knn_estep: a group of G lanes per supervoxel (32 / G supervoxels per warp; G = 4, 8, 16
 // or 32, chosen per plan, by tgmm_plan_autotune or tgmm_plan_set_knn_group; every G gives
 // the same bits).
 // Exact 5-NN of the centroid among the frame's Gaussian centres: the group's lanes split
 // each ring of grid cells, keep private top-5 lists pruned by the group's current fifth
 // distance, and after each ring the lists are merged by five rounds of a group-wide
 // (distance, index) arg-min.  Then the E-step from the supervoxel's moments, candidate j
-// on lane j of the group:
+// on lane j mod G of the group (lane 0 also takes candidate 4 when G = 4):
 //   L_j = sum_v [-1/2 (3/beta + nu d'Wd) + E ln pi + 1/2 E ln|Lambda|]
 //       = -1/2 (3 n/beta + nu tr(W D)) + n (psi(alpha) - psi(sum alpha) + 1/2 E ln|Lambda|),
 //   D = sum_v (x_v - m)(x_v - m)' = G2 - G1 u' - u G1' + n u u',  u = m - c_s,
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(256) k_order_scatter(DevPlan P) {
 // ===========================================================================
 constexpr int kKnnWarps = 4;  // warps per block; the lanes per supervoxel (G) come from the plan
 #ifndef TGMM_KNN_BLOCKS
-#define TGMM_KNN_BLOCKS 5  // 102 registers: the list path fits more warps; the rare grid search spills a little
+#define TGMM_KNN_BLOCKS 5  // 96 registers: the list path fits more warps; the rare grid search spills a little
 #endif
 constexpr int kKnnBlocks = TGMM_KNN_BLOCKS;  // resident blocks per SM the kNN/E-step is compiled for
 
@@ -854,7 +854,7 @@ __device__ __forceinline__ void knn_estep_sv(const DevPlan& P, int s, int it, in
   const double disp = S.disp_cum;
   Top5 t;
   // After the first iteration: the supervoxel's neighbour list, the kNbr nearest Gaussians
-  // when it was last searched (at displacement bound disp_b), member i on lane i.  A
+  // when it was last searched (at displacement bound disp_b), member i on lane i mod G.  A
   // Gaussian outside the list was then at scaled distance >= rho from the centroid and has
   // since moved at most disp - disp_b, so the five nearest members (current centres, the
   // same FP32 distances and (distance, index) order) are the exact five nearest whenever
