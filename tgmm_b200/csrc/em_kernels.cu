@@ -306,26 +306,30 @@ __device__ void write_sv_rec(const DevPlan& P, const FrameDesc& D, int f, int s,
 // centroid bounding box and grid geometry, EM state reset.
 // ===========================================================================
 __global__ void __launch_bounds__(kFrameThreads) k_build_maps(DevPlan P) {
+  // block (f, y): the frame's map stores split over kMapSlices blocks; block (f, 0) also
+  // checks the CSR, takes the centroids' bounding box and starts the frame's state
   const int f = blockIdx.x;
   if (f >= P.info->n_frames) return;
   const FrameDesc D = load_desc(P, f);
+  const int first = blockIdx.y * blockDim.x + threadIdx.x, stride = kMapSlices * blockDim.x;
+  for (int i = first; i < D.n_sv; i += stride) P.sv_frame[D.sv_base + i] = f;
+#pragma unroll 4
+  for (int i = first; i < D.n_gauss; i += stride) {
+    P.g_frame[D.g_base + i] = f;
+    P.bcnt[D.g_base + i] = 0;  // M-step and assignment buckets start empty
+    P.acnt[D.g_base + i] = 0;
+  }
+  for (int i = first; i < D.cell_budget; i += stride) P.cell_cnt[D.cell_base + i] = 0;
+  if (blockIdx.y != 0) return;
   FrameState* S = &P.state[f];
   __shared__ float smin[3][32], smax[3][32];
   __shared__ int sbad;
   if (threadIdx.x == 0) sbad = 0;
   __syncthreads();
-  for (int i = threadIdx.x; i < D.n_sv; i += blockDim.x) P.sv_frame[D.sv_base + i] = f;
   if (threadIdx.x < kOrderBuckets) {  // the supervoxel order's bucket counts and cursors
     P.ord_hist[f * kOrderBuckets + threadIdx.x] = 0;
     P.ord_cur[f * kOrderBuckets + threadIdx.x] = 0;
   }
-#pragma unroll 4
-  for (int i = threadIdx.x; i < D.n_gauss; i += blockDim.x) {
-    P.g_frame[D.g_base + i] = f;
-    P.bcnt[D.g_base + i] = 0;  // M-step and assignment buckets start empty
-    P.acnt[D.g_base + i] = 0;
-  }
-  for (int i = threadIdx.x; i < D.cell_budget; i += blockDim.x) P.cell_cnt[D.cell_base + i] = 0;
   int bad = 0;
   float lo[3] = {kInfF, kInfF, kInfF}, hi[3] = {-kInfF, -kInfF, -kInfF};
   // unrolled so that several supervoxels' loads are in flight at once
@@ -2454,7 +2458,7 @@ __global__ void __launch_bounds__(kGChunk) k_export(DevPlan P) {
 static inline int div_up(int a, int b) { return (a + b - 1) / b; }
 
 void launch_build_maps(const DevPlan& P, cudaStream_t st) {
-  k_build_maps<<<P.max_frames, kFrameThreads, 0, st>>>(P);
+  k_build_maps<<<dim3(P.max_frames, kMapSlices), kFrameThreads, 0, st>>>(P);
 }
 // The caller's page-locked records into the plan's device records, 16 bytes a thread, read
 // by the SMs over the bus (not a copy engine, so they do not queue behind the caller's own

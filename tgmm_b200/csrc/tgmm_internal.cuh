@@ -34,6 +34,7 @@ constexpr int kSvPerWarpV = 2;
 constexpr int kSvPerBlockV = kWarpsPerBlockV * kSvPerWarpV;
 constexpr int kNumMoments = 19;
 constexpr int kFrameThreads = 1024;
+constexpr int kMapSlices = 8;  // blocks per frame of the frame-map kernel
 constexpr int kCellCap = 32;   // Gaussian centres per kNN grid cell
 #ifndef TGMM_NBR
 #define TGMM_NBR 8
